@@ -1,0 +1,85 @@
+/*
+ * wenofv_oracle.h -- CPU restatement of the reference's WENOFV time-advance path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This oracle is the checker for the sm_100a kernels: only the
+ * tests, __graft_entry__.smoke() and the CPU-baseline leg of bench.py may load it.  The
+ * product path (the C-ABI library) never calls it and has no CPU fallback.
+ *
+ * Every function follows the reference's arithmetic in the same operation order (cited
+ * per function as path:line inside the reference project), so that for the two-phase
+ * linear-EOS system it reproduces the compiled reference bit for bit.  Linear advection,
+ * Euler and outflow boundaries are extensions that the reference does not implement;
+ * for those the oracle is the restated algorithm itself (parity unpinned by the reference).
+ *
+ * Data layout of every state array crossing this interface: SoA, U[v*ny*nx + j*nx + i],
+ * interior cells only (no ghosts), i = x index (contiguous), j = y index.
+ */
+#ifndef WENOFV_ORACLE_H
+#define WENOFV_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Equation kinds (same numbering as include/wenofv.h). */
+enum { OFV_EQ_TWO_PHASE = 0, OFV_EQ_LINEAR_ADV = 1, OFV_EQ_EULER = 2 };
+/* Boundary kinds: PERIOD = 0 as include/Equations.hpp:27; OUTFLOW is an extension. */
+enum { OFV_BC_PERIOD = 0, OFV_BC_OUTFLOW = 5 };
+
+typedef struct {
+    int kind;
+    /* TwoPhaseEquation parameters (include/Equations.hpp:67-69) */
+    double rho10, rho20, sound1, sound2, preb;
+    /* Euler ratio of specific heats */
+    double gamma;
+    /* linear advection velocity */
+    double adv_u, adv_v;
+} ofv_eq;
+
+typedef struct {
+    int nx, ny;            /* ELEMNUMX, ELEMNUMY */
+    double xl, xr, yl, yr; /* domain */
+    int bc;                /* OFV_BC_* */
+    int rk;                /* RKMETH: 0 RK1, 1 RK2, 2 RK3 */
+    double cfl;            /* CFL */
+    int scheme;            /* SCHEME: 0 WENO-JS, 1 WENO-Z */
+    int limiter;           /* PPlimiter */
+    int flux;              /* RIEMANNFLUX: 0 LLF, 1 HLLC */
+    int recon;             /* RECONSTRUCTIONTYPE: 0 conservative, 1 characteristic */
+    int ref_slabs;         /* 0: uniform cell sizes; P>0: the reference's P-slab x metric */
+    int threads;           /* OpenMP threads (0 = library default) */
+    ofv_eq eq;
+} ofv_problem;
+
+int ofv_nvar(const ofv_eq *eq);
+
+/* pointwise kernels */
+double ofv_weno_js(const double v[5], int gp);
+double ofv_weno_z(const double v[5], int gp);
+double ofv_volume_frac(const ofv_eq *eq, const double *U);
+double ofv_pressure(const ofv_eq *eq, const double *U);
+double ofv_sound_speed(const ofv_eq *eq, const double *U);
+double ofv_max_eig(const ofv_eq *eq, const double *U, double nx, double ny);
+void ofv_riemann(const ofv_eq *eq, int flux, const double *UL, const double *UR,
+                 double nx, double ny, double *F);
+void ofv_eigen_L(const ofv_eq *eq, const double *U, double nx, double ny, double *L);
+void ofv_eigen_R(const ofv_eq *eq, const double *U, double nx, double ny, double *R);
+
+/* grid metric: dxc[nx], dxl[nx], dy[ny] (see ofv_metric in the .c file) */
+void ofv_metric(const ofv_problem *p, double *dxc, double *dxl, double *dy);
+
+/* whole-grid operators */
+double ofv_compute_dt(const ofv_problem *p, const double *U, int *nan_flag);
+/* rhs of one stage; theta_flags (may be NULL) receives the per-cell limiter flag */
+void ofv_rhs(const ofv_problem *p, const double *U, double *rhs, double *theta_flags);
+/* face states after the limiter for interior cells: out[cell][face B,T,L,R][var][gp] */
+void ofv_face_states(const ofv_problem *p, const double *U, double *out);
+void ofv_step(const ofv_problem *p, double *U, double dt);
+/* time loop of CWENOFV::run to one target time; returns the number of steps taken */
+int ofv_advance(const ofv_problem *p, double *U, double t0, double t_end, double *t_out,
+                int max_steps, double *dts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
