@@ -1,0 +1,199 @@
+/*
+ * wenofv.h -- C ABI of the B200 (sm_100a) WENOFV time-advance library (libwenofv_b200.so).
+ *
+ * The library replaces the hot path of the reference solver's CWENOFV class
+ * (infinity-07/two-phase-3equation-2D-pal-column): the ghost-cell fill, the
+ * dimension-by-dimension WENO-JS/WENO-Z reconstruction at Gauss-Lobatto points, the
+ * bound-preserving theta limiter, the LLF/HLLC Riemann fluxes with Gauss-Lobatto face
+ * quadrature, the SSP-RK stage combination and the CFL max-wavespeed reduction.  The whole
+ * domain stays resident in one GPU's HBM; the reference's 4-rank MPI x-slab
+ * decomposition is not needed.
+ *
+ * Citations are path:line inside the reference project.  All entry points return a
+ * WENOFV_* status (0 = success) and never exit, trap or block on stdin.  One context is
+ * used by one host thread at a time; contexts are independent of each other.  Calls are
+ * asynchronous on the context's CUDA stream except where a function reads a result back
+ * (download, compute_dt, rhs, advance, status), which synchronise that stream.
+ */
+#ifndef WENOFV_H
+#define WENOFV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WENOFV_ABI_VERSION 1
+
+/* status codes (the reference prints, waits on std::cin and exits instead:
+ * src/WENOFV.cpp:34-38, :521-531, :1927-1932, :2287-2292; include/Equations.hpp:345-359) */
+enum {
+    WENOFV_OK = 0,
+    WENOFV_EINVAL = 1,    /* invalid configuration or argument */
+    WENOFV_ENOMEM = 2,    /* device allocation failed or the HBM budget is exceeded */
+    WENOFV_ENUMERIC = 3,  /* NaN time step, NaN flux or illegal limiter theta (see status) */
+    WENOFV_ETIMEDOUT = 4, /* a bounded wait ran out */
+    WENOFV_ECUDA = 5,     /* CUDA runtime error (message in wenofv_last_error) */
+    WENOFV_ENOTSUP = 6,   /* option combination not supported */
+    WENOFV_EBUSY = 7,     /* request still running (serving API) */
+    WENOFV_ENOTFOUND = 8  /* unknown request id (serving API) */
+};
+
+/* equation kinds; TWO_PHASE is TwoPhaseEquation (include/Equations.hpp:52-1044) */
+enum { WENOFV_EQ_TWO_PHASE = 0, WENOFV_EQ_LINEAR_ADV = 1, WENOFV_EQ_EULER = 2 };
+/* boundary kinds; PERIOD keeps the number of BOUNDARYTYPE::PERIOD (include/Equations.hpp:27);
+ * OUTFLOW (zero-gradient) has no counterpart in the reference */
+enum { WENOFV_BC_PERIOD = 0, WENOFV_BC_OUTFLOW = 5 };
+/* arithmetic forms */
+enum {
+    WENOFV_FP64 = 0,        /* FP64 with fused multiply-add contraction */
+    WENOFV_FP64_STRICT = 1, /* FP64 in the reference's operation order, no contraction */
+    WENOFV_FP32_BULK = 2    /* FP32 reconstruction/flux; FP64 pressure recovery, theta and
+                               RK accumulation */
+};
+/* host array layouts for upload/download/rhs */
+enum {
+    WENOFV_LAYOUT_SOA = 0,    /* U[v][j][i], i (x) fastest */
+    WENOFV_LAYOUT_REF_AOS = 1 /* U[i][j][v]: the order of the reference's m_Uh[ei][ej].vector[r]
+                                 over interior cells (include/WENOFV.hpp:171) */
+};
+/* bits of the device status word */
+enum {
+    WENOFV_FLAG_NAN_DT = 1u,     /* NaN in the CFL time step (src/WENOFV.cpp:502-531) */
+    WENOFV_FLAG_BAD_THETA = 2u,  /* limiter theta outside [0,1] (src/WENOFV.cpp:1927-1932) */
+    WENOFV_FLAG_NAN_FLUX = 4u,   /* NaN Riemann flux (include/Equations.hpp:345-359) */
+    WENOFV_FLAG_NAN_STATE = 8u   /* NaN in an updated cell average */
+};
+
+/* Equation parameters.  Field order and meaning of rho10..preb follow TwoPhaseEquation's
+ * g_rho10, g_rho20, g_sound1, g_sound2, g_preb (include/Equations.hpp:67-69); the linear EOS
+ * p_k = sound_k^2 (rho_k - rho_k0) drops preb exactly as getPressure does (:112-116). */
+typedef struct {
+    int eq_kind;
+    double rho10, rho20, sound1, sound2, preb;
+    double gamma;        /* Euler ratio of specific heats */
+    double adv_u, adv_v; /* linear advection velocity */
+} wenofv_eq_params;
+
+/* Solver options: the settings.cfg keys (config/settings.cfg:11-24, read at
+ * src/WENOFV.cpp:43-62) plus the domain, boundary, grid metric, arithmetic form and device. */
+typedef struct {
+    int nx, ny;            /* ELEMNUMX, ELEMNUMY */
+    double xl, xr, yl, yr; /* TwoPhaseEquation::xL, xR, yL, yR */
+    int bc;                /* WENOFV_BC_* */
+    int rk_method;         /* RKMETH: 0 RK1, 1 RK2, 2 RK3 */
+    double cfl;            /* CFL */
+    int scheme;            /* SCHEME: 0 WENO-JS, 1 WENO-Z */
+    int pp_limiter;        /* PPlimiter: 0 off, 1 on */
+    int riemann_flux;      /* RIEMANNFLUX: 0 LLF, 1 HLLC */
+    int reconstruction;    /* RECONSTRUCTIONTYPE: 0 conservative, 1 characteristic */
+    int ref_slabs;         /* 0: uniform cell sizes; P > 0: cell sizes exactly as the
+                              reference's P-slab grid generator rounds them (src/WENOFV.cpp:89-123) */
+    int precision;         /* WENOFV_FP64, WENOFV_FP64_STRICT, WENOFV_FP32_BULK */
+    int device;            /* CUDA device ordinal */
+} wenofv_config;
+
+typedef struct wenofv_ctx wenofv_ctx;
+
+int wenofv_abi_version(void);
+const char *wenofv_strerror(int code);
+/* text of the last error on the calling thread (CUDA message or argument check) */
+const char *wenofv_last_error(void);
+/* fills *cfg with the reference's shipped settings.cfg defaults (config/settings.cfg) */
+void wenofv_default_config(wenofv_config *cfg);
+
+/* CWENOFV::initializeSolver (src/WENOFV.cpp:16-231): validate options, build the grid
+ * metric and allocate the device state (three FP64 state buffers, the status block). */
+int wenofv_create(const wenofv_config *cfg, const wenofv_eq_params *eq, wenofv_ctx **out);
+/* releases every device allocation of the context */
+void wenofv_destroy(wenofv_ctx *ctx);
+
+/* writes the interior cell averages (CWENOFV::m_Uh after initializeAve, src/WENOFV.cpp:232-279) */
+int wenofv_upload(wenofv_ctx *ctx, const double *U, int layout);
+/* reads the interior cell averages (what getWorldUh gathers, src/WENOFV.cpp:2059-2117) */
+int wenofv_download(wenofv_ctx *ctx, double *U, int layout);
+
+/* CWENOFV::calculateDeltaT (src/WENOFV.cpp:474-540): min over cells of
+ * CFL / (lambda_x/dx + lambda_y/dy), starting from 1.0; WENOFV_ENUMERIC on a NaN */
+int wenofv_compute_dt(wenofv_ctx *ctx, double *dt);
+/* CWENOFV::performTimeIntegration (src/WENOFV.cpp:541-566): one SSP-RK step with this dt */
+int wenofv_step(wenofv_ctx *ctx, double dt);
+/* CWENOFV::assembleRHS (src/WENOFV.cpp:568-615) of the current state, written to host rhs */
+int wenofv_rhs(wenofv_ctx *ctx, double *rhs, int layout);
+/* the stepping loop of CWENOFV::run towards one output time (src/WENOFV.cpp:318-354):
+ * while |now - t_end| > 1e-10 { dt = min(calculateDeltaT, t_end - now); step; now += dt; }
+ * The loop runs on the device in CUDA graphs; max_steps <= 0 means no limit. */
+int wenofv_advance(wenofv_ctx *ctx, double t_now, double t_end, int64_t max_steps, double *t_out,
+                   int64_t *nsteps);
+/* device status word (WENOFV_FLAG_*) and the first offending cell (j*nx+i, -1 if none) */
+int wenofv_status(wenofv_ctx *ctx, uint32_t *flags, int64_t *first_cell);
+/* waits for all work queued on the context's stream */
+int wenofv_synchronize(wenofv_ctx *ctx);
+/* the context's cudaStream_t (for event timing by the caller) */
+void *wenofv_stream(wenofv_ctx *ctx);
+/* device pointer of the current interior state, SoA with row pitch *pitch doubles and
+ * plane stride pitch*ny (valid until the next step) */
+int wenofv_device_state(wenofv_ctx *ctx, double **U, int *pitch);
+
+/* ---- batched ensemble: many uneven instances per persistent launch (no counterpart in
+ *      the reference, which solves one grid per MPI job) ---------------------------------- */
+typedef struct wenofv_batch wenofv_batch;
+/* all instances share device and rk_method; grids, schemes, fluxes, limiter, equations
+ * and precision may differ per instance */
+int wenofv_batch_create(int n, const wenofv_config *cfgs, const wenofv_eq_params *eqs, wenofv_batch **out);
+void wenofv_batch_destroy(wenofv_batch *b);
+int wenofv_batch_upload(wenofv_batch *b, int i, const double *U, int layout);
+int wenofv_batch_download(wenofv_batch *b, int i, double *U, int layout);
+/* advances instance k from t=0 to t_end[k]; nsteps[k] receives its step count */
+int wenofv_batch_advance(wenofv_batch *b, const double *t_end, int64_t max_steps, int64_t *nsteps);
+/* rows per work item and CTAs per SM of the persistent stage kernel (0 = automatic) */
+int wenofv_batch_set_tiling(wenofv_batch *b, int rows_per_item, int ctas_per_sm);
+int wenofv_batch_stream(wenofv_batch *b, void **stream);
+/* measures candidate tilings on the batch's current state (state unchanged) and keeps the best */
+int wenofv_batch_autotune(wenofv_batch *b, int *rows_per_item, int *ctas_per_sm, double *best_ms);
+
+/* ---- serving: continuous batching of solve requests under an HBM budget (no
+ *      counterpart in the reference) ------------------------------------------------------- */
+typedef struct wenofv_server wenofv_server;
+typedef struct {
+    double t_submit, t_admit, t_done; /* host seconds on the server's clock */
+    int64_t steps;
+    uint32_t flags;
+    int status;
+} wenofv_request_info;
+int wenofv_server_create(int device, size_t hbm_budget_bytes, int max_slots, wenofv_server **out);
+void wenofv_server_destroy(wenofv_server *s);
+/* queues a solve of U0 (SoA) from t=0 to t_end, or max_steps steps if that comes first
+ * (max_steps <= 0: no limit); the server copies U0.  RKMETH must be 2 (SSP-RK3). */
+int wenofv_server_submit(wenofv_server *s, const wenofv_config *cfg, const wenofv_eq_params *eq,
+                         const double *U0, double t_end, int64_t max_steps, int64_t *request_id);
+/* WENOFV_EBUSY while the request runs; otherwise its status (WENOFV_OK copies the result,
+ * SoA) and the request is forgotten */
+int wenofv_server_poll(wenofv_server *s, int64_t request_id, double *U, wenofv_request_info *info);
+/* seconds on the server's clock */
+double wenofv_server_clock(wenofv_server *s);
+/* counters: admitted, completed, queued, active, resident bytes */
+int wenofv_server_stats(wenofv_server *s, int64_t *admitted, int64_t *completed, int64_t *queued,
+                        int64_t *active, int64_t *resident_bytes);
+
+/* ---- device probes of the pointwise kernels (test hooks; they replace calls to the
+ *      header-only reference kernels include/Utility.hpp and include/Equations.hpp) ------- */
+/* WENO5threconstruction / WENO5Zthreconstruction (include/Utility.hpp:5-95, :193-290) at
+ * the 4 Gauss-Lobatto points: stencils n x 5, out n x 4 */
+int wenofv_probe_weno(int scheme, int precision, const double *stencils, int n, double *out, int device);
+/* getRiemannFlux (include/Equations.hpp:329-483): UL, UR, F are n x nvar */
+int wenofv_probe_riemann(const wenofv_eq_params *eq, int flux, int precision, const double *UL,
+                         const double *UR, int n, double nx, double ny, double *F, int device);
+/* getLEigenMatrix / getREigenMatrix (include/Equations.hpp:189-327): L, R are n x 16 row-major */
+int wenofv_probe_eigen(const wenofv_eq_params *eq, int precision, const double *U, int n, double nx,
+                       double ny, double *L, double *R, int device);
+/* measured FMA throughput of the FP64 (or, with WENOFV_FP32_BULK, FP32) CUDA-core pipe in
+ * TFLOP/s: the denominator of the stage kernel's compute roofline (no reference counterpart) */
+int wenofv_probe_fma_peak(int precision, int device, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -199,7 +199,7 @@ def reference_available() -> bool:
 
 def run_reference(p: Problem, testcase: int = 0, U0: np.ndarray | None = None, steps: int = 0,
                   t_end: float = 0.0, want_rhs: bool = False, time: bool = False,
-                  timeout: float = 600.0) -> RefResult:
+                  timeout: float = 600.0, warmup: int = 0) -> RefResult:
     """Run the unmodified reference (4 slab ranks) on the two-phase system.
 
     ``testcase`` selects the reference's own test case (its domain, boundary and, when
@@ -228,6 +228,8 @@ def run_reference(p: Problem, testcase: int = 0, U0: np.ndarray | None = None, s
             args += ["--rhs", os.path.join(d, "rhs.bin"), "--faces", os.path.join(d, "faces.bin")]
         if time:
             args += ["--time"]
+        if warmup:
+            args += ["--warmup", str(warmup)]
         cp = subprocess.run(args, capture_output=True, text=True, timeout=timeout)
         if cp.returncode != 0:
             raise RuntimeError(f"reference failed ({cp.returncode}): {cp.stderr[-2000:]}")

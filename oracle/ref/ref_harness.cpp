@@ -11,7 +11,7 @@
 //                   [--rho10 X --rho20 X --sound1 X --sound2 X]   equation overrides
 //                   [--u0 FILE]        initial averages, SoA [v][j][i] FP64 (else the test case IC)
 //                   [--dump-u0 FILE]   the initial averages actually used
-//                   [--steps N | --tend T]
+//                   [--steps N | --tend T] [--warmup N]   (warm-up steps run untimed first)
 //                   [--rhs FILE]       one assembleRHS of the initial state, SoA FP64
 //                   [--faces FILE]     face states after that assembleRHS [cell][B,T,L,R][v][gp]
 //                   [--out FILE] [--dts FILE] [--time]
@@ -39,7 +39,7 @@ struct Args {
     std::map<std::string, std::string> opt;
     double rho10 = -1, rho20 = -1, sound1 = -1, sound2 = -1;
     std::string u0, dump_u0, rhs, faces, out, dts;
-    long steps = -1;
+    long steps = -1, warmup = 0;
     double tend = -1;
     bool time = false;
 };
@@ -115,6 +115,8 @@ void rank_main(int rank, const Args &a, Shared &sh, const std::vector<double> &u
             }
     }
 
+    // untimed warm-up steps (the state they produce is the timed steps' input)
+    for (long k = 0; k < a.warmup; k++) solver.performTimeIntegration(solver.calculateDeltaT(0.0));
     MPI_Barrier(MPI_COMM_WORLD);
     const auto t0 = std::chrono::steady_clock::now();
     double now = 0;
@@ -168,6 +170,7 @@ int main(int argc, char **argv)
         else if (s == "--out") { a.out = val; k++; }
         else if (s == "--dts") { a.dts = val; k++; }
         else if (s == "--steps") { a.steps = std::atol(val); k++; }
+        else if (s == "--warmup") { a.warmup = std::atol(val); k++; }
         else if (s == "--tend") { a.tend = std::atof(val); k++; }
         else if (s == "--time") { a.time = true; }
         else { std::fprintf(stderr, "unknown argument %s\n", s.c_str()); return 2; }

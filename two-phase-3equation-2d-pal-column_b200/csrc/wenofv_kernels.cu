@@ -1,0 +1,220 @@
+// wenofv_kernels.cu -- instantiations and host launchers of the stage, CFL and probe
+// kernels.  Built twice into the library: -DWENOFV_STRICT=1 -fmad=false (namespace
+// wenofv::strict, the reference's FP64 operation order) and -DWENOFV_STRICT=0 (namespace
+// wenofv::fast, FP64 with contraction and the FP32-bulk form).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "wenofv_stage.cuh"
+
+namespace wenofv {
+#if WENOFV_STRICT
+namespace strict {
+#else
+namespace fast {
+#endif
+
+#if WENOFV_STRICT
+#define WENOFV_HAS_FP32 0
+#else
+#define WENOFV_HAS_FP32 1
+#endif
+
+int stage_tx(int eq) { return eq == EQ_LINEAR_ADV ? StageGeom<EQ_LINEAR_ADV>::TX : StageGeom<EQ_TWO_PHASE>::TX; }
+
+template <int EQ, int RECON, class R> static const void *stage_fn() { return (const void *)stage_kernel<EQ, RECON, R>; }
+
+static const void *pick_stage(int eq, int recon, int fp32)
+{
+#if WENOFV_HAS_FP32
+    if (fp32) {
+        switch (eq) {
+        case EQ_TWO_PHASE: return recon ? stage_fn<EQ_TWO_PHASE, 1, float>() : stage_fn<EQ_TWO_PHASE, 0, float>();
+        case EQ_EULER: return recon ? stage_fn<EQ_EULER, 1, float>() : stage_fn<EQ_EULER, 0, float>();
+        case EQ_LINEAR_ADV: return stage_fn<EQ_LINEAR_ADV, 0, float>();
+        default: return nullptr;
+        }
+    }
+#else
+    if (fp32) return nullptr;
+#endif
+    switch (eq) {
+    case EQ_TWO_PHASE: return recon ? stage_fn<EQ_TWO_PHASE, 1, double>() : stage_fn<EQ_TWO_PHASE, 0, double>();
+    case EQ_EULER: return recon ? stage_fn<EQ_EULER, 1, double>() : stage_fn<EQ_EULER, 0, double>();
+    case EQ_LINEAR_ADV: return stage_fn<EQ_LINEAR_ADV, 0, double>();
+    default: return nullptr;
+    }
+}
+
+int launch_stage(int eq, int recon, int fp32, const StageLaunch &L, int grid, void *stream)
+{
+    const void *fn = pick_stage(eq, recon, fp32);
+    if (!fn) return (int)cudaErrorInvalidValue;
+    void *args[] = {(void *)&L};
+    return (int)cudaLaunchKernel(fn, dim3(grid), dim3(NT), args, 0, (cudaStream_t)stream);
+}
+
+int launch_cfl(int eq, const StageLaunch &L, int grid, void *stream)
+{
+    const void *fn = eq == EQ_TWO_PHASE ? (const void *)cfl_kernel<EQ_TWO_PHASE>
+                     : eq == EQ_EULER   ? (const void *)cfl_kernel<EQ_EULER>
+                                        : (const void *)cfl_kernel<EQ_LINEAR_ADV>;
+    void *args[] = {(void *)&L};
+    return (int)cudaLaunchKernel(fn, dim3(grid), dim3(NT), args, 0, (cudaStream_t)stream);
+}
+
+int stage_blocks_per_sm(int eq, int recon, int fp32)
+{
+    const void *fn = pick_stage(eq, recon, fp32);
+    if (!fn) return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, NT, 0) != cudaSuccess) return 0;
+    return n;
+}
+
+// ---- probes: the pointwise kernels on arrays (test hooks) -----------------------------
+template <class R> __global__ void probe_weno_kernel(int scheme, const double *st, int n, double *out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    Weno5<R> W;
+    W.init(scheme, (R)st[5 * k], (R)st[5 * k + 1], (R)st[5 * k + 2], (R)st[5 * k + 3], (R)st[5 * k + 4]);
+    out[4 * k + 0] = (double)W.template eval<0>();
+    out[4 * k + 1] = (double)W.template eval<1>();
+    out[4 * k + 2] = (double)W.template eval<2>();
+    out[4 * k + 3] = (double)W.template eval<3>();
+}
+
+template <int EQ, class R>
+__global__ void probe_riemann_kernel(EqParams P, int flux, const double *UL, const double *UR, int n, int xdir, double *F)
+{
+    constexpr int NV = EqTraits<EQ>::NV;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    R l[NV], r[NV], f[NV];
+    for (int v = 0; v < NV; v++) { l[v] = (R)UL[NV * k + v]; r[v] = (R)UR[NV * k + v]; }
+    riemann<EQ, R>(P, flux, l, r, f, xdir != 0);
+    for (int v = 0; v < NV; v++) F[NV * k + v] = (double)f[v];
+}
+
+template <int EQ, class R>
+__global__ void probe_eigen_kernel(EqParams P, const double *U, int n, int xdir, double *Lm, double *Rm)
+{
+    constexpr int NV = EqTraits<EQ>::NV;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    R u[NV];
+    for (int v = 0; v < NV; v++) u[v] = (R)U[NV * k + v];
+    for (int row = 0; row < NV; row++) {
+        R lr[NV], rr[NV];
+        eigen_rows<EQ, R>(P, u, xdir != 0, row, lr, rr);
+        for (int j = 0; j < NV; j++) {
+            Lm[16 * k + row * NV + j] = (double)lr[j];
+            Rm[16 * k + row * NV + j] = (double)rr[j];
+        }
+    }
+}
+
+int probe_weno(int scheme, int fp32, const double *d_st, int n, double *d_out, void *stream)
+{
+    const int b = 128, g = (n + b - 1) / b;
+    if (n <= 0) return 0;
+#if WENOFV_HAS_FP32
+    if (fp32) probe_weno_kernel<float><<<g, b, 0, (cudaStream_t)stream>>>(scheme, d_st, n, d_out);
+    else
+#endif
+        probe_weno_kernel<double><<<g, b, 0, (cudaStream_t)stream>>>(scheme, d_st, n, d_out);
+    return (int)cudaGetLastError();
+}
+
+int probe_riemann(const EqParams &P, int flux, int fp32, const double *d_UL, const double *d_UR, int n, int xdir, double *d_F, void *stream)
+{
+    const int b = 128, g = (n + b - 1) / b;
+    if (n <= 0) return 0;
+    cudaStream_t s = (cudaStream_t)stream;
+#if WENOFV_HAS_FP32
+    if (fp32) {
+        if (P.kind == EQ_TWO_PHASE) probe_riemann_kernel<EQ_TWO_PHASE, float><<<g, b, 0, s>>>(P, flux, d_UL, d_UR, n, xdir, d_F);
+        else if (P.kind == EQ_EULER) probe_riemann_kernel<EQ_EULER, float><<<g, b, 0, s>>>(P, flux, d_UL, d_UR, n, xdir, d_F);
+        else probe_riemann_kernel<EQ_LINEAR_ADV, float><<<g, b, 0, s>>>(P, flux, d_UL, d_UR, n, xdir, d_F);
+        return (int)cudaGetLastError();
+    }
+#endif
+    if (P.kind == EQ_TWO_PHASE) probe_riemann_kernel<EQ_TWO_PHASE, double><<<g, b, 0, s>>>(P, flux, d_UL, d_UR, n, xdir, d_F);
+    else if (P.kind == EQ_EULER) probe_riemann_kernel<EQ_EULER, double><<<g, b, 0, s>>>(P, flux, d_UL, d_UR, n, xdir, d_F);
+    else probe_riemann_kernel<EQ_LINEAR_ADV, double><<<g, b, 0, s>>>(P, flux, d_UL, d_UR, n, xdir, d_F);
+    return (int)cudaGetLastError();
+}
+
+int probe_eigen(const EqParams &P, int fp32, const double *d_U, int n, int xdir, double *d_L, double *d_R, void *stream)
+{
+    const int b = 128, g = (n + b - 1) / b;
+    if (n <= 0) return 0;
+    cudaStream_t s = (cudaStream_t)stream;
+#if WENOFV_HAS_FP32
+    if (fp32) {
+        if (P.kind == EQ_TWO_PHASE) probe_eigen_kernel<EQ_TWO_PHASE, float><<<g, b, 0, s>>>(P, d_U, n, xdir, d_L, d_R);
+        else if (P.kind == EQ_EULER) probe_eigen_kernel<EQ_EULER, float><<<g, b, 0, s>>>(P, d_U, n, xdir, d_L, d_R);
+        else probe_eigen_kernel<EQ_LINEAR_ADV, float><<<g, b, 0, s>>>(P, d_U, n, xdir, d_L, d_R);
+        return (int)cudaGetLastError();
+    }
+#endif
+    if (P.kind == EQ_TWO_PHASE) probe_eigen_kernel<EQ_TWO_PHASE, double><<<g, b, 0, s>>>(P, d_U, n, xdir, d_L, d_R);
+    else if (P.kind == EQ_EULER) probe_eigen_kernel<EQ_EULER, double><<<g, b, 0, s>>>(P, d_U, n, xdir, d_L, d_R);
+    else probe_eigen_kernel<EQ_LINEAR_ADV, double><<<g, b, 0, s>>>(P, d_U, n, xdir, d_L, d_R);
+    return (int)cudaGetLastError();
+}
+
+#if !WENOFV_STRICT
+// FMA throughput of the CUDA-core pipe: independent FMA chains per thread, enough warps to
+// fill every SM (the denominator of the stage kernel's compute roofline).
+template <class R> __global__ void __launch_bounds__(256) fma_peak_kernel(R *out, int iters, R a, R b)
+{
+    R x0 = (R)threadIdx.x, x1 = x0 + R(1), x2 = x0 + R(2), x3 = x0 + R(3), x4 = x0 + R(4), x5 = x0 + R(5), x6 = x0 + R(6), x7 = x0 + R(7);
+#pragma unroll 1
+    for (int k = 0; k < iters; k++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+            x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+        }
+    }
+    const R s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == R(-1.2345)) out[threadIdx.x] = s; // keeps the chains alive
+}
+
+int fma_peak(int fp32, double *tflops, void *stream)
+{
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    void *out = nullptr;
+    if (cudaMalloc(&out, 256 * sizeof(double)) != cudaSuccess) return (int)cudaErrorMemoryAllocation;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = sms * 8, iters = 2048;
+    double best = 0.0;
+    for (int rep = 0; rep < 4; rep++) {
+        cudaEventRecord(e0, s);
+        if (fp32) fma_peak_kernel<float><<<blocks, 256, 0, s>>>((float *)out, iters, 0.999999f, 1e-7f);
+        else fma_peak_kernel<double><<<blocks, 256, 0, s>>>((double *)out, iters, 0.9999999, 1e-9);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double flops = 2.0 * 8 * 16 * (double)iters * blocks * 256;
+        if (rep > 0 && ms > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    *tflops = best;
+    return (int)cudaGetLastError();
+}
+#endif
+
+} // namespace strict / fast
+} // namespace wenofv

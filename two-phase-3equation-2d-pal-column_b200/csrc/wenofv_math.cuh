@@ -1,0 +1,607 @@
+// wenofv_math.cuh -- pointwise device kernels of the WENOFV hot path (sm_100a).
+//
+// Compiled twice: WENOFV_STRICT=1 with -fmad=false reproduces the reference's FP64
+// operation order exactly (no contraction, every division and sqrt where the reference
+// has it); WENOFV_STRICT=0 lets the compiler contract into FMAs and uses reciprocals
+// where the reference divides repeatedly by the same value.  Real is double, or float for
+// the FP32-bulk form (whose pressure recovery stays FP64).
+//
+// Citations are path:line inside the reference project.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "wenofv_types.h"
+
+#ifndef WENOFV_STRICT
+#error "define WENOFV_STRICT (0 or 1)"
+#endif
+
+namespace wenofv {
+#if WENOFV_STRICT
+namespace strict {
+#else
+namespace fast {
+#endif
+
+// std::min / std::max (used unqualified by the reference via `using namespace std`)
+template <class R> __device__ __forceinline__ R std_min(R a, R b) { return (b < a) ? b : a; }
+template <class R> __device__ __forceinline__ R std_max(R a, R b) { return (a < b) ? b : a; }
+// sc_math::Min, third_party/scTools/MyMath.h:52-55
+template <class R> __device__ __forceinline__ R sc_min(R a, R b) { return (a < b) ? a : b; }
+
+// ------------------------------------------------------------------------------------
+// WENO at Gauss-Lobatto points (include/Utility.hpp:5-95 JS, :193-290 Z)
+// ------------------------------------------------------------------------------------
+
+// linear weights, include/Utility.hpp:12-39
+template <class R, int GP> __device__ __forceinline__ void weno_d(R &d0, R &d1, R &d2)
+{
+    if (GP == 0) { d0 = R(0.3); d1 = R(0.6); d2 = R(0.1); }
+    else if (GP == 1) { d0 = R((91.0 - 9.0 * sqrt(5.0)) / 440.0); d1 = R(129.0 / 220.0); d2 = R((91.0 + 9.0 * sqrt(5.0)) / 440.0); }
+    else if (GP == 2) { d0 = R((91.0 + 9.0 * sqrt(5.0)) / 440.0); d1 = R(129.0 / 220.0); d2 = R((91.0 - 9.0 * sqrt(5.0)) / 440.0); }
+    else { d0 = R(0.1); d1 = R(0.6); d2 = R(0.3); }
+}
+
+// candidate polynomials, include/Utility.hpp:64-90 (coefficients folded in double)
+template <class R, int GP>
+__device__ __forceinline__ void weno_h(R umm, R um, R u, R up, R upp, R &h0, R &h1, R &h2)
+{
+    if (GP == 0) {
+        h0 = R(-1.0 / 6.0) * umm + R(5.0 / 6.0) * um + R(1.0 / 3.0) * u;
+        h1 = R(1.0 / 3.0) * um + R(5.0 / 6.0) * u - R(1.0 / 6) * up;
+        h2 = R(11.0 / 6.0) * u - R(7.0 / 6.0) * up + R(1.0 / 3.0) * upp;
+    } else if (GP == 1) {
+        h0 = R(-1.0 / 60.0 - sqrt(5.0) / 20.0) * umm + R(1.0 / 30.0 + sqrt(5.0) / 5.0) * um +
+             R(59.0 / 60.0 - 3 * sqrt(5.0) / 20.0) * u;
+        h1 = R(-1.0 / 60.0 + sqrt(5.0) / 20.0) * um + R(31.0 / 30.0) * u + R(-1.0 / 60 - sqrt(5.0) / 20.0) * up;
+        h2 = R(59.0 / 60.0 + 3 * sqrt(5.0) / 20) * u + R(1.0 / 30.0 - sqrt(5.0) / 5.0) * up +
+             R(-1.0 / 60.0 + sqrt(5.0) / 20.0) * upp;
+    } else if (GP == 2) {
+        h0 = R(-1.0 / 60.0 + sqrt(5.0) / 20.0) * umm + R(1.0 / 30.0 - sqrt(5.0) / 5.0) * um +
+             R(59.0 / 60.0 + 3 * sqrt(5.0) / 20) * u;
+        h1 = R(-1.0 / 60 - sqrt(5.0) / 20.0) * um + R(31.0 / 30.0) * u + R(-1.0 / 60.0 + sqrt(5.0) / 20.0) * up;
+        h2 = R(59.0 / 60.0 - 3 * sqrt(5.0) / 20.0) * u + R(1.0 / 30.0 + sqrt(5.0) / 5.0) * up +
+             R(-1.0 / 60.0 - sqrt(5.0) / 20.0) * upp;
+    } else {
+        h0 = R(1.0 / 3.0) * umm - R(7.0 / 6.0) * um + R(11.0 / 6.0) * u;
+        h1 = R(-1.0 / 6) * um + R(5.0 / 6.0) * u + R(1.0 / 3.0) * up;
+        h2 = R(1.0 / 3.0) * u + R(5.0 / 6.0) * up - R(1.0 / 6.0) * upp;
+    }
+}
+
+template <class R> __device__ __forceinline__ void weno_betas(R umm, R um, R u, R up, R upp, R &b0, R &b1, R &b2)
+{
+    const R t0 = umm - R(4) * um + R(3) * u, s0 = umm - R(2) * um + u;
+    const R t1 = um - up, s1 = um - R(2) * u + up;
+    const R t2 = R(3) * u - R(4) * up + upp, s2 = u - R(2) * up + upp;
+    // pow(x, 2) of include/Utility.hpp:48-50 / :271-273 is x*x
+    b0 = R(0.25) * (t0 * t0) + R(13.0 / 12.0) * (s0 * s0);
+    b1 = R(0.25) * (t1 * t1) + R(13.0 / 12.0) * (s1 * s1);
+    b2 = R(0.25) * (t2 * t2) + R(13.0 / 12.0) * (s2 * s2);
+}
+
+// One 5-point stencil prepared once and evaluated at several Gauss-Lobatto points: the
+// smoothness indicators (and WENO-Z's normalisation) depend on the stencil only, so they
+// are shared across points, which reproduces the per-point reference calls bit for bit.
+template <class R> struct Weno5 {
+    R umm, um, u, up, upp; // raw values (candidate polynomials use these)
+    R g0, g1, g2;          // JS: (eps+beta_k)^2 [strict] or 1/(eps+beta_k)^2 [fast]; Z: 1 + tau/(beta_k+eps)
+    int z;
+
+    __device__ __forceinline__ void init(int scheme, R v0, R v1, R v2, R v3, R v4)
+    {
+        umm = v0; um = v1; u = v2; up = v3; upp = v4;
+        z = scheme;
+        if (scheme == 1) {
+            // WENO-Z: normalise the stencil to [0,1], include/Utility.hpp:261-268
+            const R umax = std_max(std_max(std_max(v0, v1), std_max(v4, v3)), v2);
+            const R umin = std_min(std_min(std_min(v0, v1), std_min(v4, v3)), v2);
+            R n0, n1, n2, n3, n4;
+#if WENOFV_STRICT
+            n0 = (v0 - umin) / (umax - umin + R(1e-20));
+            n1 = (v1 - umin) / (umax - umin + R(1e-20));
+            n2 = (v2 - umin) / (umax - umin + R(1e-20));
+            n3 = (v3 - umin) / (umax - umin + R(1e-20));
+            n4 = (v4 - umin) / (umax - umin + R(1e-20));
+#else
+            const R inv = R(1) / (umax - umin + R(1e-20));
+            n0 = (v0 - umin) * inv; n1 = (v1 - umin) * inv; n2 = (v2 - umin) * inv;
+            n3 = (v3 - umin) * inv; n4 = (v4 - umin) * inv;
+#endif
+            R b0, b1, b2;
+            weno_betas(n0, n1, n2, n3, n4, b0, b1, b2);
+            const R eps = R(1.0e-10);
+            const R tau = fabs(b0 - b2);
+            g0 = R(1) + tau / (b0 + eps);
+            g1 = R(1) + tau / (b1 + eps);
+            g2 = R(1) + tau / (b2 + eps);
+        } else {
+            R b0, b1, b2;
+            weno_betas(v0, v1, v2, v3, v4, b0, b1, b2);
+            const R eps = R(1.0e-6);
+#if WENOFV_STRICT
+            g0 = (eps + b0) * (eps + b0);
+            g1 = (eps + b1) * (eps + b1);
+            g2 = (eps + b2) * (eps + b2);
+#else
+            g0 = R(1) / ((eps + b0) * (eps + b0));
+            g1 = R(1) / ((eps + b1) * (eps + b1));
+            g2 = R(1) / ((eps + b2) * (eps + b2));
+#endif
+        }
+    }
+
+    template <int GP> __device__ __forceinline__ R eval() const
+    {
+        R d0, d1, d2, h0, h1, h2;
+        weno_d<R, GP>(d0, d1, d2);
+        weno_h<R, GP>(umm, um, u, up, upp, h0, h1, h2);
+        R w0, w1, w2;
+        if (z) {
+            w0 = d0 * g0; w1 = d1 * g1; w2 = d2 * g2;
+        } else {
+#if WENOFV_STRICT
+            w0 = d0 / g0; w1 = d1 / g1; w2 = d2 / g2;
+#else
+            w0 = d0 * g0; w1 = d1 * g1; w2 = d2 * g2;
+#endif
+        }
+        const R sum = w0 + w1 + w2;
+#if WENOFV_STRICT
+        w0 = w0 / sum; w1 = w1 / sum; w2 = w2 / sum;
+        return w0 * h0 + w1 * h1 + w2 * h2;
+#else
+        return (w0 * h0 + w1 * h1 + w2 * h2) / sum;
+#endif
+    }
+};
+
+// ------------------------------------------------------------------------------------
+// equations
+// ------------------------------------------------------------------------------------
+
+// Two-phase 3-equation model with linear acoustic EOS (include/Equations.hpp:84-483).
+// U = (z1 rho1, z2 rho2, rho u, rho v).  The volume fraction and pressure recovery always
+// run in FP64 (also in the FP32-bulk form): the cancellation in q - qs and the division by
+// z2 rho2 c2^2 near pure phases need it.
+struct TwoPhaseK {
+    double c1_2, c2_2, q, rho10, rho20;
+    __device__ __forceinline__ explicit TwoPhaseK(const EqParams &p)
+    {
+        c1_2 = p.sound1 * p.sound1;
+        c2_2 = p.sound2 * p.sound2;
+        q = p.rho20 * c2_2 - p.rho10 * c1_2;
+        rho10 = p.rho10;
+        rho20 = p.rho20;
+    }
+    // getVolumeFrac, include/Equations.hpp:84-99
+    __device__ __forceinline__ double volume_frac(double z1rho1, double z2rho2) const
+    {
+        const double qs = z2rho2 * c2_2 - z1rho1 * c1_2;
+        const double r = ((q - qs) + sqrt((q - qs) * (q - qs) + 4.0 * z1rho1 * c1_2 * z2rho2 * c2_2)) / (2.0 * z2rho2 * c2_2);
+        return r / (1.0 + r);
+    }
+    // getPressure, include/Equations.hpp:101-124 (dominant phase, g_preb dropped)
+    __device__ __forceinline__ double pressure(double z1rho1, double z2rho2, double z1) const
+    {
+        const double z2 = 1.0 - z1;
+        const double pre1 = c1_2 * (z1rho1 / z1 - rho10);
+        const double pre2 = c2_2 * (z2rho2 / z2 - rho20);
+        return (z1 < z2) ? pre2 : pre1;
+    }
+    // getSoundSpeed (Wood), include/Equations.hpp:126-146
+    template <class R> __device__ __forceinline__ R sound(R z1rho1, R z2rho2, R z1) const
+    {
+        const R z2 = R(1.0) - z1;
+        const R rho = z1rho1 + z2rho2;
+        const R rho1 = z1rho1 / z1;
+        const R rho2 = z2rho2 / z2;
+        const R sc = sqrt(rho * (z1 / (rho1 * R(c1_2)) + z2 / (rho2 * R(c2_2))));
+        return R(1.0) / sc;
+    }
+};
+
+// Primitive quantities of one state, computed once and reused by every consumer (the
+// reference recomputes getVolumeFrac per call; the values are identical).
+template <class R> struct TPState {
+    R z1rho1, z2rho2, rhou, rhov, rho, u, v, pre, c;
+};
+
+template <class R>
+__device__ __forceinline__ void tp_state(const TwoPhaseK &K, const R *U, TPState<R> &s)
+{
+    s.z1rho1 = U[0]; s.z2rho2 = U[1]; s.rhou = U[2]; s.rhov = U[3];
+    s.rho = s.z1rho1 + s.z2rho2;
+#if WENOFV_STRICT
+    s.u = s.rhou / s.rho;
+    s.v = s.rhov / s.rho;
+#else
+    const R ir = R(1) / s.rho;
+    s.u = s.rhou * ir;
+    s.v = s.rhov * ir;
+#endif
+    const double z1 = K.volume_frac((double)s.z1rho1, (double)s.z2rho2);
+    s.pre = (R)K.pressure((double)s.z1rho1, (double)s.z2rho2, z1);
+    s.c = K.sound<R>(s.z1rho1, s.z2rho2, (R)z1);
+}
+
+// getMaxEigenValue, include/Equations.hpp:149-156 (u from U[2]/(U[0]+U[1]) as there)
+template <class R> __device__ __forceinline__ R tp_max_eig(const TPState<R> &s, double nx, double ny)
+{
+    return fabs(s.u * R(nx) + s.v * R(ny)) + s.c;
+}
+
+// getPhyFlux, include/Equations.hpp:158-186
+template <class R> __device__ __forceinline__ void tp_phy_flux(const TPState<R> &s, R *F, bool xdir)
+{
+    if (xdir) {
+        F[0] = s.z1rho1 * s.u;
+        F[1] = s.z2rho2 * s.u;
+        F[2] = s.rho * (s.u * s.u) + s.pre;
+        F[3] = s.rho * s.u * s.v;
+    } else {
+        F[0] = s.z1rho1 * s.v;
+        F[1] = s.z2rho2 * s.v;
+        F[2] = s.rho * s.v * s.u;
+        F[3] = s.rho * (s.v * s.v) + s.pre;
+    }
+}
+
+// getLLFRiemannFlux, include/Equations.hpp:363-378
+template <class R>
+__device__ __forceinline__ void tp_llf(const TPState<R> &L, const TPState<R> &Rs, const R *UL, const R *UR, R *F, bool xdir)
+{
+    const double nx = xdir ? 1.0 : 0.0, ny = xdir ? 0.0 : 1.0;
+    const R ws = std_max(tp_max_eig(L, nx, ny), tp_max_eig(Rs, nx, ny));
+    R FUL[4], FUR[4];
+    tp_phy_flux(L, FUL, xdir);
+    tp_phy_flux(Rs, FUR, xdir);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) F[r] = R(0.5) * (FUL[r] + FUR[r] - ws * (UR[r] - UL[r]));
+}
+
+// getHLLCRiemannFlux (Zhang & Zhang 2025), include/Equations.hpp:381-483
+template <class R>
+__device__ __forceinline__ void tp_hllc(const TPState<R> &L, const TPState<R> &Rs, const R *UL, const R *UR, R *F, bool xdir)
+{
+    const R nx = xdir ? R(1.0) : R(0.0), ny = xdir ? R(0.0) : R(1.0);
+    const R vn_L = L.u * nx + L.v * ny;
+    const R vn_R = Rs.u * nx + Rs.v * ny;
+    R FUL[4], FUR[4], U[4];
+    FUL[0] = L.z1rho1 * vn_L;
+    FUL[1] = L.z2rho2 * vn_L;
+    FUL[2] = L.rhou * vn_L + L.pre * nx;
+    FUL[3] = L.rhov * vn_L + L.pre * ny;
+    FUR[0] = Rs.z1rho1 * vn_R;
+    FUR[1] = Rs.z2rho2 * vn_R;
+    FUR[2] = Rs.rhou * vn_R + Rs.pre * nx;
+    FUR[3] = Rs.rhov * vn_R + Rs.pre * ny;
+    const R sL = sqrt(L.rho), sR = sqrt(Rs.rho);
+#if WENOFV_STRICT
+    const R vn_roe = (vn_L * sL + vn_R * sR) / (sL + sR);
+    R c2_roe = (L.c * L.c * sL + Rs.c * Rs.c * sR) / (sL + sR);
+    c2_roe += R(0.5) * sL * sR / (sL + sR) / (sL + sR) * (vn_R - vn_L) * (vn_R - vn_L);
+#else
+    const R is = R(1) / (sL + sR);
+    const R vn_roe = (vn_L * sL + vn_R * sR) * is;
+    R c2_roe = (L.c * L.c * sL + Rs.c * Rs.c * sR) * is;
+    c2_roe += R(0.5) * sL * sR * is * is * (vn_R - vn_L) * (vn_R - vn_L);
+#endif
+    const R c_roe = sqrt(c2_roe);
+    const R S_L = std_min(vn_L - L.c, vn_roe - c_roe);
+    const R S_R = std_max(vn_R + Rs.c, vn_roe + c_roe);
+    const R S_star = ((S_L - vn_L) * L.rho * vn_L - (S_R - vn_R) * Rs.rho * vn_R + Rs.pre - L.pre) /
+                     ((S_L - vn_L) * L.rho - (S_R - vn_R) * Rs.rho);
+    if (S_star >= R(0)) {
+        if (S_L >= R(0.0)) {
+#pragma unroll
+            for (int r = 0; r < 4; r++) F[r] = FUL[r];
+        } else {
+            const R k = (S_L - vn_L) / (S_L - S_star);
+            U[0] = L.z1rho1;
+            U[1] = L.z2rho2;
+            U[2] = L.rho * (L.u + (S_star - vn_L) * nx);
+            U[3] = L.rho * (L.v + (S_star - vn_L) * ny);
+#pragma unroll
+            for (int r = 0; r < 4; r++) F[r] = S_L * (k * U[r] - UL[r]) + FUL[r];
+        }
+    } else {
+        if (S_R <= R(0)) {
+#pragma unroll
+            for (int r = 0; r < 4; r++) F[r] = FUR[r];
+        } else {
+            const R k = (S_R - vn_R) / (S_R - S_star);
+            U[0] = Rs.z1rho1;
+            U[1] = Rs.z2rho2;
+            U[2] = Rs.rho * (Rs.u + (S_star - vn_R) * nx);
+            U[3] = Rs.rho * (Rs.v + (S_star - vn_R) * ny);
+#pragma unroll
+            for (int r = 0; r < 4; r++) F[r] = S_R * (k * U[r] - UR[r]) + FUR[r];
+        }
+    }
+}
+
+// Characteristic matrices of the two-phase system, include/Equations.hpp:189-327.
+// Row k of L and row r of R in direction x (xdir) or y.
+template <class R> struct TPEigen {
+    R z1rho1, z2rho2, rho, u, v, c, c2, sc1_2, sc2_2;
+};
+template <class R> __device__ __forceinline__ void tp_eigen_prep(const TwoPhaseK &K, const R *U, TPEigen<R> &e)
+{
+    e.z1rho1 = U[0]; e.z2rho2 = U[1];
+    e.rho = e.z1rho1 + e.z2rho2;
+    e.u = U[2] / e.rho;
+    e.v = U[3] / e.rho;
+    const double z1d = K.volume_frac((double)U[0], (double)U[1]);
+    const R z1 = (R)z1d;
+    const R z2 = R(1.0) - z1;
+    e.c = K.sound<R>(e.z1rho1, e.z2rho2, z1);
+    e.c2 = e.c * e.c;
+    const R c1_2 = R(K.c1_2), c2_2 = R(K.c2_2);
+    const R zrho1 = e.z1rho1 * c1_2 / (z1 * z1);
+    const R zrho2 = e.z2rho2 * c2_2 / (z2 * z2);
+    e.sc1_2 = c1_2 / z1 - c1_2 / z1 * zrho1 / (zrho1 + zrho2);
+    e.sc2_2 = c2_2 / z2 - c2_2 / z2 * zrho2 / (zrho1 + zrho2);
+}
+template <class R> __device__ __forceinline__ void tp_L_row(const TPEigen<R> &e, bool xdir, int k, R *row)
+{
+    const R un = xdir ? e.u : e.v, ut = xdir ? e.v : e.u;
+    switch (k) {
+    case 0:
+        row[0] = (e.sc1_2 + e.c * un) / (R(2.0) * e.c2);
+        row[1] = (e.sc2_2 + e.c * un) / (R(2.0) * e.c2);
+        row[2] = xdir ? R(-1.0) / (R(2.0) * e.c) : R(0);
+        row[3] = xdir ? R(0) : R(-1.0) / (R(2.0) * e.c);
+        break;
+    case 1:
+        row[0] = -e.z2rho2 * (e.sc1_2 - e.sc2_2) / (e.rho * e.c2);
+        row[1] = e.z1rho1 * (e.sc1_2 - e.sc2_2) / (e.rho * e.c2);
+        row[2] = R(0);
+        row[3] = R(0);
+        break;
+    case 2:
+        row[0] = -ut;
+        row[1] = -ut;
+        row[2] = xdir ? R(0) : R(1.0);
+        row[3] = xdir ? R(1.0) : R(0);
+        break;
+    default:
+        row[0] = (e.sc1_2 - e.c * un) / (R(2.0) * e.c2);
+        row[1] = (e.sc2_2 - e.c * un) / (R(2.0) * e.c2);
+        row[2] = xdir ? R(1.0) / (R(2.0) * e.c) : R(0);
+        row[3] = xdir ? R(0) : R(1.0) / (R(2.0) * e.c);
+        break;
+    }
+}
+template <class R> __device__ __forceinline__ void tp_R_row(const TPEigen<R> &e, bool xdir, int r, R *row)
+{
+    switch (r) {
+    case 0:
+        row[0] = e.z1rho1 / e.rho;
+        row[1] = -e.sc2_2 / (e.sc1_2 - e.sc2_2);
+        row[2] = R(0);
+        row[3] = e.z1rho1 / e.rho;
+        break;
+    case 1:
+        row[0] = e.z2rho2 / e.rho;
+        row[1] = e.sc1_2 / (e.sc1_2 - e.sc2_2);
+        row[2] = R(0);
+        row[3] = e.z2rho2 / e.rho;
+        break;
+    case 2:
+        row[0] = xdir ? e.u - e.c : e.u;
+        row[1] = e.u;
+        row[2] = xdir ? R(0) : R(1);
+        row[3] = xdir ? e.u + e.c : e.u;
+        break;
+    default:
+        row[0] = xdir ? e.v : e.v - e.c;
+        row[1] = e.v;
+        row[2] = xdir ? R(1) : R(0);
+        row[3] = xdir ? e.v : e.v + e.c;
+        break;
+    }
+}
+
+// ---- Euler, gamma-law gas, U = (rho, rho u, rho v, E).  No counterpart in the reference;
+//      restated from the standard formulation (Toro, ch. 3 and 10) in the oracle's order.
+template <class R> struct EUState {
+    R rho, u, v, E, p, c, H;
+};
+template <class R> __device__ __forceinline__ void eu_state(double gamma, const R *U, EUState<R> &s)
+{
+    s.rho = U[0];
+    s.u = U[1] / U[0];
+    s.v = U[2] / U[0];
+    s.E = U[3];
+    s.p = R(gamma - 1.0) * (U[3] - R(0.5) * U[0] * (s.u * s.u + s.v * s.v));
+    s.c = sqrt(R(gamma) * s.p / U[0]);
+    s.H = (U[3] + s.p) / U[0];
+}
+template <class R> __device__ __forceinline__ void eu_phy_flux(const EUState<R> &s, const R *U, R *F, R nx, R ny)
+{
+    const R vn = s.u * nx + s.v * ny;
+    F[0] = U[0] * vn;
+    F[1] = U[1] * vn + s.p * nx;
+    F[2] = U[2] * vn + s.p * ny;
+    F[3] = (U[3] + s.p) * vn;
+}
+template <class R>
+__device__ __forceinline__ void eu_llf(const EUState<R> &L, const EUState<R> &Rs, const R *UL, const R *UR, R *F, bool xdir)
+{
+    const R nx = xdir ? R(1) : R(0), ny = xdir ? R(0) : R(1);
+    const R wl = fabs(L.u * nx + L.v * ny) + L.c, wr = fabs(Rs.u * nx + Rs.v * ny) + Rs.c;
+    const R ws = std_max(wl, wr);
+    R FL[4], FR[4];
+    eu_phy_flux(L, UL, FL, nx, ny);
+    eu_phy_flux(Rs, UR, FR, nx, ny);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) F[r] = R(0.5) * (FL[r] + FR[r] - ws * (UR[r] - UL[r]));
+}
+template <class R>
+__device__ __forceinline__ void eu_hllc(double gamma, const EUState<R> &L, const EUState<R> &Rs, const R *UL, const R *UR, R *F, bool xdir)
+{
+    const R nx = xdir ? R(1) : R(0), ny = xdir ? R(0) : R(1);
+    const R rL = L.rho, rR = Rs.rho;
+    const R vnL = L.u * nx + L.v * ny, vnR = Rs.u * nx + Rs.v * ny;
+    const R sL = sqrt(rL), sR = sqrt(rR);
+    const R inv = R(1.0) / (sL + sR);
+    const R ur = (sL * L.u + sR * Rs.u) * inv, vr = (sL * L.v + sR * Rs.v) * inv;
+    const R Hr = (sL * L.H + sR * Rs.H) * inv;
+    const R vnr = ur * nx + vr * ny;
+    const R cr = sqrt(R(gamma - 1.0) * (Hr - R(0.5) * (ur * ur + vr * vr)));
+    const R S_L = std_min(vnL - L.c, vnr - cr);
+    const R S_R = std_max(vnR + Rs.c, vnr + cr);
+    const R S_star = (Rs.p - L.p + rL * vnL * (S_L - vnL) - rR * vnR * (S_R - vnR)) / (rL * (S_L - vnL) - rR * (S_R - vnR));
+    R FL[4], FR[4];
+    eu_phy_flux(L, UL, FL, nx, ny);
+    eu_phy_flux(Rs, UR, FR, nx, ny);
+    if (S_L >= R(0.0)) {
+#pragma unroll
+        for (int r = 0; r < 4; r++) F[r] = FL[r];
+    } else if (S_star >= R(0.0)) {
+        const R k = rL * (S_L - vnL) / (S_L - S_star);
+        R Us[4];
+        Us[0] = k;
+        Us[1] = k * (L.u + (S_star - vnL) * nx);
+        Us[2] = k * (L.v + (S_star - vnL) * ny);
+        Us[3] = k * (UL[3] / rL + (S_star - vnL) * (S_star + L.p / (rL * (S_L - vnL))));
+#pragma unroll
+        for (int r = 0; r < 4; r++) F[r] = FL[r] + S_L * (Us[r] - UL[r]);
+    } else if (S_R > R(0.0)) {
+        const R k = rR * (S_R - vnR) / (S_R - S_star);
+        R Us[4];
+        Us[0] = k;
+        Us[1] = k * (Rs.u + (S_star - vnR) * nx);
+        Us[2] = k * (Rs.v + (S_star - vnR) * ny);
+        Us[3] = k * (UR[3] / rR + (S_star - vnR) * (S_star + Rs.p / (rR * (S_R - vnR))));
+#pragma unroll
+        for (int r = 0; r < 4; r++) F[r] = FR[r] + S_R * (Us[r] - UR[r]);
+    } else {
+#pragma unroll
+        for (int r = 0; r < 4; r++) F[r] = FR[r];
+    }
+}
+// Euler eigenvectors in direction n (columns of R: u-c, entropy, shear, u+c)
+template <class R> __device__ __forceinline__ void eu_L_row(double gamma, const EUState<R> &s, bool xdir, int k, R *row)
+{
+    const R nx = xdir ? R(1) : R(0), ny = xdir ? R(0) : R(1);
+    const R q2 = R(0.5) * (s.u * s.u + s.v * s.v);
+    const R vn = s.u * nx + s.v * ny, vt = s.v * nx - s.u * ny;
+    const R b1 = R(gamma - 1.0) / (s.c * s.c), b2 = q2 * b1;
+    switch (k) {
+    case 0:
+        row[0] = R(0.5) * (b2 + vn / s.c); row[1] = R(0.5) * (-b1 * s.u - nx / s.c);
+        row[2] = R(0.5) * (-b1 * s.v - ny / s.c); row[3] = R(0.5) * b1;
+        break;
+    case 1:
+        row[0] = R(1.0) - b2; row[1] = b1 * s.u; row[2] = b1 * s.v; row[3] = -b1;
+        break;
+    case 2:
+        row[0] = -vt; row[1] = -ny; row[2] = nx; row[3] = R(0.0);
+        break;
+    default:
+        row[0] = R(0.5) * (b2 - vn / s.c); row[1] = R(0.5) * (-b1 * s.u + nx / s.c);
+        row[2] = R(0.5) * (-b1 * s.v + ny / s.c); row[3] = R(0.5) * b1;
+        break;
+    }
+}
+template <class R> __device__ __forceinline__ void eu_R_row(const EUState<R> &s, bool xdir, int r, R *row)
+{
+    const R nx = xdir ? R(1) : R(0), ny = xdir ? R(0) : R(1);
+    const R q2 = R(0.5) * (s.u * s.u + s.v * s.v);
+    const R vn = s.u * nx + s.v * ny, vt = s.v * nx - s.u * ny;
+    switch (r) {
+    case 0: row[0] = R(1.0); row[1] = R(1.0); row[2] = R(0.0); row[3] = R(1.0); break;
+    case 1: row[0] = s.u - s.c * nx; row[1] = s.u; row[2] = -ny; row[3] = s.u + s.c * nx; break;
+    case 2: row[0] = s.v - s.c * ny; row[1] = s.v; row[2] = nx; row[3] = s.v + s.c * ny; break;
+    default: row[0] = s.H - s.c * vn; row[1] = q2; row[2] = vt; row[3] = s.H + s.c * vn; break;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// equation dispatch (the equation kind is a template parameter of every kernel)
+// ------------------------------------------------------------------------------------
+template <int EQ> struct EqTraits { static constexpr int NV = 4; };
+template <> struct EqTraits<EQ_LINEAR_ADV> { static constexpr int NV = 1; };
+
+// getMaxEigenValue (include/Equations.hpp:149-156) for the CFL and the limiter's mu
+template <int EQ, class R> __device__ __forceinline__ void max_eigs(const EqParams &P, const R *U, R &ax, R &ay)
+{
+    if (EQ == EQ_TWO_PHASE) {
+        TwoPhaseK K(P);
+        TPState<R> s;
+        tp_state<R>(K, U, s);
+        ax = tp_max_eig(s, 1.0, 0.0);
+        ay = tp_max_eig(s, 0.0, 1.0);
+    } else if (EQ == EQ_EULER) {
+        EUState<R> s;
+        eu_state<R>(P.gamma, U, s);
+        ax = fabs(s.u * R(1.0) + s.v * R(0.0)) + s.c;
+        ay = fabs(s.u * R(0.0) + s.v * R(1.0)) + s.c;
+    } else {
+        ax = fabs(R(P.adv_u) * R(1.0) + R(P.adv_v) * R(0.0));
+        ay = fabs(R(P.adv_u) * R(0.0) + R(P.adv_v) * R(1.0));
+    }
+}
+
+// getRiemannFlux dispatch (include/Equations.hpp:329-343); flux 0 LLF, 1 HLLC.
+// For scalar advection both are the upwind (LLF with |a.n|) flux.
+template <int EQ, class R>
+__device__ __forceinline__ void riemann(const EqParams &P, int flux, const R *UL, const R *UR, R *F, bool xdir)
+{
+    if (EQ == EQ_TWO_PHASE) {
+        TwoPhaseK K(P);
+        TPState<R> l, r;
+        tp_state<R>(K, UL, l);
+        tp_state<R>(K, UR, r);
+        if (flux == 1) tp_hllc<R>(l, r, UL, UR, F, xdir);
+        else tp_llf<R>(l, r, UL, UR, F, xdir);
+    } else if (EQ == EQ_EULER) {
+        EUState<R> l, r;
+        eu_state<R>(P.gamma, UL, l);
+        eu_state<R>(P.gamma, UR, r);
+        if (flux == 1) eu_hllc<R>(P.gamma, l, r, UL, UR, F, xdir);
+        else eu_llf<R>(l, r, UL, UR, F, xdir);
+    } else {
+        const R an = xdir ? (R(P.adv_u) * R(1.0) + R(P.adv_v) * R(0.0)) : (R(P.adv_u) * R(0.0) + R(P.adv_v) * R(1.0));
+        const R ws = std_max(fabs(an), fabs(an));
+        F[0] = R(0.5) * (an * UL[0] + an * UR[0] - ws * (UR[0] - UL[0]));
+    }
+}
+
+// Characteristic projection rows: row k of L and row k of R for the state U.
+template <int EQ, class R>
+__device__ __forceinline__ void eigen_rows(const EqParams &P, const R *U, bool xdir, int k, R *Lrow, R *Rrow)
+{
+    if (EQ == EQ_TWO_PHASE) {
+        TwoPhaseK K(P);
+        TPEigen<R> e;
+        tp_eigen_prep<R>(K, U, e);
+        tp_L_row<R>(e, xdir, k, Lrow);
+        tp_R_row<R>(e, xdir, k, Rrow);
+    } else if (EQ == EQ_EULER) {
+        EUState<R> s;
+        eu_state<R>(P.gamma, U, s);
+        eu_L_row<R>(P.gamma, s, xdir, k, Lrow);
+        eu_R_row<R>(s, xdir, k, Rrow);
+    } else {
+        Lrow[0] = R(1.0);
+        Rrow[0] = R(1.0);
+    }
+}
+
+// number of leading variables the bound-preserving limiter acts on: the two partial
+// densities of the two-phase model (src/WENOFV.cpp:1964), the density for Euler, none for
+// scalar advection
+template <int EQ> struct LimitedVars { static constexpr int N = EQ == EQ_TWO_PHASE ? 2 : (EQ == EQ_EULER ? 1 : 0); };
+
+// Gauss-Lobatto 4-point weights as written at third_party/scTools/GaussQuadratureInRef.hpp:252-262
+__device__ __forceinline__ double gl_weight(int gp)
+{
+    return (gp == 0 || gp == 3) ? 0.166666666666666666666666666667 : 0.833333333333333333333333333333;
+}
+
+} // namespace strict / fast
+} // namespace wenofv

@@ -1,0 +1,516 @@
+// wenofv_stage.cuh -- the fused RK-stage kernel of the WENOFV hot path (sm_100a).
+//
+// One launch performs one SSP-RK stage for every work item of every instance it is given:
+// ghost fill (as periodic/outflow index maps on load) -> y-direction WENO sweep ->
+// x-direction WENO sweep -> bound-preserving theta limiter -> Riemann fluxes at the face
+// Gauss-Lobatto points -> GL quadrature -> RHS -> RK combination -> (final stage) CFL
+// max-wavespeed reduction.  Nothing but the cell averages touches HBM.
+//
+// A work item is a strip of TX columns and a run of rows of one instance.  The CTA streams
+// through the rows: iteration r loads row r+3 (cp.async into an 8-row ring), sweeps row r
+// in y, reconstructs the face states of row r in x, solves the Riemann problems of row r's
+// x-faces and of the y-faces between rows r-1 and r, and updates row r-1.  The y-sweep of a
+// column is shared by the 7 cells whose stencils contain it (the reference recomputes it
+// per cell, src/WENOFV.cpp:670-687 and :796-833, with identical operands).
+//
+// Thread mapping (NT = 128 threads): a unit of the y-sweep is (position, variable), of the
+// x-sweep (cell, variable), of the Riemann phase (face, Gauss point) and of the update
+// (cell, variable); groups of NV (or 4) consecutive lanes belong to the same position, cell
+// or face, so characteristic projections, the limiter's theta and the GL quadrature sums
+// exchange values by warp shuffles.  TX = NT/NV - 6 makes the y-sweep exactly one unit per
+// thread.
+#pragma once
+#include "wenofv_math.cuh"
+
+namespace wenofv {
+#if WENOFV_STRICT
+namespace strict {
+#else
+namespace fast {
+#endif
+
+constexpr int NT = 128;
+constexpr int G = 3; // ghost layers / stencil half-width, src/WENOFV.cpp:59
+
+__device__ __forceinline__ int map_index(int k, int n, int bc)
+{
+    if (bc == 5) return k < 0 ? 0 : (k >= n ? n - 1 : k); // outflow: zero-gradient copy
+    k %= n;
+    return k < 0 ? k + n : k; // periodic wrap (2-D, corners included)
+}
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+__device__ __forceinline__ void flag_error(InstState *st, unsigned int f, long long cell)
+{
+    atomicOr(&st->flags, f);
+    atomicCAS((unsigned long long *)&st->bad_cell, (unsigned long long)-1LL, (unsigned long long)cell);
+}
+
+// finalize one instance after its final stage (or after the initial CFL pass): the
+// bookkeeping of CWENOFV::run's loop, src/WENOFV.cpp:323-332
+__device__ __forceinline__ void finalize_instance(InstState *st, int fin_kind, int out_buf)
+{
+    if (st->done) return;
+    const double dtcfl = __longlong_as_double((long long)st->accum);
+    st->accum = (unsigned long long)__double_as_longlong(1.0); // calculateDeltaT starts from 1.0 (:477)
+    st->dtcfl = dtcfl;
+    if (fin_kind == FIN_STEP) st->cur_buf = out_buf;
+    if (st->mode != MODE_ADVANCE) return;
+    if (fin_kind == FIN_STEP) {
+        st->now += st->dt;
+        st->nsteps++;
+    }
+    if (st->flags & 1u) { st->done = 1; return; } // NaN time step: stop (the reference aborts)
+    if (fabs(st->now - st->t_end) <= 1e-10 || (st->max_steps > 0 && st->nsteps >= st->max_steps)) {
+        st->done = 1;
+        return;
+    }
+    const double remaining = st->t_end - st->now;
+    st->dt = (remaining < dtcfl) ? remaining : dtcfl; // std::min(timestep, remainingTime)
+}
+
+// last-CTA-done pattern: the CTA that finishes last finalizes the launch's instances
+__device__ __forceinline__ void launch_epilogue(const StageLaunch &L, int fin_kind, int *s_last)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int t = atomicAdd(L.counter, 1u);
+        *s_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (*s_last) {
+        __threadfence();
+        for (int k = threadIdx.x; k < L.nfin; k += blockDim.x) finalize_instance(&L.state[L.fin_ids[k]], fin_kind, L.bout);
+        __syncthreads();
+        if (threadIdx.x == 0) *L.counter = 0u;
+    }
+}
+
+__device__ __forceinline__ void cfl_atomic_min(InstState *st, double v)
+{
+    if (v >= 0.0) atomicMin(&st->accum, (unsigned long long)__double_as_longlong(v));
+}
+
+// block-wide minimum of a non-negative double (+inf for idle threads)
+__device__ __forceinline__ double block_min(double v, double *s_red)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) s_red[w] = v;
+    __syncthreads();
+    double m = s_red[0];
+    for (int k = 1; k < (int)(blockDim.x >> 5); k++) m = fmin(m, s_red[k]);
+    return m;
+}
+
+template <int EQ> struct StageGeom {
+    static constexpr int NV = EqTraits<EQ>::NV;
+    static constexpr int TX = NT / NV - 2 * G; // interior columns per strip
+    static constexpr int P = TX + 2 * G;       // y-sweep positions per row
+};
+
+// shared memory of one CTA (doubles)
+template <int EQ> struct StageSmem {
+    static constexpr int NV = StageGeom<EQ>::NV, TX = StageGeom<EQ>::TX, P = StageGeom<EQ>::P;
+    double su[8][NV][P];          // ring of stage-input rows
+    double sun[2][NV][P];         // U^n rows (stages after the first)
+    double sy[P][4][NV];          // y-sweep of the current row: [position][y GL point][var]
+    double sxf[TX + 1][2][4][NV]; // x-face states: [face][minus/plus side][GL point][var]
+    double syb[TX][4][NV];        // bottom face states of the current row
+    double syt[2][TX][4][NV];     // top face states of the current and previous row
+    double sfx[2][TX + 1][NV];    // x-face quadrature sums of two rows
+    double sfy[2][TX][NV];        // y-face quadrature sums below the current and previous row
+    double sdxc[TX], sdxl[TX];    // column widths of the strip
+    double sred[NT / 32];
+    int s_last;
+};
+
+// one row of NV x P stage values into shared memory (ghost fill = index map), cp.async 8 B
+template <int EQ>
+__device__ __forceinline__ void load_row(double (*dst)[StageGeom<EQ>::P], const double *buf, const InstDesc &D, int row, int i0)
+{
+    constexpr int P = StageGeom<EQ>::P, NV = StageGeom<EQ>::NV;
+    const int jj = map_index(row, D.ny, D.bc);
+    const size_t plane = (size_t)D.ny * D.pitch;
+#pragma unroll
+    for (int e = threadIdx.x; e < NV * P; e += NT) {
+        const int v = e / P, p = e - v * P;
+        const int ii = map_index(i0 - G + p, D.nx, D.bc);
+        cp_async8(&dst[v][p], buf + v * plane + (size_t)jj * D.pitch + ii);
+    }
+}
+
+// ---- phase 1: y-direction sweep of row r (src/WENOFV.cpp:670-687, :796-833) ------------
+template <int EQ, int RECON, class R>
+__device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D, int r)
+{
+    constexpr int NV = StageGeom<EQ>::NV;
+    const int t = threadIdx.x;
+    const int p = t / NV, v = t - p * NV;
+    if (RECON == 0 || NV == 1) {
+        Weno5<R> W;
+        W.init(D.scheme, (R)S.su[(r - 2) & 7][v][p], (R)S.su[(r - 1) & 7][v][p], (R)S.su[r & 7][v][p],
+               (R)S.su[(r + 1) & 7][v][p], (R)S.su[(r + 2) & 7][v][p]);
+        S.sy[p][0][v] = (double)W.template eval<0>();
+        S.sy[p][1][v] = (double)W.template eval<1>();
+        S.sy[p][2][v] = (double)W.template eval<2>();
+        S.sy[p][3][v] = (double)W.template eval<3>();
+    } else {
+        // characteristic: project with L(U_centre, y), reconstruct, project back with R(U_centre, y)
+        R Uc[NV], Lrow[NV], Rrow[NV], pr[5];
+#pragma unroll
+        for (int j = 0; j < NV; j++) Uc[j] = (R)S.su[r & 7][j][p];
+        eigen_rows<EQ, R>(D.eq, Uc, false, v, Lrow, Rrow);
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            R s = R(0.0);
+#pragma unroll
+            for (int j = 0; j < NV; j++) s += Lrow[j] * (R)S.su[(r - 2 + m) & 7][j][p];
+            pr[m] = s;
+        }
+        Weno5<R> W;
+        W.init(D.scheme, pr[0], pr[1], pr[2], pr[3], pr[4]);
+        R cg[4];
+        cg[0] = W.template eval<0>();
+        cg[1] = W.template eval<1>();
+        cg[2] = W.template eval<2>();
+        cg[3] = W.template eval<3>();
+        const int lane = t & 31, gbase = lane & ~(NV - 1);
+#pragma unroll
+        for (int gp = 0; gp < 4; gp++) {
+            R s = R(0.0);
+#pragma unroll
+            for (int k = 0; k < NV; k++) s += Rrow[k] * __shfl_sync(0xffffffffu, cg[gp], gbase + k);
+            S.sy[p][gp][v] = (double)s;
+        }
+    }
+}
+
+// ---- phase 2: x-direction sweep + limiter of row r (src/WENOFV.cpp:690-721, :836-880,
+//      limiter :1895-2000) -> face states -----------------------------------------------
+template <int EQ, int RECON, class R>
+__device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D, InstState *st, int r, int i0, int TXe)
+{
+    constexpr int NV = StageGeom<EQ>::NV, TX = StageGeom<EQ>::TX;
+    const int t = threadIdx.x;
+    const int cu = t / NV, v = t - cu * NV;
+    const bool active = cu < TX + 2;
+    const int c = (active ? cu : TX + 1) - 1; // cell in [-1, TX]
+    const int lane = t & 31, gbase = lane & ~(NV - 1);
+    R ug[4][4]; // [gpi][gpj] of variable v (boundary points only)
+
+    if (RECON == 0 || NV == 1) {
+#pragma unroll
+        for (int gpj = 0; gpj < 4; gpj++) {
+            Weno5<R> W;
+            W.init(D.scheme, (R)S.sy[c + 1][gpj][v], (R)S.sy[c + 2][gpj][v], (R)S.sy[c + 3][gpj][v],
+                   (R)S.sy[c + 4][gpj][v], (R)S.sy[c + 5][gpj][v]);
+            ug[0][gpj] = W.template eval<0>();
+            ug[3][gpj] = W.template eval<3>();
+            if (gpj == 0 || gpj == 3) {
+                ug[1][gpj] = W.template eval<1>();
+                ug[2][gpj] = W.template eval<2>();
+            }
+        }
+    } else {
+        R Uc[NV], Lrow[NV], Rrow[NV];
+#pragma unroll
+        for (int j = 0; j < NV; j++) Uc[j] = (R)S.su[r & 7][j][c + G];
+        eigen_rows<EQ, R>(D.eq, Uc, true, v, Lrow, Rrow);
+        R cg[4][4];
+#pragma unroll
+        for (int gpj = 0; gpj < 4; gpj++) {
+            R pr[5];
+#pragma unroll
+            for (int m = 0; m < 5; m++) {
+                R s = R(0.0);
+#pragma unroll
+                for (int j = 0; j < NV; j++) s += Lrow[j] * (R)S.sy[c + 1 + m][gpj][j];
+                pr[m] = s;
+            }
+            Weno5<R> W;
+            W.init(D.scheme, pr[0], pr[1], pr[2], pr[3], pr[4]);
+            cg[0][gpj] = W.template eval<0>();
+            cg[3][gpj] = W.template eval<3>();
+            if (gpj == 0 || gpj == 3) {
+                cg[1][gpj] = W.template eval<1>();
+                cg[2][gpj] = W.template eval<2>();
+            }
+        }
+#pragma unroll
+        for (int gpj = 0; gpj < 4; gpj++)
+#pragma unroll
+            for (int gpi = 0; gpi < 4; gpi++) {
+                if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
+                R s = R(0.0);
+#pragma unroll
+                for (int k = 0; k < NV; k++) s += Rrow[k] * __shfl_sync(0xffffffffu, cg[gpi][gpj], gbase + k);
+                ug[gpi][gpj] = s;
+            }
+    }
+
+    // bound-preserving limiter: theta from the partial densities, in FP64 in every form
+    constexpr int NLIM = LimitedVars<EQ>::N;
+    if (NLIM > 0 && D.limiter) {
+        double ub[NV];
+#pragma unroll
+        for (int j = 0; j < NV; j++) ub[j] = S.su[r & 7][j][c + G];
+        double a1, a2;
+        max_eigs<EQ, double>(D.eq, ub, a1, a2);
+        const double mu1 = (a1 / D.dX) / (a1 / D.dX + a2 / D.dY);
+        const double mu2 = (a2 / D.dY) / (a1 / D.dX + a2 / D.dY);
+        double th = 1.0;
+        if (v < NLIM) {
+            const double uave = ub[v];
+            const double zeps = 1e-12, omega1 = 0.1, omegaR = 1.0 - 2 * omega1;
+            const double eps = std_min(zeps, uave);
+            double rem = uave;
+#pragma unroll
+            for (int gp = 0; gp < 4; gp++) {
+                const double w = gl_weight(gp);
+                rem -= omega1 * w / 2 * mu2 * (double)ug[gp][0];
+                rem -= omega1 * w / 2 * mu2 * (double)ug[gp][3];
+                rem -= omega1 * w / 2 * mu1 * (double)ug[0][gp];
+                rem -= omega1 * w / 2 * mu1 * (double)ug[3][gp];
+            }
+            rem /= omegaR;
+            double mloc = rem;
+#pragma unroll
+            for (int gp = 0; gp < 4; gp++) {
+                mloc = sc_min(mloc, (double)ug[gp][0]);
+                mloc = sc_min(mloc, (double)ug[gp][3]);
+                mloc = sc_min(mloc, (double)ug[0][gp]);
+                mloc = sc_min(mloc, (double)ug[3][gp]);
+            }
+            th = sc_min(fabs((uave - eps) / (uave - mloc)), th);
+        }
+        const double t0 = __shfl_sync(0xffffffffu, th, gbase + 0);
+        const double t1 = __shfl_sync(0xffffffffu, th, gbase + (NLIM > 1 ? 1 : 0));
+        const double theta = NLIM == 2 ? sc_min(t0, t1) : t0;
+        if (theta >= 0.0 && theta <= 1.0) {
+            const double u0 = ub[v];
+#pragma unroll
+            for (int gpj = 0; gpj < 4; gpj++)
+#pragma unroll
+                for (int gpi = 0; gpi < 4; gpi++) {
+                    if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
+                    ug[gpi][gpj] = (R)(theta * ((double)ug[gpi][gpj] - u0) + u0);
+                }
+        } else if (active && v == 0 && c >= 0 && c < TXe) {
+            flag_error(st, 2u, (long long)map_index(r, D.ny, D.bc) * D.nx + i0 + c);
+        }
+    }
+
+    if (active) {
+#pragma unroll
+        for (int gp = 0; gp < 4; gp++) {
+            if (c >= 0) S.sxf[c][1][gp][v] = (double)ug[0][gp];     // left face: plus side of face c
+            if (c < TX) S.sxf[c + 1][0][gp][v] = (double)ug[3][gp]; // right face: minus side of face c+1
+            if (c >= 0 && c < TX) {
+                S.syb[c][gp][v] = (double)ug[gp][0];
+                S.syt[r & 1][c][gp][v] = (double)ug[gp][3];
+            }
+        }
+    }
+}
+
+// ---- phase 3: Riemann fluxes + Gauss-Lobatto quadrature (src/WENOFV.cpp:1707-1799) -----
+// x-faces of row r (when r is an interior row of the item) and y-faces between rows r-1
+// and r (when r-1 >= j0-1 and r <= j1).  Four consecutive lanes hold the four Gauss
+// points of one face; lane gp = 0 sums them in the reference's order.
+template <int EQ, class R>
+__device__ __forceinline__ void phase_riemann(StageSmem<EQ> &S, const InstDesc &D, InstState *st, int r, int i0, int j0, int j1, int TXe)
+{
+    constexpr int NV = StageGeom<EQ>::NV, TX = StageGeom<EQ>::TX;
+    const int nxf = (r >= j0 && r < j1) ? (TX + 1) * 4 : 0;
+    const int nyf = (r >= j0 && r <= j1) ? TX * 4 : 0;
+    const int total = nxf + nyf;
+    if (total == 0) return;
+    const int lane = threadIdx.x & 31, g4 = lane & ~3;
+    const double dyr = (r >= j0 && r < j1) ? D.dy[r] : 1.0;
+    for (int base = 0; base < total; base += NT) {
+        const int u = base + threadIdx.x;
+        const bool act = u < total;
+        const int uu = act ? u : total - 1;
+        const bool xf = uu < nxf;
+        const int f = xf ? (uu >> 2) : ((uu - nxf) >> 2);
+        const int gp = uu & 3;
+        R UL[NV], UR[NV], F[NV];
+        if (xf) {
+#pragma unroll
+            for (int v = 0; v < NV; v++) { UL[v] = (R)S.sxf[f][0][gp][v]; UR[v] = (R)S.sxf[f][1][gp][v]; }
+        } else {
+#pragma unroll
+            for (int v = 0; v < NV; v++) { UL[v] = (R)S.syt[(r - 1) & 1][f][gp][v]; UR[v] = (R)S.syb[f][gp][v]; }
+        }
+        riemann<EQ, R>(D.eq, D.flux, UL, UR, F, xf);
+        // gWeight = m_gweights_ref[gp] * (cell size) / 2.0 (src/WENOFV.cpp:1774, :1793)
+        const double wq = xf ? gl_weight(gp) * dyr / 2.0 : gl_weight(gp) * S.sdxc[f] / 2.0;
+        bool bad = false;
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            const double pv = (double)F[v] * wq;
+            bad |= isnan(pv);
+            const double p1 = __shfl_sync(0xffffffffu, pv, g4 + 1);
+            const double p2 = __shfl_sync(0xffffffffu, pv, g4 + 2);
+            const double p3 = __shfl_sync(0xffffffffu, pv, g4 + 3);
+            double ave = 0.0;
+            ave += pv;
+            ave += p1;
+            ave += p2;
+            ave += p3;
+            if (act && gp == 0) {
+                if (xf) S.sfx[r & 1][f][v] = ave;
+                else S.sfy[r & 1][f][v] = ave;
+            }
+        }
+        if (bad && act && f < TXe + (xf ? 1 : 0)) flag_error(st, 4u, (long long)map_index(r, D.ny, D.bc) * D.nx + i0 + (f < TXe ? f : TXe - 1));
+    }
+}
+
+// ---- phase 4: RHS scatter (src/WENOFV.cpp:1802-1827) + SSP-RK combination (:376-473)
+//      of row q = r-1, and on the final stage the per-cell CFL step (:486-514) ---------
+template <int EQ>
+__device__ __forceinline__ double phase_update(StageSmem<EQ> &S, const InstDesc &D, InstState *st, const StageLaunch &L,
+                                               int q, int i0, int TXe, double dt, double cmin)
+{
+    constexpr int NV = StageGeom<EQ>::NV;
+    const int t = threadIdx.x;
+    const int cu = t / NV, v = t - cu * NV;
+    const bool act = cu < TXe;
+    const int c = act ? cu : 0;
+    const double aL = S.sfx[q & 1][c][v], aR = S.sfx[q & 1][c + 1][v];
+    const double aB = S.sfy[q & 1][c][v], aT = S.sfy[(q + 1) & 1][c][v];
+    const double dyq = D.dy[q], dxc = S.sdxc[c], dxl = S.sdxl[c];
+    double rhs = 0.0;
+#if WENOFV_STRICT
+    rhs += aL / dxl / dyq;
+    rhs += -aR / dxc / dyq;
+    rhs += aB / dxc / dyq;
+    rhs -= aT / dxc / dyq;
+#else
+    const double idy = 1.0 / dyq, idxc = 1.0 / dxc, idxl = 1.0 / dxl;
+    rhs = ((aL * idxl - aR * idxc) + (aB - aT) * idxc) * idy;
+#endif
+    const double U = S.su[q & 7][v][c + G];
+    const double Un = L.first_stage ? U : S.sun[q & 1][v][c + G];
+    double Unew;
+    if (L.rk1) Unew = U + dt * rhs;
+    else Unew = L.A * Un + L.B * U + L.C * dt * rhs;
+    const size_t plane = (size_t)D.ny * D.pitch;
+    const size_t off = v * plane + (size_t)q * D.pitch + i0 + c;
+    if (act) {
+        if (L.rhs_out) L.rhs_out[off] = rhs;
+        else D.buf[L.bout][off] = Unew;
+        if (isnan(Unew)) flag_error(st, 8u, (long long)q * D.nx + i0 + c);
+    }
+    if (L.final_stage && !L.rhs_out) {
+        double u[NV];
+        const int g = (t & 31) & ~(NV - 1);
+#pragma unroll
+        for (int k = 0; k < NV; k++) u[k] = __shfl_sync(0xffffffffu, Unew, g + k);
+        double ax, ay;
+        max_eigs<EQ, double>(D.eq, u, ax, ay);
+        const double tmp = D.cfl / (ax / D.dX + ay / D.dY);
+        if (act && v == 0) {
+            if (isnan(tmp)) flag_error(st, 1u, (long long)q * D.nx + i0 + c);
+            else cmin = fmin(cmin, tmp);
+        }
+    }
+    return cmin;
+}
+
+template <int EQ, int RECON, class R>
+__global__ void __launch_bounds__(NT) stage_kernel(const StageLaunch L)
+{
+    constexpr int TX = StageGeom<EQ>::TX;
+    __shared__ StageSmem<EQ> S;
+    for (int w = blockIdx.x; w < L.nwork; w += gridDim.x) {
+        const WorkItem it = L.work[w];
+        const InstDesc &D = L.inst[it.inst];
+        InstState *st = &L.state[it.inst];
+        if (st->done) continue;
+        const double dt = st->dt;
+        const int TXe = min(TX, D.nx - it.i0);
+        for (int c = threadIdx.x; c < TX; c += NT) {
+            const int i = min(it.i0 + c, D.nx - 1);
+            S.sdxc[c] = D.dxc[i];
+            S.sdxl[c] = D.dxl[i];
+        }
+        const double *bin = D.buf[L.bin];
+        const double *bun = D.buf[L.bun];
+#pragma unroll 1
+        for (int m = 0; m < 5; m++) load_row<EQ>(S.su[(it.j0 - G + m) & 7], bin, D, it.j0 - G + m, it.i0);
+        cp_async_commit();
+        double cmin = __longlong_as_double(0x7ff0000000000000LL);
+#pragma unroll 1
+        for (int r = it.j0 - 1; r <= it.j1; r++) {
+            cp_async_wait_all();
+            __syncthreads();
+            if (r + 3 <= it.j1 + 2) load_row<EQ>(S.su[(r + 3) & 7], bin, D, r + 3, it.i0);
+            if (!L.first_stage && r >= it.j0 && r < it.j1) load_row<EQ>(S.sun[r & 1], bun, D, r, it.i0);
+            cp_async_commit();
+            phase_ysweep<EQ, RECON, R>(S, D, r);
+            __syncthreads();
+            phase_xsweep<EQ, RECON, R>(S, D, st, r, it.i0, TXe);
+            __syncthreads();
+            phase_riemann<EQ, R>(S, D, st, r, it.i0, it.j0, it.j1, TXe);
+            __syncthreads();
+            if (r - 1 >= it.j0) cmin = phase_update<EQ>(S, D, st, L, r - 1, it.i0, TXe, dt, cmin);
+        }
+        if (L.final_stage && !L.rhs_out) {
+            const double m = block_min(cmin, S.sred);
+            if (threadIdx.x == 0) cfl_atomic_min(st, m);
+        }
+        __syncthreads();
+    }
+    if (L.final_stage && !L.rhs_out) launch_epilogue(L, FIN_STEP, &S.s_last);
+}
+
+// calculateDeltaT of the current state (src/WENOFV.cpp:474-540) for every instance of the
+// launch, then the loop bookkeeping (FIN_INIT) by the last CTA.
+template <int EQ>
+__global__ void __launch_bounds__(NT) cfl_kernel(const StageLaunch L)
+{
+    constexpr int NV = EqTraits<EQ>::NV;
+    __shared__ double sred[NT / 32];
+    __shared__ int s_last;
+    for (int w = blockIdx.x; w < L.nwork; w += gridDim.x) {
+        const WorkItem it = L.work[w];
+        const InstDesc &D = L.inst[it.inst];
+        InstState *st = &L.state[it.inst];
+        if (st->done) continue;
+        const double *U = D.buf[st->cur_buf];
+        const size_t plane = (size_t)D.ny * D.pitch;
+        const int width = min(StageGeom<EQ>::TX, D.nx - it.i0);
+        double cmin = __longlong_as_double(0x7ff0000000000000LL);
+        for (int e = threadIdx.x; e < width * (it.j1 - it.j0); e += NT) {
+            const int j = it.j0 + e / width, i = it.i0 + e % width;
+            double u[NV];
+#pragma unroll
+            for (int k = 0; k < NV; k++) u[k] = U[k * plane + (size_t)j * D.pitch + i];
+            double ax, ay;
+            max_eigs<EQ, double>(D.eq, u, ax, ay);
+            const double tmp = D.cfl / (ax / D.dX + ay / D.dY);
+            if (isnan(tmp)) flag_error(st, 1u, (long long)j * D.nx + i);
+            else cmin = fmin(cmin, tmp);
+        }
+        const double m = block_min(cmin, sred);
+        if (threadIdx.x == 0) cfl_atomic_min(st, m);
+        __syncthreads();
+    }
+    launch_epilogue(L, FIN_INIT, &s_last);
+}
+
+} // namespace strict / fast
+} // namespace wenofv
