@@ -1,0 +1,730 @@
+// wenofv_engine.cu -- host side of the C ABI: instances, work lists, buffer rotation and
+// the device-resident time loop in captured CUDA graphs.
+#include "wenofv_engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+namespace wenofv {
+
+static thread_local char g_err[512];
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+const char *last_error_text() { return g_err; }
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? WENOFV_ENOMEM : WENOFV_ECUDA;
+}
+
+int nvar_of(int k) { return k == WENOFV_EQ_LINEAR_ADV ? 1 : 4; }
+
+int validate(const wenofv_config *c, const wenofv_eq_params *e)
+{
+    if (!c || !e) { set_error("null config or equation"); return WENOFV_EINVAL; }
+    if (c->nx < 1 || c->ny < 1) { set_error("nx, ny must be positive (got %d, %d)", c->nx, c->ny); return WENOFV_EINVAL; }
+    if (!(c->xr > c->xl) || !(c->yr > c->yl)) { set_error("empty domain"); return WENOFV_EINVAL; }
+    if (c->rk_method < 0 || c->rk_method > 2) { set_error("RKMETH must be 0, 1 or 2"); return WENOFV_EINVAL; }
+    if (!(c->cfl > 0)) { set_error("CFL must be positive"); return WENOFV_EINVAL; }
+    if (c->scheme == 2) { set_error("SCHEME 2 (WENOEXP) is not supported"); return WENOFV_ENOTSUP; }
+    if (c->scheme < 0 || c->scheme > 1) { set_error("SCHEME must be 0 or 1"); return WENOFV_EINVAL; }
+    if (c->reconstruction >= 2 && c->reconstruction <= 5) { set_error("RECONSTRUCTIONTYPE %d is not supported", c->reconstruction); return WENOFV_ENOTSUP; }
+    if (c->reconstruction < 0 || c->reconstruction > 1) { set_error("RECONSTRUCTIONTYPE must be 0 or 1"); return WENOFV_EINVAL; }
+    if (c->riemann_flux < 0 || c->riemann_flux > 1) { set_error("RIEMANNFLUX must be 0 or 1"); return WENOFV_EINVAL; }
+    if (c->pp_limiter < 0 || c->pp_limiter > 1) { set_error("PPlimiter must be 0 or 1"); return WENOFV_EINVAL; }
+    if (c->bc != WENOFV_BC_PERIOD && c->bc != WENOFV_BC_OUTFLOW) { set_error("boundary kind %d is not supported", c->bc); return WENOFV_ENOTSUP; }
+    if (c->precision < 0 || c->precision > 2) { set_error("unknown precision %d", c->precision); return WENOFV_EINVAL; }
+    if (c->ref_slabs < 0 || (c->ref_slabs > 0 && c->nx % c->ref_slabs != 0)) {
+        set_error("ELEMNUMX (%d) must be divisible by the slab count (%d)", c->nx, c->ref_slabs);
+        return WENOFV_EINVAL;
+    }
+    if (e->eq_kind < 0 || e->eq_kind > 2) { set_error("unknown equation kind %d", e->eq_kind); return WENOFV_EINVAL; }
+    if (e->eq_kind == WENOFV_EQ_TWO_PHASE && !(e->sound1 > 0 && e->sound2 > 0)) { set_error("sound speeds must be positive"); return WENOFV_EINVAL; }
+    if (e->eq_kind == WENOFV_EQ_EULER && !(e->gamma > 1.0)) { set_error("gamma must exceed 1"); return WENOFV_EINVAL; }
+    if ((size_t)c->nx * c->ny > (size_t)1 << 31) { set_error("grid too large"); return WENOFV_EINVAL; }
+    return WENOFV_OK;
+}
+
+// Cell sizes exactly as the reference's grid generator rounds them (src/WENOFV.cpp:89-123):
+// rank p of a P-slab decomposition builds its cells from its own ghost origin.
+void grid_metric(const wenofv_config &c, double *dxc, double *dxl, double *dy)
+{
+    const double dX = (c.xr - c.xl) / c.nx, dY = (c.yr - c.yl) / c.ny;
+    const int G = 3;
+    if (c.ref_slabs <= 0) {
+        for (int i = 0; i < c.nx; i++) dxc[i] = dxl[i] = dX;
+        for (int j = 0; j < c.ny; j++) dy[j] = dY;
+        return;
+    }
+    const int m = c.nx / c.ref_slabs;
+    for (int g = 0; g < c.nx; g++) {
+        const int rank = g / m, ei = g - rank * m + G;
+        const double procXLeft = c.xl + rank * m * dX;
+        const double ghostLeft = procXLeft - dX * G;
+        dxc[g] = (ghostLeft + (ei + 1) * dX) - (ghostLeft + ei * dX);
+        dxl[g] = (ghostLeft + ei * dX) - (ghostLeft + (ei - 1) * dX);
+    }
+    const double procYLeft = c.yl + 0 * c.ny * dY;
+    const double ghostBottom = procYLeft - dY * G;
+    for (int j = 0; j < c.ny; j++) dy[j] = (ghostBottom + (j + G + 1) * dY) - (ghostBottom + (j + G) * dY);
+}
+
+int stage_count(int rk) { return rk + 1; }
+
+Roles stage_roles(int rk, int parity, int stage)
+{
+    static const Roles r3[2][3] = {{{0, 0, 1}, {1, 0, 2}, {2, 0, 1}}, {{1, 1, 0}, {0, 1, 2}, {2, 1, 0}}};
+    static const Roles r2[2][2] = {{{0, 0, 1}, {1, 0, 2}}, {{2, 2, 1}, {1, 2, 0}}};
+    static const Roles r1[2][1] = {{{0, 0, 1}}, {{1, 1, 0}}};
+    if (rk == 2) return r3[parity][stage];
+    if (rk == 1) return r2[parity][stage];
+    return r1[parity][stage];
+}
+static int end_buffer(int rk, int parity) { return stage_roles(rk, parity, stage_count(rk) - 1).bout; }
+
+// SSP-RK stage coefficients of RunRK2/RunRK3, src/WENOFV.cpp:402-418, :443-465
+void stage_coeffs(int rk, int stage, double &A, double &B, double &C)
+{
+    if (rk == 2) {
+        static const double a[3] = {1.0, 3.0 / 4.0, 1.0 / 3.0}, b[3] = {0.0, 1.0 / 4.0, 2.0 / 3.0}, c[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+        A = a[stage]; B = b[stage]; C = c[stage];
+    } else if (rk == 1) {
+        static const double a[2] = {1.0, 0.5}, b[2] = {0.0, 0.5}, c[2] = {1.0, 0.5};
+        A = a[stage]; B = b[stage]; C = c[stage];
+    } else {
+        A = 0.0; B = 1.0; C = 1.0;
+    }
+}
+
+static InstState fresh_state(int cur)
+{
+    InstState s;
+    std::memset(&s, 0, sizeof s);
+    const double one = 1.0;
+    std::memcpy(&s.accum, &one, sizeof one);
+    s.bad_cell = -1;
+    s.cur_buf = cur;
+    s.mode = MODE_MANUAL;
+    return s;
+}
+
+Engine::~Engine()
+{
+    if (device >= 0) cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    drop_graphs();
+    free_work();
+    for (int i = 0; i < cap_; i++) free_instance(i);
+    cudaFree(d_desc_);
+    cudaFree(d_state_);
+    cudaFree(d_rhs_);
+    if (h_state_) cudaFreeHost(h_state_);
+    if (h_stage_) cudaFreeHost(h_stage_);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+size_t Engine::bytes_needed(const wenofv_config &c, const wenofv_eq_params &e)
+{
+    const size_t pitch = (size_t)(c.nx + 15) / 16 * 16;
+    return 3 * (size_t)nvar_of(e.eq_kind) * c.ny * pitch * sizeof(double) + (2 * (size_t)c.nx + c.ny) * sizeof(double);
+}
+
+int Engine::init_slots(int capacity, int dev, int rk_method)
+{
+    if (capacity < 1) { set_error("capacity must be positive"); return WENOFV_EINVAL; }
+    device = dev;
+    rk = rk_method;
+    int ndev = 0;
+    WENOFV_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) { set_error("no CUDA device %d", device); return WENOFV_EINVAL; }
+    WENOFV_CUDA(cudaSetDevice(device));
+    WENOFV_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device));
+    WENOFV_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    cap_ = capacity;
+    cfg_.assign(cap_, wenofv_config{});
+    eq_.assign(cap_, wenofv_eq_params{});
+    desc_.assign(cap_, InstDesc{});
+    dmem_.assign(cap_, nullptr);
+    dmetric_.assign(cap_, nullptr);
+    live_.assign(cap_, 0);
+    WENOFV_CUDA(cudaMalloc(&d_desc_, cap_ * sizeof(InstDesc)));
+    WENOFV_CUDA(cudaMemset(d_desc_, 0, cap_ * sizeof(InstDesc)));
+    WENOFV_CUDA(cudaMalloc(&d_state_, cap_ * sizeof(InstState)));
+    WENOFV_CUDA(cudaMallocHost(&h_state_, cap_ * sizeof(InstState)));
+    for (int i = 0; i < cap_; i++) {
+        h_state_[i] = fresh_state(0);
+        h_state_[i].done = 1; // an empty slot is never stepped
+    }
+    return push_state();
+}
+
+int Engine::alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params &e)
+{
+    const int nv = nvar_of(e.eq_kind);
+    const int pitch = (c.nx + 15) / 16 * 16;
+    const size_t per = (size_t)nv * c.ny * pitch;
+    if (per * sizeof(double) > h_stage_bytes_) {
+        WENOFV_CUDA(cudaStreamSynchronize(stream));
+        if (h_stage_) cudaFreeHost(h_stage_);
+        h_stage_ = nullptr;
+        h_stage_bytes_ = 0;
+        WENOFV_CUDA(cudaMallocHost(&h_stage_, per * sizeof(double)));
+        h_stage_bytes_ = per * sizeof(double);
+    }
+    WENOFV_CUDA(cudaMalloc(&dmem_[i], 3 * per * sizeof(double)));
+    WENOFV_CUDA(cudaMemsetAsync(dmem_[i], 0, 3 * per * sizeof(double), stream));
+    std::vector<double> met(2 * (size_t)c.nx + c.ny);
+    grid_metric(c, met.data(), met.data() + c.nx, met.data() + 2 * c.nx);
+    WENOFV_CUDA(cudaMalloc(&dmetric_[i], met.size() * sizeof(double)));
+    WENOFV_CUDA(cudaMemcpyAsync(dmetric_[i], met.data(), met.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    InstDesc &d = desc_[i];
+    std::memset(&d, 0, sizeof d);
+    for (int b = 0; b < 3; b++) d.buf[b] = dmem_[i] + b * per;
+    d.dxc = dmetric_[i];
+    d.dxl = dmetric_[i] + c.nx;
+    d.dy = dmetric_[i] + 2 * c.nx;
+    d.nx = c.nx; d.ny = c.ny; d.pitch = pitch; d.bc = c.bc;
+    d.scheme = c.scheme; d.flux = c.riemann_flux; d.limiter = c.pp_limiter;
+    d.recon = e.eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : c.reconstruction;
+    d.eq_kind = e.eq_kind;
+    d.cfl = c.cfl;
+    d.dX = (c.xr - c.xl) / c.nx;
+    d.dY = (c.yr - c.yl) / c.ny;
+    d.eq = EqParams{e.eq_kind, e.rho10, e.rho20, e.sound1, e.sound2, e.preb, e.gamma, e.adv_u, e.adv_v};
+    WENOFV_CUDA(cudaMemcpyAsync(d_desc_ + i, &d, sizeof(InstDesc), cudaMemcpyHostToDevice, stream));
+    WENOFV_CUDA(cudaStreamSynchronize(stream)); // the metric staging above is a host local
+    cfg_[i] = c;
+    eq_[i] = e;
+    live_[i] = 1;
+    h_state_[i] = fresh_state(0);
+    work_dirty_ = true;
+    return WENOFV_OK;
+}
+
+void Engine::free_instance(int i)
+{
+    if (i < 0 || i >= cap_) return;
+    if (dmem_[i]) cudaFree(dmem_[i]);
+    if (dmetric_[i]) cudaFree(dmetric_[i]);
+    dmem_[i] = nullptr;
+    dmetric_[i] = nullptr;
+    if (live_[i]) work_dirty_ = true;
+    live_[i] = 0;
+    if (h_state_) {
+        h_state_[i] = fresh_state(0);
+        h_state_[i].done = 1;
+    }
+}
+
+int Engine::init(int count, const wenofv_config *cfgs, const wenofv_eq_params *eqs)
+{
+    if (count < 1) { set_error("instance count must be positive"); return WENOFV_EINVAL; }
+    for (int i = 0; i < count; i++) {
+        const int rc = validate(&cfgs[i], &eqs[i]);
+        if (rc) return rc;
+        if (cfgs[i].device != cfgs[0].device || cfgs[i].rk_method != cfgs[0].rk_method) {
+            set_error("all instances of a batch share the device and RKMETH");
+            return WENOFV_EINVAL;
+        }
+    }
+    int rc = init_slots(count, cfgs[0].device, cfgs[0].rk_method);
+    if (rc) return rc;
+    n = count;
+    for (int i = 0; i < n && !rc; i++) rc = alloc_instance(i, cfgs[i], eqs[i]);
+    if (!rc) rc = push_state();
+    if (!rc) rc = ensure_work();
+    return rc;
+}
+
+int Engine::ensure_work()
+{
+    if (!work_dirty_) return WENOFV_OK;
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    drop_graphs();
+    const int rc = build_work();
+    if (!rc) work_dirty_ = false;
+    return rc;
+}
+
+int Engine::add(const wenofv_config &c, const wenofv_eq_params &e, int *slot)
+{
+    int rc = validate(&c, &e);
+    if (rc) return rc;
+    if (c.rk_method != rk || c.device != device) { set_error("slot RKMETH/device differ from the server's"); return WENOFV_ENOTSUP; }
+    int k = -1;
+    for (int i = 0; i < cap_; i++)
+        if (!live_[i]) { k = i; break; }
+    if (k < 0) { set_error("no free slot"); return WENOFV_EBUSY; }
+    WENOFV_CUDA(cudaSetDevice(device));
+    rc = alloc_instance(k, c, e);
+    if (rc) { free_instance(k); return rc; }
+    n = std::max(n, k + 1);
+    *slot = k;
+    return WENOFV_OK;
+}
+
+int Engine::remove(int slot)
+{
+    if (!live(slot)) { set_error("slot %d is not live", slot); return WENOFV_EINVAL; }
+    WENOFV_CUDA(cudaSetDevice(device));
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    free_instance(slot);
+    WENOFV_CUDA(cudaMemcpyAsync(d_state_ + slot, &h_state_[slot], sizeof(InstState), cudaMemcpyHostToDevice, stream));
+    return WENOFV_OK;
+}
+
+int Engine::start(int slot, double t_end, int64_t max_steps)
+{
+    if (!live(slot)) { set_error("slot %d is not live", slot); return WENOFV_EINVAL; }
+    WENOFV_CUDA(cudaSetDevice(device));
+    int rc = ensure_work();
+    if (rc) return rc;
+    h_state_[slot] = fresh_state(0);
+    h_state_[slot].mode = MODE_ADVANCE;
+    h_state_[slot].t_end = t_end;
+    h_state_[slot].max_steps = max_steps > 0 ? max_steps : 0;
+    WENOFV_CUDA(cudaMemcpyAsync(d_state_ + slot, &h_state_[slot], sizeof(InstState), cudaMemcpyHostToDevice, stream));
+    // the CFL pass also re-derives the (unchanged) step of the slots already running
+    return launch_cfl_all();
+}
+
+int Engine::run_pairs(int K)
+{
+    WENOFV_CUDA(cudaSetDevice(device));
+    int rc = ensure_work();
+    for (int k = 0; k < K && !rc; k++)
+        for (int p = 0; p < 2 && !rc; p++)
+            for (int s = 0; s < stage_count(rk) && !rc; s++) rc = launch_stage_all(p, s, nullptr);
+    return rc;
+}
+
+int Engine::refresh() { return pull_state(); }
+
+void Engine::free_work()
+{
+    for (Group &g : groups_) {
+        cudaFree(g.d_work);
+        cudaFree(g.d_fin);
+        cudaFree(g.d_counter);
+    }
+    groups_.clear();
+}
+
+// one launch group per (form, equation, reconstruction); work items are strips of TX
+// columns by `seg` rows; the grid is a persistent one (at most the resident CTA count)
+int Engine::build_work()
+{
+    free_work();
+    std::map<long, int> key2g;
+    for (int i = 0; i < cap_; i++) {
+        if (!live_[i]) continue;
+        const int strict = cfg_[i].precision == WENOFV_FP64_STRICT;
+        const int fp32 = cfg_[i].precision == WENOFV_FP32_BULK;
+        const long key = ((long)strict << 24) | (fp32 << 16) | (desc_[i].eq_kind << 8) | desc_[i].recon;
+        auto it = key2g.find(key);
+        if (it == key2g.end()) {
+            Group g;
+            g.ns_strict = strict; g.fp32 = fp32; g.eq = desc_[i].eq_kind; g.recon = desc_[i].recon;
+            key2g[key] = (int)groups_.size();
+            groups_.push_back(g);
+            it = key2g.find(key);
+        }
+        groups_[it->second].inst.push_back(i);
+    }
+    for (Group &g : groups_) {
+        const int tx = g.ns_strict ? strict::stage_tx(g.eq) : fast::stage_tx(g.eq);
+        const int bps = std::max(1, g.ns_strict ? strict::stage_blocks_per_sm(g.eq, g.recon, g.fp32)
+                                                : fast::stage_blocks_per_sm(g.eq, g.recon, g.fp32));
+        const int slots = sms_ * (ctas_per_sm_ > 0 ? std::min(ctas_per_sm_, bps) : bps);
+        long strips_rows = 0;
+        for (int i : g.inst) strips_rows += (long)((cfg_[i].nx + tx - 1) / tx) * cfg_[i].ny;
+        int seg = rows_per_item_;
+        if (seg <= 0) {
+            // rows per item: long enough to amortise the 2 halo rows, short enough to fill the GPU
+            seg = 32;
+            while (seg > 8 && strips_rows / seg < 2L * slots) seg /= 2;
+        }
+        std::vector<WorkItem> work;
+        for (int i : g.inst)
+            for (int j0 = 0; j0 < cfg_[i].ny; j0 += seg)
+                for (int i0 = 0; i0 < cfg_[i].nx; i0 += tx)
+                    work.push_back(WorkItem{i, i0, j0, std::min(cfg_[i].ny, j0 + seg)});
+        g.nwork = (int)work.size();
+        g.grid = std::min(g.nwork, slots);
+        WENOFV_CUDA(cudaMalloc(&g.d_work, work.size() * sizeof(WorkItem)));
+        WENOFV_CUDA(cudaMemcpy(g.d_work, work.data(), work.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
+        WENOFV_CUDA(cudaMalloc(&g.d_fin, g.inst.size() * sizeof(int)));
+        WENOFV_CUDA(cudaMemcpy(g.d_fin, g.inst.data(), g.inst.size() * sizeof(int), cudaMemcpyHostToDevice));
+        WENOFV_CUDA(cudaMalloc(&g.d_counter, sizeof(unsigned int)));
+        WENOFV_CUDA(cudaMemset(g.d_counter, 0, sizeof(unsigned int)));
+    }
+    return WENOFV_OK;
+}
+
+int Engine::push_state()
+{
+    WENOFV_CUDA(cudaMemcpyAsync(d_state_, h_state_, cap_ * sizeof(InstState), cudaMemcpyHostToDevice, stream));
+    return WENOFV_OK;
+}
+int Engine::pull_state()
+{
+    WENOFV_CUDA(cudaMemcpyAsync(h_state_, d_state_, cap_ * sizeof(InstState), cudaMemcpyDeviceToHost, stream));
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    return WENOFV_OK;
+}
+
+int Engine::launch_stage_all(int parity, int stage, double *rhs_out)
+{
+    const Roles ro = stage_roles(rk, parity, stage);
+    for (Group &g : groups_) {
+        StageLaunch L;
+        std::memset(&L, 0, sizeof L);
+        L.inst = d_desc_;
+        L.state = d_state_;
+        L.work = g.d_work;
+        L.nwork = g.nwork;
+        L.fin_ids = g.d_fin;
+        L.nfin = (int)g.inst.size();
+        L.counter = g.d_counter;
+        if (rhs_out) {
+            L.bin = L.bun = L.bout = cur_;
+            L.first_stage = 1;
+            L.final_stage = 0;
+            L.rhs_out = rhs_out;
+        } else {
+            L.bin = ro.bin; L.bun = ro.bun; L.bout = ro.bout;
+            L.first_stage = stage == 0;
+            L.final_stage = stage == stage_count(rk) - 1;
+            L.rk1 = rk == 0;
+            stage_coeffs(rk, stage, L.A, L.B, L.C);
+        }
+        const int rc = g.ns_strict ? strict::launch_stage(g.eq, g.recon, g.fp32, L, g.grid, stream)
+                                   : fast::launch_stage(g.eq, g.recon, g.fp32, L, g.grid, stream);
+        if (rc) return cuda_fail((cudaError_t)rc, "stage kernel launch");
+    }
+    return WENOFV_OK;
+}
+
+int Engine::launch_cfl_all()
+{
+    for (Group &g : groups_) {
+        StageLaunch L;
+        std::memset(&L, 0, sizeof L);
+        L.inst = d_desc_;
+        L.state = d_state_;
+        L.work = g.d_work;
+        L.nwork = g.nwork;
+        L.fin_ids = g.d_fin;
+        L.nfin = (int)g.inst.size();
+        L.counter = g.d_counter;
+        const int rc = g.ns_strict ? strict::launch_cfl(g.eq, L, g.grid, stream) : fast::launch_cfl(g.eq, L, g.grid, stream);
+        if (rc) return cuda_fail((cudaError_t)rc, "cfl kernel launch");
+    }
+    return WENOFV_OK;
+}
+
+static void to_pitch(const double *U, int layout, int nv, int nx, int ny, int pitch, double *dst)
+{
+    for (int v = 0; v < nv; v++)
+        for (int j = 0; j < ny; j++) {
+            double *row = dst + ((size_t)v * ny + j) * pitch;
+            if (layout == WENOFV_LAYOUT_SOA) {
+                std::memcpy(row, U + ((size_t)v * ny + j) * nx, nx * sizeof(double));
+            } else {
+                for (int i = 0; i < nx; i++) row[i] = U[((size_t)i * ny + j) * nv + v];
+            }
+            for (int i = nx; i < pitch; i++) row[i] = 0.0;
+        }
+}
+static void from_pitch(const double *src, int layout, int nv, int nx, int ny, int pitch, double *U)
+{
+    for (int v = 0; v < nv; v++)
+        for (int j = 0; j < ny; j++) {
+            const double *row = src + ((size_t)v * ny + j) * pitch;
+            if (layout == WENOFV_LAYOUT_SOA) std::memcpy(U + ((size_t)v * ny + j) * nx, row, nx * sizeof(double));
+            else
+                for (int i = 0; i < nx; i++) U[((size_t)i * ny + j) * nv + v] = row[i];
+        }
+}
+
+int Engine::upload(int i, const double *U, int layout)
+{
+    if (!live(i) || !U) { set_error("bad instance index or null array"); return WENOFV_EINVAL; }
+    if (layout != WENOFV_LAYOUT_SOA && layout != WENOFV_LAYOUT_REF_AOS) { set_error("unknown layout"); return WENOFV_EINVAL; }
+    WENOFV_CUDA(cudaSetDevice(device));
+    const InstDesc &d = desc_[i];
+    const int nv = nvar_of(d.eq_kind);
+    const int b = slot_mode ? 0 : cur_;
+    WENOFV_CUDA(cudaStreamSynchronize(stream)); // the staging buffer may still feed a copy
+    to_pitch(U, layout, nv, d.nx, d.ny, d.pitch, h_stage_);
+    WENOFV_CUDA(cudaMemcpyAsync(d.buf[b], h_stage_, (size_t)nv * d.ny * d.pitch * sizeof(double), cudaMemcpyHostToDevice, stream));
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    return WENOFV_OK;
+}
+
+int Engine::download(int i, double *U, int layout)
+{
+    if (!live(i) || !U) { set_error("bad instance index or null array"); return WENOFV_EINVAL; }
+    if (layout != WENOFV_LAYOUT_SOA && layout != WENOFV_LAYOUT_REF_AOS) { set_error("unknown layout"); return WENOFV_EINVAL; }
+    WENOFV_CUDA(cudaSetDevice(device));
+    const InstDesc &d = desc_[i];
+    const int nv = nvar_of(d.eq_kind);
+    const int b = slot_mode ? h_state_[i].cur_buf : cur_;
+    WENOFV_CUDA(cudaMemcpyAsync(h_stage_, d.buf[b], (size_t)nv * d.ny * d.pitch * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    from_pitch(h_stage_, layout, nv, d.nx, d.ny, d.pitch, U);
+    return WENOFV_OK;
+}
+
+int Engine::compute_dt(double *dt_out)
+{
+    WENOFV_CUDA(cudaSetDevice(device));
+    for (int i = 0; i < n; i++) h_state_[i] = fresh_state(cur_);
+    int rc = push_state();
+    if (!rc) rc = launch_cfl_all();
+    if (!rc) rc = pull_state();
+    if (rc) return rc;
+    int bad = 0;
+    for (int i = 0; i < n; i++) {
+        dt_out[i] = h_state_[i].dtcfl;
+        if (h_state_[i].flags & WENOFV_FLAG_NAN_DT) bad = 1;
+    }
+    if (bad) { set_error("NaN in the CFL time step"); return WENOFV_ENUMERIC; }
+    return WENOFV_OK;
+}
+
+int Engine::step(double dt)
+{
+    WENOFV_CUDA(cudaSetDevice(device));
+    for (int i = 0; i < n; i++) {
+        h_state_[i] = fresh_state(cur_);
+        h_state_[i].dt = dt;
+    }
+    int rc = push_state();
+    if (rc) return rc;
+    const int parity = cur_ == 0 ? 0 : 1;
+    for (int s = 0; s < stage_count(rk) && !rc; s++) rc = launch_stage_all(parity, s, nullptr);
+    if (rc) return rc;
+    cur_ = end_buffer(rk, parity);
+    return WENOFV_OK;
+}
+
+int Engine::rhs(double *out, int layout)
+{
+    if (n != 1) { set_error("rhs is defined for a single instance"); return WENOFV_EINVAL; }
+    WENOFV_CUDA(cudaSetDevice(device));
+    const InstDesc &d = desc_[0];
+    const int nv = nvar_of(d.eq_kind);
+    const size_t bytes = (size_t)nv * d.ny * d.pitch * sizeof(double);
+    if (!d_rhs_) WENOFV_CUDA(cudaMalloc(&d_rhs_, bytes));
+    h_state_[0] = fresh_state(cur_);
+    int rc = push_state();
+    if (!rc) rc = launch_stage_all(0, 0, d_rhs_);
+    if (rc) return rc;
+    WENOFV_CUDA(cudaMemcpyAsync(h_stage_, d_rhs_, bytes, cudaMemcpyDeviceToHost, stream));
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    from_pitch(h_stage_, layout, nv, d.nx, d.ny, d.pitch, out);
+    return WENOFV_OK;
+}
+
+void Engine::drop_graphs()
+{
+    for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+    for (auto &kv : graph_defs_) cudaGraphDestroy(kv.second);
+    graphs_.clear();
+    graph_defs_.clear();
+}
+
+// K captured pairs of RK steps (buffer roles return to buffer 0 after each pair)
+int Engine::run_graph(int K)
+{
+    auto it = graphs_.find(K);
+    if (it == graphs_.end()) {
+        cudaGraph_t g;
+        WENOFV_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        int rc = 0;
+        for (int k = 0; k < K && !rc; k++)
+            for (int p = 0; p < 2 && !rc; p++)
+                for (int s = 0; s < stage_count(rk) && !rc; s++) rc = launch_stage_all(p, s, nullptr);
+        const cudaError_t e = cudaStreamEndCapture(stream, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        cudaGraphExec_t ex;
+        WENOFV_CUDA(cudaGraphInstantiate(&ex, g, 0));
+        graph_defs_[K] = g;
+        graphs_[K] = ex;
+        it = graphs_.find(K);
+    }
+    WENOFV_CUDA(cudaGraphLaunch(it->second, stream));
+    return WENOFV_OK;
+}
+
+int Engine::normalize_buffers()
+{
+    for (int i = 0; i < n; i++) {
+        const int cb = h_state_[i].cur_buf;
+        if (cb == 0) continue;
+        const InstDesc &d = desc_[i];
+        const size_t bytes = (size_t)nvar_of(d.eq_kind) * d.ny * d.pitch * sizeof(double);
+        WENOFV_CUDA(cudaMemcpyAsync(d.buf[0], d.buf[cb], bytes, cudaMemcpyDeviceToDevice, stream));
+        h_state_[i].cur_buf = 0;
+    }
+    cur_ = 0;
+    return push_state();
+}
+
+int Engine::advance(const double *t0, const double *t_end, int64_t max_steps, double *t_out, int64_t *nsteps)
+{
+    WENOFV_CUDA(cudaSetDevice(device));
+    // every instance's state into buffer 0, where the captured step pairs start
+    for (int i = 0; i < n; i++) h_state_[i].cur_buf = cur_;
+    int rc = normalize_buffers();
+    if (rc) return rc;
+    for (int i = 0; i < n; i++) {
+        h_state_[i] = fresh_state(0);
+        h_state_[i].mode = MODE_ADVANCE;
+        h_state_[i].now = t0 ? t0[i] : 0.0;
+        h_state_[i].t_end = t_end[i];
+        h_state_[i].max_steps = max_steps > 0 ? max_steps : 0;
+    }
+    rc = push_state();
+    if (!rc) rc = launch_cfl_all();
+    if (!rc) rc = pull_state();
+    if (rc) return rc;
+    for (;;) {
+        // pairs of steps for the next graph launch: from the slowest instance's estimate
+        double most = 0.0;
+        bool all_done = true;
+        for (int i = 0; i < n; i++) {
+            const InstState &s = h_state_[i];
+            if (s.done) continue;
+            all_done = false;
+            double left = s.dt > 0 ? std::ceil((s.t_end - s.now) / s.dt) : 1.0;
+            if (s.max_steps > 0) left = std::min(left, (double)(s.max_steps - s.nsteps));
+            most = std::max(most, left);
+        }
+        if (all_done) break;
+        int K = (int)std::ceil(most / 2.0);
+        K = std::max(1, std::min(K, 64));
+        // round K up to a power of two so that few distinct graphs are instantiated
+        int Kp = 1;
+        while (Kp < K) Kp <<= 1;
+        rc = run_graph(Kp);
+        if (!rc) rc = pull_state();
+        if (rc) return rc;
+    }
+    uint32_t flags = 0;
+    for (int i = 0; i < n; i++) {
+        if (t_out) t_out[i] = h_state_[i].now;
+        if (nsteps) nsteps[i] = h_state_[i].nsteps;
+        flags |= h_state_[i].flags;
+    }
+    rc = normalize_buffers();
+    if (rc) return rc;
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    if (flags & (WENOFV_FLAG_NAN_DT | WENOFV_FLAG_BAD_THETA | WENOFV_FLAG_NAN_FLUX | WENOFV_FLAG_NAN_STATE)) {
+        set_error("numerical error flags 0x%x", flags);
+        return WENOFV_ENUMERIC;
+    }
+    return WENOFV_OK;
+}
+
+int Engine::status(int i, uint32_t *flags, int64_t *cell)
+{
+    if (!live(i)) { set_error("bad instance index"); return WENOFV_EINVAL; }
+    WENOFV_CUDA(cudaSetDevice(device));
+    const int rc = pull_state();
+    if (rc) return rc;
+    if (flags) *flags = h_state_[i].flags;
+    if (cell) *cell = h_state_[i].bad_cell;
+    return WENOFV_OK;
+}
+
+int Engine::set_tiling(int rows, int ctas)
+{
+    WENOFV_CUDA(cudaSetDevice(device));
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    rows_per_item_ = rows;
+    ctas_per_sm_ = ctas;
+    work_dirty_ = true;
+    return ensure_work();
+}
+
+int Engine::device_state(int i, double **U, int *pitch)
+{
+    if (!live(i)) { set_error("bad instance index"); return WENOFV_EINVAL; }
+    if (U) *U = desc_[i].buf[cur_];
+    if (pitch) *pitch = desc_[i].pitch;
+    return WENOFV_OK;
+}
+
+// Times candidate tilings with a few manual steps on a copy of the current state and keeps
+// the fastest; the state is restored afterwards.
+int Engine::autotune(int *rows_out, int *ctas_out, double *best_ms)
+{
+    WENOFV_CUDA(cudaSetDevice(device));
+    std::vector<double *> saved(n, nullptr);
+    for (int i = 0; i < n; i++) {
+        const InstDesc &d = desc_[i];
+        const size_t bytes = (size_t)nvar_of(d.eq_kind) * d.ny * d.pitch * sizeof(double);
+        WENOFV_CUDA(cudaMalloc(&saved[i], bytes));
+        WENOFV_CUDA(cudaMemcpyAsync(saved[i], d.buf[cur_], bytes, cudaMemcpyDeviceToDevice, stream));
+    }
+    const int cur0 = cur_;
+    cudaEvent_t e0, e1;
+    WENOFV_CUDA(cudaEventCreate(&e0));
+    WENOFV_CUDA(cudaEventCreate(&e1));
+    double dt = 0.0;
+    {
+        std::vector<double> dts(n);
+        const int rc = compute_dt(dts.data());
+        if (rc) return rc;
+        dt = *std::min_element(dts.begin(), dts.end()) * 0.5;
+    }
+    const int rows_c[] = {8, 16, 32, 64};
+    const int ctas_c[] = {0, 2, 1};
+    double best = 1e30;
+    int br = 32, bc = 0;
+    for (int r : rows_c)
+        for (int c : ctas_c) {
+            int rc = set_tiling(r, c);
+            if (!rc) rc = step(dt); // warm-up
+            if (rc) return rc;
+            WENOFV_CUDA(cudaEventRecord(e0, stream));
+            for (int k = 0; k < 2 && !rc; k++) rc = step(dt);
+            if (rc) return rc;
+            WENOFV_CUDA(cudaEventRecord(e1, stream));
+            WENOFV_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            WENOFV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) { best = ms; br = r; bc = c; }
+        }
+    cur_ = cur0;
+    for (int i = 0; i < n; i++) {
+        const InstDesc &d = desc_[i];
+        const size_t bytes = (size_t)nvar_of(d.eq_kind) * d.ny * d.pitch * sizeof(double);
+        WENOFV_CUDA(cudaMemcpyAsync(d.buf[cur_], saved[i], bytes, cudaMemcpyDeviceToDevice, stream));
+    }
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    for (double *p : saved) cudaFree(p);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const int rc = set_tiling(br, bc);
+    if (rc) return rc;
+    if (rows_out) *rows_out = br;
+    if (ctas_out) *ctas_out = bc;
+    if (best_ms) *best_ms = best / 2.0;
+    return WENOFV_OK;
+}
+
+} // namespace wenofv

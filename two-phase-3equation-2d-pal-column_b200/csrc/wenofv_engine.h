@@ -1,0 +1,116 @@
+// wenofv_engine.h -- host-side engine behind the C ABI: a set of instances on one device
+// advanced together by the fused stage kernels.  A single-grid context is an engine with one
+// instance; the batch API exposes several; the server adds and removes instances in slots.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/wenofv.h"
+#include "wenofv_types.h"
+
+namespace wenofv {
+
+void set_error(const char *fmt, ...);
+const char *last_error_text();
+int cuda_fail(cudaError_t e, const char *what);
+#define WENOFV_CUDA(call)                                                   \
+    do {                                                                    \
+        cudaError_t _e = (call);                                            \
+        if (_e != cudaSuccess) return cuda_fail(_e, #call);                 \
+    } while (0)
+
+int validate(const wenofv_config *cfg, const wenofv_eq_params *eq);
+int nvar_of(int eq_kind);
+// the reference's grid metric (src/WENOFV.cpp:89-123), see wenofv_create
+void grid_metric(const wenofv_config &c, double *dxc, double *dxl, double *dy);
+
+// buffer roles of one RK stage for a step starting at parity p (the state returns to
+// buffer 0 after two steps, so a captured pair of steps has fixed roles)
+struct Roles { int bin, bun, bout; };
+Roles stage_roles(int rk, int parity, int stage);
+int stage_count(int rk);
+void stage_coeffs(int rk, int stage, double &A, double &B, double &C);
+
+class Engine {
+public:
+    ~Engine();
+    // all instances live (context and batch)
+    int init(int n, const wenofv_config *cfgs, const wenofv_eq_params *eqs);
+
+    int upload(int i, const double *U, int layout);
+    int download(int i, double *U, int layout);
+    int compute_dt(double *dt_out);                // per instance, synchronises
+    int step(double dt);                           // one manual RK step of every instance
+    int rhs(double *out, int layout);              // instance 0
+    int advance(const double *t0, const double *t_end, int64_t max_steps, double *t_out, int64_t *nsteps);
+    int status(int i, uint32_t *flags, int64_t *cell);
+    int set_tiling(int rows, int ctas_per_sm);
+    int autotune(int *rows, int *ctas_per_sm, double *best_ms);
+    int device_state(int i, double **U, int *pitch);
+
+    // ---- slots (serving): capacity fixed at init_slots, instances added and removed ----
+    int init_slots(int capacity, int device, int rk_method);
+    int add(const wenofv_config &cfg, const wenofv_eq_params &eq, int *slot);
+    int remove(int slot);
+    int start(int slot, double t_end, int64_t max_steps); // device loop of one slot: t = 0 -> t_end
+    int run_pairs(int K);                                 // K pairs of steps of every live, unfinished slot
+    int refresh();                                        // pull the device loop state
+    const InstState &slot_state(int slot) const { return h_state_[slot]; }
+    bool live(int slot) const { return slot >= 0 && slot < cap_ && live_[slot]; }
+    static size_t bytes_needed(const wenofv_config &cfg, const wenofv_eq_params &eq);
+
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    int n = 0;
+    int rk = 2;
+    bool slot_mode = false; // serving: every slot keeps its own current buffer
+
+private:
+    struct Group {
+        int ns_strict, fp32, eq, recon;
+        std::vector<int> inst;
+        WorkItem *d_work = nullptr;
+        int nwork = 0;
+        int *d_fin = nullptr;
+        unsigned int *d_counter = nullptr;
+        int grid = 0;
+    };
+    int build_work();
+    void free_work();
+    int ensure_work();
+    int alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params &e);
+    void free_instance(int i);
+    int launch_stage_all(int parity, int stage, double *rhs_out);
+    int launch_cfl_all();
+    int pull_state();
+    int push_state();
+    int normalize_buffers();
+    int run_graph(int double_steps);
+    void drop_graphs();
+
+    std::vector<wenofv_config> cfg_;
+    std::vector<wenofv_eq_params> eq_;
+    std::vector<InstDesc> desc_;
+    std::vector<double *> dmem_;    // per instance: 3 state buffers
+    std::vector<double *> dmetric_; // per instance: dxc, dxl, dy
+    std::vector<char> live_;
+    std::vector<Group> groups_;
+    InstDesc *d_desc_ = nullptr;
+    InstState *d_state_ = nullptr;
+    InstState *h_state_ = nullptr; // pinned mirror
+    double *h_stage_ = nullptr;    // pinned staging for upload/download
+    size_t h_stage_bytes_ = 0;
+    double *d_rhs_ = nullptr;
+    int rows_per_item_ = 0, ctas_per_sm_ = 0;
+    int sms_ = 148;
+    int cap_ = 0;
+    int cur_ = 0; // buffer holding every instance's state between calls (context/batch)
+    bool work_dirty_ = true;
+    std::map<int, cudaGraphExec_t> graphs_;
+    std::map<int, cudaGraph_t> graph_defs_;
+};
+
+} // namespace wenofv
