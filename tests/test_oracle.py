@@ -1,0 +1,125 @@
+"""The CPU oracle against the reference: committed golden vectors (bit for bit), live runs
+of the compiled reference when it is built here, and properties of the restated kernels."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+from oracle import EQ_EULER, EQ_LINEAR_ADV, BC_OUTFLOW, Problem, reference_available, run_reference
+import cases
+
+GOLD = golden_cases()
+
+
+def problem_of(meta) -> Problem:
+    return Problem(nx=meta["nx"], ny=meta["ny"], rk=meta["rk"], cfl=meta["cfl"], scheme=meta["scheme"],
+                   flux=meta["flux"], recon=meta["recon"], limiter=meta["limiter"], ref_slabs=meta["ref_slabs"],
+                   rho10=meta["rho10"], rho20=meta["rho20"], sound1=meta["sound1"], sound2=meta["sound2"])
+
+
+@pytest.mark.parametrize("name", sorted(GOLD))
+def test_oracle_matches_reference_golden(name, oracle_lib):
+    meta, g = GOLD[name], load_golden(name)
+    p = problem_of(meta)
+    assert np.array_equal(oracle_lib.rhs(p, g["U0"]), g["rhs"])
+    if meta["t_end"] > 0:
+        U, n, t, dts = oracle_lib.advance(p, g["U0"], t_end=meta["t_end"])
+    else:
+        U, n, t, dts = oracle_lib.advance(p, g["U0"], t_end=1e9, max_steps=meta["steps"])
+    assert n == meta["nsteps_taken"]
+    assert np.array_equal(dts, g["dts"])
+    assert np.array_equal(U, g["U"])
+
+
+@pytest.mark.skipif(not reference_available(), reason="compiled reference not built (make -C oracle ref)")
+@pytest.mark.parametrize("scheme,flux,recon,lim,rk", [(1, 1, 1, 1, 2), (0, 0, 0, 1, 1), (1, 0, 0, 0, 0)])
+def test_oracle_matches_live_reference(scheme, flux, recon, lim, rk, oracle_lib):
+    U0, prm = cases.liquid_column(36, 20, seed=5)
+    p = Problem(nx=36, ny=20, rk=rk, scheme=scheme, flux=flux, recon=recon, limiter=lim, ref_slabs=4,
+                rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"])
+    r = run_reference(p, testcase=2, U0=U0, steps=3, want_rhs=True)
+    assert np.array_equal(oracle_lib.face_states(p, U0), r.faces)
+    assert np.array_equal(oracle_lib.rhs(p, U0), r.rhs)
+    U, n, _, dts = oracle_lib.advance(p, U0, t_end=1e9, max_steps=3)
+    assert np.array_equal(dts, r.dts) and np.array_equal(U, r.U)
+
+
+def test_weno_reproduces_quadratics(oracle_lib):
+    # both schemes are exact for cell averages of a quadratic on a uniform stencil at the
+    # Gauss-Lobatto points (their candidate polynomials are)
+    xg = np.array([-1.0, -0.447213595499957939281834733746, 0.447213595499957939281834733746, 1.0]) / 2
+    c = np.arange(-2, 3)
+    f = lambda x: 0.3 + 1.7 * x - 0.9 * x * x
+    F = lambda a, b: (0.3 * (b - a) + 0.85 * (b * b - a * a) - 0.3 * (b ** 3 - a ** 3))
+    avg = np.array([F(k - 0.5, k + 0.5) for k in c])
+    for scheme in (0, 1):
+        for gp in range(4):
+            assert abs(oracle_lib.weno(scheme, avg, gp) - f(xg[gp])) < 1e-9
+
+
+def test_weno_flat_stencil(oracle_lib):
+    for scheme in (0, 1):
+        for gp in range(4):
+            # the candidate coefficients sum to 1 up to their rounding
+            assert oracle_lib.weno(scheme, np.full(5, 7.25), gp) == pytest.approx(7.25, rel=4e-16)
+
+
+@pytest.mark.parametrize("kind", [0, 2])
+def test_eigenvectors_are_inverse(kind, oracle_lib):
+    rng = np.random.default_rng(7)
+    p = Problem(nx=8, ny=8, eq_kind=kind, rho10=1000.0, rho20=1.0, sound1=70.0, sound2=70.0)
+    for _ in range(20):
+        if kind == 0:
+            z1 = rng.uniform(1e-6, 1 - 1e-6)
+            U = np.array([z1 * 1000.0, (1 - z1) * 1.0, 0, 0])
+            rho = U[0] + U[1]
+            U[2:] = rho * rng.uniform(-1, 1, 2)
+        else:
+            rho, u, v, pr = rng.uniform(0.1, 2), *rng.uniform(-1, 1, 2), rng.uniform(0.1, 2)
+            U = np.array([rho, rho * u, rho * v, pr / 0.4 + 0.5 * rho * (u * u + v * v)])
+        for n in ((1.0, 0.0), (0.0, 1.0)):
+            L, R = oracle_lib.eigen(p, U, *n)
+            assert np.allclose(L @ R, np.eye(4), atol=1e-8)
+
+
+def test_fluxes_consistent(oracle_lib):
+    # F(U, U) is the physical flux for both LLF and HLLC
+    rng = np.random.default_rng(8)
+    p = Problem(nx=8, ny=8, rho10=1000.0, rho20=1.0, sound1=70.0, sound2=70.0)
+    for _ in range(20):
+        z1 = rng.uniform(0.01, 0.99)
+        U = np.array([z1 * 1000.0, (1 - z1), 0, 0])
+        U[2:] = (U[0] + U[1]) * rng.uniform(-1, 1, 2)
+        for nrm in ((1.0, 0.0), (0.0, 1.0)):
+            a = oracle_lib.riemann(p, 0, U, U, *nrm)
+            b = oracle_lib.riemann(p, 1, U, U, *nrm)
+            assert np.allclose(a, b, rtol=1e-12, atol=1e-9)
+
+
+def test_conservation_periodic(oracle_lib):
+    U0, prm = cases.liquid_column(24, 20, seed=9)
+    p = Problem(nx=24, ny=20, scheme=1, flux=1, recon=1, limiter=1, **prm)
+    U, n, _, _ = oracle_lib.advance(p, U0, t_end=1e9, max_steps=4)
+    m0, m1 = U0.sum(axis=(1, 2)), U.sum(axis=(1, 2))
+    assert np.allclose(m0, m1, rtol=1e-13, atol=1e-10)
+
+
+def test_outflow_and_euler_run(oracle_lib):
+    U0, _ = cases.euler_quadrants(32, 32)
+    p = Problem(nx=32, ny=32, bc=BC_OUTFLOW, eq_kind=EQ_EULER, scheme=1, flux=1, recon=0, cfl=0.4)
+    U, n, t, _ = oracle_lib.advance(p, U0, t_end=0.02)
+    assert abs(t - 0.02) < 1e-12 and np.isfinite(U).all() and (U[0] > 0).all()
+
+
+def test_advection_converges(oracle_lib):
+    # one full period of u_t + u_x + u_y = 0: the L1 error against the initial averages
+    # falls at (at least) third order, the SSP-RK3 time order with dt ~ dx
+    err = []
+    for n in (32, 64):
+        U0 = cases.advection_sine(n, n)
+        p = Problem(nx=n, ny=n, eq_kind=EQ_LINEAR_ADV, scheme=0, flux=0, recon=0, cfl=0.5)
+        U, k, t, _ = oracle_lib.advance(p, U0, t_end=1.0)
+        assert k == 4 * n and abs(t - 1.0) < 1e-12  # dt = CFL / (1/dx + 1/dy)
+        err.append(np.abs(U - U0).mean())
+    assert err[0] < 1e-3 and np.log2(err[0] / err[1]) > 3.0
