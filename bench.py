@@ -1,0 +1,375 @@
+"""Benchmark of the WENOFV time-advance hot path on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload column1024|euler512|advection128] [--form fp64|fp64_strict|fp32_bulk]
+
+A step is one SSP-RK3 time step (3 fused stage launches, the last with the CFL
+reduction) over the whole grid of the workload.  The metric is cell-stage updates per
+second: interior cells x RK stages x steps / time.
+
+* value: K steps on the device-resident state, each timed with CUDA events on the solver's
+  stream; L2 (126 MB) is flushed by a 256 MiB write between steps, outside the timed events.
+* e2e: the same K steps through the public C-ABI calls with host arrays: upload of the
+  step's input state, the step, download of its result.
+* roofline: the stage kernel is bound by the FP64 CUDA-core pipe (the path is a stencil,
+  not a contraction); achieved = counted algorithmic flops per launch (profiles/flop_table.txt)
+  / average launch time; peak = FMA throughput measured in this run by the library's probe.
+* cpu_baseline: the unmodified reference (oracle/_ref, 4 slab ranks per process, as many
+  processes as the host has groups of 4 cores) on a bounded sample of the same workload.
+* --impl reference: that reference arm alone, on rank 0 (other ranks exit 0).
+
+Multi-GPU (torchrun): replicas only -- each rank advances its own copy of the workload on
+its own GPU with no collective on the data path; the barrier and the max over ranks of the
+timed duration use torch.distributed.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import cases  # noqa: E402
+
+# option sets of the workloads, for the flop table lookup
+FLOP_KEYS = {
+    "column1024": ("two_phase", 1, 1, 1, 1),    # characteristic, WENO-Z, HLLC, limiter
+    "euler512": ("euler", 0, 1, 1, 0),          # conservative, WENO-Z, HLLC
+    "advection128": ("linear_advection", 0, 0, 0, 0),
+}
+BYTES_PER_CELL_STAGE = {"column1024": 96.0, "euler512": 96.0, "advection128": 24.0}
+
+
+def flops_per_cell_stage(name: str) -> float:
+    eq, recon, scheme, flux, lim = FLOP_KEYS[name]
+    for line in open(os.path.join(ROOT, "profiles", "flop_table.txt")):
+        if not line.startswith("{"):
+            continue
+        d = json.loads(line)
+        if (d["eq"], d["recon"], d["scheme"], d["flux"], d["limiter"]) == (eq, recon, scheme, flux, lim):
+            return float(d["flops_per_cell_stage"])
+    raise KeyError(name)
+
+
+def workload(name: str, wb, form: int):
+    """(U0, config, eq, description dict) of a named workload"""
+    if name == "column1024":
+        U0, prm = cases.liquid_column(1024, 1024, seed=3)
+        cfg = wb.make_config(1024, 1024, rk=2, cfl=0.5, scheme=1, limiter=1, flux=1, recon=1, precision=form)
+        eq = wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"])
+        desc = dict(workload="liquid_column_1024_ref_eos", grid="1024x1024", equation="two-phase 3-equation, linear EOS "
+                    "linearised from stiffened gas (g1=4.4, pinf1=6e3, g2=1.4, pinf2=0) at p=1, density ratio 1000",
+                    bc="periodic", scheme="WENO-Z", flux="HLLC", reconstruction="characteristic", limiter=True,
+                    rk="SSP-RK3", cfl=0.5, ic="disk r=0.2 tanh-smoothed over 2 cells, eps=1e-6, seeded periodic "
+                    "Gaussian velocity field amplitude 1e-2 (seed 3)")
+    elif name == "euler512":
+        U0, _ = cases.euler_quadrants(512, 512, seed=2)
+        cfg = wb.make_config(512, 512, bc=wb.BC_OUTFLOW, rk=2, cfl=0.4, scheme=1, flux=1, recon=0, precision=form)
+        eq = wb.make_eq(kind=wb.EQ_EULER, gamma=1.4)
+        desc = dict(workload="euler_quadrants_512", grid="512x512", equation="Euler gamma=1.4", bc="outflow",
+                    scheme="WENO-Z", flux="HLLC", reconstruction="conservative", limiter=False, rk="SSP-RK3", cfl=0.4,
+                    ic="four quadrants, (rho,u,v,p) from seed 2")
+    elif name == "advection128":
+        U0 = cases.advection_sine(128, 128)
+        cfg = wb.make_config(128, 128, rk=2, cfl=0.5, scheme=0, flux=0, recon=0, precision=form)
+        eq = wb.make_eq(kind=wb.EQ_LINEAR_ADV)
+        desc = dict(workload="linear_advection_128", grid="128x128", equation="u_t+u_x+u_y=0", bc="periodic",
+                    scheme="WENO-JS", flux="LLF", reconstruction="conservative", limiter=False, rk="SSP-RK3", cfl=0.5,
+                    ic="sin(2 pi (x+y))")
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return U0, cfg, eq, desc
+
+
+# ---- host CPU baseline ------------------------------------------------------------------------
+def cpu_baseline(name: str, steps: int, warmup: int, sample_n: int = 256):
+    """The reference (or, where it cannot run the workload, the oracle port) on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    ncores = os.cpu_count() or 1
+    if name == "column1024" and O.reference_available():
+        U0, prm = cases.liquid_column(sample_n, sample_n, seed=3)
+        nproc = max(1, ncores // 4)
+        with tempfile.TemporaryDirectory() as d:
+            U0.tofile(os.path.join(d, "u0.bin"))
+            args = [O.REF_BIN, "--testcase", "2", "--nx", str(sample_n), "--ny", str(sample_n), "--rk", "2",
+                    "--cfl", "0.5", "--scheme", "1", "--limiter", "1", "--flux", "1", "--recon", "1",
+                    "--rho10", O._f(prm["rho10"]), "--rho20", O._f(prm["rho20"]), "--sound1", O._f(prm["sound1"]),
+                    "--sound2", O._f(prm["sound2"]), "--u0", os.path.join(d, "u0.bin"), "--steps", str(steps),
+                    "--warmup", str(warmup), "--time"]
+            t0 = time.perf_counter()
+            procs = [subprocess.Popen(args, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+                     for _ in range(nproc)]
+            outs = [pr.communicate(timeout=1800) for pr in procs]
+            wall = time.perf_counter() - t0
+            secs = []
+            for (o, e), pr in zip(outs, procs):
+                if pr.returncode != 0:
+                    raise RuntimeError(e[-500:])
+                secs.append(json.loads(o.strip().splitlines()[-1])["seconds"])
+        units = nproc * sample_n * sample_n * 3 * steps
+        return dict(value=units / max(secs), unit="cell-stage updates/s", cores=4 * nproc, kind="reference",
+                    sample=f"{nproc} concurrent processes of the unmodified reference (4 slab ranks each, "
+                           f"threads over an in-process MPI shim), {steps} timed SSP-RK3 steps after {warmup} "
+                           f"warm-up steps each, on the same workload at {sample_n}x{sample_n} "
+                           f"(same equation, options and initial data); {ncores} host cores; wall {wall:.1f} s",
+                    seconds=max(secs))
+    # the oracle port on all host threads (the reference has no Euler or scalar advection)
+    if name == "euler512":
+        U0, _ = cases.euler_quadrants(sample_n, sample_n, seed=2)
+        p = O.Problem(nx=sample_n, ny=sample_n, bc=O.BC_OUTFLOW, eq_kind=O.EQ_EULER, rk=2, cfl=0.4, scheme=1,
+                      flux=1, recon=0, threads=ncores)
+    elif name == "advection128":
+        sample_n = 128
+        U0 = cases.advection_sine(128, 128)
+        p = O.Problem(nx=128, ny=128, eq_kind=O.EQ_LINEAR_ADV, rk=2, cfl=0.5, scheme=0, flux=0, recon=0,
+                      threads=ncores)
+    else:
+        U0, prm = cases.liquid_column(sample_n, sample_n, seed=3)
+        p = O.Problem(nx=sample_n, ny=sample_n, rk=2, cfl=0.5, scheme=1, flux=1, recon=1, limiter=1,
+                      threads=ncores, **prm)
+    orc = O.Oracle()
+    dt = orc.compute_dt(p, U0)
+    V = U0
+    for _ in range(warmup):
+        V = orc.step(p, V, dt)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        V = orc.step(p, V, dt)
+    secs = time.perf_counter() - t0
+    return dict(value=sample_n * sample_n * 3 * steps / secs, unit="cell-stage updates/s", cores=ncores, kind="port",
+                sample=f"the C restatement (oracle/wenofv_oracle.c, OpenMP over {ncores} threads), {steps} SSP-RK3 "
+                       f"steps at {sample_n}x{sample_n} of the same workload",
+                seconds=secs)
+
+
+# ---- clocks ------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            self.f = os.fdopen(fd, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.path:
+            return None
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        pw = [num(r[3]) for r in rows if num(r[3]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return dict(sm_mhz=float(np.median(sm)) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                    reasons=reasons, samples=len(rows), power_w_max=max(pw) if pw else None)
+
+
+def read_traffic(workload_name: str):
+    """DRAM bytes per stage-kernel launch from the committed ncu summary, when there is one"""
+    path = os.path.join(ROOT, "profiles", f"stage_kernel_{workload_name}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ---- our arm --------------------------------------------------------------------------------------
+def run_ours(args, rank, world, dist):
+    import importlib.util
+
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    spec = importlib.util.spec_from_file_location("wenofv_b200", os.path.join(ROOT, "two-phase-3equation-2d-pal-column_b200", "__init__.py"))
+    wb = importlib.util.module_from_spec(spec)
+    sys.modules["wenofv_b200"] = wb
+    spec.loader.exec_module(wb)
+
+    form = {"fp64": wb.FP64, "fp64_strict": wb.FP64_STRICT, "fp32_bulk": wb.FP32_BULK}[args.form]
+    U0, cfg, eq, desc = workload(args.workload, wb, form)
+    cfg.device = local
+    s = wb.Solver(cfg, eq)
+    s.upload(U0)
+    ncells = cfg.nx * cfg.ny
+    nstages = 3
+    peak = wb.fma_peak_tflops(wb.FP32_BULK if form == wb.FP32_BULK else wb.FP64, local)
+    dt = s.compute_dt()
+
+    stream = torch.cuda.ExternalStream(s.stream())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        s.step(dt)
+    s.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # device-resident timing
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.zero_()  # L2 flush, outside the timed events
+                evs[k][0].record(stream)
+                s.step(dt)
+                evs[k][1].record(stream)
+        s.synchronize()
+        torch.cuda.synchronize()
+    barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = float(np.sum(step_ms))
+    if dist is not None:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * ncells * nstages * args.steps / (total_ms * 1e-3)
+    flags, _ = s.status()
+
+    # end to end through the public API with host arrays
+    U_host = s.download()
+    nbytes = U_host.nbytes
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        s.upload(U_host)
+        s.step(dt)
+        U_host = s.download()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = dict(value=world * ncells * nstages * args.steps / e2e_s, unit="cell-stage updates/s",
+               h2d_bytes_per_step=nbytes, d2h_bytes_per_step=nbytes)
+
+    launch_ms = total_ms / (args.steps * nstages)  # a step is the stage kernel 3x (+ a 100-byte H2D)
+    fpcs = flops_per_cell_stage(args.workload)
+    achieved_tf = fpcs * ncells / (launch_ms * 1e-3) / 1e12
+    hbm_gbs = BYTES_PER_CELL_STAGE[args.workload] * ncells / (launch_ms * 1e-3) / 1e9
+    mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    measured = json.load(open(mp)) if os.path.exists(mp) else {}
+    hbm_peak = measured.get("hbm_gbs", 6650.0)
+    roofline = dict(bound="fp32" if form == wb.FP32_BULK else "fp64", achieved=achieved_tf, peak=peak,
+                    unit="TFLOP/s", frac=achieved_tf / peak, traffic=read_traffic(args.workload),
+                    kernel="wenofv::stage_kernel", launch_ms=launch_ms, flops_per_launch=fpcs * ncells,
+                    flops_per_cell_stage=fpcs,
+                    peak_source=f"FMA throughput of the {'FP32' if form == wb.FP32_BULK else 'FP64'} CUDA-core pipe "
+                                f"measured in this run (wenofv_probe_fma_peak)",
+                    hbm_view=dict(achieved=hbm_gbs, peak=hbm_peak, unit="GB/s", frac=hbm_gbs / hbm_peak,
+                                  bytes_per_cell_stage=BYTES_PER_CELL_STAGE[args.workload],
+                                  peak_source="MEASURED_PEAKS.json hbm_gbs (of measured)" if measured else "fallback"))
+    out = dict(metric="cell-stage updates/s", value=value, unit="cell-stage updates/s", n_gpus=world,
+               steps=args.steps, warmup=args.warmup, ms_per_step=total_ms / args.steps, higher_is_better=True,
+               scaling="weak", vs_baseline=None,
+               dtype={"fp64": "f64", "fp64_strict": "f64", "fp32_bulk": "f32+f64"}[args.form], data="synthetic",
+               config=dict(desc, form=args.form, l2="flushed between steps by a 256 MiB write outside the timed "
+                           "events", parallelism=f"replicas x{world}"),
+               roofline=roofline, e2e=e2e, gpu_launches=args.steps * nstages, status_flags=flags)
+    out["clocks"] = clk.summary()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args.workload, steps=args.cpu_steps, warmup=1)
+    s.close()
+    return out
+
+
+def run_reference_arm(args):
+    cb = cpu_baseline(args.workload, steps=max(1, args.steps), warmup=args.warmup)
+    return dict(metric="cell-stage updates/s", value=cb["value"], unit="cell-stage updates/s", n_gpus=args.gpus,
+                steps=args.steps, warmup=args.warmup, ms_per_step=1e3 * cb["seconds"] / max(1, args.steps),
+                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+                impl="reference", config=dict(workload=args.workload, sample=cb["sample"]),
+                cpu_baseline=dict(value=cb["value"], unit=cb["unit"], cores=cb["cores"], kind=cb["kind"],
+                                  sample=cb["sample"]),
+                e2e=dict(value=cb["value"], unit=cb["unit"], h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="column1024", choices=sorted(FLOP_KEYS))
+    ap.add_argument("--form", default="fp64", choices=["fp64", "fp64_strict", "fp32_bulk"])
+    ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference_arm(args)), flush=True)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    out = run_ours(args, rank, world, dist)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,178 @@
+"""Batched ensembles and the serving loop (no counterpart in the reference).
+
+* Every instance of a batch equals the same instance solved alone (bit for bit in
+  FP64_STRICT, where neighbouring instances cannot change an instance's arithmetic).
+* Every served request equals the same solve run alone through the single-grid API, however
+  it was mixed with other requests (bit for bit in FP64_STRICT).
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import pytest
+
+import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def column_cfg(wb, nx, ny, prm, precision, scheme=1, limiter=1):
+    cfg = wb.make_config(nx, ny, scheme=scheme, flux=1, recon=1, limiter=limiter, precision=precision)
+    eq = wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"])
+    return cfg, eq
+
+
+def alone(wb, cfg, eq, U0, t_end=1e9, max_steps=0):
+    with wb.Solver(cfg, eq) as s:
+        s.upload(U0)
+        t, n = s.advance(t_end, max_steps=max_steps)
+        return s.download(), n
+
+
+@pytest.mark.parametrize("precision", ["FP64_STRICT", "FP64"])
+def test_batch_equals_alone(wb, precision):
+    prec = getattr(wb, precision)
+    ens = cases.ensemble(6, seed=5, grids=[(64, 64), (96, 40), (130, 33), (52, 70)])
+    cfgs, eqs = [], []
+    for U0, prm in ens:
+        c, e = column_cfg(wb, prm["nx"], prm["ny"], prm, prec, scheme=prm["scheme"])
+        cfgs.append(c)
+        eqs.append(e)
+    b = wb.Batch(cfgs, eqs)
+    for k, (U0, _) in enumerate(ens):
+        b.upload(k, U0)
+    t_end = [0.002 * (k + 1) for k in range(len(ens))]  # uneven end times
+    ns = b.advance(t_end)
+    for k, (U0, _) in enumerate(ens):
+        ref, n = alone(wb, cfgs[k], eqs[k], U0, t_end=t_end[k])
+        assert ns[k] == n
+        got = b.download(k)
+        if prec == wb.FP64_STRICT:
+            assert np.array_equal(got, ref)
+        else:
+            assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    b.close()
+
+
+def test_batch_mixed_equations_and_tiling(wb):
+    # a two-phase instance, an Euler instance (outflow) and an advection instance in one batch
+    U1, prm = cases.liquid_column(64, 48, seed=7)
+    c1, e1 = column_cfg(wb, 64, 48, prm, wb.FP64_STRICT)
+    U2, _ = cases.euler_quadrants(40, 40)
+    c2 = wb.make_config(40, 40, bc=wb.BC_OUTFLOW, cfl=0.4, scheme=1, flux=1, recon=0, precision=wb.FP64_STRICT)
+    e2 = wb.make_eq(kind=wb.EQ_EULER)
+    U3 = cases.advection_sine(150, 20)
+    c3 = wb.make_config(150, 20, scheme=0, flux=0, recon=0, precision=wb.FP64_STRICT)
+    e3 = wb.make_eq(kind=wb.EQ_LINEAR_ADV)
+    refs = [alone(wb, c, e, U, max_steps=5)[0] for c, e, U in ((c1, e1, U1), (c2, e2, U2), (c3, e3, U3))]
+    for rows, ctas in ((8, 1), (16, 0), (64, 2)):
+        b = wb.Batch([c1, c2, c3], [e1, e2, e3])
+        for k, U in enumerate((U1, U2, U3)):
+            b.upload(k, U)
+        b.set_tiling(rows, ctas)
+        ns = b.advance([1e9] * 3, max_steps=5)
+        assert list(ns) == [5, 5, 5]
+        for k in range(3):
+            assert np.array_equal(b.download(k), refs[k])
+        b.close()
+
+
+def test_batch_autotune_keeps_state(wb):
+    ens = cases.ensemble(4, seed=9, grids=[(64, 64), (96, 48)])
+    cfgs, eqs = [], []
+    for U0, prm in ens:
+        c, e = column_cfg(wb, prm["nx"], prm["ny"], prm, wb.FP64_STRICT, scheme=prm["scheme"])
+        cfgs.append(c)
+        eqs.append(e)
+    b = wb.Batch(cfgs, eqs)
+    for k, (U0, _) in enumerate(ens):
+        b.upload(k, U0)
+    rows, ctas, ms = b.autotune()
+    assert rows in (8, 16, 32, 64) and ms > 0
+    for k, (U0, _) in enumerate(ens):
+        assert np.array_equal(b.download(k), U0)  # the autotuner restores the state
+    b.advance([1e9] * len(ens), max_steps=3)
+    for k, (U0, _) in enumerate(ens):
+        ref, _ = alone(wb, cfgs[k], eqs[k], U0, max_steps=3)
+        assert np.array_equal(b.download(k), ref)
+    b.close()
+
+
+def _drain(srv, ids, timeout=300.0):
+    out = {}
+    t0 = time.time()
+    while len(out) < len(ids):
+        for rid in ids:
+            if rid in out:
+                continue
+            got = srv.poll(rid)
+            if got is not None:
+                out[rid] = got
+        if time.time() - t0 > timeout:
+            raise TimeoutError("server did not finish")
+        time.sleep(0.002)
+    return out
+
+
+def test_server_alone_equals_mixed(wb):
+    rng = np.random.default_rng(11)
+    reqs = []
+    for k in range(10):
+        nx, ny = [(64, 64), (96, 48), (128, 64), (40, 40)][k % 4]
+        if k % 3 == 2:
+            U0, _ = cases.euler_quadrants(nx, ny, seed=k)
+            cfg = wb.make_config(nx, ny, bc=wb.BC_OUTFLOW, cfl=0.4, scheme=1, flux=1, recon=0, precision=wb.FP64_STRICT)
+            eq = wb.make_eq(kind=wb.EQ_EULER)
+        else:
+            U0, prm = cases.liquid_column(nx, ny, seed=k)
+            cfg, eq = column_cfg(wb, nx, ny, prm, wb.FP64_STRICT)
+        reqs.append((cfg, eq, U0, int(rng.integers(6, 30))))
+    srv = wb.Server(0, hbm_budget_bytes=3 << 20, max_slots=4)  # small budget: requests queue
+    ids = []
+    for cfg, eq, U0, ns in reqs:
+        ids.append(srv.submit(cfg, eq, U0, 1e9, max_steps=ns))
+        time.sleep(0.001 * rng.integers(0, 3))  # arrivals while others run
+    res = _drain(srv, ids)
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["active"] == 0 and st["resident_bytes"] == 0
+    for rid, (cfg, eq, U0, ns) in zip(ids, reqs):
+        U, info = res[rid]
+        assert info.status == 0 and info.steps == ns
+        assert info.t_submit <= info.t_admit <= info.t_done
+        ref, n = alone(wb, cfg, eq, U0, max_steps=ns)
+        assert np.array_equal(U, ref)
+    srv.close()
+
+
+def test_server_rejects_and_isolates_failures(wb):
+    srv = wb.Server(0, hbm_budget_bytes=1 << 20, max_slots=2)
+    U0, prm = cases.liquid_column(256, 256, seed=1)
+    cfg, eq = column_cfg(wb, 256, 256, prm, wb.FP64)
+    with pytest.raises(wb.WenofvError) as e:
+        srv.submit(cfg, eq, U0, 0.01)  # over the budget
+    assert e.value.code == wb.ENOMEM
+    U1, prm = cases.liquid_column(16, 16, seed=2)
+    c1, e1 = column_cfg(wb, 16, 16, prm, wb.FP64)
+    U1[1, 3, 3] = np.nan  # a failing request does not disturb the others
+    bad = srv.submit(c1, e1, U1, 1e9, max_steps=3)
+    U2, prm2 = cases.liquid_column(16, 16, seed=3)
+    c2, e2 = column_cfg(wb, 16, 16, prm2, wb.FP64)
+    good = srv.submit(c2, e2, U2, 1e9, max_steps=3)
+    t0 = time.time()
+    failed = False
+    while time.time() - t0 < 60:
+        try:
+            if srv.poll(bad) is not None:
+                break
+        except wb.WenofvError as err:
+            assert err.code == wb.ENUMERIC
+            failed = True
+            break
+        time.sleep(0.002)
+    assert failed
+    res = _drain(srv, [good])
+    U, info = res[good]
+    ref, _ = alone(wb, c2, e2, U2, max_steps=3)
+    assert np.abs(U - ref).max() <= 1e-12 * np.abs(ref).max()
+    srv.close()

@@ -1,0 +1,261 @@
+"""Parity of the sm_100a path (through the C ABI) with the oracle and the reference.
+
+* FP64_STRICT (the reference's operation order, no contraction) must equal the oracle and
+  the reference's golden vectors bit for bit.
+* FP64 (contracted, reciprocal form) must agree with the oracle to 1e-11 of max |U| after
+  a few steps (tolerances stated per test).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+from oracle import BC_OUTFLOW, EQ_EULER, EQ_LINEAR_ADV, Problem, reference_available, run_reference
+import cases
+
+pytestmark = pytest.mark.gpu
+GOLD = golden_cases()
+FAST_RTOL = 1e-11  # max |GPU - oracle| / max |U| after a few FP64 steps with FMA contraction
+
+
+def relerr(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def solver_for(wb, p: Problem, precision):
+    cfg = wb.make_config(p.nx, p.ny, xl=p.xl, xr=p.xr, yl=p.yl, yr=p.yr, bc=p.bc, rk=p.rk, cfl=p.cfl,
+                         scheme=p.scheme, limiter=p.limiter, flux=p.flux, recon=p.recon,
+                         ref_slabs=p.ref_slabs, precision=precision)
+    eq = wb.make_eq(kind=p.eq_kind, rho10=p.rho10, rho20=p.rho20, sound1=p.sound1, sound2=p.sound2,
+                    gamma=p.gamma, adv_u=p.adv_u, adv_v=p.adv_v)
+    return wb.Solver(cfg, eq)
+
+
+def problem_of(meta) -> Problem:
+    return Problem(nx=meta["nx"], ny=meta["ny"], rk=meta["rk"], cfl=meta["cfl"], scheme=meta["scheme"],
+                   flux=meta["flux"], recon=meta["recon"], limiter=meta["limiter"], ref_slabs=meta["ref_slabs"],
+                   rho10=meta["rho10"], rho20=meta["rho20"], sound1=meta["sound1"], sound2=meta["sound2"])
+
+
+# ---- pointwise kernels ------------------------------------------------------------------------
+def stencils(rng, n):
+    s = [rng.standard_normal((n, 5)),                                     # generic
+         rng.uniform(0, 1, (n, 5)) * 1e3 + 1e3,                           # large offset, small spread
+         np.repeat(rng.standard_normal((n, 1)), 5, axis=1),                # flat
+         np.where(rng.uniform(size=(n, 5)) < 0.5, 1e-6, 1000.0),           # jumps 1e-6 .. 1e3
+         rng.standard_normal((n, 5)) * 1e-12]                              # tiny
+    return np.concatenate(s)
+
+
+@pytest.mark.parametrize("scheme", [0, 1])
+def test_weno_probe(wb, oracle_lib, scheme):
+    st = stencils(np.random.default_rng(1), 400)
+    ref = np.array([[oracle_lib.weno(scheme, s, gp) for gp in range(4)] for s in st])
+    strict = wb.probe_weno(scheme, st, precision=wb.FP64_STRICT)
+    assert np.array_equal(strict, ref)
+    fast = wb.probe_weno(scheme, st, precision=wb.FP64)
+    scale = np.abs(st).max(axis=1, keepdims=True)
+    assert np.all(np.abs(fast - ref) <= 1e-13 * scale)
+    f32 = wb.probe_weno(scheme, st, precision=wb.FP32_BULK)
+    assert np.all(np.abs(f32 - ref) <= 2e-5 * scale)
+
+
+def two_phase_states(rng, n, rho10=1000.0, rho20=1.0):
+    z1 = np.concatenate([rng.uniform(1e-8, 1e-6, n // 4), rng.uniform(1 - 1e-6, 1 - 1e-8, n // 4),
+                         rng.uniform(0.01, 0.99, n - n // 2)])
+    a1 = z1 * rho10 * (1 + rng.uniform(-1e-4, 1e-4, n))
+    a2 = (1 - z1) * rho20 * (1 + rng.uniform(-1e-4, 1e-4, n))
+    rho = a1 + a2
+    return np.stack([a1, a2, rho * rng.uniform(-2, 2, n), rho * rng.uniform(-2, 2, n)], axis=1)
+
+
+@pytest.mark.parametrize("flux", [0, 1])
+@pytest.mark.parametrize("normal", [(1.0, 0.0), (0.0, 1.0)])
+def test_two_phase_riemann_probe(wb, oracle_lib, flux, normal):
+    rng = np.random.default_rng(2)
+    UL, UR = two_phase_states(rng, 800), two_phase_states(rng, 800)
+    p = Problem(nx=8, ny=8, rho10=1000.0, rho20=1.0, sound1=70.0, sound2=70.0)
+    eq = wb.make_eq(rho10=1000.0, rho20=1.0, sound1=70.0, sound2=70.0)
+    ref = np.array([oracle_lib.riemann(p, flux, a, b, *normal) for a, b in zip(UL, UR)])
+    assert np.array_equal(wb.probe_riemann(eq, flux, UL, UR, *normal, precision=wb.FP64_STRICT), ref)
+    fast = wb.probe_riemann(eq, flux, UL, UR, *normal, precision=wb.FP64)
+    scale = np.abs(ref).max(axis=1, keepdims=True) + 1.0
+    assert np.all(np.abs(fast - ref) <= 1e-11 * scale)
+
+
+@pytest.mark.parametrize("flux", [0, 1])
+def test_euler_riemann_probe(wb, oracle_lib, flux):
+    rng = np.random.default_rng(3)
+
+    def st(n):
+        rho, p = rng.uniform(0.1, 1.5, n), rng.uniform(0.03, 1.5, n)
+        u, v = rng.uniform(-1.2, 1.2, n), rng.uniform(-1.2, 1.2, n)
+        return np.stack([rho, rho * u, rho * v, p / 0.4 + 0.5 * rho * (u * u + v * v)], axis=1)
+    UL, UR = st(500), st(500)
+    p = Problem(nx=8, ny=8, eq_kind=EQ_EULER)
+    eq = wb.make_eq(kind=wb.EQ_EULER)
+    for nrm in ((1.0, 0.0), (0.0, 1.0)):
+        ref = np.array([oracle_lib.riemann(p, flux, a, b, *nrm) for a, b in zip(UL, UR)])
+        assert np.array_equal(wb.probe_riemann(eq, flux, UL, UR, *nrm, precision=wb.FP64_STRICT), ref)
+        got = wb.probe_riemann(eq, flux, UL, UR, *nrm, precision=wb.FP64)
+        assert np.allclose(got, ref, rtol=1e-12, atol=1e-13)
+
+
+@pytest.mark.parametrize("normal", [(1.0, 0.0), (0.0, 1.0)])
+def test_eigen_probe(wb, oracle_lib, normal):
+    rng = np.random.default_rng(4)
+    U = two_phase_states(rng, 200)
+    p = Problem(nx=8, ny=8, rho10=1000.0, rho20=1.0, sound1=70.0, sound2=70.0)
+    eq = wb.make_eq(rho10=1000.0, rho20=1.0, sound1=70.0, sound2=70.0)
+    L, R = wb.probe_eigen(eq, U, *normal, precision=wb.FP64_STRICT)
+    for k in range(len(U)):
+        Lr, Rr = oracle_lib.eigen(p, U[k], *normal)
+        assert np.array_equal(L[k], Lr) and np.array_equal(R[k], Rr)
+
+
+# ---- whole stages and steps against the reference's golden vectors ------------------------------
+@pytest.mark.parametrize("name", sorted(GOLD))
+def test_strict_matches_reference_golden(wb, name):
+    meta, g = GOLD[name], load_golden(name)
+    p = problem_of(meta)
+    with solver_for(wb, p, wb.FP64_STRICT) as s:
+        s.upload(g["U0"])
+        assert np.array_equal(s.rhs(), g["rhs"])
+        if meta["t_end"] > 0:
+            t, n = s.advance(meta["t_end"])
+        else:
+            t, n = s.advance(1e9, max_steps=meta["steps"])
+        assert n == meta["nsteps_taken"]
+        assert np.array_equal(s.download(), g["U"])
+
+
+@pytest.mark.parametrize("name", sorted(GOLD))
+def test_fast_matches_reference_golden(wb, oracle_lib, name):
+    meta, g = GOLD[name], load_golden(name)
+    p = problem_of(meta)
+    with solver_for(wb, p, wb.FP64) as s:
+        s.upload(g["U0"])
+        # the RHS is a difference of fluxes much larger than itself: its error is measured as
+        # the change it makes to U over one CFL step, relative to max |U|
+        dt = oracle_lib.compute_dt(p, g["U0"])
+        assert np.abs(s.rhs() - g["rhs"]).max() * dt <= 1e-11 * np.abs(g["U0"]).max()
+        if meta["t_end"] > 0:
+            s.advance(meta["t_end"])
+        else:
+            s.advance(1e9, max_steps=meta["steps"])
+        assert relerr(s.download(), g["U"]) <= FAST_RTOL
+
+
+def test_manual_steps_and_dt(wb, oracle_lib):
+    U0, prm = cases.liquid_column(52, 36, seed=21)
+    p = Problem(nx=52, ny=36, scheme=1, flux=1, recon=1, limiter=1, ref_slabs=4, **prm)
+    with solver_for(wb, p, wb.FP64_STRICT) as s:
+        s.upload(U0)
+        V = U0
+        for _ in range(3):
+            dt = s.compute_dt()
+            assert dt == oracle_lib.compute_dt(p, V)
+            s.step(dt)
+            V = oracle_lib.step(p, V, dt)
+        assert np.array_equal(s.download(), V)
+
+
+@pytest.mark.skipif(not reference_available(), reason="compiled reference not present")
+def test_strict_matches_live_reference(wb):
+    U0, prm = cases.liquid_column(64, 48, seed=31)
+    p = Problem(nx=64, ny=48, scheme=1, flux=1, recon=1, limiter=1, ref_slabs=4, **prm)
+    r = run_reference(p, testcase=2, U0=U0, steps=10)
+    with solver_for(wb, p, wb.FP64_STRICT) as s:
+        s.upload(U0)
+        s.advance(1e9, max_steps=10)
+        assert np.array_equal(s.download(), r.U)
+
+
+# ---- edge cases: ragged strips, short row runs, tiny and non-square grids --------------------
+@pytest.mark.parametrize("nx,ny", [(8, 8), (12, 8), (27, 5), (53, 70), (130, 9)])
+@pytest.mark.parametrize("recon,lim", [(0, 0), (1, 1)])
+def test_ragged_sizes_strict(wb, oracle_lib, nx, ny, recon, lim):
+    U0, prm = cases.liquid_column(nx, ny, seed=nx * 100 + ny)
+    p = Problem(nx=nx, ny=ny, scheme=1, flux=1, recon=recon, limiter=lim, **prm)
+    V, n, _, _ = oracle_lib.advance(p, U0, t_end=1e9, max_steps=3)
+    with solver_for(wb, p, wb.FP64_STRICT) as s:
+        s.upload(U0)
+        assert np.array_equal(s.rhs(), oracle_lib.rhs(p, U0))
+        s.advance(1e9, max_steps=3)
+        assert np.array_equal(s.download(), V)
+
+
+@pytest.mark.parametrize("recon", [0, 1])
+@pytest.mark.parametrize("flux", [0, 1])
+def test_euler_outflow_strict(wb, oracle_lib, recon, flux):
+    U0, _ = cases.euler_quadrants(40, 30)
+    p = Problem(nx=40, ny=30, bc=BC_OUTFLOW, eq_kind=EQ_EULER, scheme=1, flux=flux, recon=recon, cfl=0.4)
+    V, n, t, _ = oracle_lib.advance(p, U0, t_end=0.01)
+    with solver_for(wb, p, wb.FP64_STRICT) as s:
+        s.upload(U0)
+        t2, n2 = s.advance(0.01)
+        assert n2 == n and t2 == t
+        assert np.array_equal(s.download(), V)
+
+
+@pytest.mark.parametrize("nx", [64, 130])
+def test_advection_strict(wb, oracle_lib, nx):
+    U0 = cases.advection_sine(nx, 32)
+    p = Problem(nx=nx, ny=32, eq_kind=EQ_LINEAR_ADV, scheme=0, flux=0, recon=0, cfl=0.5)
+    V, n, t, _ = oracle_lib.advance(p, U0, t_end=0.25)
+    with solver_for(wb, p, wb.FP64_STRICT) as s:
+        s.upload(U0)
+        t2, n2 = s.advance(0.25)
+        assert n2 == n
+        assert np.array_equal(s.download(), V)
+
+
+def test_layout_round_trip(wb):
+    U0, prm = cases.liquid_column(20, 12, seed=2)
+    p = Problem(nx=20, ny=12, **prm)
+    with solver_for(wb, p, wb.FP64) as s:
+        aos = np.ascontiguousarray(np.transpose(U0, (2, 1, 0)))  # [i][j][v]
+        s.upload(aos, layout=wb.LAYOUT_REF_AOS)
+        assert np.array_equal(s.download(), U0)
+        assert np.array_equal(s.download(layout=wb.LAYOUT_REF_AOS), aos)
+
+
+def test_nan_is_reported(wb):
+    U0, prm = cases.liquid_column(32, 32, seed=3)
+    U0[2, 5, 7] = np.nan
+    p = Problem(nx=32, ny=32, **prm)
+    with solver_for(wb, p, wb.FP64) as s:
+        s.upload(U0)
+        with pytest.raises(wb.WenofvError) as e:
+            s.advance(1e9, max_steps=2)
+        assert e.value.code == wb.ENUMERIC
+        flags, cell = s.status()
+        assert flags & wb.FLAG_NAN_DT and cell >= 0
+
+
+# ---- full size: properties the domain offers ------------------------------------------------------
+def test_column_1024_conservation_and_bounds(wb):
+    U0, prm = cases.liquid_column(1024, 1024, seed=3)
+    p = Problem(nx=1024, ny=1024, scheme=1, flux=1, recon=1, limiter=1, **prm)
+    with solver_for(wb, p, wb.FP64) as s:
+        s.upload(U0)
+        t, n = s.advance(1e9, max_steps=6)
+        U = s.download()
+    m0, m1 = U0.sum(axis=(1, 2)), U.sum(axis=(1, 2))
+    assert np.all(np.abs(m1 - m0) <= 1e-12 * np.abs(U0).sum(axis=(1, 2)))  # mass and momentum, periodic
+    assert (U[0] > 0).all() and (U[1] > 0).all()
+
+
+def test_advection_128_full_period(wb, oracle_lib):
+    # config 1 at its full size: one period, FP64 vs oracle and vs the exact solution
+    U0 = cases.advection_sine(128, 128)
+    p = Problem(nx=128, ny=128, eq_kind=EQ_LINEAR_ADV, scheme=0, flux=0, recon=0, cfl=0.5)
+    with solver_for(wb, p, wb.FP64) as s:
+        s.upload(U0)
+        t, n = s.advance(1.0)
+        U = s.download()
+    assert n == 512 and abs(t - 1.0) < 1e-12
+    V, *_ = oracle_lib.advance(p, U0, t_end=1.0)
+    assert relerr(U, V) <= 1e-10
+    assert np.abs(U - U0).mean() < 1e-5  # L1 error of WENO-JS5 + SSP-RK3 after one period
