@@ -176,7 +176,11 @@ def test_strict_matches_live_reference(wb):
 @pytest.mark.parametrize("nx,ny", [(8, 8), (12, 8), (27, 5), (53, 70), (130, 9)])
 @pytest.mark.parametrize("recon,lim", [(0, 0), (1, 1)])
 def test_ragged_sizes_strict(wb, oracle_lib, nx, ny, recon, lim):
-    U0, prm = cases.liquid_column(nx, ny, seed=nx * 100 + ny)
+    # without the limiter a density ratio of 1000 on these coarse grids drives the partial
+    # densities negative (the oracle and the reference then produce NaN too), so that case
+    # uses a mild column
+    mild = dict(ratio=2.0, eps=0.05) if not lim else {}
+    U0, prm = cases.liquid_column(nx, ny, seed=nx * 100 + ny, **mild)
     p = Problem(nx=nx, ny=ny, scheme=1, flux=1, recon=recon, limiter=lim, **prm)
     V, n, _, _ = oracle_lib.advance(p, U0, t_end=1e9, max_steps=3)
     with solver_for(wb, p, wb.FP64_STRICT) as s:
