@@ -137,6 +137,24 @@ void *wenofv_stream(wenofv_ctx *ctx);
  * plane stride pitch*ny (valid until the next step) */
 int wenofv_device_state(wenofv_ctx *ctx, double **U, int *pitch);
 
+/* One SSP-RK step (cfg->rk_method) of a caller-owned device state without allocating any
+ * device memory: for callers that cannot call cudaMalloc (they manage GPU memory through
+ * their own pool or framework allocator, which a direct cudaMalloc would bypass and may
+ * exceed; they reserve all free device memory at start-up; or they cannot afford the device
+ * synchronisation of cudaMalloc/cudaFree inside a latency-bound loop).  d_U and
+ * d_U_next are distinct device arrays, SoA [v][ny][pitch] with pitch >= nx; d_U is only
+ * read.  The stage kernel's scratch (one intermediate RK state, grid metric, descriptor,
+ * loop state, work list, counter) is a fixed 4.2 MiB device array inside the library, held
+ * by every GPU that loads it until exit; so nvar*ny*pitch <= 524288, 2*nx + ny <= 8192 and
+ * ceil(nx/strip)*ceil(ny/16) <= 8192, otherwise WENOFV_EINVAL.  The first call on a device
+ * looks up that array's address and should come before any stream capture.  Calls share
+ * the array: calls whose work overlaps on the GPU race.  The call synchronises `stream`
+ * (a cudaStream_t, NULL = default stream) once after its host-to-device set-up copies, and
+ * again at the end when flags is non-NULL (then *flags receives the WENOFV_FLAG_* word).
+ * No counterpart in the reference. */
+int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_params *eq, const double *d_U, double *d_U_next,
+                        int pitch, double dt, void *stream, uint32_t *flags);
+
 /* ---- batched ensemble: many uneven instances per persistent launch (no counterpart in
  *      the reference, which solves one grid per MPI job) ---------------------------------- */
 typedef struct wenofv_batch wenofv_batch;

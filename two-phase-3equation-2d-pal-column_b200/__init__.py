@@ -29,7 +29,7 @@ EXPORTS = (
     "wenofv_abi_version", "wenofv_strerror", "wenofv_last_error", "wenofv_default_config",
     "wenofv_create", "wenofv_destroy", "wenofv_upload", "wenofv_download", "wenofv_compute_dt",
     "wenofv_step", "wenofv_rhs", "wenofv_advance", "wenofv_status", "wenofv_synchronize",
-    "wenofv_stream", "wenofv_device_state",
+    "wenofv_stream", "wenofv_device_state", "wenofv_step_noalloc",
     "wenofv_batch_create", "wenofv_batch_destroy", "wenofv_batch_upload", "wenofv_batch_download",
     "wenofv_batch_advance", "wenofv_batch_set_tiling", "wenofv_batch_stream", "wenofv_batch_autotune",
     "wenofv_server_create", "wenofv_server_destroy", "wenofv_server_submit", "wenofv_server_poll",
@@ -120,6 +120,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.wenofv_probe_riemann.argtypes = [C.POINTER(EqParams), I, I, DP, DP, I, D, D, DP, I]
     L.wenofv_probe_eigen.argtypes = [C.POINTER(EqParams), I, DP, I, D, D, DP, DP, I]
     L.wenofv_probe_fma_peak.argtypes = [I, I, DP]
+    L.wenofv_step_noalloc.argtypes = [C.POINTER(Config), C.POINTER(EqParams), P, P, I, D, P, C.POINTER(C.c_uint32)]
     _lib = L
     return L
 
