@@ -92,10 +92,10 @@ __global__ void probe_riemann_kernel(EqParams P, int flux, const double *UL, con
     constexpr int NV = EqTraits<EQ>::NV;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    R l[NV], r[NV], f[NV];
-    for (int v = 0; v < NV; v++) { l[v] = (R)UL[NV * k + v]; r[v] = (R)UR[NV * k + v]; }
+    double l[NV], r[NV], f[NV];
+    for (int v = 0; v < NV; v++) { l[v] = UL[NV * k + v]; r[v] = UR[NV * k + v]; }
     riemann<EQ, R>(P, flux, l, r, f, xdir != 0);
-    for (int v = 0; v < NV; v++) F[NV * k + v] = (double)f[v];
+    for (int v = 0; v < NV; v++) F[NV * k + v] = f[v];
 }
 
 template <int EQ, class R>
@@ -104,8 +104,8 @@ __global__ void probe_eigen_kernel(EqParams P, const double *U, int n, int xdir,
     constexpr int NV = EqTraits<EQ>::NV;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    R u[NV];
-    for (int v = 0; v < NV; v++) u[v] = (R)U[NV * k + v];
+    double u[NV];
+    for (int v = 0; v < NV; v++) u[v] = U[NV * k + v];
     for (int row = 0; row < NV; row++) {
         R lr[NV], rr[NV];
         eigen_rows<EQ, R>(P, u, xdir != 0, row, lr, rr);

@@ -191,9 +191,9 @@ struct TwoPhaseK {
         return (z1 < z2) ? pre2 : pre1;
     }
     // getSoundSpeed (Wood), include/Equations.hpp:126-146
-    template <class R> __device__ __forceinline__ R sound(R z1rho1, R z2rho2, R z1) const
+    // z2 comes in as 1 - z1 rounded from FP64: in FP32, 1 - (float)z1 loses z2 near pure phase 1
+    template <class R> __device__ __forceinline__ R sound(R z1rho1, R z2rho2, R z1, R z2) const
     {
-        const R z2 = R(1.0) - z1;
         const R rho = z1rho1 + z2rho2;
         const R rho1 = z1rho1 / z1;
         const R rho2 = z2rho2 / z2;
@@ -206,12 +206,15 @@ struct TwoPhaseK {
 // reference recomputes getVolumeFrac per call; the values are identical).
 template <class R> struct TPState {
     R z1rho1, z2rho2, rhou, rhov, rho, u, v, pre, c;
+    double pd; // the FP64 pressure (pre is pd rounded to R)
 };
 
+// The state comes in FP64 in every form: the volume fraction and the pressure are
+// recovered from the FP64 values.
 template <class R>
-__device__ __forceinline__ void tp_state(const TwoPhaseK &K, const R *U, TPState<R> &s)
+__device__ __forceinline__ void tp_state(const TwoPhaseK &K, const double *U, TPState<R> &s)
 {
-    s.z1rho1 = U[0]; s.z2rho2 = U[1]; s.rhou = U[2]; s.rhov = U[3];
+    s.z1rho1 = (R)U[0]; s.z2rho2 = (R)U[1]; s.rhou = (R)U[2]; s.rhov = (R)U[3];
     s.rho = s.z1rho1 + s.z2rho2;
 #if WENOFV_STRICT
     s.u = s.rhou / s.rho;
@@ -221,9 +224,10 @@ __device__ __forceinline__ void tp_state(const TwoPhaseK &K, const R *U, TPState
     s.u = s.rhou * ir;
     s.v = s.rhov * ir;
 #endif
-    const double z1 = K.volume_frac((double)s.z1rho1, (double)s.z2rho2);
-    s.pre = (R)K.pressure((double)s.z1rho1, (double)s.z2rho2, z1);
-    s.c = K.sound<R>(s.z1rho1, s.z2rho2, (R)z1);
+    const double z1 = K.volume_frac(U[0], U[1]);
+    s.pd = K.pressure(U[0], U[1], z1);
+    s.pre = (R)s.pd;
+    s.c = K.sound<R>(s.z1rho1, s.z2rho2, (R)z1, (R)(1.0 - z1));
 }
 
 // getMaxEigenValue, include/Equations.hpp:149-156 (u from U[2]/(U[0]+U[1]) as there)
@@ -322,31 +326,140 @@ __device__ __forceinline__ void tp_hllc(const TPState<R> &L, const TPState<R> &R
     }
 }
 
+// FP32-bulk forms of the two fluxes.  The same fluxes, rearranged so that FP32 rounds only
+// small quantities: the pressure terms of the momentum fluxes are added in FP64 (the
+// pressure of a weakly compressible flow is a large constant plus small variations, and
+// its FP32 rounding would not cancel between the two faces of a cell), the pressure jump of
+// S* and the state jump of LLF are formed in FP64, and the HLLC star fluxes use the exact
+// identities S_K (k U*_K - U_K) + F_K = k S* U_K + k rho_K S_K (S* - vn_K) n + p_K n
+// (k = (S_K - vn_K) / (S_K - S*)), which need no difference of nearly equal terms.
+__device__ __forceinline__ void tp_llf_f32(const TPState<float> &L, const TPState<float> &Rs, const double *ULd,
+                                           const double *URd, double *F, bool xdir)
+{
+    const double nx = xdir ? 1.0 : 0.0, ny = xdir ? 0.0 : 1.0;
+    const float ws = std_max(tp_max_eig(L, nx, ny), tp_max_eig(Rs, nx, ny));
+    const float vn_L = xdir ? L.u : L.v, vn_R = xdir ? Rs.u : Rs.v;
+    const float ut_L = xdir ? L.v : L.u, ut_R = xdir ? Rs.v : Rs.u;
+    float FD[4]; // FUL + FUR without the pressure terms
+    FD[0] = L.z1rho1 * vn_L + Rs.z1rho1 * vn_R;
+    FD[1] = L.z2rho2 * vn_L + Rs.z2rho2 * vn_R;
+    FD[2] = L.rho * vn_L * (xdir ? vn_L : ut_L) + Rs.rho * vn_R * (xdir ? vn_R : ut_R);
+    FD[3] = L.rho * vn_L * (xdir ? ut_L : vn_L) + Rs.rho * vn_R * (xdir ? ut_R : vn_R);
+    const double pm = 0.5 * (L.pd + Rs.pd);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) F[r] = (double)(0.5f * (FD[r] - ws * (float)(URd[r] - ULd[r])));
+    F[2] += pm * nx;
+    F[3] += pm * ny;
+}
+
+__device__ __forceinline__ void tp_hllc_f32(const TPState<float> &L, const TPState<float> &Rs, double *F, bool xdir)
+{
+    const float vn_L = xdir ? L.u : L.v, vn_R = xdir ? Rs.u : Rs.v;
+    const float sL = sqrtf(L.rho), sR = sqrtf(Rs.rho);
+    const float is = 1.0f / (sL + sR);
+    const float vn_roe = (vn_L * sL + vn_R * sR) * is;
+    float c2_roe = (L.c * L.c * sL + Rs.c * Rs.c * sR) * is;
+    c2_roe += 0.5f * sL * sR * is * is * (vn_R - vn_L) * (vn_R - vn_L);
+    const float c_roe = sqrtf(c2_roe);
+    const float S_L = std_min(vn_L - L.c, vn_roe - c_roe);
+    const float S_R = std_max(vn_R + Rs.c, vn_roe + c_roe);
+    const float dp = (float)(Rs.pd - L.pd);
+    const float S_star = ((S_L - vn_L) * L.rho * vn_L - (S_R - vn_R) * Rs.rho * vn_R + dp) /
+                         ((S_L - vn_L) * L.rho - (S_R - vn_R) * Rs.rho);
+    const bool left = S_star >= 0.0f;
+    const TPState<float> &K = left ? L : Rs;
+    const float S_K = left ? S_L : S_R, vn_K = left ? vn_L : vn_R;
+    const bool super = left ? (S_L >= 0.0f) : (S_R <= 0.0f);
+    float a, b; // F = a U_K + b n (+ p_K n in FP64)
+    if (super) {
+        a = vn_K;
+        b = 0.0f;
+    } else {
+        const float k = (S_K - vn_K) / (S_K - S_star);
+        a = k * S_star;
+        b = k * K.rho * S_K * (S_star - vn_K);
+    }
+    F[0] = (double)(a * K.z1rho1);
+    F[1] = (double)(a * K.z2rho2);
+    F[2] = (double)(a * K.rhou + (xdir ? b : 0.0f)) + (xdir ? K.pd : 0.0);
+    F[3] = (double)(a * K.rhov + (xdir ? 0.0f : b)) + (xdir ? 0.0 : K.pd);
+}
+
 // Characteristic matrices of the two-phase system, include/Equations.hpp:189-327.
 // Row k of L and row r of R in direction x (xdir) or y.
 template <class R> struct TPEigen {
     R z1rho1, z2rho2, rho, u, v, c, c2, sc1_2, sc2_2;
+    R i2c2, i2c, irc2, idsc, irho, pad; // reciprocals of the contracted build; pad: odd size in smem
 };
-template <class R> __device__ __forceinline__ void tp_eigen_prep(const TwoPhaseK &K, const R *U, TPEigen<R> &e)
+template <class R> __device__ __forceinline__ void tp_eigen_prep(const TwoPhaseK &K, const double *U, TPEigen<R> &e)
 {
-    e.z1rho1 = U[0]; e.z2rho2 = U[1];
+    e.z1rho1 = (R)U[0]; e.z2rho2 = (R)U[1];
     e.rho = e.z1rho1 + e.z2rho2;
-    e.u = U[2] / e.rho;
-    e.v = U[3] / e.rho;
-    const double z1d = K.volume_frac((double)U[0], (double)U[1]);
+#if WENOFV_STRICT
+    e.u = (R)U[2] / e.rho;
+    e.v = (R)U[3] / e.rho;
+#else
+    e.irho = R(1) / e.rho;
+    e.u = (R)U[2] * e.irho;
+    e.v = (R)U[3] * e.irho;
+#endif
+    const double z1d = K.volume_frac(U[0], U[1]);
     const R z1 = (R)z1d;
-    const R z2 = R(1.0) - z1;
-    e.c = K.sound<R>(e.z1rho1, e.z2rho2, z1);
+    const R z2 = (R)(1.0 - z1d);
+    e.c = K.sound<R>(e.z1rho1, e.z2rho2, z1, z2);
     e.c2 = e.c * e.c;
     const R c1_2 = R(K.c1_2), c2_2 = R(K.c2_2);
-    const R zrho1 = e.z1rho1 * c1_2 / (z1 * z1);
-    const R zrho2 = e.z2rho2 * c2_2 / (z2 * z2);
-    e.sc1_2 = c1_2 / z1 - c1_2 / z1 * zrho1 / (zrho1 + zrho2);
-    e.sc2_2 = c2_2 / z2 - c2_2 / z2 * zrho2 / (zrho1 + zrho2);
+    if constexpr (sizeof(R) < sizeof(double)) {
+        // FP32: the same quantities without the cancellation 1 - zrho1/(zrho1+zrho2) and
+        // without dividing by z_k^2 (exact algebra: multiply zrho_k through by z1^2 z2^2)
+        const R a = e.z1rho1 * c1_2 * (z2 * z2), b = e.z2rho2 * c2_2 * (z1 * z1);
+        const R g = c1_2 * c2_2 / (a + b);
+        e.sc1_2 = g * (z1 * e.z2rho2);
+        e.sc2_2 = g * (z2 * e.z1rho1);
+    } else {
+        const R zrho1 = e.z1rho1 * c1_2 / (z1 * z1);
+        const R zrho2 = e.z2rho2 * c2_2 / (z2 * z2);
+        e.sc1_2 = c1_2 / z1 - c1_2 / z1 * zrho1 / (zrho1 + zrho2);
+        e.sc2_2 = c2_2 / z2 - c2_2 / z2 * zrho2 / (zrho1 + zrho2);
+    }
+#if !WENOFV_STRICT
+    e.i2c2 = R(1) / (R(2.0) * e.c2);
+    e.i2c = e.c * e.i2c2; // c / (2 c^2) = 1/(2c)
+    e.irc2 = R(1) / (e.rho * e.c2);
+    e.idsc = R(1) / (e.sc1_2 - e.sc2_2);
+#endif
 }
 template <class R> __device__ __forceinline__ void tp_L_row(const TPEigen<R> &e, bool xdir, int k, R *row)
 {
     const R un = xdir ? e.u : e.v, ut = xdir ? e.v : e.u;
+#if !WENOFV_STRICT // contracted build: multiplications by the prepared reciprocals
+    switch (k) {
+    case 0:
+        row[0] = (e.sc1_2 + e.c * un) * e.i2c2;
+        row[1] = (e.sc2_2 + e.c * un) * e.i2c2;
+        row[2] = xdir ? -e.i2c : R(0);
+        row[3] = xdir ? R(0) : -e.i2c;
+        break;
+    case 1:
+        row[0] = -e.z2rho2 * (e.sc1_2 - e.sc2_2) * e.irc2;
+        row[1] = e.z1rho1 * (e.sc1_2 - e.sc2_2) * e.irc2;
+        row[2] = R(0);
+        row[3] = R(0);
+        break;
+    case 2:
+        row[0] = -ut;
+        row[1] = -ut;
+        row[2] = xdir ? R(0) : R(1.0);
+        row[3] = xdir ? R(1.0) : R(0);
+        break;
+    default:
+        row[0] = (e.sc1_2 - e.c * un) * e.i2c2;
+        row[1] = (e.sc2_2 - e.c * un) * e.i2c2;
+        row[2] = xdir ? e.i2c : R(0);
+        row[3] = xdir ? R(0) : e.i2c;
+        break;
+    }
+#else
     switch (k) {
     case 0:
         row[0] = (e.sc1_2 + e.c * un) / (R(2.0) * e.c2);
@@ -373,21 +486,34 @@ template <class R> __device__ __forceinline__ void tp_L_row(const TPEigen<R> &e,
         row[3] = xdir ? R(0) : R(1.0) / (R(2.0) * e.c);
         break;
     }
+#endif
 }
 template <class R> __device__ __forceinline__ void tp_R_row(const TPEigen<R> &e, bool xdir, int r, R *row)
 {
     switch (r) {
     case 0:
+#if WENOFV_STRICT
         row[0] = e.z1rho1 / e.rho;
         row[1] = -e.sc2_2 / (e.sc1_2 - e.sc2_2);
-        row[2] = R(0);
         row[3] = e.z1rho1 / e.rho;
+#else
+        row[0] = e.z1rho1 * e.irho;
+        row[1] = -e.sc2_2 * e.idsc;
+        row[3] = row[0];
+#endif
+        row[2] = R(0);
         break;
     case 1:
+#if WENOFV_STRICT
         row[0] = e.z2rho2 / e.rho;
         row[1] = e.sc1_2 / (e.sc1_2 - e.sc2_2);
-        row[2] = R(0);
         row[3] = e.z2rho2 / e.rho;
+#else
+        row[0] = e.z2rho2 * e.irho;
+        row[1] = e.sc1_2 * e.idsc;
+        row[3] = row[0];
+#endif
+        row[2] = R(0);
         break;
     case 2:
         row[0] = xdir ? e.u - e.c : e.u;
@@ -408,16 +534,24 @@ template <class R> __device__ __forceinline__ void tp_R_row(const TPEigen<R> &e,
 //      restated from the standard formulation (Toro, ch. 3 and 10) in the oracle's order.
 template <class R> struct EUState {
     R rho, u, v, E, p, c, H;
+    R ic, b1; // 1/c and (gamma-1)/c^2 of the contracted build (eigenvectors); odd size in smem
 };
-template <class R> __device__ __forceinline__ void eu_state(double gamma, const R *U, EUState<R> &s)
+template <class R> __device__ __forceinline__ void eu_state(double gamma, const double *U, EUState<R> &s)
 {
-    s.rho = U[0];
-    s.u = U[1] / U[0];
-    s.v = U[2] / U[0];
-    s.E = U[3];
-    s.p = R(gamma - 1.0) * (U[3] - R(0.5) * U[0] * (s.u * s.u + s.v * s.v));
-    s.c = sqrt(R(gamma) * s.p / U[0]);
-    s.H = (U[3] + s.p) / U[0];
+    // velocity and pressure recovered in FP64 in every form
+    const double ud = U[1] / U[0], vd = U[2] / U[0];
+    const double pd = (gamma - 1.0) * (U[3] - 0.5 * U[0] * (ud * ud + vd * vd));
+    s.rho = (R)U[0];
+    s.u = (R)ud;
+    s.v = (R)vd;
+    s.E = (R)U[3];
+    s.p = (R)pd;
+    s.c = sqrt(R(gamma) * s.p / s.rho);
+    s.H = (s.E + s.p) / s.rho;
+#if !WENOFV_STRICT
+    s.ic = R(1.0) / s.c;
+    s.b1 = R(gamma - 1.0) * s.ic * s.ic;
+#endif
 }
 template <class R> __device__ __forceinline__ void eu_phy_flux(const EUState<R> &s, const R *U, R *F, R nx, R ny)
 {
@@ -489,11 +623,17 @@ template <class R> __device__ __forceinline__ void eu_L_row(double gamma, const 
     const R nx = xdir ? R(1) : R(0), ny = xdir ? R(0) : R(1);
     const R q2 = R(0.5) * (s.u * s.u + s.v * s.v);
     const R vn = s.u * nx + s.v * ny, vt = s.v * nx - s.u * ny;
+#if WENOFV_STRICT
     const R b1 = R(gamma - 1.0) / (s.c * s.c), b2 = q2 * b1;
+    const R vnc = vn / s.c, nxc = nx / s.c, nyc = ny / s.c;
+#else
+    const R b1 = s.b1, b2 = q2 * b1;
+    const R vnc = vn * s.ic, nxc = nx * s.ic, nyc = ny * s.ic;
+#endif
     switch (k) {
     case 0:
-        row[0] = R(0.5) * (b2 + vn / s.c); row[1] = R(0.5) * (-b1 * s.u - nx / s.c);
-        row[2] = R(0.5) * (-b1 * s.v - ny / s.c); row[3] = R(0.5) * b1;
+        row[0] = R(0.5) * (b2 + vnc); row[1] = R(0.5) * (-b1 * s.u - nxc);
+        row[2] = R(0.5) * (-b1 * s.v - nyc); row[3] = R(0.5) * b1;
         break;
     case 1:
         row[0] = R(1.0) - b2; row[1] = b1 * s.u; row[2] = b1 * s.v; row[3] = -b1;
@@ -502,8 +642,8 @@ template <class R> __device__ __forceinline__ void eu_L_row(double gamma, const 
         row[0] = -vt; row[1] = -ny; row[2] = nx; row[3] = R(0.0);
         break;
     default:
-        row[0] = R(0.5) * (b2 - vn / s.c); row[1] = R(0.5) * (-b1 * s.u + nx / s.c);
-        row[2] = R(0.5) * (-b1 * s.v + ny / s.c); row[3] = R(0.5) * b1;
+        row[0] = R(0.5) * (b2 - vnc); row[1] = R(0.5) * (-b1 * s.u + nxc);
+        row[2] = R(0.5) * (-b1 * s.v + nyc); row[3] = R(0.5) * b1;
         break;
     }
 }
@@ -527,7 +667,7 @@ template <int EQ> struct EqTraits { static constexpr int NV = 4; };
 template <> struct EqTraits<EQ_LINEAR_ADV> { static constexpr int NV = 1; };
 
 // getMaxEigenValue (include/Equations.hpp:149-156) for the CFL and the limiter's mu
-template <int EQ, class R> __device__ __forceinline__ void max_eigs(const EqParams &P, const R *U, R &ax, R &ay)
+template <int EQ, class R> __device__ __forceinline__ void max_eigs(const EqParams &P, const double *U, R &ax, R &ay)
 {
     if (EQ == EQ_TWO_PHASE) {
         TwoPhaseK K(P);
@@ -548,32 +688,47 @@ template <int EQ, class R> __device__ __forceinline__ void max_eigs(const EqPara
 
 // getRiemannFlux dispatch (include/Equations.hpp:329-343); flux 0 LLF, 1 HLLC.
 // For scalar advection both are the upwind (LLF with |a.n|) flux.
+// The face states come in FP64 and the flux goes out in FP64 in every form.
 template <int EQ, class R>
-__device__ __forceinline__ void riemann(const EqParams &P, int flux, const R *UL, const R *UR, R *F, bool xdir)
+__device__ __forceinline__ void riemann(const EqParams &P, int flux, const double *ULd, const double *URd, double *F, bool xdir)
 {
-    if (EQ == EQ_TWO_PHASE) {
+    constexpr int NV = EqTraits<EQ>::NV;
+    constexpr bool F32 = sizeof(R) < sizeof(double);
+    R UL[NV], UR[NV], Fr[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) { UL[v] = (R)ULd[v]; UR[v] = (R)URd[v]; }
+    if constexpr (EQ == EQ_TWO_PHASE) {
         TwoPhaseK K(P);
         TPState<R> l, r;
-        tp_state<R>(K, UL, l);
-        tp_state<R>(K, UR, r);
-        if (flux == 1) tp_hllc<R>(l, r, UL, UR, F, xdir);
-        else tp_llf<R>(l, r, UL, UR, F, xdir);
-    } else if (EQ == EQ_EULER) {
+        tp_state<R>(K, ULd, l);
+        tp_state<R>(K, URd, r);
+        if constexpr (F32) {
+            if (flux == 1) tp_hllc_f32(l, r, F, xdir);
+            else tp_llf_f32(l, r, ULd, URd, F, xdir);
+        } else {
+            if (flux == 1) tp_hllc<R>(l, r, UL, UR, Fr, xdir);
+            else tp_llf<R>(l, r, UL, UR, Fr, xdir);
+        }
+    } else if constexpr (EQ == EQ_EULER) {
         EUState<R> l, r;
-        eu_state<R>(P.gamma, UL, l);
-        eu_state<R>(P.gamma, UR, r);
-        if (flux == 1) eu_hllc<R>(P.gamma, l, r, UL, UR, F, xdir);
-        else eu_llf<R>(l, r, UL, UR, F, xdir);
+        eu_state<R>(P.gamma, ULd, l);
+        eu_state<R>(P.gamma, URd, r);
+        if (flux == 1) eu_hllc<R>(P.gamma, l, r, UL, UR, Fr, xdir);
+        else eu_llf<R>(l, r, UL, UR, Fr, xdir);
     } else {
         const R an = xdir ? (R(P.adv_u) * R(1.0) + R(P.adv_v) * R(0.0)) : (R(P.adv_u) * R(0.0) + R(P.adv_v) * R(1.0));
         const R ws = std_max(fabs(an), fabs(an));
-        F[0] = R(0.5) * (an * UL[0] + an * UR[0] - ws * (UR[0] - UL[0]));
+        Fr[0] = R(0.5) * (an * UL[0] + an * UR[0] - ws * (UR[0] - UL[0]));
+    }
+    if constexpr (!(F32 && EQ == EQ_TWO_PHASE)) { // the FP32 two-phase fluxes write F themselves
+#pragma unroll
+        for (int v = 0; v < NV; v++) F[v] = (double)Fr[v];
     }
 }
 
 // Characteristic projection rows: row k of L and row k of R for the state U.
 template <int EQ, class R>
-__device__ __forceinline__ void eigen_rows(const EqParams &P, const R *U, bool xdir, int k, R *Lrow, R *Rrow)
+__device__ __forceinline__ void eigen_rows(const EqParams &P, const double *U, bool xdir, int k, R *Lrow, R *Rrow)
 {
     if (EQ == EQ_TWO_PHASE) {
         TwoPhaseK K(P);
@@ -590,6 +745,42 @@ __device__ __forceinline__ void eigen_rows(const EqParams &P, const R *U, bool x
         Lrow[0] = R(1.0);
         Rrow[0] = R(1.0);
     }
+}
+
+// Per-cell eigensystem data, computed once per cell and row in FP64 (every form) and shared
+// by the lanes that build its rows of L and R and by the limiter's wave speeds.
+template <int EQ> struct CellEigen { using type = TPEigen<double>; };
+template <> struct CellEigen<EQ_EULER> { using type = EUState<double>; };
+
+template <int EQ> __device__ __forceinline__ void cell_eigen(const EqParams &P, const double *U, typename CellEigen<EQ>::type &e)
+{
+    if constexpr (EQ == EQ_TWO_PHASE) {
+        TwoPhaseK K(P);
+        tp_eigen_prep<double>(K, U, e);
+    } else if constexpr (EQ == EQ_EULER) {
+        eu_state<double>(P.gamma, U, e);
+    }
+}
+template <int EQ>
+__device__ __forceinline__ void eigen_rows_of(const EqParams &P, const typename CellEigen<EQ>::type &e, bool xdir, int k,
+                                              double *Lrow, double *Rrow)
+{
+    if constexpr (EQ == EQ_TWO_PHASE) {
+        tp_L_row<double>(e, xdir, k, Lrow);
+        tp_R_row<double>(e, xdir, k, Rrow);
+    } else if constexpr (EQ == EQ_EULER) {
+        eu_L_row<double>(P.gamma, e, xdir, k, Lrow);
+        eu_R_row<double>(e, xdir, k, Rrow);
+    } else {
+        Lrow[0] = 1.0;
+        Rrow[0] = 1.0;
+    }
+}
+// getMaxEigenValue in x and y from the cell data (the same expressions as max_eigs)
+template <int EQ> __device__ __forceinline__ void max_eigs_of(const typename CellEigen<EQ>::type &e, double &ax, double &ay)
+{
+    ax = fabs(e.u * 1.0 + e.v * 0.0) + e.c;
+    ay = fabs(e.u * 0.0 + e.v * 1.0) + e.c;
 }
 
 // number of leading variables the bound-preserving limiter acts on: the two partial

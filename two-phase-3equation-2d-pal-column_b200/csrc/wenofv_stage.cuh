@@ -130,6 +130,8 @@ template <int EQ> struct StageSmem {
     double syt[2][TX][4][NV];     // top face states of the current and previous row
     double sfx[2][TX + 1][NV];    // x-face quadrature sums of two rows
     double sfy[2][TX][NV];        // y-face quadrature sums below the current and previous row
+    static constexpr int PE = NV > 1 ? P : 1;
+    typename CellEigen<EQ>::type se[PE]; // per-cell eigensystem data of one row, by position
     double sdxc[TX], sdxl[TX];    // column widths of the strip
     double sred[NT / 32];
     int s_last;
@@ -150,33 +152,69 @@ __device__ __forceinline__ void load_row(double (*dst)[StageGeom<EQ>::P], const 
     }
 }
 
+// value of a reconstruction: in the deviation form the anchor plus the FP32 deviation, in
+// FP64 the reconstructed value itself (unchanged, so the FP64 forms keep their bits)
+template <bool DEV, class R> __device__ __forceinline__ double anchor(double c, R d)
+{
+    if constexpr (DEV) return c + (double)d;
+    else return (double)d;
+}
+
+// ---- phase 0: the per-cell eigensystem data (L/R rows, wave speeds) of row r at the
+// strip's P positions, computed once per cell by one thread each (threads t0 .. t0+n-1)
+// instead of by every lane that needs it.  Identical arithmetic to the per-lane form.
+template <int EQ, int RECON>
+__device__ __forceinline__ void phase_eigen(StageSmem<EQ> &S, const InstDesc &D, int r, int t0, int n)
+{
+    constexpr int NV = StageGeom<EQ>::NV, P = StageGeom<EQ>::P;
+    if constexpr (NV > 1) {
+        if (!(RECON == 1 || D.limiter)) return;
+        for (int p = (int)threadIdx.x - t0; p < P; p += n) {
+            double u[NV];
+#pragma unroll
+            for (int j = 0; j < NV; j++) u[j] = S.su[r & 7][j][p];
+            cell_eigen<EQ>(D.eq, u, S.se[p]);
+        }
+    }
+}
+
 // ---- phase 1: y-direction sweep of row r (src/WENOFV.cpp:670-687, :796-833) ------------
+// FP64: the reference's arithmetic on the averages.  FP32 bulk: the same reconstruction on
+// the deviations from the column's centre average (WENO is translation invariant), so that
+// FP32 rounds the small differences, not the large averages; the result is re-anchored in
+// FP64.
 template <int EQ, int RECON, class R>
 __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D, int r)
 {
     constexpr int NV = StageGeom<EQ>::NV;
+    constexpr bool DEV = sizeof(R) < sizeof(double); // deviation form
     const int t = threadIdx.x;
     const int p = t / NV, v = t - p * NV;
     if (RECON == 0 || NV == 1) {
+        const double c0 = DEV ? S.su[r & 7][v][p] : 0.0;
         Weno5<R> W;
-        W.init(D.scheme, (R)S.su[(r - 2) & 7][v][p], (R)S.su[(r - 1) & 7][v][p], (R)S.su[r & 7][v][p],
-               (R)S.su[(r + 1) & 7][v][p], (R)S.su[(r + 2) & 7][v][p]);
-        S.sy[p][0][v] = (double)W.template eval<0>();
-        S.sy[p][1][v] = (double)W.template eval<1>();
-        S.sy[p][2][v] = (double)W.template eval<2>();
-        S.sy[p][3][v] = (double)W.template eval<3>();
+        W.init(D.scheme, (R)(S.su[(r - 2) & 7][v][p] - c0), (R)(S.su[(r - 1) & 7][v][p] - c0), (R)(S.su[r & 7][v][p] - c0),
+               (R)(S.su[(r + 1) & 7][v][p] - c0), (R)(S.su[(r + 2) & 7][v][p] - c0));
+        S.sy[p][0][v] = anchor<DEV>(c0, W.template eval<0>());
+        S.sy[p][1][v] = anchor<DEV>(c0, W.template eval<1>());
+        S.sy[p][2][v] = anchor<DEV>(c0, W.template eval<2>());
+        S.sy[p][3][v] = anchor<DEV>(c0, W.template eval<3>());
     } else {
-        // characteristic: project with L(U_centre, y), reconstruct, project back with R(U_centre, y)
-        R Uc[NV], Lrow[NV], Rrow[NV], pr[5];
+        // characteristic: project with L(U_centre, y), reconstruct, project back with R(U_centre, y).
+        // The eigenvectors and both projections are FP64 in every form: the two-phase
+        // eigenvector matrices reach condition numbers of ~5e3 near pure phases, so FP32
+        // rows or FP32 mat-vecs would mix the large partial density into the small momenta.
+        double Uc[NV], Lrow[NV], Rrow[NV];
+        R pr[5];
 #pragma unroll
-        for (int j = 0; j < NV; j++) Uc[j] = (R)S.su[r & 7][j][p];
-        eigen_rows<EQ, R>(D.eq, Uc, false, v, Lrow, Rrow);
+        for (int j = 0; j < NV; j++) Uc[j] = S.su[r & 7][j][p];
+        eigen_rows_of<EQ>(D.eq, S.se[p], false, v, Lrow, Rrow);
 #pragma unroll
         for (int m = 0; m < 5; m++) {
-            R s = R(0.0);
+            double s = 0.0;
 #pragma unroll
-            for (int j = 0; j < NV; j++) s += Lrow[j] * (R)S.su[(r - 2 + m) & 7][j][p];
-            pr[m] = s;
+            for (int j = 0; j < NV; j++) s += Lrow[j] * (S.su[(r - 2 + m) & 7][j][p] - (DEV ? Uc[j] : 0.0));
+            pr[m] = (R)s;
         }
         Weno5<R> W;
         W.init(D.scheme, pr[0], pr[1], pr[2], pr[3], pr[4]);
@@ -188,55 +226,57 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
         const int lane = t & 31, gbase = lane & ~(NV - 1);
 #pragma unroll
         for (int gp = 0; gp < 4; gp++) {
-            R s = R(0.0);
+            double s = 0.0;
 #pragma unroll
-            for (int k = 0; k < NV; k++) s += Rrow[k] * __shfl_sync(0xffffffffu, cg[gp], gbase + k);
-            S.sy[p][gp][v] = (double)s;
+            for (int k = 0; k < NV; k++) s += Rrow[k] * (double)__shfl_sync(0xffffffffu, cg[gp], gbase + k);
+            S.sy[p][gp][v] = anchor<DEV>(Uc[v], s);
         }
     }
 }
 
 // ---- phase 2: x-direction sweep + limiter of row r (src/WENOFV.cpp:690-721, :836-880,
-//      limiter :1895-2000) -> face states -----------------------------------------------
+//      limiter :1895-2000) -> face states (FP64 in every form) ------------------------------
 template <int EQ, int RECON, class R>
 __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D, InstState *st, int r, int i0, int TXe)
 {
     constexpr int NV = StageGeom<EQ>::NV, TX = StageGeom<EQ>::TX;
+    constexpr bool DEV = sizeof(R) < sizeof(double);
     const int t = threadIdx.x;
     const int cu = t / NV, v = t - cu * NV;
     const bool active = cu < TX + 2;
     const int c = (active ? cu : TX + 1) - 1; // cell in [-1, TX]
     const int lane = t & 31, gbase = lane & ~(NV - 1);
-    R ug[4][4]; // [gpi][gpj] of variable v (boundary points only)
+    double fv[4][4]; // face values [gpi][gpj] of variable v (boundary points only)
 
     if (RECON == 0 || NV == 1) {
+        const double cc = DEV ? S.su[r & 7][v][c + G] : 0.0;
 #pragma unroll
         for (int gpj = 0; gpj < 4; gpj++) {
             Weno5<R> W;
-            W.init(D.scheme, (R)S.sy[c + 1][gpj][v], (R)S.sy[c + 2][gpj][v], (R)S.sy[c + 3][gpj][v],
-                   (R)S.sy[c + 4][gpj][v], (R)S.sy[c + 5][gpj][v]);
-            ug[0][gpj] = W.template eval<0>();
-            ug[3][gpj] = W.template eval<3>();
+            W.init(D.scheme, (R)(S.sy[c + 1][gpj][v] - cc), (R)(S.sy[c + 2][gpj][v] - cc), (R)(S.sy[c + 3][gpj][v] - cc),
+                   (R)(S.sy[c + 4][gpj][v] - cc), (R)(S.sy[c + 5][gpj][v] - cc));
+            fv[0][gpj] = anchor<DEV>(cc, W.template eval<0>());
+            fv[3][gpj] = anchor<DEV>(cc, W.template eval<3>());
             if (gpj == 0 || gpj == 3) {
-                ug[1][gpj] = W.template eval<1>();
-                ug[2][gpj] = W.template eval<2>();
+                fv[1][gpj] = anchor<DEV>(cc, W.template eval<1>());
+                fv[2][gpj] = anchor<DEV>(cc, W.template eval<2>());
             }
         }
     } else {
-        R Uc[NV], Lrow[NV], Rrow[NV];
+        double Uc[NV], Lrow[NV], Rrow[NV]; // FP64 in every form, as in the y-sweep
 #pragma unroll
-        for (int j = 0; j < NV; j++) Uc[j] = (R)S.su[r & 7][j][c + G];
-        eigen_rows<EQ, R>(D.eq, Uc, true, v, Lrow, Rrow);
+        for (int j = 0; j < NV; j++) Uc[j] = S.su[r & 7][j][c + G];
+        eigen_rows_of<EQ>(D.eq, S.se[c + G], true, v, Lrow, Rrow);
         R cg[4][4];
 #pragma unroll
         for (int gpj = 0; gpj < 4; gpj++) {
             R pr[5];
 #pragma unroll
             for (int m = 0; m < 5; m++) {
-                R s = R(0.0);
+                double s = 0.0;
 #pragma unroll
-                for (int j = 0; j < NV; j++) s += Lrow[j] * (R)S.sy[c + 1 + m][gpj][j];
-                pr[m] = s;
+                for (int j = 0; j < NV; j++) s += Lrow[j] * (S.sy[c + 1 + m][gpj][j] - (DEV ? Uc[j] : 0.0));
+                pr[m] = (R)s;
             }
             Weno5<R> W;
             W.init(D.scheme, pr[0], pr[1], pr[2], pr[3], pr[4]);
@@ -252,10 +292,10 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
 #pragma unroll
             for (int gpi = 0; gpi < 4; gpi++) {
                 if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
-                R s = R(0.0);
+                double s = 0.0;
 #pragma unroll
-                for (int k = 0; k < NV; k++) s += Rrow[k] * __shfl_sync(0xffffffffu, cg[gpi][gpj], gbase + k);
-                ug[gpi][gpj] = s;
+                for (int k = 0; k < NV; k++) s += Rrow[k] * (double)__shfl_sync(0xffffffffu, cg[gpi][gpj], gbase + k);
+                fv[gpi][gpj] = anchor<DEV>(Uc[v], s);
             }
     }
 
@@ -266,7 +306,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
 #pragma unroll
         for (int j = 0; j < NV; j++) ub[j] = S.su[r & 7][j][c + G];
         double a1, a2;
-        max_eigs<EQ, double>(D.eq, ub, a1, a2);
+        max_eigs_of<EQ>(S.se[c + G], a1, a2);
         const double mu1 = (a1 / D.dX) / (a1 / D.dX + a2 / D.dY);
         const double mu2 = (a2 / D.dY) / (a1 / D.dX + a2 / D.dY);
         double th = 1.0;
@@ -278,19 +318,19 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
 #pragma unroll
             for (int gp = 0; gp < 4; gp++) {
                 const double w = gl_weight(gp);
-                rem -= omega1 * w / 2 * mu2 * (double)ug[gp][0];
-                rem -= omega1 * w / 2 * mu2 * (double)ug[gp][3];
-                rem -= omega1 * w / 2 * mu1 * (double)ug[0][gp];
-                rem -= omega1 * w / 2 * mu1 * (double)ug[3][gp];
+                rem -= omega1 * w / 2 * mu2 * fv[gp][0];
+                rem -= omega1 * w / 2 * mu2 * fv[gp][3];
+                rem -= omega1 * w / 2 * mu1 * fv[0][gp];
+                rem -= omega1 * w / 2 * mu1 * fv[3][gp];
             }
             rem /= omegaR;
             double mloc = rem;
 #pragma unroll
             for (int gp = 0; gp < 4; gp++) {
-                mloc = sc_min(mloc, (double)ug[gp][0]);
-                mloc = sc_min(mloc, (double)ug[gp][3]);
-                mloc = sc_min(mloc, (double)ug[0][gp]);
-                mloc = sc_min(mloc, (double)ug[3][gp]);
+                mloc = sc_min(mloc, fv[gp][0]);
+                mloc = sc_min(mloc, fv[gp][3]);
+                mloc = sc_min(mloc, fv[0][gp]);
+                mloc = sc_min(mloc, fv[3][gp]);
             }
             th = sc_min(fabs((uave - eps) / (uave - mloc)), th);
         }
@@ -304,7 +344,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
 #pragma unroll
                 for (int gpi = 0; gpi < 4; gpi++) {
                     if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
-                    ug[gpi][gpj] = (R)(theta * ((double)ug[gpi][gpj] - u0) + u0);
+                    fv[gpi][gpj] = theta * (fv[gpi][gpj] - u0) + u0;
                 }
         } else if (active && v == 0 && c >= 0 && c < TXe) {
             flag_error(st, 2u, (long long)map_index(r, D.ny, D.bc) * D.nx + i0 + c);
@@ -314,11 +354,11 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
     if (active) {
 #pragma unroll
         for (int gp = 0; gp < 4; gp++) {
-            if (c >= 0) S.sxf[c][1][gp][v] = (double)ug[0][gp];     // left face: plus side of face c
-            if (c < TX) S.sxf[c + 1][0][gp][v] = (double)ug[3][gp]; // right face: minus side of face c+1
+            if (c >= 0) S.sxf[c][1][gp][v] = fv[0][gp];     // left face: plus side of face c
+            if (c < TX) S.sxf[c + 1][0][gp][v] = fv[3][gp]; // right face: minus side of face c+1
             if (c >= 0 && c < TX) {
-                S.syb[c][gp][v] = (double)ug[gp][0];
-                S.syt[r & 1][c][gp][v] = (double)ug[gp][3];
+                S.syb[c][gp][v] = fv[gp][0];
+                S.syt[r & 1][c][gp][v] = fv[gp][3];
             }
         }
     }
@@ -339,19 +379,20 @@ __device__ __forceinline__ void phase_riemann(StageSmem<EQ> &S, const InstDesc &
     const int lane = threadIdx.x & 31, g4 = lane & ~3;
     const double dyr = (r >= j0 && r < j1) ? D.dy[r] : 1.0;
     for (int base = 0; base < total; base += NT) {
+        if (base + (int)(threadIdx.x & ~31u) >= total) break; // the whole warp is idle: leave (warp-uniform)
         const int u = base + threadIdx.x;
         const bool act = u < total;
         const int uu = act ? u : total - 1;
         const bool xf = uu < nxf;
         const int f = xf ? (uu >> 2) : ((uu - nxf) >> 2);
         const int gp = uu & 3;
-        R UL[NV], UR[NV], F[NV];
+        double UL[NV], UR[NV], F[NV];
         if (xf) {
 #pragma unroll
-            for (int v = 0; v < NV; v++) { UL[v] = (R)S.sxf[f][0][gp][v]; UR[v] = (R)S.sxf[f][1][gp][v]; }
+            for (int v = 0; v < NV; v++) { UL[v] = S.sxf[f][0][gp][v]; UR[v] = S.sxf[f][1][gp][v]; }
         } else {
 #pragma unroll
-            for (int v = 0; v < NV; v++) { UL[v] = (R)S.syt[(r - 1) & 1][f][gp][v]; UR[v] = (R)S.syb[f][gp][v]; }
+            for (int v = 0; v < NV; v++) { UL[v] = S.syt[(r - 1) & 1][f][gp][v]; UR[v] = S.syb[f][gp][v]; }
         }
         riemann<EQ, R>(D.eq, D.flux, UL, UR, F, xf);
         // gWeight = m_gweights_ref[gp] * (cell size) / 2.0 (src/WENOFV.cpp:1774, :1793)
@@ -359,7 +400,7 @@ __device__ __forceinline__ void phase_riemann(StageSmem<EQ> &S, const InstDesc &
         bool bad = false;
 #pragma unroll
         for (int v = 0; v < NV; v++) {
-            const double pv = (double)F[v] * wq;
+            const double pv = F[v] * wq;
             bad |= isnan(pv);
             const double p1 = __shfl_sync(0xffffffffu, pv, g4 + 1);
             const double p2 = __shfl_sync(0xffffffffu, pv, g4 + 2);
@@ -430,8 +471,15 @@ __device__ __forceinline__ double phase_update(StageSmem<EQ> &S, const InstDesc 
     return cmin;
 }
 
+// resident CTAs per SM the register allocation is bounded for: 4 for the FP32-bulk form
+// (no spills at 128 registers); the FP64 forms at 3 keep all values in registers
+#ifndef WENOFV_FP64_MIN_BLOCKS
+#define WENOFV_FP64_MIN_BLOCKS 3
+#endif
+template <class R> struct StageMinBlocks { static constexpr int value = sizeof(R) < sizeof(double) ? 4 : WENOFV_FP64_MIN_BLOCKS; };
+
 template <int EQ, int RECON, class R>
-__global__ void __launch_bounds__(NT) stage_kernel(const StageLaunch L)
+__global__ void __launch_bounds__(NT, StageMinBlocks<R>::value) stage_kernel(const StageLaunch L)
 {
     constexpr int TX = StageGeom<EQ>::TX;
     __shared__ StageSmem<EQ> S;
@@ -460,11 +508,18 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageLaunch L)
             if (r + 3 <= it.j1 + 2) load_row<EQ>(S.su[(r + 3) & 7], bin, D, r + 3, it.i0);
             if (!L.first_stage && r >= it.j0 && r < it.j1) load_row<EQ>(S.sun[r & 1], bun, D, r, it.i0);
             cp_async_commit();
+            if (r == it.j0 - 1) { // eigensystems of the first row; later rows come from phase 3
+                phase_eigen<EQ, RECON>(S, D, r, 0, NT);
+                __syncthreads();
+            }
             phase_ysweep<EQ, RECON, R>(S, D, r);
             __syncthreads();
             phase_xsweep<EQ, RECON, R>(S, D, st, r, it.i0, TXe);
             __syncthreads();
             phase_riemann<EQ, R>(S, D, st, r, it.i0, it.j0, it.j1, TXe);
+            // the last warp, idle in the second round of Riemann units, prepares the next
+            // row's eigensystems (row r+1 is resident; se is not read until the next row)
+            if (threadIdx.x >= NT - 32) phase_eigen<EQ, RECON>(S, D, r + 1, NT - 32, 32);
             __syncthreads();
             if (r - 1 >= it.j0) cmin = phase_update<EQ>(S, D, st, L, r - 1, it.i0, TXe, dt, cmin);
         }
