@@ -191,9 +191,30 @@ struct TwoPhaseK {
         return (z1 < z2) ? pre2 : pre1;
     }
     // getSoundSpeed (Wood), include/Equations.hpp:126-146
+    // getVolumeFrac + getPressure in one pass, contracted build: the same quadratic root with
+    // z1 = r/(1+r) = N/(N+D) and the pressures rewritten with 1/z2 = 1+r, 1/z1 = 1+1/r
+    // (r = N/D), i.e. one sqrt and two divisions instead of one sqrt and four
+    __device__ __forceinline__ void recover(double z1rho1, double z2rho2, double &z1, double &p) const
+    {
+        const double qs = z2rho2 * c2_2 - z1rho1 * c1_2;
+        const double N = (q - qs) + sqrt((q - qs) * (q - qs) + 4.0 * z1rho1 * c1_2 * z2rho2 * c2_2);
+        const double Dn = 2.0 * z2rho2 * c2_2;
+        z1 = N / (N + Dn);
+        const double z2 = 1.0 - z1;
+        const double pre2 = c2_2 * (z2rho2 - rho20) + 0.5 * N; // c2^2 (z2rho2 / z2 - rho20)
+        const double pre1 = c1_2 * (z1rho1 + z1rho1 * Dn / N - rho10); // c1^2 (z1rho1 / z1 - rho10)
+        p = (z1 < z2) ? pre2 : pre1;
+    }
     // z2 comes in as 1 - z1 rounded from FP64: in FP32, 1 - (float)z1 loses z2 near pure phase 1
     template <class R> __device__ __forceinline__ R sound(R z1rho1, R z2rho2, R z1, R z2) const
     {
+#if !WENOFV_STRICT
+        if constexpr (sizeof(R) == sizeof(double)) {
+            // 1/c^2 = rho (z1^2/(z1rho1 c1^2) + z2^2/(z2rho2 c2^2)): one division, one sqrt
+            const double a1 = z1rho1 * c1_2, a2 = z2rho2 * c2_2;
+            return sqrt(a1 * a2 / ((z1rho1 + z2rho2) * (z1 * z1 * a2 + z2 * z2 * a1)));
+        }
+#endif
         const R rho = z1rho1 + z2rho2;
         const R rho1 = z1rho1 / z1;
         const R rho2 = z2rho2 / z2;
@@ -224,8 +245,13 @@ __device__ __forceinline__ void tp_state(const TwoPhaseK &K, const double *U, TP
     s.u = s.rhou * ir;
     s.v = s.rhov * ir;
 #endif
+#if WENOFV_STRICT
     const double z1 = K.volume_frac(U[0], U[1]);
     s.pd = K.pressure(U[0], U[1], z1);
+#else
+    double z1;
+    K.recover(U[0], U[1], z1, s.pd);
+#endif
     s.pre = (R)s.pd;
     s.c = K.sound<R>(s.z1rho1, s.z2rho2, (R)z1, (R)(1.0 - z1));
 }
@@ -403,7 +429,12 @@ template <class R> __device__ __forceinline__ void tp_eigen_prep(const TwoPhaseK
     e.u = (R)U[2] * e.irho;
     e.v = (R)U[3] * e.irho;
 #endif
+#if WENOFV_STRICT
     const double z1d = K.volume_frac(U[0], U[1]);
+#else
+    double z1d, pdummy;
+    K.recover(U[0], U[1], z1d, pdummy);
+#endif
     const R z1 = (R)z1d;
     const R z2 = (R)(1.0 - z1d);
     e.c = K.sound<R>(e.z1rho1, e.z2rho2, z1, z2);

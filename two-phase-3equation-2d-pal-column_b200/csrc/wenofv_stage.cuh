@@ -132,6 +132,7 @@ template <int EQ> struct StageSmem {
     double sfy[2][TX][NV];        // y-face quadrature sums below the current and previous row
     static constexpr int PE = NV > 1 ? P : 1;
     typename CellEigen<EQ>::type se[PE]; // per-cell eigensystem data of one row, by position
+    double smu[PE][2];                   // the limiter's wave-speed weights mu1, mu2 by position
     double sdxc[TX], sdxl[TX];    // column widths of the strip
     double sred[NT / 32];
     int s_last;
@@ -174,6 +175,12 @@ __device__ __forceinline__ void phase_eigen(StageSmem<EQ> &S, const InstDesc &D,
 #pragma unroll
             for (int j = 0; j < NV; j++) u[j] = S.su[r & 7][j][p];
             cell_eigen<EQ>(D.eq, u, S.se[p]);
+            if (D.limiter) { // src/WENOFV.cpp:1954-1957
+                double a1, a2;
+                max_eigs_of<EQ>(S.se[p], a1, a2);
+                S.smu[p][0] = (a1 / D.dX) / (a1 / D.dX + a2 / D.dY);
+                S.smu[p][1] = (a2 / D.dY) / (a1 / D.dX + a2 / D.dY);
+            }
         }
     }
 }
@@ -305,10 +312,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
         double ub[NV];
 #pragma unroll
         for (int j = 0; j < NV; j++) ub[j] = S.su[r & 7][j][c + G];
-        double a1, a2;
-        max_eigs_of<EQ>(S.se[c + G], a1, a2);
-        const double mu1 = (a1 / D.dX) / (a1 / D.dX + a2 / D.dY);
-        const double mu2 = (a2 / D.dY) / (a1 / D.dX + a2 / D.dY);
+        const double mu1 = S.smu[c + G][0], mu2 = S.smu[c + G][1];
         double th = 1.0;
         if (v < NLIM) {
             const double uave = ub[v];
