@@ -280,15 +280,23 @@ def run_ours(args, rank, world, dist):
     value = world * ncells * nstages * args.steps / (total_ms * 1e-3)
     flags, _ = s.status()
 
-    # end to end through the public API with host arrays
-    U_host = s.download()
+    U_dev_end = s.download()
+    # FP32-bulk beside FP64: the same steps from the same state, device-timed the same way,
+    # and the error of its result against the FP64 one
+    fp32 = None
+    if form == wb.FP64 and args.workload != "advection128" and not args.no_fp32:
+        fp32 = compare_fp32(args, wb, cfg, eq, U0, dt, U_dev_end, ncells, nstages, flush, barrier, dist, world, local)
+
+    # end to end through the public API with host arrays (pinned host memory)
+    U_host = torch.empty(U_dev_end.shape, dtype=torch.float64, pin_memory=True).numpy()
+    U_host[...] = U_dev_end
     nbytes = U_host.nbytes
     barrier()
     t0 = time.perf_counter()
     for k in range(args.steps):
         s.upload(U_host)
         s.step(dt)
-        U_host = s.download()
+        s.download_into(U_host)
     e2e_s = time.perf_counter() - t0
     if dist is not None:
         t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
@@ -319,12 +327,57 @@ def run_ours(args, rank, world, dist):
                dtype={"fp64": "f64", "fp64_strict": "f64", "fp32_bulk": "f32+f64"}[args.form], data="synthetic",
                config=dict(desc, form=args.form, l2="flushed between steps by a 256 MiB write outside the timed "
                            "events", parallelism=f"replicas x{world}"),
-               roofline=roofline, e2e=e2e, gpu_launches=args.steps * nstages, status_flags=flags)
+               roofline=roofline, e2e=e2e, gpu_launches=args.steps * nstages * (2 if fp32 else 1), status_flags=flags)
+    if fp32:
+        fp32["roofline"] = dict(bound="fp64+fp32", achieved=fpcs * ncells / (fp32["launch_ms"] * 1e-3) / 1e12,
+                                unit="TFLOP/s", note="counted flops of the FP64 algorithm per launch / launch time; "
+                                "the FP32-bulk form mixes both pipes, so no single peak bounds it")
+        out["fp32_bulk"] = fp32
     out["clocks"] = clk.summary()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args.workload, steps=args.cpu_steps, warmup=1)
     s.close()
     return out
+
+
+def compare_fp32(args, wb, cfg, eq, U0, dt, U64, ncells, nstages, flush, barrier, dist, world, local):
+    import torch
+
+    cfg32 = wb.Config.from_buffer_copy(cfg)
+    cfg32.precision = wb.FP32_BULK
+    s = wb.Solver(cfg32, eq)
+    s.upload(U0)
+    for _ in range(args.warmup):
+        s.step(dt)
+    s.synchronize()
+    stream = torch.cuda.ExternalStream(s.stream())
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()
+            evs[k][0].record(stream)
+            s.step(dt)
+            evs[k][1].record(stream)
+    s.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    total_ms = float(np.sum([a.elapsed_time(b) for a, b in evs]))
+    if dist is not None:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    U32 = s.download()
+    flags, _ = s.status()
+    s.close()
+    per = [float(np.abs(U32[v] - U64[v]).sum() / max(np.abs(U64[v]).sum(), 1e-300)) for v in range(U64.shape[0])]
+    return dict(value=world * ncells * nstages * args.steps / (total_ms * 1e-3), unit="cell-stage updates/s",
+                ms_per_step=total_ms / args.steps, launch_ms=total_ms / (args.steps * nstages),
+                rel_l1_vs_fp64=float(np.abs(U32 - U64).sum() / np.abs(U64).sum()), rel_l1_vs_fp64_per_var=per,
+                error_note=f"relative L1 of the FP32-bulk state against the FP64 state after the same "
+                           f"{args.warmup + args.steps} steps from the same initial data and dt",
+                status_flags=flags)
 
 
 def run_reference_arm(args):
@@ -348,6 +401,7 @@ def main():
     ap.add_argument("--form", default="fp64", choices=["fp64", "fp64_strict", "fp32_bulk"])
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-bulk comparison of the FP64 form")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 

@@ -187,6 +187,13 @@ class Solver:
         _check(self.L.wenofv_download(self.h, _dp(out), layout), "wenofv_download")
         return out
 
+    def download_into(self, out: np.ndarray, layout=LAYOUT_SOA) -> np.ndarray:
+        """download into a caller's C-contiguous float64 array (e.g. pinned host memory)"""
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != int(np.prod(self.shape)):
+            raise ValueError("need a C-contiguous float64 array of the state's size")
+        _check(self.L.wenofv_download(self.h, _dp(out), layout), "wenofv_download")
+        return out
+
     def compute_dt(self) -> float:
         d = C.c_double()
         _check(self.L.wenofv_compute_dt(self.h, C.byref(d)), "wenofv_compute_dt")

@@ -465,6 +465,14 @@ int Engine::upload(int i, const double *U, int layout)
     const InstDesc &d = desc_[i];
     const int nv = nvar_of(d.eq_kind);
     const int b = slot_mode ? 0 : cur_;
+    if (layout == WENOFV_LAYOUT_SOA) {
+        // one strided copy straight from the caller's array (the pitch padding is never read);
+        // from pinned memory this is a single DMA without a host-side repack
+        WENOFV_CUDA(cudaMemcpy2DAsync(d.buf[b], (size_t)d.pitch * sizeof(double), U, (size_t)d.nx * sizeof(double),
+                                      (size_t)d.nx * sizeof(double), (size_t)nv * d.ny, cudaMemcpyHostToDevice, stream));
+        WENOFV_CUDA(cudaStreamSynchronize(stream));
+        return WENOFV_OK;
+    }
     WENOFV_CUDA(cudaStreamSynchronize(stream)); // the staging buffer may still feed a copy
     to_pitch(U, layout, nv, d.nx, d.ny, d.pitch, h_stage_);
     WENOFV_CUDA(cudaMemcpyAsync(d.buf[b], h_stage_, (size_t)nv * d.ny * d.pitch * sizeof(double), cudaMemcpyHostToDevice, stream));
@@ -480,6 +488,12 @@ int Engine::download(int i, double *U, int layout)
     const InstDesc &d = desc_[i];
     const int nv = nvar_of(d.eq_kind);
     const int b = slot_mode ? h_state_[i].cur_buf : cur_;
+    if (layout == WENOFV_LAYOUT_SOA) {
+        WENOFV_CUDA(cudaMemcpy2DAsync(U, (size_t)d.nx * sizeof(double), d.buf[b], (size_t)d.pitch * sizeof(double),
+                                      (size_t)d.nx * sizeof(double), (size_t)nv * d.ny, cudaMemcpyDeviceToHost, stream));
+        WENOFV_CUDA(cudaStreamSynchronize(stream));
+        return WENOFV_OK;
+    }
     WENOFV_CUDA(cudaMemcpyAsync(h_stage_, d.buf[b], (size_t)nv * d.ny * d.pitch * sizeof(double), cudaMemcpyDeviceToHost, stream));
     WENOFV_CUDA(cudaStreamSynchronize(stream));
     from_pitch(h_stage_, layout, nv, d.nx, d.ny, d.pitch, U);
