@@ -1,0 +1,99 @@
+"""The C++ host mirror of the reference's driver (CConfig / TwoPhaseEquation / CWENOFV on
+the CUDA backend, two-phase-3equation-2d-pal-column_b200/host).
+
+CPU: it builds, reads settings.cfg with the reference's key = value rules, rejects the
+cases the CUDA backend does not run, and its initial cell averages (initializeAve on the
+reference's slab grid) equal the reference's own bit for bit.
+GPU: `run()` of the mirror with PRECISION = FP64_STRICT reproduces the reference's final
+state of SMOOTH and SHARP bit for bit.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import PKG_DIR
+from oracle import Problem, reference_available, run_reference
+
+HOST = os.path.join(PKG_DIR, "host")
+BIN = os.path.join(HOST, "_build", "wenofv_host")
+CFG = os.path.join(HOST, "config", "settings.cfg")
+# TwoPhaseEquation parameters of the periodic test cases (rho10, rho20, sound1, sound2)
+CASE_PARAMS = {0: (1.2, 1.0, 1.0, 1.0), 1: (1000.0, 1.0, 30.0, 30.0), 2: (1000.0, 1.0, 70.0, 70.0)}
+
+
+@pytest.fixture(scope="module")
+def host_bin():
+    if not os.path.exists(os.path.join(PKG_DIR, "lib", "libwenofv_b200.so")):
+        pytest.skip("libwenofv_b200.so not built")
+    subprocess.run(["make", "-C", HOST], check=True, capture_output=True)
+    return BIN
+
+
+def run_host(host_bin, *kv, dump_ic=None, cwd=None, timeout=600):
+    args = [host_bin, CFG] + list(kv)
+    if dump_ic:
+        args += ["--dump-ic", dump_ic]
+    return subprocess.run(args, capture_output=True, text=True, timeout=timeout, cwd=cwd)
+
+
+def to_soa(raw, nx, ny):
+    return np.ascontiguousarray(raw.reshape(nx, ny, 4).transpose(2, 1, 0))
+
+
+def test_host_builds_and_rejects_unsupported(host_bin, tmp_path):
+    cp = run_host(host_bin, "TESTCASE=3", dump_ic=str(tmp_path / "x.bin"))
+    assert cp.returncode == 1 and "non-periodic" in cp.stderr
+    cp = run_host(host_bin, "BACKEND=CPU", dump_ic=str(tmp_path / "x.bin"))
+    assert cp.returncode == 1 and "CUDA backend only" in cp.stderr
+    cp = run_host(host_bin, "ELEMNUMX=30", dump_ic=str(tmp_path / "x.bin"))
+    assert cp.returncode == 1 and "REFSLABS" in cp.stderr
+    cp = subprocess.run([host_bin, str(tmp_path / "missing.cfg")], capture_output=True, text=True)
+    assert cp.returncode == 1 and "Failed to open" in cp.stderr
+
+
+def test_settings_reader_rules(host_bin, tmp_path):
+    # comments, blank lines, CR line ends and blanks around '=' as the reference accepts them
+    cfg = tmp_path / "s.cfg"
+    cfg.write_bytes(b"# c\n\nTESTCASE =  2 \r\nELEMNUMX=16\nELEMNUMY = 8\r\n\rjunk\nnot a key\n")
+    cp = subprocess.run([host_bin, str(cfg), "--dump-ic", str(tmp_path / "ic.bin")], capture_output=True, text=True)
+    assert cp.returncode == 0, cp.stderr
+    assert "Invalid line: not a key" in cp.stderr
+    U = to_soa(np.fromfile(tmp_path / "ic.bin"), 16, 8)
+    assert U[0].max() > 500 and np.isclose(U[0].min(), 1000 * 1e-8)  # SHARP: the square of phase 1 in phase 2
+
+
+@pytest.mark.skipif(not reference_available(), reason="the compiled reference is not built here")
+@pytest.mark.parametrize("testcase", [0, 1, 2])
+def test_initial_averages_equal_reference(host_bin, tmp_path, testcase):
+    nx, ny = 32, 24
+    path = str(tmp_path / "ic.bin")
+    cp = run_host(host_bin, f"TESTCASE={testcase}", f"ELEMNUMX={nx}", f"ELEMNUMY={ny}", dump_ic=path)
+    assert cp.returncode == 0, cp.stderr
+    mine = to_soa(np.fromfile(path), nx, ny)
+    r10, r20, c1, c2 = CASE_PARAMS[testcase]
+    p = Problem(nx=nx, ny=ny, rho10=r10, rho20=r20, sound1=c1, sound2=c2)
+    ref = run_reference(p, testcase=testcase, steps=1)
+    assert np.array_equal(mine, ref.U0)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not reference_available(), reason="the compiled reference binary is not present")
+@pytest.mark.parametrize("testcase,kv", [(0, ("RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=0", "PPlimiter=0")),
+                                         (2, ("RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=1", "PPlimiter=1"))])
+def test_host_run_equals_reference(host_bin, tmp_path, testcase, kv):
+    nx, ny, tend = 32, 32, 0.01
+    out = str(tmp_path / "u.bin")
+    cp = run_host(host_bin, f"TESTCASE={testcase}", f"ELEMNUMX={nx}", f"ELEMNUMY={ny}", "PRECISION=FP64_STRICT",
+                  "REFSLABS=4", f"ENDTIME={tend}", f"OUTPUT={out}", *kv)
+    assert cp.returncode == 0, cp.stderr
+    mine = to_soa(np.fromfile(out), nx, ny)
+    opts = dict(x.split("=") for x in kv)
+    r10, r20, c1, c2 = CASE_PARAMS[testcase]
+    p = Problem(nx=nx, ny=ny, rho10=r10, rho20=r20, sound1=c1, sound2=c2, recon=int(opts["RECONSTRUCTIONTYPE"]),
+                flux=int(opts["RIEMANNFLUX"]), limiter=int(opts["PPlimiter"]), scheme=1, rk=2, cfl=0.5)
+    ref = run_reference(p, testcase=testcase, t_end=tend)
+    assert np.array_equal(mine, ref.U)
