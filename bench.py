@@ -380,6 +380,180 @@ def compare_fp32(args, wb, cfg, eq, U0, dt, U64, ncells, nstages, flush, barrier
                 status_flags=flags)
 
 
+def _load_package():
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("wenofv_b200", os.path.join(ROOT, "two-phase-3equation-2d-pal-column_b200", "__init__.py"))
+    wb = importlib.util.module_from_spec(spec)
+    sys.modules["wenofv_b200"] = wb
+    spec.loader.exec_module(wb)
+    return wb
+
+
+def _pctl(x, q):
+    return float(np.percentile(np.asarray(x, dtype=np.float64), q)) if len(x) else None
+
+
+# ---- config 4: batched ensemble ------------------------------------------------------------------
+def run_batch(args, rank, world, dist):
+    """256 uneven two-phase instances, one persistent launch per RK stage for all of them,
+    captured step pairs, autotuned tiling; FP64 and FP32-bulk on the same inputs."""
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    wb = _load_package()
+    ens = cases.ensemble(args.instances, seed=4)
+    cells = sum(prm["nx"] * prm["ny"] for _, prm in ens)
+    steps = args.steps
+    res, finals = {}, {}
+    for name, form in (("fp64", wb.FP64), ("fp32_bulk", wb.FP32_BULK)):
+        cfgs, eqs = [], []
+        for U0, prm in ens:
+            c = wb.make_config(prm["nx"], prm["ny"], rk=2, cfl=0.5, scheme=prm["scheme"], flux=1, recon=1, limiter=1,
+                               precision=form)
+            c.device = local
+            cfgs.append(c)
+            eqs.append(wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"]))
+        b = wb.Batch(cfgs, eqs)
+        for k, (U0, _) in enumerate(ens):
+            b.upload(k, U0)
+        rows, ctas, tune_ms = b.autotune()
+        b.advance(1e9, max_steps=args.warmup)
+        for k, (U0, _) in enumerate(ens):
+            b.upload(k, U0)
+        stream = torch.cuda.ExternalStream(b.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        ns = b.advance(1e9, max_steps=steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        assert int(ns.min()) == int(ns.max()) == steps
+        finals[name] = [b.download(k) for k in range(len(ens))]
+        res[name] = dict(value=world * cells * 3 * steps / (ms * 1e-3), unit="cell-stage updates/s",
+                         solves_per_s=world * len(ens) / (ms * 1e-3), seconds=ms * 1e-3,
+                         tiling=dict(rows_per_item=rows, ctas_per_sm=ctas, autotune_best_stage_ms=tune_ms))
+        b.close()
+    errs = [float(np.abs(a - b_).sum() / np.abs(b_).sum()) for a, b_ in zip(finals["fp32_bulk"], finals["fp64"])]
+    res["fp32_bulk"]["rel_l1_vs_fp64"] = dict(median=_pctl(errs, 50), p90=_pctl(errs, 90), max=max(errs),
+                                             note="pooled relative L1 of each instance's final state")
+    out = dict(metric="cell-stage updates/s", value=res["fp64"]["value"], unit="cell-stage updates/s", n_gpus=world,
+               steps=steps, warmup=args.warmup, ms_per_step=res["fp64"]["seconds"] * 1e3 / steps,
+               higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+               config=dict(workload=f"batched_ensemble_{len(ens)}", instances=len(ens), cells=cells,
+                           grids="U{64,96,128,192,256}^2 and {256x64, 512x128} (seed 4)",
+                           ic="liquid columns, radius U[0.1,0.3], density ratio U[10,1000], eps in {1e-8,1e-6}",
+                           scheme="WENO-JS/WENO-Z mixed", flux="HLLC", reconstruction="characteristic",
+                           limiter=True, rk="SSP-RK3", steps_per_solve=steps,
+                           l2=f"working set {cells * 32 * 3 / 1e6:.0f} MB > L2", parallelism=f"replicas x{world}"),
+               solves_per_s=res["fp64"]["solves_per_s"], fp64=res["fp64"], fp32_bulk=res["fp32_bulk"],
+               gpu_launches=2 * 3 * steps)
+    return out
+
+
+# ---- config 5: serving stream --------------------------------------------------------------------
+def run_serve(args, rank, world, dist):
+    """Poisson arrivals of mixed Euler / two-phase solves into the continuous-batching
+    server; latency from submission to completion on the server clock."""
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    wb = _load_package()
+    rng = np.random.default_rng(5 + rank)
+    n = args.requests
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
+    reqs = []
+    for k in range(n):
+        nx = int(round(2 ** rng.uniform(6, 11) / 8)) * 8
+        ny = int(round(2 ** rng.uniform(6, 9) / 8)) * 8
+        steps = int(rng.integers(args.min_steps, args.max_steps + 1))
+        if rng.uniform() < 0.5:
+            U0, _ = cases.euler_quadrants(nx, ny, seed=100 + k)
+            mk = lambda f, nx=nx, ny=ny: wb.make_config(nx, ny, bc=wb.BC_OUTFLOW, rk=2, cfl=0.4, scheme=1, flux=1,
+                                                         recon=0, precision=f)
+            eq = wb.make_eq(kind=wb.EQ_EULER, gamma=1.4)
+            kind = "euler"
+        else:
+            U0, prm = cases.point_column(nx, ny, seed=100 + k)
+            mk = lambda f, nx=nx, ny=ny: wb.make_config(nx, ny, rk=2, cfl=0.5, scheme=1, flux=1, recon=1, limiter=1,
+                                                         precision=f)
+            eq = wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"])
+            kind = "two_phase"
+        reqs.append((mk, eq, U0, steps, nx * ny, kind))
+    res, finals = {}, {}
+    for name, form in (("fp64", wb.FP64), ("fp32_bulk", wb.FP32_BULK)):
+        srv = wb.Server(local, hbm_budget_bytes=args.hbm_budget_gb << 30, max_slots=256)
+        if dist is not None:
+            dist.barrier()
+        t0 = srv.clock()
+        ids, done, failed = [], {}, set()
+        k = 0
+        while len(done) < n:
+            now = srv.clock() - t0
+            while k < n and arrivals[k] <= now:
+                mk, eq, U0, steps, _, _ = reqs[k]
+                cfg = mk(form)
+                cfg.device = local
+                ids.append(srv.submit(cfg, eq, U0, 1e9, max_steps=steps))
+                k += 1
+            for j, rid in enumerate(ids):
+                if j in done:
+                    continue
+                try:
+                    got = srv.poll(rid)
+                except wb.WenofvError:  # a numerically failed solve is a result too
+                    got = (None, None)
+                    failed.add(j)
+                if got is not None:
+                    done[j] = got
+            time.sleep(0.0005)
+        ok = [j for j in range(n) if j not in failed]
+        lat = [done[j][1].t_done - done[j][1].t_submit for j in ok]
+        qwait = [done[j][1].t_admit - done[j][1].t_submit for j in ok]
+        span = max(done[j][1].t_done for j in ok) - min(done[j][1].t_submit for j in ok)
+        if dist is not None:
+            t = torch.tensor([span], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            span = float(t.item())
+        assert all(done[j][1].steps == reqs[j][3] for j in ok)
+        finals[name] = [done[j][0] for j in range(n)]
+        work_ok = sum(reqs[j][3] * reqs[j][4] * 3 for j in ok)
+        res[name] = dict(value=world * work_ok / span, unit="cell-stage updates/s", solves_per_s=world * len(ok) / span,
+                         failed_requests=sorted(failed),
+                         p50_latency_s=_pctl(lat, 50), p99_latency_s=_pctl(lat, 99), p50_queue_s=_pctl(qwait, 50),
+                         makespan_s=span)
+        srv.close()
+    errs = {"euler": [], "two_phase": []}
+    for j in range(n):
+        a, b_ = finals["fp32_bulk"][j], finals["fp64"][j]
+        if a is not None and b_ is not None:
+            errs[reqs[j][5]].append(float(np.abs(a - b_).sum() / np.abs(b_).sum()))
+    res["fp32_bulk"]["rel_l1_vs_fp64"] = {k: dict(median=_pctl(v, 50), max=max(v) if v else None, n=len(v))
+                                          for k, v in errs.items()}
+    out = dict(metric="cell-stage updates/s", value=res["fp64"]["value"], unit="cell-stage updates/s", n_gpus=world,
+               steps=n, warmup=0, ms_per_step=None, higher_is_better=True, scaling="weak", vs_baseline=None,
+               dtype="f64", data="synthetic",
+               config=dict(workload=f"serving_stream_{n}", requests=n, arrival=f"Poisson, mean {args.rate} req/s "
+                           f"(seed {5 + rank})", grids="nx log-uniform 64..2048, ny log-uniform 64..512 (multiples of 8)",
+                           steps=f"uniform {args.min_steps}..{args.max_steps} per request",
+                           mix="Euler quadrants (outflow, conservative WENO-Z/HLLC) and two-phase columns "
+                               "(periodic, characteristic WENO-Z/HLLC/limiter), 50/50",
+                           hbm_budget_gb=args.hbm_budget_gb, parallelism=f"replicas x{world}",
+                           latency="server clock, submission to completion"),
+               solves_per_s=res["fp64"]["solves_per_s"], p50_latency_s=res["fp64"]["p50_latency_s"],
+               p99_latency_s=res["fp64"]["p99_latency_s"], fp64=res["fp64"], fp32_bulk=res["fp32_bulk"])
+    return out
+
+
 def run_reference_arm(args):
     cb = cpu_baseline(args.workload, steps=max(1, args.steps), warmup=args.warmup)
     return dict(metric="cell-stage updates/s", value=cb["value"], unit="cell-stage updates/s", n_gpus=args.gpus,
@@ -397,7 +571,13 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="column1024", choices=sorted(FLOP_KEYS))
+    ap.add_argument("--workload", default="column1024", choices=sorted(FLOP_KEYS) + ["batch256", "serve"])
+    ap.add_argument("--instances", type=int, default=256, help="batch256: instances")
+    ap.add_argument("--requests", type=int, default=32, help="serve: requests")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: mean arrival rate, requests/s")
+    ap.add_argument("--min-steps", type=int, default=50, help="serve: fewest steps of a request")
+    ap.add_argument("--max-steps", type=int, default=2000, help="serve: most steps of a request")
+    ap.add_argument("--hbm-budget-gb", type=int, default=150, help="serve: HBM budget of the server")
     ap.add_argument("--form", default="fp64", choices=["fp64", "fp64_strict", "fp32_bulk"])
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -418,7 +598,12 @@ def main():
         import torch.distributed as tdist
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
-    out = run_ours(args, rank, world, dist)
+    if args.workload == "batch256":
+        out = run_batch(args, rank, world, dist)
+    elif args.workload == "serve":
+        out = run_serve(args, rank, world, dist)
+    else:
+        out = run_ours(args, rank, world, dist)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist is not None:
