@@ -89,10 +89,44 @@ template <class R> struct Weno5 {
     R g0, g1, g2;          // JS: (eps+beta_k)^2 [strict] or 1/(eps+beta_k)^2 [fast]; Z: 1 + tau/(beta_k+eps)
     int z;
 
+    // contracted FP64 build: one division for the three weights of a stencil and one for
+    // the normalisations of all Gauss points evaluated from it (products of the
+    // denominators, all bounded away from 0 and far below overflow), and WENO-Z without
+    // normalising the stencil: beta is quadratic and translation invariant, so beta(n) =
+    // beta(v) / s^2 with s = umax - umin + 1e-20, and tau/(beta(n) + eps) =
+    // tau(v)/(beta(v) + eps s^2)
+    static constexpr bool SHARED = !WENOFV_STRICT && sizeof(R) == sizeof(double);
+
     __device__ __forceinline__ void init(int scheme, R v0, R v1, R v2, R v3, R v4)
     {
         umm = v0; um = v1; u = v2; up = v3; upp = v4;
         z = scheme;
+        if constexpr (SHARED) {
+            R b0, b1, b2;
+            weno_betas(v0, v1, v2, v3, v4, b0, b1, b2);
+            R a0, a1, a2;
+            if (scheme == 1) {
+                const R umax = std_max(std_max(std_max(v0, v1), std_max(v4, v3)), v2);
+                const R umin = std_min(std_min(std_min(v0, v1), std_min(v4, v3)), v2);
+                const R sc = umax - umin + R(1e-20);
+                const R e2 = R(1.0e-10) * sc * sc;
+                a0 = b0 + e2; a1 = b1 + e2; a2 = b2 + e2;
+            } else {
+                a0 = (R(1.0e-6) + b0) * (R(1.0e-6) + b0);
+                a1 = (R(1.0e-6) + b1) * (R(1.0e-6) + b1);
+                a2 = (R(1.0e-6) + b2) * (R(1.0e-6) + b2);
+            }
+            const R a01 = a0 * a1;
+            const R inv = R(1) / (a01 * a2);
+            const R r0 = a1 * a2 * inv, r1 = a0 * a2 * inv, r2 = a01 * inv;
+            if (scheme == 1) {
+                const R tau = fabs(b0 - b2);
+                g0 = R(1) + tau * r0; g1 = R(1) + tau * r1; g2 = R(1) + tau * r2;
+            } else {
+                g0 = r0; g1 = r1; g2 = r2;
+            }
+            return;
+        }
         if (scheme == 1) {
             // WENO-Z: normalise the stencil to [0,1], include/Utility.hpp:261-268
             const R umax = std_max(std_max(std_max(v0, v1), std_max(v4, v3)), v2);
@@ -154,6 +188,46 @@ template <class R> struct Weno5 {
 #else
         return (w0 * h0 + w1 * h1 + w2 * h2) / sum;
 #endif
+    }
+
+    // numerator and denominator of the value at GP (the shared-division form)
+    template <int GP> __device__ __forceinline__ R num_den(R &den) const
+    {
+        R d0, d1, d2, h0, h1, h2;
+        weno_d<R, GP>(d0, d1, d2);
+        weno_h<R, GP>(umm, um, u, up, upp, h0, h1, h2);
+        const R w0 = d0 * g0, w1 = d1 * g1, w2 = d2 * g2;
+        den = w0 + w1 + w2;
+        return w0 * h0 + w1 * h1 + w2 * h2;
+    }
+    // the values at all four Gauss-Lobatto points
+    __device__ __forceinline__ void eval4(R *o) const
+    {
+        if constexpr (SHARED) {
+            R q0, q1, q2, q3;
+            const R n0 = num_den<0>(q0), n1 = num_den<1>(q1), n2 = num_den<2>(q2), n3 = num_den<3>(q3);
+            const R q01 = q0 * q1, q23 = q2 * q3;
+            const R inv = R(1) / (q01 * q23);
+            o[0] = n0 * (q1 * q23) * inv;
+            o[1] = n1 * (q0 * q23) * inv;
+            o[2] = n2 * (q01 * q3) * inv;
+            o[3] = n3 * (q01 * q2) * inv;
+        } else {
+            o[0] = eval<0>(); o[1] = eval<1>(); o[2] = eval<2>(); o[3] = eval<3>();
+        }
+    }
+    // the values at the two end points (the cell faces)
+    __device__ __forceinline__ void eval03(R &o0, R &o3) const
+    {
+        if constexpr (SHARED) {
+            R q0, q3;
+            const R n0 = num_den<0>(q0), n3 = num_den<3>(q3);
+            const R inv = R(1) / (q0 * q3);
+            o0 = n0 * q3 * inv;
+            o3 = n3 * q0 * inv;
+        } else {
+            o0 = eval<0>(); o3 = eval<3>();
+        }
     }
 };
 

@@ -134,6 +134,7 @@ template <int EQ> struct StageSmem {
     typename CellEigen<EQ>::type se[PE]; // per-cell eigensystem data of one row, by position
     double smu[PE][2];                   // the limiter's wave-speed weights mu1, mu2 by position
     double sdxc[TX], sdxl[TX];    // column widths of the strip
+    double sidxc[TX], sidxl[TX];  // their reciprocals (contracted build)
     double sred[NT / 32];
     int s_last;
 };
@@ -202,10 +203,10 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
         Weno5<R> W;
         W.init(D.scheme, (R)(S.su[(r - 2) & 7][v][p] - c0), (R)(S.su[(r - 1) & 7][v][p] - c0), (R)(S.su[r & 7][v][p] - c0),
                (R)(S.su[(r + 1) & 7][v][p] - c0), (R)(S.su[(r + 2) & 7][v][p] - c0));
-        S.sy[p][0][v] = anchor<DEV>(c0, W.template eval<0>());
-        S.sy[p][1][v] = anchor<DEV>(c0, W.template eval<1>());
-        S.sy[p][2][v] = anchor<DEV>(c0, W.template eval<2>());
-        S.sy[p][3][v] = anchor<DEV>(c0, W.template eval<3>());
+        R o[4];
+        W.eval4(o);
+#pragma unroll
+        for (int gp = 0; gp < 4; gp++) S.sy[p][gp][v] = anchor<DEV>(c0, o[gp]);
     } else {
         // characteristic: project with L(U_centre, y), reconstruct, project back with R(U_centre, y).
         // The eigenvectors and both projections are FP64 in every form: the two-phase
@@ -226,10 +227,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
         Weno5<R> W;
         W.init(D.scheme, pr[0], pr[1], pr[2], pr[3], pr[4]);
         R cg[4];
-        cg[0] = W.template eval<0>();
-        cg[1] = W.template eval<1>();
-        cg[2] = W.template eval<2>();
-        cg[3] = W.template eval<3>();
+        W.eval4(cg);
         const int lane = t & 31, gbase = lane & ~(NV - 1);
 #pragma unroll
         for (int gp = 0; gp < 4; gp++) {
@@ -262,11 +260,16 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
             Weno5<R> W;
             W.init(D.scheme, (R)(S.sy[c + 1][gpj][v] - cc), (R)(S.sy[c + 2][gpj][v] - cc), (R)(S.sy[c + 3][gpj][v] - cc),
                    (R)(S.sy[c + 4][gpj][v] - cc), (R)(S.sy[c + 5][gpj][v] - cc));
-            fv[0][gpj] = anchor<DEV>(cc, W.template eval<0>());
-            fv[3][gpj] = anchor<DEV>(cc, W.template eval<3>());
             if (gpj == 0 || gpj == 3) {
-                fv[1][gpj] = anchor<DEV>(cc, W.template eval<1>());
-                fv[2][gpj] = anchor<DEV>(cc, W.template eval<2>());
+                R o[4];
+                W.eval4(o);
+#pragma unroll
+                for (int gpi = 0; gpi < 4; gpi++) fv[gpi][gpj] = anchor<DEV>(cc, o[gpi]);
+            } else {
+                R o0, o3;
+                W.eval03(o0, o3);
+                fv[0][gpj] = anchor<DEV>(cc, o0);
+                fv[3][gpj] = anchor<DEV>(cc, o3);
             }
         }
     } else {
@@ -287,11 +290,13 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
             }
             Weno5<R> W;
             W.init(D.scheme, pr[0], pr[1], pr[2], pr[3], pr[4]);
-            cg[0][gpj] = W.template eval<0>();
-            cg[3][gpj] = W.template eval<3>();
             if (gpj == 0 || gpj == 3) {
-                cg[1][gpj] = W.template eval<1>();
-                cg[2][gpj] = W.template eval<2>();
+                R o[4];
+                W.eval4(o);
+#pragma unroll
+                for (int gpi = 0; gpi < 4; gpi++) cg[gpi][gpj] = o[gpi];
+            } else {
+                W.eval03(cg[0][gpj], cg[3][gpj]);
             }
         }
 #pragma unroll
@@ -444,7 +449,7 @@ __device__ __forceinline__ double phase_update(StageSmem<EQ> &S, const InstDesc 
     rhs += aB / dxc / dyq;
     rhs -= aT / dxc / dyq;
 #else
-    const double idy = 1.0 / dyq, idxc = 1.0 / dxc, idxl = 1.0 / dxl;
+    const double idy = 1.0 / dyq, idxc = S.sidxc[c], idxl = S.sidxl[c];
     rhs = ((aL * idxl - aR * idxc) + (aB - aT) * idxc) * idy;
 #endif
     const double U = S.su[q & 7][v][c + G];
@@ -498,6 +503,10 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<R>::value) stage_kernel(con
             const int i = min(it.i0 + c, D.nx - 1);
             S.sdxc[c] = D.dxc[i];
             S.sdxl[c] = D.dxl[i];
+#if !WENOFV_STRICT
+            S.sidxc[c] = 1.0 / D.dxc[i];
+            S.sidxl[c] = 1.0 / D.dxl[i];
+#endif
         }
         const double *bin = D.buf[L.bin];
         const double *bun = D.buf[L.bun];
