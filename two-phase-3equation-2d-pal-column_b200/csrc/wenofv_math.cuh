@@ -279,6 +279,22 @@ struct TwoPhaseK {
         const double pre1 = c1_2 * (z1rho1 + z1rho1 * Dn / N - rho10); // c1^2 (z1rho1 / z1 - rho10)
         p = (z1 < z2) ? pre2 : pre1;
     }
+    // recover plus 1/rho of the same state with one division for 1/rho and 1/(N+D)
+    __device__ __forceinline__ void recover_rho(double z1rho1, double z2rho2, double rho, double &irho, double &z1,
+                                                double &p) const
+    {
+        const double qs = z2rho2 * c2_2 - z1rho1 * c1_2;
+        const double N = (q - qs) + sqrt((q - qs) * (q - qs) + 4.0 * z1rho1 * c1_2 * z2rho2 * c2_2);
+        const double Dn = 2.0 * z2rho2 * c2_2;
+        const double ND = N + Dn;
+        const double inv = 1.0 / (rho * ND);
+        irho = ND * inv;
+        z1 = N * (rho * inv);
+        const double z2 = 1.0 - z1;
+        const double pre2 = c2_2 * (z2rho2 - rho20) + 0.5 * N;
+        const double pre1 = c1_2 * (z1rho1 + z1rho1 * Dn / N - rho10);
+        p = (z1 < z2) ? pre2 : pre1;
+    }
     // z2 comes in as 1 - z1 rounded from FP64: in FP32, 1 - (float)z1 loses z2 near pure phase 1
     template <class R> __device__ __forceinline__ R sound(R z1rho1, R z2rho2, R z1, R z2) const
     {
@@ -314,17 +330,21 @@ __device__ __forceinline__ void tp_state(const TwoPhaseK &K, const double *U, TP
 #if WENOFV_STRICT
     s.u = s.rhou / s.rho;
     s.v = s.rhov / s.rho;
-#else
-    const R ir = R(1) / s.rho;
-    s.u = s.rhou * ir;
-    s.v = s.rhov * ir;
-#endif
-#if WENOFV_STRICT
     const double z1 = K.volume_frac(U[0], U[1]);
     s.pd = K.pressure(U[0], U[1], z1);
 #else
     double z1;
-    K.recover(U[0], U[1], z1, s.pd);
+    if constexpr (sizeof(R) == sizeof(double)) {
+        double ir;
+        K.recover_rho(U[0], U[1], s.rho, ir, z1, s.pd);
+        s.u = s.rhou * ir;
+        s.v = s.rhov * ir;
+    } else {
+        const R ir = R(1) / s.rho;
+        s.u = s.rhou * ir;
+        s.v = s.rhov * ir;
+        K.recover(U[0], U[1], z1, s.pd);
+    }
 #endif
     s.pre = (R)s.pd;
     s.c = K.sound<R>(s.z1rho1, s.z2rho2, (R)z1, (R)(1.0 - z1));
@@ -395,6 +415,36 @@ __device__ __forceinline__ void tp_hllc(const TPState<R> &L, const TPState<R> &R
     const R c_roe = sqrt(c2_roe);
     const R S_L = std_min(vn_L - L.c, vn_roe - c_roe);
     const R S_R = std_max(vn_R + Rs.c, vn_roe + c_roe);
+#if !WENOFV_STRICT
+    if constexpr (sizeof(R) == sizeof(double)) {
+        // S* = num/den and the star factor k = (S_K - vn_K)/(S_K - S*) = (S_K - vn_K) den /
+        // (S_K den - num) from one division; the side is the sign of S* (num over den)
+        const R num = (S_L - vn_L) * L.rho * vn_L - (S_R - vn_R) * Rs.rho * vn_R + Rs.pre - L.pre;
+        const R den = (S_L - vn_L) * L.rho - (S_R - vn_R) * Rs.rho;
+        const bool left = (den < R(0)) ? (num <= R(0)) : (num >= R(0));
+        const bool super = left ? (S_L >= R(0.0)) : (S_R <= R(0));
+        const TPState<R> &K = left ? L : Rs;
+        const R *UK = left ? UL : UR;
+        const R *FK = left ? FUL : FUR;
+        if (super) {
+#pragma unroll
+            for (int r = 0; r < 4; r++) F[r] = FK[r];
+            return;
+        }
+        const R S_K = left ? S_L : S_R, vn_K = left ? vn_L : vn_R;
+        const R m = S_K * den - num;
+        const R inv = R(1) / (den * m);
+        const R S_star = num * m * inv;
+        const R k = (S_K - vn_K) * den * den * inv;
+        U[0] = K.z1rho1;
+        U[1] = K.z2rho2;
+        U[2] = K.rho * (K.u + (S_star - vn_K) * nx);
+        U[3] = K.rho * (K.v + (S_star - vn_K) * ny);
+#pragma unroll
+        for (int r = 0; r < 4; r++) F[r] = S_K * (k * U[r] - UK[r]) + FK[r];
+        return;
+    }
+#endif
     const R S_star = ((S_L - vn_L) * L.rho * vn_L - (S_R - vn_R) * Rs.rho * vn_R + Rs.pre - L.pre) /
                      ((S_L - vn_L) * L.rho - (S_R - vn_R) * Rs.rho);
     if (S_star >= R(0)) {
