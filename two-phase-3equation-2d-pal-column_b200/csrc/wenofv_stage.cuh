@@ -122,12 +122,20 @@ template <int EQ> struct StageGeom {
 // shared memory of one CTA (doubles)
 template <int EQ> struct StageSmem {
     static constexpr int NV = StageGeom<EQ>::NV, TX = StageGeom<EQ>::TX, P = StageGeom<EQ>::P;
-    double su[8][NV][P];          // ring of stage-input rows
-    double sun[2][NV][P];         // U^n rows (stages after the first)
-    double sy[P][4][NV];          // y-sweep of the current row: [position][y GL point][var]
-    double sxf[TX + 1][2][4][NV]; // x-face states: [face][minus/plus side][GL point][var]
-    double syb[TX][4][NV];        // bottom face states of the current row
-    double syt[2][TX][4][NV];     // top face states of the current and previous row
+    // Strides are padded so that the lanes of a half-warp (8-byte accesses are served 16
+    // lanes at a time) hit distinct bank pairs: rows of 4 variables at P+4 doubles
+    // (variable v of 4 neighbouring positions: banks 8v + 2p), positions and cells at an odd
+    // number of doubles (neighbouring positions 2 banks apart).
+    static constexpr int PS = NV > 1 ? P + 4 : P; // row stride of su / sun
+    static constexpr int YS = 4 * NV + 1;         // position stride of sy
+    static constexpr int FS = 8 * NV + 1;         // face stride of sxf
+    static constexpr int BS = 4 * NV + 1;         // cell stride of syb / syt
+    double su[8][NV][PS];   // ring of stage-input rows
+    double sun[2][NV][PS];  // U^n rows (stages after the first)
+    double sy[P][YS];       // y-sweep of the current row: [position][y GL point * NV + var]
+    double sxf[TX + 1][FS]; // x-face states: [face][(minus/plus side * 4 + GL point) * NV + var]
+    double syb[TX][BS];     // bottom face states of the current row: [cell][GL point * NV + var]
+    double syt[2][TX][BS];  // top face states of the current and previous row
     double sfx[2][TX + 1][NV];    // x-face quadrature sums of two rows
     double sfy[2][TX][NV];        // y-face quadrature sums below the current and previous row
     static constexpr int PE = NV > 1 ? P : 1;
@@ -141,7 +149,7 @@ template <int EQ> struct StageSmem {
 
 // one row of NV x P stage values into shared memory (ghost fill = index map), cp.async 8 B
 template <int EQ>
-__device__ __forceinline__ void load_row(double (*dst)[StageGeom<EQ>::P], const double *buf, const InstDesc &D, int row, int i0)
+__device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ>::PS], const double *buf, const InstDesc &D, int row, int i0)
 {
     constexpr int P = StageGeom<EQ>::P, NV = StageGeom<EQ>::NV;
     const int jj = map_index(row, D.ny, D.bc);
@@ -206,7 +214,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
         R o[4];
         W.eval4(o);
 #pragma unroll
-        for (int gp = 0; gp < 4; gp++) S.sy[p][gp][v] = anchor<DEV>(c0, o[gp]);
+        for (int gp = 0; gp < 4; gp++) S.sy[p][gp * NV + v] = anchor<DEV>(c0, o[gp]);
     } else {
         // characteristic: project with L(U_centre, y), reconstruct, project back with R(U_centre, y).
         // The eigenvectors and both projections are FP64 in every form: the two-phase
@@ -241,7 +249,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
             double s = 0.0;
 #pragma unroll
             for (int k = 0; k < NV; k++) s += Rrow[k] * (double)__shfl_sync(0xffffffffu, cg[gp], gbase + k);
-            S.sy[p][gp][v] = anchor<DEV>(Uc[v], s);
+            S.sy[p][gp * NV + v] = anchor<DEV>(Uc[v], s);
         }
     }
 }
@@ -265,8 +273,8 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
 #pragma unroll
         for (int gpj = 0; gpj < 4; gpj++) {
             Weno5<R> W;
-            W.init(D.scheme, (R)(S.sy[c + 1][gpj][v] - cc), (R)(S.sy[c + 2][gpj][v] - cc), (R)(S.sy[c + 3][gpj][v] - cc),
-                   (R)(S.sy[c + 4][gpj][v] - cc), (R)(S.sy[c + 5][gpj][v] - cc));
+            W.init(D.scheme, (R)(S.sy[c + 1][gpj * NV + v] - cc), (R)(S.sy[c + 2][gpj * NV + v] - cc), (R)(S.sy[c + 3][gpj * NV + v] - cc),
+                   (R)(S.sy[c + 4][gpj * NV + v] - cc), (R)(S.sy[c + 5][gpj * NV + v] - cc));
             if (gpj == 0 || gpj == 3) {
                 R o[4];
                 W.eval4(o);
@@ -297,7 +305,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
             for (int m = 0; m < 5; m++) {
                 double s = 0.0;
 #pragma unroll
-                for (int j = 0; j < NV; j++) s += Lrow[j] * S.sy[c + 1 + m][gpj][j];
+                for (int j = 0; j < NV; j++) s += Lrow[j] * S.sy[c + 1 + m][gpj * NV + j];
                 pr[m] = DEV ? (R)(s - lc) : (R)s;
             }
             Weno5<R> W;
@@ -375,11 +383,11 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
     if (active) {
 #pragma unroll
         for (int gp = 0; gp < 4; gp++) {
-            if (c >= 0) S.sxf[c][1][gp][v] = fv[0][gp];     // left face: plus side of face c
-            if (c < TX) S.sxf[c + 1][0][gp][v] = fv[3][gp]; // right face: minus side of face c+1
+            if (c >= 0) S.sxf[c][(4 + gp) * NV + v] = fv[0][gp];     // left face: plus side of face c
+            if (c < TX) S.sxf[c + 1][gp * NV + v] = fv[3][gp]; // right face: minus side of face c+1
             if (c >= 0 && c < TX) {
-                S.syb[c][gp][v] = fv[gp][0];
-                S.syt[r & 1][c][gp][v] = fv[gp][3];
+                S.syb[c][gp * NV + v] = fv[gp][0];
+                S.syt[r & 1][c][gp * NV + v] = fv[gp][3];
             }
         }
     }
@@ -410,10 +418,10 @@ __device__ __forceinline__ void phase_riemann(StageSmem<EQ> &S, const InstDesc &
         double UL[NV], UR[NV], F[NV];
         if (xf) {
 #pragma unroll
-            for (int v = 0; v < NV; v++) { UL[v] = S.sxf[f][0][gp][v]; UR[v] = S.sxf[f][1][gp][v]; }
+            for (int v = 0; v < NV; v++) { UL[v] = S.sxf[f][gp * NV + v]; UR[v] = S.sxf[f][(4 + gp) * NV + v]; }
         } else {
 #pragma unroll
-            for (int v = 0; v < NV; v++) { UL[v] = S.syt[(r - 1) & 1][f][gp][v]; UR[v] = S.syb[f][gp][v]; }
+            for (int v = 0; v < NV; v++) { UL[v] = S.syt[(r - 1) & 1][f][gp * NV + v]; UR[v] = S.syb[f][gp * NV + v]; }
         }
         riemann<EQ, R>(D.eq, D.flux, UL, UR, F, xf);
         // gWeight = m_gweights_ref[gp] * (cell size) / 2.0 (src/WENOFV.cpp:1774, :1793)
