@@ -153,6 +153,26 @@ def cpu_baseline(name: str, steps: int, warmup: int, sample_n: int = 256):
                 seconds=secs)
 
 
+# ---- ranks ------------------------------------------------------------------------------------------
+def max_over_ranks(x: float, dist, local: int = 0) -> float:
+    """the largest value over all ranks (times are taken on each rank's own device, and the
+    job's duration is the slowest rank's); the reduction runs on the rank's GPU under NCCL
+    and on the CPU under gloo"""
+    if dist is None:
+        return float(x)
+    import torch
+
+    dev = f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world: int, units_per_rank: float, seconds: float) -> float:
+    """whole-job throughput of independent replicas: all ranks' units over the slowest time"""
+    return world * units_per_rank / seconds
+
+
 # ---- clocks ------------------------------------------------------------------------------------
 class ClockSampler:
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
@@ -273,10 +293,7 @@ def run_ours(args, rank, world, dist):
     barrier()
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = float(np.sum(step_ms))
-    if dist is not None:
-        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, local)
     value = world * ncells * nstages * args.steps / (total_ms * 1e-3)
     flags, _ = s.status()
 
@@ -298,10 +315,7 @@ def run_ours(args, rank, world, dist):
         s.step(dt)
         s.download_into(U_host)
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist, local)
     e2e = dict(value=world * ncells * nstages * args.steps / e2e_s, unit="cell-stage updates/s",
                h2d_bytes_per_step=nbytes, d2h_bytes_per_step=nbytes)
 
@@ -364,10 +378,7 @@ def compare_fp32(args, wb, cfg, eq, U0, dt, U64, ncells, nstages, flush, barrier
     torch.cuda.synchronize()
     barrier()
     total_ms = float(np.sum([a.elapsed_time(b) for a, b in evs]))
-    if dist is not None:
-        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, local)
     U32 = s.download()
     flags, _ = s.status()
     s.close()
@@ -432,10 +443,7 @@ def run_batch(args, rank, world, dist):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dist, local)
         assert int(ns.min()) == int(ns.max()) == steps
         finals[name] = [b.download(k) for k in range(len(ens))]
         res[name] = dict(value=world * cells * 3 * steps / (ms * 1e-3), unit="cell-stage updates/s",
@@ -520,10 +528,7 @@ def run_serve(args, rank, world, dist):
         lat = [done[j][1].t_done - done[j][1].t_submit for j in ok]
         qwait = [done[j][1].t_admit - done[j][1].t_submit for j in ok]
         span = max(done[j][1].t_done for j in ok) - min(done[j][1].t_submit for j in ok)
-        if dist is not None:
-            t = torch.tensor([span], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            span = float(t.item())
+        span = max_over_ranks(span, dist, local)
         assert all(done[j][1].steps == reqs[j][3] for j in ok)
         finals[name] = [done[j][0] for j in range(n)]
         work_ok = sum(reqs[j][3] * reqs[j][4] * 3 for j in ok)
