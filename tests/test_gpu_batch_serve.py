@@ -176,3 +176,39 @@ def test_server_rejects_and_isolates_failures(wb):
     ref, _ = alone(wb, c2, e2, U2, max_steps=3)
     assert np.abs(U - ref).max() <= 1e-12 * np.abs(ref).max()
     srv.close()
+
+
+def test_batch_member_with_nan_is_isolated(wb):
+    # a corrupted instance stops with a NaN flag; the others finish as if alone
+    ens = cases.ensemble(3, seed=8, grids=[(64, 64), (48, 40)])
+    cfgs, eqs = [], []
+    for U0, prm in ens:
+        c, e = column_cfg(wb, prm["nx"], prm["ny"], prm, wb.FP64_STRICT, scheme=prm["scheme"])
+        cfgs.append(c)
+        eqs.append(e)
+    b = wb.Batch(cfgs, eqs)
+    bad = ens[1][0].copy()
+    bad[2, 5, 7] = np.nan
+    for k, (U0, _) in enumerate(ens):
+        b.upload(k, bad if k == 1 else U0)
+    with pytest.raises(wb.WenofvError) as e:
+        b.advance(1e9, max_steps=5)
+    assert e.value.code == wb.ENUMERIC
+    for k in (0, 2):
+        ref, n = alone(wb, cfgs[k], eqs[k], ens[k][0], max_steps=5)
+        assert np.array_equal(b.download(k), ref)
+    b.close()
+
+
+def test_device_allocation_failure_is_reported(wb):
+    # 46000^2 cells x 4 variables x 3 buffers x 8 B = 203 GB: more than the GPU holds
+    cfg = wb.make_config(46000, 46000, precision=wb.FP64)
+    eq = wb.make_eq()
+    with pytest.raises(wb.WenofvError) as e:
+        wb.Solver(cfg, eq)
+    assert e.value.code == wb.ENOMEM
+    # the device stays usable afterwards
+    U0, prm = cases.liquid_column(32, 32, seed=1)
+    c, q = column_cfg(wb, 32, 32, prm, wb.FP64_STRICT)
+    ref, n = alone(wb, c, q, U0, max_steps=2)
+    assert n == 2 and np.isfinite(ref).all()

@@ -24,6 +24,7 @@ const char *last_error_text() { return g_err; }
 int cuda_fail(cudaError_t e, const char *what)
 {
     set_error("%s: %s", what, cudaGetErrorString(e));
+    (void)cudaGetLastError(); // a failed allocation is not sticky: do not let a later check see it
     return e == cudaErrorMemoryAllocation ? WENOFV_ENOMEM : WENOFV_ECUDA;
 }
 
@@ -173,14 +174,6 @@ int Engine::alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params
     const int nv = nvar_of(e.eq_kind);
     const int pitch = (c.nx + 15) / 16 * 16;
     const size_t per = (size_t)nv * c.ny * pitch;
-    if (per * sizeof(double) > h_stage_bytes_) {
-        WENOFV_CUDA(cudaStreamSynchronize(stream));
-        if (h_stage_) cudaFreeHost(h_stage_);
-        h_stage_ = nullptr;
-        h_stage_bytes_ = 0;
-        WENOFV_CUDA(cudaMallocHost(&h_stage_, per * sizeof(double)));
-        h_stage_bytes_ = per * sizeof(double);
-    }
     WENOFV_CUDA(cudaMalloc(&dmem_[i], 3 * per * sizeof(double)));
     WENOFV_CUDA(cudaMemsetAsync(dmem_[i], 0, 3 * per * sizeof(double), stream));
     std::vector<double> met(2 * (size_t)c.nx + c.ny);
@@ -457,6 +450,19 @@ static void from_pitch(const double *src, int layout, int nv, int nx, int ny, in
         }
 }
 
+// pinned staging for the layouts that need a host-side repack, allocated on first use
+int Engine::ensure_stage(size_t bytes)
+{
+    if (bytes <= h_stage_bytes_) return WENOFV_OK;
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    if (h_stage_) cudaFreeHost(h_stage_);
+    h_stage_ = nullptr;
+    h_stage_bytes_ = 0;
+    WENOFV_CUDA(cudaMallocHost(&h_stage_, bytes));
+    h_stage_bytes_ = bytes;
+    return WENOFV_OK;
+}
+
 int Engine::upload(int i, const double *U, int layout)
 {
     if (!live(i) || !U) { set_error("bad instance index or null array"); return WENOFV_EINVAL; }
@@ -473,6 +479,8 @@ int Engine::upload(int i, const double *U, int layout)
         WENOFV_CUDA(cudaStreamSynchronize(stream));
         return WENOFV_OK;
     }
+    const int src = ensure_stage((size_t)nv * d.ny * d.pitch * sizeof(double));
+    if (src) return src;
     WENOFV_CUDA(cudaStreamSynchronize(stream)); // the staging buffer may still feed a copy
     to_pitch(U, layout, nv, d.nx, d.ny, d.pitch, h_stage_);
     WENOFV_CUDA(cudaMemcpyAsync(d.buf[b], h_stage_, (size_t)nv * d.ny * d.pitch * sizeof(double), cudaMemcpyHostToDevice, stream));
@@ -494,6 +502,8 @@ int Engine::download(int i, double *U, int layout)
         WENOFV_CUDA(cudaStreamSynchronize(stream));
         return WENOFV_OK;
     }
+    const int src = ensure_stage((size_t)nv * d.ny * d.pitch * sizeof(double));
+    if (src) return src;
     WENOFV_CUDA(cudaMemcpyAsync(h_stage_, d.buf[b], (size_t)nv * d.ny * d.pitch * sizeof(double), cudaMemcpyDeviceToHost, stream));
     WENOFV_CUDA(cudaStreamSynchronize(stream));
     from_pitch(h_stage_, layout, nv, d.nx, d.ny, d.pitch, U);
@@ -544,6 +554,14 @@ int Engine::rhs(double *out, int layout)
     h_state_[0] = fresh_state(cur_);
     int rc = push_state();
     if (!rc) rc = launch_stage_all(0, 0, d_rhs_);
+    if (rc) return rc;
+    if (layout == WENOFV_LAYOUT_SOA) {
+        WENOFV_CUDA(cudaMemcpy2DAsync(out, (size_t)d.nx * sizeof(double), d_rhs_, (size_t)d.pitch * sizeof(double),
+                                      (size_t)d.nx * sizeof(double), (size_t)nv * d.ny, cudaMemcpyDeviceToHost, stream));
+        WENOFV_CUDA(cudaStreamSynchronize(stream));
+        return WENOFV_OK;
+    }
+    rc = ensure_stage(bytes);
     if (rc) return rc;
     WENOFV_CUDA(cudaMemcpyAsync(h_stage_, d_rhs_, bytes, cudaMemcpyDeviceToHost, stream));
     WENOFV_CUDA(cudaStreamSynchronize(stream));

@@ -84,6 +84,7 @@ private:
     int alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params &e);
     void free_instance(int i);
     int launch_stage_all(int parity, int stage, double *rhs_out);
+    int ensure_stage(size_t bytes);
     int launch_cfl_all();
     int pull_state();
     int push_state();
