@@ -20,7 +20,9 @@
 //    waiting on stdin and exiting.
 // Added keys: BACKEND (CUDA, the only backend), PRECISION (FP64 | FP64_STRICT | FP32BULK),
 // REFSLABS, DEVICE, ENDTIME (replaces the case's last output time), MAXSTEPS (bound on
-// the steps of each output interval, 0 = none), OUTPUT (file for the final state, FP64 [i][j][r]).
+// the steps of each output interval, 0 = none), OUTPUT (file for the final state, FP64 [i][j][r]),
+// STEPMODE (1: run's time loop on the host through calculateDeltaT / performTimeIntegration,
+// as the reference loops; 0, the default: the loop on the device).
 #pragma once
 #include <cstdint>
 #include <map>

@@ -2,6 +2,7 @@
 // call structure; the per-cell work runs in libwenofv_b200).
 #include "../include/WENOFV.hpp"
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -189,12 +190,27 @@ void CWENOFV::run()
     const auto t0 = std::chrono::steady_clock::now();
     initializeSolver();
     const auto t1 = std::chrono::steady_clock::now();
+    const bool hostLoop = opt("STEPMODE", "0") == "1";
     for (size_t k = 1; k < m_timeMoments.size(); k++) {
-        double tout = m_now;
-        int64_t n = 0;
-        check(wenofv_advance(m_ctx, m_now, m_timeMoments[k], m_maxSteps, &tout, &n), "run");
-        m_now = tout;
-        m_stepCount += n;
+        const double targetTime = m_timeMoments[k];
+        if (hostLoop) {
+            // the reference's loop on the host, one C-ABI call per method (src/WENOFV.cpp:318-331)
+            int64_t n = 0;
+            while (std::abs(m_now - targetTime) > 1e-10 && (m_maxSteps <= 0 || n < m_maxSteps)) {
+                const double remainingTime = targetTime - m_now;
+                double timestep = calculateDeltaT(m_now);
+                timestep = std::min(timestep, remainingTime);
+                performTimeIntegration(timestep);
+                m_now += timestep;
+                n++;
+            }
+        } else {
+            double tout = m_now;
+            int64_t n = 0;
+            check(wenofv_advance(m_ctx, m_now, targetTime, m_maxSteps, &tout, &n), "run");
+            m_now = tout;
+            m_stepCount += n;
+        }
         downloadUh();
     }
     const auto t2 = std::chrono::steady_clock::now();
