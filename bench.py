@@ -118,7 +118,20 @@ def cpu_baseline(name: str, steps: int, warmup: int, sample_n: int = 256):
                     raise RuntimeError(e[-500:])
                 secs.append(json.loads(o.strip().splitlines()[-1])["seconds"])
         units = nproc * sample_n * sample_n * 3 * steps
+        single = None
+        if shutil.which("taskset"):
+            # the same reference process pinned to one core (its 4 slab ranks share it)
+            with tempfile.TemporaryDirectory() as d1:
+                U0.tofile(os.path.join(d1, "u0.bin"))
+                a1 = list(args)
+                a1[a1.index("--u0") + 1] = os.path.join(d1, "u0.bin")
+                a1[a1.index("--steps") + 1] = "2"
+                cp = subprocess.run(["taskset", "-c", "0"] + a1, capture_output=True, text=True, timeout=1800)
+                if cp.returncode == 0:
+                    s1 = json.loads(cp.stdout.strip().splitlines()[-1])["seconds"]
+                    single = dict(value=sample_n * sample_n * 3 * 2 / s1, cores=1, steps=2)
         return dict(value=units / max(secs), unit="cell-stage updates/s", cores=4 * nproc, kind="reference",
+                    single_core=single,
                     sample=f"{nproc} concurrent processes of the unmodified reference (4 slab ranks each, "
                            f"threads over an in-process MPI shim), {steps} timed SSP-RK3 steps after {warmup} "
                            f"warm-up steps each, on the same workload at {sample_n}x{sample_n} "
@@ -584,7 +597,7 @@ def main():
     ap.add_argument("--max-steps", type=int, default=2000, help="serve: most steps of a request")
     ap.add_argument("--hbm-budget-gb", type=int, default=150, help="serve: HBM budget of the server")
     ap.add_argument("--form", default="fp64", choices=["fp64", "fp64_strict", "fp32_bulk"])
-    ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-bulk comparison of the FP64 form")
     args = ap.parse_args()

@@ -82,6 +82,35 @@ def test_two_phase_riemann_probe(wb, oracle_lib, flux, normal):
     fast = wb.probe_riemann(eq, flux, UL, UR, *normal, precision=wb.FP64)
     scale = np.abs(ref).max(axis=1, keepdims=True) + 1.0
     assert np.all(np.abs(fast - ref) <= 1e-11 * scale)
+    f32 = wb.probe_riemann(eq, flux, UL, UR, *normal, precision=wb.FP32_BULK)  # near-pure phases
+    assert np.all(np.abs(f32 - ref) <= 1e-5 * scale)
+
+
+@pytest.mark.parametrize("flux", [0, 1])
+@pytest.mark.parametrize("normal", [(1.0, 0.0), (0.0, 1.0)])
+def test_two_phase_riemann_probe_supersonic(wb, oracle_lib, flux, normal):
+    # sound speeds of 1 and velocities up to 4: every HLLC branch (F_L, F*_L, F*_R, F_R) occurs
+    rng = np.random.default_rng(7)
+    n = 1200
+
+    def st():
+        z1 = rng.uniform(0.01, 0.99, n)
+        a1, a2 = z1 * 1.2 * (1 + rng.uniform(-0.1, 0.1, n)), (1 - z1) * (1 + rng.uniform(-0.1, 0.1, n))
+        rho = a1 + a2
+        return np.stack([a1, a2, rho * rng.uniform(-4, 4, n), rho * rng.uniform(-4, 4, n)], axis=1)
+    UL, UR = st(), st()
+    p = Problem(nx=8, ny=8, rho10=1.2, rho20=1.0, sound1=1.0, sound2=1.0)
+    eq = wb.make_eq(rho10=1.2, rho20=1.0, sound1=1.0, sound2=1.0)
+    k = 2 if normal[0] == 1.0 else 3
+    vn_l, vn_r = UL[:, k] / UL[:, :2].sum(1), UR[:, k] / UR[:, :2].sum(1)
+    assert (vn_l > 1.5).sum() > 50 and (vn_r < -1.5).sum() > 50  # supersonic from both sides
+    ref = np.array([oracle_lib.riemann(p, flux, a, b, *normal) for a, b in zip(UL, UR)])
+    assert np.array_equal(wb.probe_riemann(eq, flux, UL, UR, *normal, precision=wb.FP64_STRICT), ref)
+    scale = np.abs(ref).max(axis=1, keepdims=True) + 1.0
+    fast = wb.probe_riemann(eq, flux, UL, UR, *normal, precision=wb.FP64)
+    assert np.all(np.abs(fast - ref) <= 1e-11 * scale)
+    f32 = wb.probe_riemann(eq, flux, UL, UR, *normal, precision=wb.FP32_BULK)
+    assert np.all(np.abs(f32 - ref) <= 1e-5 * scale)
 
 
 @pytest.mark.parametrize("flux", [0, 1])
