@@ -98,3 +98,54 @@ def test_host_run_equals_reference(host_bin, tmp_path, testcase, kv):
                 flux=int(opts["RIEMANNFLUX"]), limiter=int(opts["PPlimiter"]), scheme=1, rk=2, cfl=0.5)
     ref = run_reference(p, testcase=testcase, t_end=tend)
     assert np.array_equal(mine, ref.U)
+
+
+# Accuracy of z1 against the exact solution on SMOOTH at t = 0.05, as the reference's
+# outputAccuracy computes it (src/WENOFV.cpp:3152-3251), for runs of the reference made with
+# a one-rank build (so REFSLABS = 1): (L_inf, L1, L2) to 15 digits.
+SMOOTH_KNOWN = [
+    ((100, "SCHEME=1", "RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=0"),
+     (3.841719623982887e-07, 2.400853109961034e-07, 2.689826478231563e-07)),
+    ((128, "SCHEME=0", "RECONSTRUCTIONTYPE=0", "RIEMANNFLUX=0"),
+     (9.072026528854360e-07, 4.452180407799647e-07, 5.149646872224241e-07)),
+    ((128, "SCHEME=1", "RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=1"),
+     (7.220356113869786e-08, 4.566660819012802e-08, 5.089875840234343e-08)),
+]
+
+
+def smooth_accuracy(U, n, t):
+    """(L_inf, L1, L2) of z1 = getVolumeFrac(U) against the 4x4 Gauss-Legendre average of the
+    translated initial volume fraction (rho10 = 1.2, rho20 = 1, c1 = c2 = 1, eps = 1e-8)"""
+    from cases import GLEG_W, GLEG_X
+
+    eps, c1, c2, r10, r20 = 1e-8, 1.0, 1.0, 1.2, 1.0
+    d = 1.0 / n
+    xl = 0.0 - 3 * d + (np.arange(n) + 3) * d
+    xr = 0.0 - 3 * d + (np.arange(n) + 4) * d
+    xc = (xl + xr) / 2
+    ex = np.zeros((n, n))  # [j][i]
+    for a in range(4):
+        for b in range(4):
+            X = xc[None, :] + 0.5 * d * GLEG_X[a]
+            Y = xc[:, None] + 0.5 * d * GLEG_X[b]
+            z = eps + (1 - 2 * eps) * np.sin(2.0 * np.pi * (X - t)) ** 2 + 0 * Y
+            ex += z * (0.5 * d * GLEG_W[a]) * (0.5 * d * GLEG_W[b]) / d / d
+    a1, a2 = U[0], U[1]
+    q = r20 * c2 * c2 - r10 * c1 * c1
+    qs = a2 * c2 * c2 - a1 * c1 * c1
+    r = ((q - qs) + np.sqrt((q - qs) ** 2 + 4.0 * a1 * c1 * c1 * a2 * c2 * c2)) / (2.0 * a2 * c2 * c2)
+    err = np.abs(ex - r / (1 + r))
+    return err.max(), err.mean(), np.sqrt((err ** 2).mean())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case,known", SMOOTH_KNOWN)
+def test_smooth_accuracy_known_answers(host_bin, tmp_path, case, known):
+    n, *kv = case
+    out = str(tmp_path / "u.bin")
+    cp = run_host(host_bin, "TESTCASE=0", f"ELEMNUMX={n}", f"ELEMNUMY={n}", "RKMETH=2", "CFL=0.5", "PPlimiter=0",
+                  "PRECISION=FP64_STRICT", "REFSLABS=1", f"OUTPUT={out}", *kv)
+    assert cp.returncode == 0, cp.stderr
+    U = to_soa(np.fromfile(out), n, n)
+    got = smooth_accuracy(U, n, 0.05)
+    assert np.allclose(got, known, rtol=1e-6, atol=0), (got, known)

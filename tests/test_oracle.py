@@ -2,11 +2,13 @@
 of the compiled reference when it is built here, and properties of the restated kernels."""
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 
 from conftest import golden_cases, load_golden
-from oracle import EQ_EULER, EQ_LINEAR_ADV, BC_OUTFLOW, Problem, reference_available, run_reference
+from oracle import EQ_EULER, EQ_LINEAR_ADV, BC_OUTFLOW, Oracle, Problem, reference_available, run_reference
 import cases
 
 GOLD = golden_cases()
@@ -123,3 +125,27 @@ def test_advection_converges(oracle_lib):
         assert k == 4 * n and abs(t - 1.0) < 1e-12  # dt = CFL / (1/dx + 1/dy)
         err.append(np.abs(U - U0).mean())
     assert err[0] < 1e-3 and np.log2(err[0] / err[1]) > 3.0
+
+
+def test_oracle_reproduces_smooth_known_answer():
+    # the reference's own accuracy report for SMOOTH 128^2, WENO-JS, conservative, LLF, RK3 at
+    # t = 0.05 (a one-rank run of the reference): the oracle from the reference's initial
+    # averages reproduces (L_inf, L1, L2) of z1
+    import subprocess
+
+    import test_host_mirror as T
+
+    if not os.path.exists(os.path.join(T.PKG_DIR, "lib", "libwenofv_b200.so")):
+        pytest.skip("the host mirror needs the built library")
+    subprocess.run(["make", "-C", T.HOST], check=True, capture_output=True)
+    n = 128
+    ic = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"smooth_ic_{os.getpid()}.bin")
+    subprocess.run([T.BIN, T.CFG, "TESTCASE=0", f"ELEMNUMX={n}", f"ELEMNUMY={n}", "REFSLABS=1", "--dump-ic", ic],
+                   check=True, capture_output=True)
+    U0 = T.to_soa(np.fromfile(ic), n, n)
+    os.unlink(ic)
+    p = Problem(nx=n, ny=n, rk=2, cfl=0.5, scheme=0, flux=0, recon=0, limiter=0, ref_slabs=1,
+                threads=os.cpu_count() or 1, rho10=1.2, rho20=1.0, sound1=1.0, sound2=1.0)
+    V, k, t, _ = Oracle().advance(p, U0, t_end=0.05)
+    got = T.smooth_accuracy(V, n, 0.05)
+    assert np.allclose(got, T.SMOOTH_KNOWN[1][1], rtol=1e-12, atol=0), got
