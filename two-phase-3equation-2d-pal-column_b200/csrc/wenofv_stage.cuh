@@ -217,9 +217,10 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
         for (int gp = 0; gp < 4; gp++) S.sy[p][gp * NV + v] = anchor<DEV>(c0, o[gp]);
     } else {
         // characteristic: project with L(U_centre, y), reconstruct, project back with R(U_centre, y).
-        // The eigenvectors and both projections are FP64 in every form: the two-phase
-        // eigenvector matrices reach condition numbers of ~5e3 near pure phases, so FP32
-        // rows or FP32 mat-vecs would mix the large partial density into the small momenta.
+        // The eigenvectors and the forward projection are FP64 in every form: the two-phase
+        // eigenvector matrices reach condition numbers of ~5e3 near pure phases, so FP32 rows
+        // of L against FP32 rows of R (|R L - I| ~ 3e-4) would mix the large partial density
+        // into the small momenta.
         double Uc[NV], Lrow[NV], Rrow[NV];
         R pr[5];
 #pragma unroll
@@ -246,10 +247,19 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
         const int lane = t & 31, gbase = lane & ~(NV - 1);
 #pragma unroll
         for (int gp = 0; gp < 4; gp++) {
-            double s = 0.0;
+            // back-projection: FP32 in the bulk form (it adds an error of the same order as the
+            // FP32 WENO's own, eps * sum_k |R_vk w_k|), FP64 otherwise
+            if constexpr (DEV) {
+                R s = R(0);
 #pragma unroll
-            for (int k = 0; k < NV; k++) s += Rrow[k] * (double)__shfl_sync(0xffffffffu, cg[gp], gbase + k);
-            S.sy[p][gp * NV + v] = anchor<DEV>(Uc[v], s);
+                for (int k = 0; k < NV; k++) s += (R)Rrow[k] * __shfl_sync(0xffffffffu, cg[gp], gbase + k);
+                S.sy[p][gp * NV + v] = Uc[v] + (double)s;
+            } else {
+                double s = 0.0;
+#pragma unroll
+                for (int k = 0; k < NV; k++) s += Rrow[k] * (double)__shfl_sync(0xffffffffu, cg[gp], gbase + k);
+                S.sy[p][gp * NV + v] = s;
+            }
         }
     }
 }
@@ -324,10 +334,17 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
 #pragma unroll
             for (int gpi = 0; gpi < 4; gpi++) {
                 if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
-                double s = 0.0;
+                if constexpr (DEV) { // as in the y-sweep
+                    R s = R(0);
 #pragma unroll
-                for (int k = 0; k < NV; k++) s += Rrow[k] * (double)__shfl_sync(0xffffffffu, cg[gpi][gpj], gbase + k);
-                fv[gpi][gpj] = anchor<DEV>(Uc[v], s);
+                    for (int k = 0; k < NV; k++) s += (R)Rrow[k] * __shfl_sync(0xffffffffu, cg[gpi][gpj], gbase + k);
+                    fv[gpi][gpj] = Uc[v] + (double)s;
+                } else {
+                    double s = 0.0;
+#pragma unroll
+                    for (int k = 0; k < NV; k++) s += Rrow[k] * (double)__shfl_sync(0xffffffffu, cg[gpi][gpj], gbase + k);
+                    fv[gpi][gpj] = s;
+                }
             }
     }
 
@@ -500,15 +517,15 @@ __device__ __forceinline__ double phase_update(StageSmem<EQ> &S, const InstDesc 
     return cmin;
 }
 
-// resident CTAs per SM the register allocation is bounded for: 4 for the FP32-bulk form
-// (no spills at 128 registers); the FP64 forms at 3 keep all values in registers
-#ifndef WENOFV_FP64_MIN_BLOCKS
-#define WENOFV_FP64_MIN_BLOCKS 3
-#endif
-template <class R> struct StageMinBlocks { static constexpr int value = sizeof(R) < sizeof(double) ? 4 : WENOFV_FP64_MIN_BLOCKS; };
+// resident CTAs per SM the register allocation is bounded for (measured best): the FP64
+// forms at 3 keep all values in registers (4 spills and runs slower); the FP32-bulk form
+// runs 4 (conservative) or 5 (characteristic, a few spilled values) CTAs
+template <int RECON, class R> struct StageMinBlocks {
+    static constexpr int value = sizeof(R) < sizeof(double) ? (RECON == 1 ? 5 : 4) : 3;
+};
 
 template <int EQ, int RECON, class R>
-__global__ void __launch_bounds__(NT, StageMinBlocks<R>::value) stage_kernel(const StageLaunch L)
+__global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_kernel(const StageLaunch L)
 {
     constexpr int TX = StageGeom<EQ>::TX;
     __shared__ StageSmem<EQ> S;
