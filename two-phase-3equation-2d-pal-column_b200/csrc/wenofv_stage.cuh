@@ -307,7 +307,8 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
 #pragma unroll
             for (int j = 0; j < NV; j++) lc += Lrow[j] * Uc[j];
         }
-        R cg[4][4];
+        // per y Gauss point: project, reconstruct, and project back at once, so that only
+        // that point's characteristic values are live (not all twelve)
 #pragma unroll
         for (int gpj = 0; gpj < 4; gpj++) {
             R pr[5];
@@ -320,32 +321,26 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
             }
             Weno5<R> W;
             W.init(D.scheme, pr[0], pr[1], pr[2], pr[3], pr[4]);
-            if (gpj == 0 || gpj == 3) {
-                R o[4];
-                W.eval4(o);
-#pragma unroll
-                for (int gpi = 0; gpi < 4; gpi++) cg[gpi][gpj] = o[gpi];
-            } else {
-                W.eval03(cg[0][gpj], cg[3][gpj]);
-            }
-        }
-#pragma unroll
-        for (int gpj = 0; gpj < 4; gpj++)
+            R cg[4];
+            const bool all4 = gpj == 0 || gpj == 3;
+            if (all4) W.eval4(cg);
+            else W.eval03(cg[0], cg[3]);
 #pragma unroll
             for (int gpi = 0; gpi < 4; gpi++) {
-                if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
+                if (!(gpi == 0 || gpi == 3 || all4)) continue;
                 if constexpr (DEV) { // as in the y-sweep
                     R s = R(0);
 #pragma unroll
-                    for (int k = 0; k < NV; k++) s += (R)Rrow[k] * __shfl_sync(0xffffffffu, cg[gpi][gpj], gbase + k);
+                    for (int k = 0; k < NV; k++) s += (R)Rrow[k] * __shfl_sync(0xffffffffu, cg[gpi], gbase + k);
                     fv[gpi][gpj] = Uc[v] + (double)s;
                 } else {
                     double s = 0.0;
 #pragma unroll
-                    for (int k = 0; k < NV; k++) s += Rrow[k] * (double)__shfl_sync(0xffffffffu, cg[gpi][gpj], gbase + k);
+                    for (int k = 0; k < NV; k++) s += Rrow[k] * (double)__shfl_sync(0xffffffffu, cg[gpi], gbase + k);
                     fv[gpi][gpj] = s;
                 }
             }
+        }
     }
 
     // bound-preserving limiter: theta from the partial densities, in FP64 in every form
