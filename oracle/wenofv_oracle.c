@@ -706,8 +706,49 @@ static void cell_avg(ofv_ws *w, int i, int j, real_t *u)
     for (int v = 0; v < w->nv; v++) u[v] = *Ecell(w, v, i, j);
 }
 
+/* Primitive variables of the two-phase model for RECONSTRUCTIONTYPE 2 (PRIMITIVE: z1,
+ * rho1, u, v; src/WENOFV.cpp:944-959) and 3 (PRIMITIVE2: z1, p, u, v; :1102-1121), and
+ * their inverse at the Gauss points (:1002-1025 and :1178-1189). */
+static void to_primitive(const ofv_eq *e, int recon, const real_t *U, real_t *P)
+{
+    const real_t z1 = tp_volume_frac(e, U);
+    P[0] = z1;
+    if (recon == 2) {
+        P[1] = U[0] / z1;
+    } else {
+        const real_t c1_2 = (real_t)e->sound1 * e->sound1, c2_2 = (real_t)e->sound2 * e->sound2;
+        if (z1 > 0.5)
+            P[1] = e->preb + c1_2 * (U[0] / z1 - e->rho10);
+        else
+            P[1] = e->preb + c2_2 * (U[1] / (1.0 - z1) - e->rho20);
+    }
+    P[2] = U[2] / (U[0] + U[1]);
+    P[3] = U[3] / (U[0] + U[1]);
+}
+static void from_primitive(const ofv_eq *e, int recon, const real_t *P, real_t *U)
+{
+    const real_t z1 = P[0];
+    const real_t c1_2 = (real_t)e->sound1 * e->sound1, c2_2 = (real_t)e->sound2 * e->sound2;
+    real_t z1rho1, z2rho2;
+    if (recon == 2) {
+        const real_t rho1 = P[1];
+        z2rho2 = c1_2 / c2_2 * (rho1 - e->rho10) + e->rho20;
+        z2rho2 = z2rho2 * (1.0 - z1);
+        z1rho1 = z1 * rho1;
+    } else {
+        const real_t pr = P[1];
+        z1rho1 = ((pr - e->preb) / c1_2 + e->rho10) * z1;
+        z2rho2 = ((pr - e->preb) / c2_2 + e->rho20) * (1.0 - z1);
+    }
+    const real_t rho = z1rho1 + z2rho2;
+    U[0] = z1rho1;
+    U[1] = z2rho2;
+    U[2] = rho * P[2];
+    U[3] = rho * P[3];
+}
+
 /* y-direction sweep of one column position (src/WENOFV.cpp:670-687 conservative,
- * :796-833 characteristic): 4 Gauss-Lobatto y points x nv variables */
+ * :796-833 characteristic, :963-979 primitive): 4 Gauss-Lobatto y points x nv variables */
 static void y_sweep(ofv_ws *w, int i, int j)
 {
     const ofv_problem *p = w->p;
@@ -730,6 +771,16 @@ static void y_sweep(ofv_ws *w, int i, int j)
             real_t phys[4];
             matvec(nv, R, cg[gp], phys);
             for (int v = 0; v < nv; v++) out[gp * 4 + v] = phys[v];
+        }
+    } else if (p->recon >= 2 && nv > 1) {
+        real_t col[5][4], prim[5][4], st[5];
+        for (int m = 0; m < 5; m++) {
+            cell_avg(w, i, j - 2 + m, col[m]);
+            to_primitive(&p->eq, p->recon, col[m], prim[m]);
+        }
+        for (int v = 0; v < nv; v++) {
+            for (int m = 0; m < 5; m++) st[m] = prim[m][v];
+            for (int gp = 0; gp < 4; gp++) out[gp * 4 + v] = weno(p->scheme, st, gp);
         }
     } else {
         real_t st[5];
@@ -827,6 +878,14 @@ static int x_sweep(ofv_ws *w, int i, int j)
                     ugp[gpi][gpj][v] = weno(p->scheme, st, gpi);
                 }
             }
+        if (p->recon >= 2 && nv > 1) /* the primitive values back to conservative ones */
+            for (int gpi = 0; gpi < 4; gpi++)
+                for (int gpj = 0; gpj < 4; gpj++) {
+                    if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
+                    real_t prim[4];
+                    for (int v = 0; v < 4; v++) prim[v] = ugp[gpi][gpj][v];
+                    from_primitive(&p->eq, p->recon, prim, ugp[gpi][gpj]);
+                }
     }
     for (int v = 0; v < nv; v++)
         for (int gp = 0; gp < 4; gp++) {

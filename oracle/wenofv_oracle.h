@@ -45,7 +45,8 @@ typedef struct {
     int scheme;            /* SCHEME: 0 WENO-JS, 1 WENO-Z */
     int limiter;           /* PPlimiter */
     int flux;              /* RIEMANNFLUX: 0 LLF, 1 HLLC */
-    int recon;             /* RECONSTRUCTIONTYPE: 0 conservative, 1 characteristic */
+    int recon;             /* RECONSTRUCTIONTYPE: 0 conservative, 1 characteristic, 2 primitive
+                              (z1, rho1, u, v), 3 primitive2 (z1, p, u, v); 2-3 two-phase only */
     int ref_slabs;         /* 0: uniform cell sizes; P>0: the reference's P-slab x metric */
     int threads;           /* OpenMP threads (0 = library default) */
     ofv_eq eq;

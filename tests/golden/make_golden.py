@@ -37,6 +37,9 @@ CASES = [
     ("sharp_js_cons_llf_lim_rk3", 2, 40, 24, 0, 0, 0, 1, 2, 8, 0.0, False),
     ("column_z_char_hllc_lim_rk3", 2, 48, 32, 1, 1, 1, 1, 2, 6, 0.0, True),
     ("column_js_cons_llf_lim_rk3", 2, 48, 32, 0, 0, 0, 1, 2, 6, 0.0, True),
+    ("sharp_z_prim_hllc_lim_rk3", 2, 40, 24, 1, 1, 2, 1, 2, 8, 0.0, False),
+    ("smooth_js_prim2_llf_rk3", 0, 32, 16, 0, 0, 3, 0, 2, 5, 0.0, False),
+    ("column_z_prim2_hllc_lim_rk3", 2, 48, 32, 1, 1, 3, 1, 2, 6, 0.0, True),
 ]
 
 PARAMS = {0: dict(rho10=1.2, rho20=1.0, sound1=1.0, sound2=1.0),

@@ -35,7 +35,8 @@ def test_oracle_matches_reference_golden(name, oracle_lib):
 
 
 @pytest.mark.skipif(not reference_available(), reason="compiled reference not built (make -C oracle ref)")
-@pytest.mark.parametrize("scheme,flux,recon,lim,rk", [(1, 1, 1, 1, 2), (0, 0, 0, 1, 1), (1, 0, 0, 0, 0)])
+@pytest.mark.parametrize("scheme,flux,recon,lim,rk", [(1, 1, 1, 1, 2), (0, 0, 0, 1, 1), (1, 0, 0, 0, 0),
+                                                      (1, 1, 2, 1, 2), (0, 0, 2, 0, 1), (1, 1, 3, 1, 2), (0, 1, 3, 0, 2)])
 def test_oracle_matches_live_reference(scheme, flux, recon, lim, rk, oracle_lib):
     U0, prm = cases.liquid_column(36, 20, seed=5)
     p = Problem(nx=36, ny=20, rk=rk, scheme=scheme, flux=flux, recon=recon, limiter=lim, ref_slabs=4,
