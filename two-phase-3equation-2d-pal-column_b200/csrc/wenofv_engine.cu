@@ -39,8 +39,12 @@ int validate(const wenofv_config *c, const wenofv_eq_params *e)
     if (!(c->cfl > 0)) { set_error("CFL must be positive"); return WENOFV_EINVAL; }
     if (c->scheme == 2) { set_error("SCHEME 2 (WENOEXP) is not supported"); return WENOFV_ENOTSUP; }
     if (c->scheme < 0 || c->scheme > 1) { set_error("SCHEME must be 0 or 1"); return WENOFV_EINVAL; }
-    if (c->reconstruction >= 2 && c->reconstruction <= 5) { set_error("RECONSTRUCTIONTYPE %d is not supported", c->reconstruction); return WENOFV_ENOTSUP; }
-    if (c->reconstruction < 0 || c->reconstruction > 1) { set_error("RECONSTRUCTIONTYPE must be 0 or 1"); return WENOFV_EINVAL; }
+    if (c->reconstruction >= 4 && c->reconstruction <= 5) { set_error("RECONSTRUCTIONTYPE %d is not supported", c->reconstruction); return WENOFV_ENOTSUP; }
+    if (c->reconstruction < 0 || c->reconstruction > 3) { set_error("RECONSTRUCTIONTYPE must be 0, 1, 2 or 3"); return WENOFV_EINVAL; }
+    if (c->reconstruction >= 2 && e && e->eq_kind != WENOFV_EQ_TWO_PHASE) {
+        set_error("RECONSTRUCTIONTYPE %d (primitive variables) is defined for the two-phase model only", c->reconstruction);
+        return WENOFV_ENOTSUP;
+    }
     if (c->riemann_flux < 0 || c->riemann_flux > 1) { set_error("RIEMANNFLUX must be 0 or 1"); return WENOFV_EINVAL; }
     if (c->pp_limiter < 0 || c->pp_limiter > 1) { set_error("PPlimiter must be 0 or 1"); return WENOFV_EINVAL; }
     if (c->bc != WENOFV_BC_PERIOD && c->bc != WENOFV_BC_OUTFLOW) { set_error("boundary kind %d is not supported", c->bc); return WENOFV_ENOTSUP; }

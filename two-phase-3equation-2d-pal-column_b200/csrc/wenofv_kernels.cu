@@ -30,7 +30,9 @@ static const void *pick_stage(int eq, int recon, int fp32)
 #if WENOFV_HAS_FP32
     if (fp32) {
         switch (eq) {
-        case EQ_TWO_PHASE: return recon ? stage_fn<EQ_TWO_PHASE, 1, float>() : stage_fn<EQ_TWO_PHASE, 0, float>();
+        case EQ_TWO_PHASE:
+            return recon == 1 ? stage_fn<EQ_TWO_PHASE, 1, float>() : recon == 2 ? stage_fn<EQ_TWO_PHASE, 2, float>()
+                 : recon == 3 ? stage_fn<EQ_TWO_PHASE, 3, float>() : stage_fn<EQ_TWO_PHASE, 0, float>();
         case EQ_EULER: return recon ? stage_fn<EQ_EULER, 1, float>() : stage_fn<EQ_EULER, 0, float>();
         case EQ_LINEAR_ADV: return stage_fn<EQ_LINEAR_ADV, 0, float>();
         default: return nullptr;
@@ -40,7 +42,9 @@ static const void *pick_stage(int eq, int recon, int fp32)
     if (fp32) return nullptr;
 #endif
     switch (eq) {
-    case EQ_TWO_PHASE: return recon ? stage_fn<EQ_TWO_PHASE, 1, double>() : stage_fn<EQ_TWO_PHASE, 0, double>();
+    case EQ_TWO_PHASE:
+        return recon == 1 ? stage_fn<EQ_TWO_PHASE, 1, double>() : recon == 2 ? stage_fn<EQ_TWO_PHASE, 2, double>()
+             : recon == 3 ? stage_fn<EQ_TWO_PHASE, 3, double>() : stage_fn<EQ_TWO_PHASE, 0, double>();
     case EQ_EULER: return recon ? stage_fn<EQ_EULER, 1, double>() : stage_fn<EQ_EULER, 0, double>();
     case EQ_LINEAR_ADV: return stage_fn<EQ_LINEAR_ADV, 0, double>();
     default: return nullptr;

@@ -902,6 +902,40 @@ __device__ __forceinline__ void eigen_rows(const EqParams &P, const double *U, b
     }
 }
 
+// Primitive variables of the two-phase model (FP64 in every form) for RECONSTRUCTIONTYPE 2
+// (PRIMITIVE: z1, rho1, u, v; src/WENOFV.cpp:944-959) and 3 (PRIMITIVE2: z1, p, u, v;
+// :1102-1121), and back to conserved variables at the Gauss points (:1002-1025, :1178-1189).
+__device__ __forceinline__ void tp_to_primitive(const EqParams &P, int recon, const double *U, double *W)
+{
+    const TwoPhaseK K(P);
+    const double z1 = K.volume_frac(U[0], U[1]);
+    W[0] = z1;
+    if (recon == 2) W[1] = U[0] / z1;
+    else if (z1 > 0.5) W[1] = P.preb + K.c1_2 * (U[0] / z1 - P.rho10);
+    else W[1] = P.preb + K.c2_2 * (U[1] / (1.0 - z1) - P.rho20);
+    W[2] = U[2] / (U[0] + U[1]);
+    W[3] = U[3] / (U[0] + U[1]);
+}
+__device__ __forceinline__ void tp_from_primitive(const EqParams &P, int recon, const double *W, double *U)
+{
+    const TwoPhaseK K(P);
+    const double z1 = W[0];
+    double z1rho1, z2rho2;
+    if (recon == 2) {
+        z2rho2 = K.c1_2 / K.c2_2 * (W[1] - P.rho10) + P.rho20;
+        z2rho2 = z2rho2 * (1.0 - z1);
+        z1rho1 = z1 * W[1];
+    } else {
+        z1rho1 = ((W[1] - P.preb) / K.c1_2 + P.rho10) * z1;
+        z2rho2 = ((W[1] - P.preb) / K.c2_2 + P.rho20) * (1.0 - z1);
+    }
+    const double rho = z1rho1 + z2rho2;
+    U[0] = z1rho1;
+    U[1] = z2rho2;
+    U[2] = rho * W[2];
+    U[3] = rho * W[3];
+}
+
 // Per-cell eigensystem data, computed once per cell and row in FP64 (every form) and shared
 // by the lanes that build its rows of L and R and by the limiter's wave speeds.
 template <int EQ> struct CellEigen { using type = TPEigen<double>; };

@@ -206,11 +206,25 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
     constexpr bool DEV = sizeof(R) < sizeof(double); // deviation form
     const int t = threadIdx.x;
     const int p = t / NV, v = t - p * NV;
-    if (RECON == 0 || NV == 1) {
-        const double c0 = DEV ? S.su[r & 7][v][p] : 0.0;
+    if (RECON != 1 || NV == 1) {
+        // conservative: the averages; primitive (RECONSTRUCTIONTYPE 2, 3): the primitive
+        // variables of each of the 5 cells (src/WENOFV.cpp:944-979)
+        double st[5];
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            if constexpr (RECON >= 2 && NV == 4) {
+                double U4[4], W4[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) U4[j] = S.su[(r - 2 + m) & 7][j][p];
+                tp_to_primitive(D.eq, RECON, U4, W4);
+                st[m] = W4[v];
+            } else {
+                st[m] = S.su[(r - 2 + m) & 7][v][p];
+            }
+        }
+        const double c0 = DEV ? st[2] : 0.0;
         Weno5<R> W;
-        W.init(D.scheme, (R)(S.su[(r - 2) & 7][v][p] - c0), (R)(S.su[(r - 1) & 7][v][p] - c0), (R)(S.su[r & 7][v][p] - c0),
-               (R)(S.su[(r + 1) & 7][v][p] - c0), (R)(S.su[(r + 2) & 7][v][p] - c0));
+        W.init(D.scheme, (R)(st[0] - c0), (R)(st[1] - c0), (R)(st[2] - c0), (R)(st[3] - c0), (R)(st[4] - c0));
         R o[4];
         W.eval4(o);
 #pragma unroll
@@ -278,8 +292,19 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
     const int lane = t & 31, gbase = lane & ~(NV - 1);
     double fv[4][4]; // face values [gpi][gpj] of variable v (boundary points only)
 
-    if (RECON == 0 || NV == 1) {
-        const double cc = DEV ? S.su[r & 7][v][c + G] : 0.0;
+    if (RECON != 1 || NV == 1) {
+        double cc = 0.0; // deviation anchor: the cell's own (primitive) average
+        if constexpr (DEV) {
+            if constexpr (RECON >= 2 && NV == 4) {
+                double U4[4], W4[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) U4[j] = S.su[r & 7][j][c + G];
+                tp_to_primitive(D.eq, RECON, U4, W4);
+                cc = W4[v];
+            } else {
+                cc = S.su[r & 7][v][c + G];
+            }
+        }
 #pragma unroll
         for (int gpj = 0; gpj < 4; gpj++) {
             Weno5<R> W;
@@ -296,6 +321,20 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
                 fv[0][gpj] = anchor<DEV>(cc, o0);
                 fv[3][gpj] = anchor<DEV>(cc, o3);
             }
+        }
+        if constexpr (RECON >= 2 && NV == 4) {
+            // the primitive face values back to conserved ones (src/WENOFV.cpp:1002-1025, :1178-1189)
+#pragma unroll
+            for (int gpj = 0; gpj < 4; gpj++)
+#pragma unroll
+                for (int gpi = 0; gpi < 4; gpi++) {
+                    if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
+                    double W4[4], U4[4];
+#pragma unroll
+                    for (int k = 0; k < 4; k++) W4[k] = __shfl_sync(0xffffffffu, fv[gpi][gpj], gbase + k);
+                    tp_from_primitive(D.eq, RECON, W4, U4);
+                    fv[gpi][gpj] = U4[v];
+                }
         }
     } else {
         double Uc[NV], Lrow[NV], Rrow[NV]; // FP64 in every form, as in the y-sweep
