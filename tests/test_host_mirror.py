@@ -151,3 +151,23 @@ def test_smooth_accuracy_known_answers(host_bin, tmp_path, case, known):
     U = to_soa(np.fromfile(out), n, n)
     got = smooth_accuracy(U, n, 0.05)
     assert np.allclose(got, known, rtol=1e-6, atol=0), (got, known)
+
+
+@pytest.mark.gpu
+def test_host_writes_the_reference_output_files(host_bin, tmp_path):
+    # the shipped settings (SMOOTH 100^2, WENO-Z, characteristic, LLF) with the output of
+    # outputResults: average_*.plt and accuracy_*.csv, as the reference writes them
+    out = tmp_path / "out"
+    cp = run_host(host_bin, "PRECISION=FP64_STRICT", "REFSLABS=1", f"OUTPUTDIR={out}")
+    assert cp.returncode == 0, cp.stderr
+    names = sorted(os.listdir(out))
+    assert "average_initial.plt" in names and "average_final.plt" in names and "average_0.05_intermediate.plt" in names
+    lines = (out / "average_final.plt").read_text().splitlines()
+    assert lines[0] == "TITLE=FvSolution" and lines[1].split()[:4] == ["VARIABLES=X", "Y", "RHO1Z1", "RHO2Z2"]
+    assert lines[2].startswith("ZONE T=TA, I=100, J=100")
+    rows = [list(map(float, ln.split())) for ln in lines[3:]]
+    assert len(rows) == 100 * 100 and all(len(r) == 11 for r in rows)
+    acc = (out / "accuracy_final.csv").read_text().splitlines()
+    assert acc[0] == "Cell Number, Linf-norm, L1-norm, L2-norm"
+    vals = [float(x) for x in acc[1].split(",")]
+    assert vals[0] == 100 and np.allclose(vals[1:], SMOOTH_KNOWN[0][1], rtol=1e-6, atol=0)

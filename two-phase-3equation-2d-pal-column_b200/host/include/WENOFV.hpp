@@ -21,6 +21,7 @@
 // Added keys: BACKEND (CUDA, the only backend), PRECISION (FP64 | FP64_STRICT | FP32BULK),
 // REFSLABS, DEVICE, ENDTIME (replaces the case's last output time), MAXSTEPS (bound on
 // the steps of each output interval, 0 = none), OUTPUT (file for the final state, FP64 [i][j][r]),
+// OUTPUTDIR (directory for the reference's .plt / .csv output; none by default),
 // STEPMODE (1: run's time loop on the host through calculateDeltaT / performTimeIntegration,
 // as the reference loops; 0, the default: the loop on the device).
 #pragma once
@@ -90,6 +91,15 @@ public:
 
     void downloadUh();
     void uploadUh();
+
+    // the reference's output files (src/WENOFV.cpp:2447-2601, :3152-3251), written when the
+    // key OUTPUTDIR names a directory: average_<prefix>.plt (Tecplot point data of the
+    // cell averages and the derived variables) and, for SMOOTH and VORTEX,
+    // accuracy_<prefix>.csv (L_inf, L1, L2 of z1 against the translated initial data)
+    void outputResults(int count, double now, const std::string &specialCase);
+    void outputAve(const std::string &prefix);
+    void outputAccuracy(const std::string &prefix, double now);
+    std::string m_outputDir;
     double &Uh(int i, int j, int r) { return m_Uh[((size_t)i * m_worldElemNumY + j) * m_varNum + r]; }
     wenofv_config config() const;
 

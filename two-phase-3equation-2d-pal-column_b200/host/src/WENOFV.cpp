@@ -6,8 +6,11 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <filesystem>
 #include <fstream>
+#include <iomanip>
 #include <iostream>
+#include <sstream>
 #include <stdexcept>
 
 namespace {
@@ -155,6 +158,109 @@ void CWENOFV::initializeSolver()
     m_stepCount = 0;
 }
 
+namespace {
+// getVolumeFrac / getPressure (include/Equations.hpp:84-124) of the host-side output
+double volume_frac(const TwoPhaseEquation &e, const double *U)
+{
+    const double c1_2 = e.g_sound1 * e.g_sound1, c2_2 = e.g_sound2 * e.g_sound2;
+    const double q = e.g_rho20 * c2_2 - e.g_rho10 * c1_2;
+    const double qs = U[1] * c2_2 - U[0] * c1_2;
+    const double r = ((q - qs) + std::sqrt((q - qs) * (q - qs) + 4.0 * U[0] * c1_2 * U[1] * c2_2)) / (2.0 * U[1] * c2_2);
+    return r / (1.0 + r);
+}
+double pressure(const TwoPhaseEquation &e, const double *U, double z1)
+{
+    const double z2 = 1.0 - z1;
+    const double pre1 = e.g_sound1 * e.g_sound1 * (U[0] / z1 - e.g_rho10);
+    const double pre2 = e.g_sound2 * e.g_sound2 * (U[1] / z2 - e.g_rho20);
+    return (z1 < z2) ? pre2 : pre1;
+}
+std::string num_str(double v)
+{
+    std::ostringstream o;
+    o << v;
+    return o.str();
+}
+} // namespace
+
+// outputResults (src/WENOFV.cpp:2447-2523) at the initial, intermediate and final moments
+void CWENOFV::outputResults(int count, double now, const std::string &specialCase)
+{
+    (void)count;
+    if (m_outputDir.empty()) return;
+    const bool exact = m_testcase == SMOOTH || m_testcase == VORTEX;
+    if (specialCase == "initial") {
+        outputAve("initial");
+        if (exact) outputAccuracy("initial", now);
+    } else if (specialCase == "final") {
+        outputAve("final");
+        if (exact) outputAccuracy("final", now);
+    } else if (specialCase == "intermediate") {
+        outputAve(num_str(now) + "_intermediate");
+    }
+}
+
+// outputAve (src/WENOFV.cpp:2525-2601): cell centres and the variables of getVitalVarVal
+// (include/Equations.hpp:1005-1043). The reference also writes the limiter's theta and a
+// pressure diagnostic of its primitive reconstructions per cell; those stay on the GPU here.
+void CWENOFV::outputAve(const std::string &prefix)
+{
+    const std::string filename = m_outputDir + "average_" + prefix + ".plt";
+    std::ofstream f(filename);
+    if (!f) throw std::runtime_error("cannot write " + filename);
+    f << "TITLE=FvSolution" << std::endl;
+    f << "VARIABLES=X Y RHO1Z1 RHO2Z2 Z1 RHO1 RHO2 RHO U V PRE " << std::endl;
+    f << "ZONE T=TA, I=" << m_worldElemNumY << ", J=" << m_worldElemNumX << ", DATAPACKING = POINT" << std::endl;
+    const int G = m_ghostCellNum;
+    for (int i = 0; i < m_worldElemNumX; i++) {
+        const double xl = equation->xL - G * m_deltaX + (i + G) * m_deltaX, xr = equation->xL - G * m_deltaX + (i + G + 1) * m_deltaX;
+        for (int j = 0; j < m_worldElemNumY; j++) {
+            const double yl = equation->yL - G * m_deltaY + (j + G) * m_deltaY, yr = equation->yL - G * m_deltaY + (j + G + 1) * m_deltaY;
+            const double *U = &m_Uh[((size_t)i * m_worldElemNumY + j) * m_varNum];
+            const double z1 = volume_frac(*equation, U), rho = U[0] + U[1];
+            f << (xl + xr) / 2 << " " << (yl + yr) / 2 << " " << U[0] << " " << U[1] << " " << z1 << " " << U[0] / z1
+              << " " << U[1] / (1.0 - z1) << " " << rho << " " << U[2] / rho << " " << U[3] / rho << " "
+              << pressure(*equation, U, z1) << " " << std::endl;
+        }
+    }
+}
+
+// outputAccuracy (src/WENOFV.cpp:3152-3251): z1 against the 4x4 Gauss-Legendre average of
+// the initial volume fraction translated by (u0, v0) t
+void CWENOFV::outputAccuracy(const std::string &prefix, double now)
+{
+    const int G = m_ghostCellNum;
+    double e1 = 0.0, e2 = 0.0, einf = 0.0;
+    for (int i = 0; i < m_worldElemNumX; i++) {
+        const double xl = equation->xL - G * m_deltaX + (i + G) * m_deltaX, xr = equation->xL - G * m_deltaX + (i + G + 1) * m_deltaX;
+        const double xc = (xl + xr) / 2;
+        for (int j = 0; j < m_worldElemNumY; j++) {
+            const double yl = equation->yL - G * m_deltaY + (j + G) * m_deltaY, yr = equation->yL - G * m_deltaY + (j + G + 1) * m_deltaY;
+            const double yc = (yl + yr) / 2;
+            double ex = 0.0;
+            for (int a = 0; a < 4; a++)
+                for (int b = 0; b < 4; b++) {
+                    const double gx = xc + 0.5 * m_deltaX * kGLegX[a], gy = yc + 0.5 * m_deltaY * kGLegX[b];
+                    const double wx = 0.5 * m_deltaX * kGLegW[a], wy = 0.5 * m_deltaY * kGLegW[b];
+                    ex += equation->z1_0(gx - equation->g_u0 * now, gy - equation->g_v0 * now) * wx * wy / m_deltaX / m_deltaY;
+                }
+            const double err = std::fabs(ex - volume_frac(*equation, &m_Uh[((size_t)i * m_worldElemNumY + j) * m_varNum]));
+            e1 += err;
+            e2 += std::pow(err, 2);
+            if (err > einf) einf = err;
+        }
+    }
+    e1 = e1 / m_worldElemNumX / m_worldElemNumY;
+    e2 = std::sqrt(e2 / m_worldElemNumX / m_worldElemNumY);
+    const std::string filename = m_outputDir + "accuracy_" + prefix + ".csv";
+    const bool exists = std::filesystem::exists(filename);
+    std::ofstream f(filename, exists ? std::ios::app : std::ios::out);
+    if (!f) throw std::runtime_error("cannot write " + filename);
+    if (!exists) f << "Cell Number, Linf-norm, L1-norm, L2-norm" << std::endl;
+    f << m_worldElemNumX << ", " << std::setprecision(15) << std::setw(20) << std::scientific << einf << ", "
+      << std::setw(20) << e1 << ", " << std::setw(20) << e2 << std::endl;
+}
+
 void CWENOFV::uploadUh() { check(wenofv_upload(m_ctx, m_Uh.data(), WENOFV_LAYOUT_REF_AOS), "wenofv_upload"); }
 void CWENOFV::downloadUh() { check(wenofv_download(m_ctx, m_Uh.data(), WENOFV_LAYOUT_REF_AOS), "wenofv_download"); }
 
@@ -189,6 +295,12 @@ void CWENOFV::run()
 {
     const auto t0 = std::chrono::steady_clock::now();
     initializeSolver();
+    m_outputDir = opt("OUTPUTDIR", "");
+    if (!m_outputDir.empty()) {
+        if (m_outputDir.back() != '/') m_outputDir += '/';
+        std::filesystem::create_directories(m_outputDir);
+    }
+    outputResults(0, m_now, "initial");
     const auto t1 = std::chrono::steady_clock::now();
     const bool hostLoop = opt("STEPMODE", "0") == "1";
     for (size_t k = 1; k < m_timeMoments.size(); k++) {
@@ -212,8 +324,10 @@ void CWENOFV::run()
             m_stepCount += n;
         }
         downloadUh();
+        outputResults((int)m_stepCount, m_now, "intermediate");
     }
     const auto t2 = std::chrono::steady_clock::now();
+    outputResults((int)m_stepCount, m_now, "final");
     const double solve = std::chrono::duration<double>(t2 - t1).count();
     const double init = std::chrono::duration<double>(t1 - t0).count();
     const double updates = (double)m_worldElemNumX * m_worldElemNumY * (m_rkMeth + 1) * m_stepCount;
