@@ -1,5 +1,7 @@
 // wenofv_engine.cu -- host side of the C ABI: instances, work lists, buffer rotation and
 // the device-resident time loop in captured CUDA graphs.
+#include <nvtx3/nvToolsExt.h> // header-only NVTX ranges: the host phases show up in nsys/ncu timelines
+
 #include "wenofv_engine.h"
 
 #include <algorithm>
@@ -514,8 +516,16 @@ int Engine::download(int i, double *U, int layout)
     return WENOFV_OK;
 }
 
+namespace {
+struct Range { // one NVTX range for the lifetime of the object
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+};
+} // namespace
+
 int Engine::compute_dt(double *dt_out)
 {
+    Range nvtx_range("wenofv::compute_dt");
     WENOFV_CUDA(cudaSetDevice(device));
     for (int i = 0; i < n; i++) h_state_[i] = fresh_state(cur_);
     int rc = push_state();
@@ -533,6 +543,7 @@ int Engine::compute_dt(double *dt_out)
 
 int Engine::step(double dt)
 {
+    Range nvtx_range("wenofv::step");
     WENOFV_CUDA(cudaSetDevice(device));
     for (int i = 0; i < n; i++) {
         h_state_[i] = fresh_state(cur_);
@@ -549,6 +560,7 @@ int Engine::step(double dt)
 
 int Engine::rhs(double *out, int layout)
 {
+    Range nvtx_range("wenofv::rhs");
     if (n != 1) { set_error("rhs is defined for a single instance"); return WENOFV_EINVAL; }
     WENOFV_CUDA(cudaSetDevice(device));
     const InstDesc &d = desc_[0];
@@ -584,6 +596,7 @@ void Engine::drop_graphs()
 // K captured pairs of RK steps (buffer roles return to buffer 0 after each pair)
 int Engine::run_graph(int K)
 {
+    Range nvtx_range("wenofv::run_graph");
     auto it = graphs_.find(K);
     if (it == graphs_.end()) {
         cudaGraph_t g;
@@ -621,6 +634,7 @@ int Engine::normalize_buffers()
 
 int Engine::advance(const double *t0, const double *t_end, int64_t max_steps, double *t_out, int64_t *nsteps)
 {
+    Range nvtx_range("wenofv::advance");
     WENOFV_CUDA(cudaSetDevice(device));
     // every instance's state into buffer 0, where the captured step pairs start
     for (int i = 0; i < n; i++) h_state_[i].cur_buf = cur_;
