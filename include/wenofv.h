@@ -64,7 +64,8 @@ enum {
     WENOFV_FLAG_NAN_DT = 1u,     /* NaN in the CFL time step (src/WENOFV.cpp:502-531) */
     WENOFV_FLAG_BAD_THETA = 2u,  /* limiter theta outside [0,1] (src/WENOFV.cpp:1927-1932) */
     WENOFV_FLAG_NAN_FLUX = 4u,   /* NaN Riemann flux (include/Equations.hpp:345-359) */
-    WENOFV_FLAG_NAN_STATE = 8u   /* NaN in an updated cell average */
+    WENOFV_FLAG_NAN_STATE = 8u,  /* NaN in an updated cell average */
+    WENOFV_FLAG_BOUNDS = 16u     /* an index outside its buffer (self-checking build only) */
 };
 
 /* Equation parameters.  Field order and meaning of rho10..preb follow TwoPhaseEquation's

@@ -693,9 +693,9 @@ static void fill_ghosts(ofv_ws *w, const double *U)
                 if (w->p->bc == OFV_BC_OUTFLOW) {
                     si = i < 0 ? 0 : (i >= nx ? nx - 1 : i);
                     sj = j < 0 ? 0 : (j >= ny ? ny - 1 : j);
-                } else {
-                    si = (i + nx) % nx;
-                    sj = (j + ny) % ny;
+                } else { /* a true modulo: grids narrower than the 3 ghost layers wrap more than once */
+                    si = ((i % nx) + nx) % nx;
+                    sj = ((j % ny) + ny) % ny;
                 }
                 *Ecell(w, v, i, j) = U[(size_t)v * nx * ny + (size_t)sj * nx + si];
             }

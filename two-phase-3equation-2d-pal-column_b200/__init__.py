@@ -15,14 +15,15 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libwenofv_b200.so")
+# WENOFV_LIB selects another build of the library, e.g. lib/libwenofv_b200_checked.so
+LIB_PATH = os.environ.get("WENOFV_LIB") or os.path.join(HERE, "lib", "libwenofv_b200.so")
 
 OK, EINVAL, ENOMEM, ENUMERIC, ETIMEDOUT, ECUDA, ENOTSUP, EBUSY, ENOTFOUND = range(9)
 EQ_TWO_PHASE, EQ_LINEAR_ADV, EQ_EULER = 0, 1, 2
 BC_PERIOD, BC_OUTFLOW = 0, 5
 FP64, FP64_STRICT, FP32_BULK = 0, 1, 2
 LAYOUT_SOA, LAYOUT_REF_AOS = 0, 1
-FLAG_NAN_DT, FLAG_BAD_THETA, FLAG_NAN_FLUX, FLAG_NAN_STATE = 1, 2, 4, 8
+FLAG_NAN_DT, FLAG_BAD_THETA, FLAG_NAN_FLUX, FLAG_NAN_STATE, FLAG_BOUNDS = 1, 2, 4, 8, 16
 
 # every entry point declared in include/wenofv.h
 EXPORTS = (

@@ -682,7 +682,7 @@ int Engine::advance(const double *t0, const double *t_end, int64_t max_steps, do
     rc = normalize_buffers();
     if (rc) return rc;
     WENOFV_CUDA(cudaStreamSynchronize(stream));
-    if (flags & (WENOFV_FLAG_NAN_DT | WENOFV_FLAG_BAD_THETA | WENOFV_FLAG_NAN_FLUX | WENOFV_FLAG_NAN_STATE)) {
+    if (flags & (WENOFV_FLAG_NAN_DT | WENOFV_FLAG_BAD_THETA | WENOFV_FLAG_NAN_FLUX | WENOFV_FLAG_NAN_STATE | WENOFV_FLAG_BOUNDS)) {
         set_error("numerical error flags 0x%x", flags);
         return WENOFV_ENUMERIC;
     }

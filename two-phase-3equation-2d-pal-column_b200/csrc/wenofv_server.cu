@@ -135,7 +135,7 @@ int wenofv_server::round()
         const InstState s = eng.slot_state(r->slot);
         if (!s.done) continue;
         int st = eng.download(r->slot, r->U.data(), WENOFV_LAYOUT_SOA);
-        if (!st && (s.flags & (WENOFV_FLAG_NAN_DT | WENOFV_FLAG_BAD_THETA | WENOFV_FLAG_NAN_FLUX | WENOFV_FLAG_NAN_STATE)))
+        if (!st && (s.flags & (WENOFV_FLAG_NAN_DT | WENOFV_FLAG_BAD_THETA | WENOFV_FLAG_NAN_FLUX | WENOFV_FLAG_NAN_STATE | WENOFV_FLAG_BOUNDS)))
             st = WENOFV_ENUMERIC;
         eng.remove(r->slot);
         std::lock_guard<std::mutex> lk(mu);

@@ -22,6 +22,13 @@
 #pragma once
 #include "wenofv_math.cuh"
 
+// WENOFV_CHECK_BOUNDS=1 builds the self-checking variant (lib/libwenofv_b200_checked.so):
+// every global index of the stage kernel is checked against its buffer before the access,
+// and a violation sets WENOFV_FLAG_BOUNDS with the cell instead of touching the memory
+#ifndef WENOFV_CHECK_BOUNDS
+#define WENOFV_CHECK_BOUNDS 0
+#endif
+
 namespace wenofv {
 #if WENOFV_STRICT
 namespace strict {
@@ -149,7 +156,8 @@ template <int EQ> struct StageSmem {
 
 // one row of NV x P stage values into shared memory (ghost fill = index map), cp.async 8 B
 template <int EQ>
-__device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ>::PS], const double *buf, const InstDesc &D, int row, int i0)
+__device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ>::PS], const double *buf, const InstDesc &D, int row, int i0,
+                                         InstState *st)
 {
     constexpr int P = StageGeom<EQ>::P, NV = StageGeom<EQ>::NV;
     const int jj = map_index(row, D.ny, D.bc);
@@ -158,6 +166,14 @@ __device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ>::PS], const
     for (int e = threadIdx.x; e < NV * P; e += NT) {
         const int v = e / P, p = e - v * P;
         const int ii = map_index(i0 - G + p, D.nx, D.bc);
+#if WENOFV_CHECK_BOUNDS
+        if (jj < 0 || jj >= D.ny || ii < 0 || ii >= D.nx) { // record and skip the access
+            flag_error(st, 16u /* WENOFV_FLAG_BOUNDS */, (long long)row * D.nx + (i0 - G + p));
+            continue;
+        }
+#else
+        (void)st;
+#endif
         cp_async8(&dst[v][p], buf + v * plane + (size_t)jj * D.pitch + ii);
     }
 }
@@ -530,6 +546,12 @@ __device__ __forceinline__ double phase_update(StageSmem<EQ> &S, const InstDesc 
     else Unew = L.A * Un + L.B * U + L.C * dt * rhs;
     const size_t plane = (size_t)D.ny * D.pitch;
     const size_t off = v * plane + (size_t)q * D.pitch + i0 + c;
+#if WENOFV_CHECK_BOUNDS
+    if (act && (q < 0 || q >= D.ny || i0 + c >= D.nx || off >= (size_t)NV * plane)) {
+        flag_error(st, 16u /* WENOFV_FLAG_BOUNDS */, (long long)q * D.nx + i0 + c);
+        return cmin;
+    }
+#endif
     if (act) {
         if (L.rhs_out) L.rhs_out[off] = rhs;
         else D.buf[L.bout][off] = Unew;
@@ -570,6 +592,12 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
         if (st->done) continue;
         const double dt = st->dt;
         const int TXe = min(TX, D.nx - it.i0);
+#if WENOFV_CHECK_BOUNDS
+        if (it.i0 < 0 || it.i0 >= D.nx || it.j0 < 0 || it.j1 > D.ny || it.j0 >= it.j1) { // a malformed work item
+            if (threadIdx.x == 0) flag_error(st, 16u /* WENOFV_FLAG_BOUNDS */, (long long)it.j0 * D.nx + it.i0);
+            continue;
+        }
+#endif
         for (int c = threadIdx.x; c < TX; c += NT) {
             const int i = min(it.i0 + c, D.nx - 1);
             S.sdxc[c] = D.dxc[i];
@@ -582,15 +610,15 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
         const double *bin = D.buf[L.bin];
         const double *bun = D.buf[L.bun];
 #pragma unroll 1
-        for (int m = 0; m < 5; m++) load_row<EQ>(S.su[(it.j0 - G + m) & 7], bin, D, it.j0 - G + m, it.i0);
+        for (int m = 0; m < 5; m++) load_row<EQ>(S.su[(it.j0 - G + m) & 7], bin, D, it.j0 - G + m, it.i0, st);
         cp_async_commit();
         double cmin = __longlong_as_double(0x7ff0000000000000LL);
 #pragma unroll 1
         for (int r = it.j0 - 1; r <= it.j1; r++) {
             cp_async_wait_all();
             __syncthreads();
-            if (r + 3 <= it.j1 + 2) load_row<EQ>(S.su[(r + 3) & 7], bin, D, r + 3, it.i0);
-            if (!L.first_stage && r >= it.j0 && r < it.j1) load_row<EQ>(S.sun[r & 1], bun, D, r, it.i0);
+            if (r + 3 <= it.j1 + 2) load_row<EQ>(S.su[(r + 3) & 7], bin, D, r + 3, it.i0, st);
+            if (!L.first_stage && r >= it.j0 && r < it.j1) load_row<EQ>(S.sun[r & 1], bun, D, r, it.i0, st);
             cp_async_commit();
             if (r == it.j0 - 1) { // eigensystems of the first row; later rows come from phase 3
                 phase_eigen<EQ, RECON>(S, D, r, 0, NT);
