@@ -140,6 +140,20 @@ void *wenofv_stream(wenofv_ctx *ctx);
  * plane stride pitch*ny (valid until the next step) */
 int wenofv_device_state(wenofv_ctx *ctx, double **U, int *pitch);
 
+/* The reference's periodic test cases (TESTCASE 0 SMOOTH, 1 VORTEX, 2 SHARP) with the
+ * velocity and volume-fraction floor of TwoPhaseEquation::setEquationParameters
+ * (include/Equations.hpp:490-689); the phase parameters are the context's. */
+typedef struct {
+    int testcase;
+    double u0, v0, epsa;
+} wenofv_testcase;
+/* CWENOFV::initializeAve (src/WENOFV.cpp:232-279) on the GPU: the 4x4 Gauss-Legendre
+ * averages of getU0 (include/Equations.hpp:979-1002) over the slab grid, written as the
+ * context's state (the device sin/exp differ from the host C library's by a few ulp) */
+int wenofv_init_testcase(wenofv_ctx *ctx, const wenofv_testcase *tc);
+/* CWENOFV::outputAccuracy (src/WENOFV.cpp:3152-3251) on the GPU: norms = (L_inf, L1, L2) of
+ * the volume fraction against the initial data translated by (u0, v0) t */
+int wenofv_accuracy(wenofv_ctx *ctx, const wenofv_testcase *tc, double t, double norms[3]);
 /* One SSP-RK step (cfg->rk_method) of a caller-owned device state without allocating any
  * device memory: for callers that cannot call cudaMalloc (they manage GPU memory through
  * their own pool or framework allocator, which a direct cudaMalloc would bypass and may

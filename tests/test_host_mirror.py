@@ -171,3 +171,44 @@ def test_host_writes_the_reference_output_files(host_bin, tmp_path):
     assert acc[0] == "Cell Number, Linf-norm, L1-norm, L2-norm"
     vals = [float(x) for x in acc[1].split(",")]
     assert vals[0] == 100 and np.allclose(vals[1:], SMOOTH_KNOWN[0][1], rtol=1e-6, atol=0)
+
+
+# the periodic cases' (u0, v0, epsa): include/Equations.hpp:490-689
+CASE_FLOW = {0: (1.0, 1.0, 1e-8), 1: (2.0, 2.0, 1e-4), 2: (1.0, 1.0, 1e-8)}
+CASE_BOX = {0: (0.0, 1.0, 0.0, 1.0), 1: (-1.0, 1.0, -1.0, 1.0), 2: (0.0, 1.0, 0.0, 1.0)}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("testcase", [0, 1, 2])
+def test_device_initial_averages(wb, host_bin, tmp_path, testcase):
+    # wenofv_init_testcase against the host mirror's averages (which equal the reference's)
+    nx, ny = 32, 24
+    path = str(tmp_path / "ic.bin")
+    assert run_host(host_bin, f"TESTCASE={testcase}", f"ELEMNUMX={nx}", f"ELEMNUMY={ny}", dump_ic=path).returncode == 0
+    host = to_soa(np.fromfile(path), nx, ny)
+    r10, r20, c1, c2 = CASE_PARAMS[testcase]
+    xl, xr, yl, yr = CASE_BOX[testcase]
+    cfg = wb.make_config(nx, ny, xl=xl, xr=xr, yl=yl, yr=yr, ref_slabs=4)
+    with wb.Solver(cfg, wb.make_eq(rho10=r10, rho20=r20, sound1=c1, sound2=c2)) as s:
+        s.init_testcase(testcase, *CASE_FLOW[testcase])
+        dev = s.download()
+    assert np.abs(dev - host).max() <= 1e-14 * np.abs(host).max()
+
+
+@pytest.mark.gpu
+def test_device_accuracy_known_answer(wb):
+    # SMOOTH 128^2, WENO-JS, conservative, LLF, RK3 to t = 0.05, initialised and measured on
+    # the GPU: the reference's own accuracy report (one-rank run)
+    n = 128
+    cfg = wb.make_config(n, n, rk=2, cfl=0.5, scheme=0, flux=0, recon=0, limiter=0, ref_slabs=1,
+                         precision=wb.FP64_STRICT)
+    with wb.Solver(cfg, wb.make_eq(rho10=1.2, rho20=1.0, sound1=1.0, sound2=1.0)) as s:
+        s.init_testcase(0, *CASE_FLOW[0])
+        t, k = s.advance(0.05)
+        norms = s.accuracy(0, *CASE_FLOW[0], t)
+        U = s.download()
+    assert k == 52
+    assert np.allclose(norms, SMOOTH_KNOWN[1][1], rtol=1e-6, atol=0)
+    # the errors are ~1e-7 differences of O(1) averages, so a 1-ulp change of the exact
+    # solution's sin (device against numpy) moves them by ~1e-9 relative
+    assert np.allclose(norms, smooth_accuracy(U, n, t), rtol=1e-8, atol=0)

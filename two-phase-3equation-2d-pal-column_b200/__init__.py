@@ -30,7 +30,7 @@ EXPORTS = (
     "wenofv_abi_version", "wenofv_strerror", "wenofv_last_error", "wenofv_default_config",
     "wenofv_create", "wenofv_destroy", "wenofv_upload", "wenofv_download", "wenofv_compute_dt",
     "wenofv_step", "wenofv_rhs", "wenofv_advance", "wenofv_status", "wenofv_synchronize",
-    "wenofv_stream", "wenofv_device_state", "wenofv_step_noalloc",
+    "wenofv_stream", "wenofv_device_state", "wenofv_step_noalloc", "wenofv_init_testcase", "wenofv_accuracy",
     "wenofv_batch_create", "wenofv_batch_destroy", "wenofv_batch_upload", "wenofv_batch_download",
     "wenofv_batch_advance", "wenofv_batch_set_tiling", "wenofv_batch_stream", "wenofv_batch_autotune",
     "wenofv_server_create", "wenofv_server_destroy", "wenofv_server_submit", "wenofv_server_poll",
@@ -53,6 +53,10 @@ class Config(C.Structure):
                 ("cfl", C.c_double), ("scheme", C.c_int), ("pp_limiter", C.c_int),
                 ("riemann_flux", C.c_int), ("reconstruction", C.c_int), ("ref_slabs", C.c_int),
                 ("precision", C.c_int), ("device", C.c_int)]
+
+
+class TestCase(C.Structure):
+    _fields_ = [("testcase", C.c_int), ("u0", C.c_double), ("v0", C.c_double), ("epsa", C.c_double)]
 
 
 class RequestInfo(C.Structure):
@@ -121,6 +125,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.wenofv_probe_riemann.argtypes = [C.POINTER(EqParams), I, I, DP, DP, I, D, D, DP, I]
     L.wenofv_probe_eigen.argtypes = [C.POINTER(EqParams), I, DP, I, D, D, DP, DP, I]
     L.wenofv_probe_fma_peak.argtypes = [I, I, DP]
+    L.wenofv_init_testcase.argtypes = [P, C.POINTER(TestCase)]
+    L.wenofv_accuracy.argtypes = [P, C.POINTER(TestCase), D, DP]
     L.wenofv_step_noalloc.argtypes = [C.POINTER(Config), C.POINTER(EqParams), P, P, I, D, P, C.POINTER(C.c_uint32)]
     _lib = L
     return L
@@ -194,6 +200,18 @@ class Solver:
             raise ValueError("need a C-contiguous float64 array of the state's size")
         _check(self.L.wenofv_download(self.h, _dp(out), layout), "wenofv_download")
         return out
+
+    def init_testcase(self, testcase: int, u0: float, v0: float, epsa: float):
+        """the reference's initial averages of a periodic test case, computed on the GPU"""
+        tc = TestCase(testcase, u0, v0, epsa)
+        _check(self.L.wenofv_init_testcase(self.h, C.byref(tc)), "wenofv_init_testcase")
+
+    def accuracy(self, testcase: int, u0: float, v0: float, epsa: float, t: float):
+        """(L_inf, L1, L2) of z1 against the translated initial data, computed on the GPU"""
+        tc = TestCase(testcase, u0, v0, epsa)
+        out = np.zeros(3)
+        _check(self.L.wenofv_accuracy(self.h, C.byref(tc), t, _dp(out)), "wenofv_accuracy")
+        return tuple(out)
 
     def compute_dt(self) -> float:
         d = C.c_double()

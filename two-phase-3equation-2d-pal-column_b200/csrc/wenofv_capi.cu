@@ -75,6 +75,17 @@ int wenofv_create(const wenofv_config *cfg, const wenofv_eq_params *eq, wenofv_c
 
 void wenofv_destroy(wenofv_ctx *ctx) { delete ctx; }
 
+int wenofv_init_testcase(wenofv_ctx *ctx, const wenofv_testcase *tc)
+{
+    if (!ctx || !tc) { set_error("null argument"); return WENOFV_EINVAL; }
+    return ctx->eng.init_testcase(0, tc);
+}
+int wenofv_accuracy(wenofv_ctx *ctx, const wenofv_testcase *tc, double t, double norms[3])
+{
+    if (!ctx || !tc || !norms) { set_error("null argument"); return WENOFV_EINVAL; }
+    return ctx->eng.accuracy(0, tc, t, norms);
+}
+
 int wenofv_upload(wenofv_ctx *ctx, const double *U, int layout)
 {
     if (!ctx) { set_error("null context"); return WENOFV_EINVAL; }

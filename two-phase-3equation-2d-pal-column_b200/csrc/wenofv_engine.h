@@ -50,6 +50,8 @@ public:
     int set_tiling(int rows, int ctas_per_sm);
     int autotune(int *rows, int *ctas_per_sm, double *best_ms);
     int device_state(int i, double **U, int *pitch);
+    int init_testcase(int i, const wenofv_testcase *tc);                      // wenofv_init.cu
+    int accuracy(int i, const wenofv_testcase *tc, double t, double *norms); // wenofv_init.cu
 
     // ---- slots (serving): capacity fixed at init_slots, instances added and removed ----
     int init_slots(int capacity, int device, int rk_method);
