@@ -329,11 +329,14 @@ int Engine::build_work()
         if (!live_[i]) continue;
         const int strict = cfg_[i].precision == WENOFV_FP64_STRICT;
         const int fp32 = cfg_[i].precision == WENOFV_FP32_BULK;
-        const long key = ((long)strict << 24) | (fp32 << 16) | (desc_[i].eq_kind << 8) | desc_[i].recon;
+        const int sch = desc_[i].scheme, flx = desc_[i].eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : desc_[i].flux;
+        const long key = ((long)strict << 32) | ((long)fp32 << 24) | (desc_[i].eq_kind << 16) | (desc_[i].recon << 8) |
+                         (sch << 4) | flx;
         auto it = key2g.find(key);
         if (it == key2g.end()) {
             Group g;
             g.ns_strict = strict; g.fp32 = fp32; g.eq = desc_[i].eq_kind; g.recon = desc_[i].recon;
+            g.scheme = sch; g.flux = flx;
             key2g[key] = (int)groups_.size();
             groups_.push_back(g);
             it = key2g.find(key);
@@ -342,8 +345,8 @@ int Engine::build_work()
     }
     for (Group &g : groups_) {
         const int tx = g.ns_strict ? strict::stage_tx(g.eq) : fast::stage_tx(g.eq);
-        const int bps = std::max(1, g.ns_strict ? strict::stage_blocks_per_sm(g.eq, g.recon, g.fp32)
-                                                : fast::stage_blocks_per_sm(g.eq, g.recon, g.fp32));
+        const int bps = std::max(1, g.ns_strict ? strict::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux)
+                                                : fast::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux));
         const int slots = sms_ * (ctas_per_sm_ > 0 ? std::min(ctas_per_sm_, bps) : bps);
         long strips_rows = 0;
         for (int i : g.inst) strips_rows += (long)((cfg_[i].nx + tx - 1) / tx) * cfg_[i].ny;
@@ -407,8 +410,8 @@ int Engine::launch_stage_all(int parity, int stage, double *rhs_out)
             L.rk1 = rk == 0;
             stage_coeffs(rk, stage, L.A, L.B, L.C);
         }
-        const int rc = g.ns_strict ? strict::launch_stage(g.eq, g.recon, g.fp32, L, g.grid, stream)
-                                   : fast::launch_stage(g.eq, g.recon, g.fp32, L, g.grid, stream);
+        const int rc = g.ns_strict ? strict::launch_stage(g.eq, g.recon, g.fp32, g.scheme, g.flux, L, g.grid, stream)
+                                   : fast::launch_stage(g.eq, g.recon, g.fp32, g.scheme, g.flux, L, g.grid, stream);
         if (rc) return cuda_fail((cudaError_t)rc, "stage kernel launch");
     }
     return WENOFV_OK;

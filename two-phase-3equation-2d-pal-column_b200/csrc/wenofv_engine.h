@@ -72,7 +72,7 @@ public:
 
 private:
     struct Group {
-        int ns_strict, fp32, eq, recon;
+        int ns_strict, fp32, eq, recon, scheme, flux;
         std::vector<int> inst;
         WorkItem *d_work = nullptr;
         int nwork = 0;

@@ -23,37 +23,43 @@ namespace fast {
 
 int stage_tx(int eq) { return eq == EQ_LINEAR_ADV ? StageGeom<EQ_LINEAR_ADV>::TX : StageGeom<EQ_TWO_PHASE>::TX; }
 
-template <int EQ, int RECON, class R> static const void *stage_fn() { return (const void *)stage_kernel<EQ, RECON, R>; }
-
-static const void *pick_stage(int eq, int recon, int fp32)
+template <int EQ, int RECON, class R, int SCH, int FLX> static const void *stage_fn()
 {
-#if WENOFV_HAS_FP32
-    if (fp32) {
-        switch (eq) {
-        case EQ_TWO_PHASE:
-            return recon == 1 ? stage_fn<EQ_TWO_PHASE, 1, float>() : recon == 2 ? stage_fn<EQ_TWO_PHASE, 2, float>()
-                 : recon == 3 ? stage_fn<EQ_TWO_PHASE, 3, float>() : stage_fn<EQ_TWO_PHASE, 0, float>();
-        case EQ_EULER: return recon ? stage_fn<EQ_EULER, 1, float>() : stage_fn<EQ_EULER, 0, float>();
-        case EQ_LINEAR_ADV: return stage_fn<EQ_LINEAR_ADV, 0, float>();
-        default: return nullptr;
-        }
-    }
-#else
-    if (fp32) return nullptr;
-#endif
+    return (const void *)stage_kernel<EQ, RECON, R, SCH, FLX>;
+}
+// the scheme and flux of a launch group as template arguments (scalar advection has one flux)
+template <int EQ, int RECON, class R> static const void *pick_sf(int scheme, int flux)
+{
+    if (EQ == EQ_LINEAR_ADV) return scheme ? stage_fn<EQ, RECON, R, 1, 0>() : stage_fn<EQ, RECON, R, 0, 0>();
+    if (scheme) return flux ? stage_fn<EQ, RECON, R, 1, 1>() : stage_fn<EQ, RECON, R, 1, 0>();
+    return flux ? stage_fn<EQ, RECON, R, 0, 1>() : stage_fn<EQ, RECON, R, 0, 0>();
+}
+template <class R> static const void *pick_eq(int eq, int recon, int scheme, int flux)
+{
     switch (eq) {
     case EQ_TWO_PHASE:
-        return recon == 1 ? stage_fn<EQ_TWO_PHASE, 1, double>() : recon == 2 ? stage_fn<EQ_TWO_PHASE, 2, double>()
-             : recon == 3 ? stage_fn<EQ_TWO_PHASE, 3, double>() : stage_fn<EQ_TWO_PHASE, 0, double>();
-    case EQ_EULER: return recon ? stage_fn<EQ_EULER, 1, double>() : stage_fn<EQ_EULER, 0, double>();
-    case EQ_LINEAR_ADV: return stage_fn<EQ_LINEAR_ADV, 0, double>();
+        return recon == 1 ? pick_sf<EQ_TWO_PHASE, 1, R>(scheme, flux) : recon == 2 ? pick_sf<EQ_TWO_PHASE, 2, R>(scheme, flux)
+             : recon == 3 ? pick_sf<EQ_TWO_PHASE, 3, R>(scheme, flux) : pick_sf<EQ_TWO_PHASE, 0, R>(scheme, flux);
+    case EQ_EULER: return recon ? pick_sf<EQ_EULER, 1, R>(scheme, flux) : pick_sf<EQ_EULER, 0, R>(scheme, flux);
+    case EQ_LINEAR_ADV: return pick_sf<EQ_LINEAR_ADV, 0, R>(scheme, flux);
     default: return nullptr;
     }
 }
 
-int launch_stage(int eq, int recon, int fp32, const StageLaunch &L, int grid, void *stream)
+static const void *pick_stage(int eq, int recon, int fp32, int scheme, int flux)
 {
-    const void *fn = pick_stage(eq, recon, fp32);
+    if (scheme < 0 || scheme > 1 || flux < 0 || flux > 1) return nullptr;
+#if WENOFV_HAS_FP32
+    if (fp32) return pick_eq<float>(eq, recon, scheme, flux);
+#else
+    if (fp32) return nullptr;
+#endif
+    return pick_eq<double>(eq, recon, scheme, flux);
+}
+
+int launch_stage(int eq, int recon, int fp32, int scheme, int flux, const StageLaunch &L, int grid, void *stream)
+{
+    const void *fn = pick_stage(eq, recon, fp32, scheme, flux);
     if (!fn) return (int)cudaErrorInvalidValue;
     void *args[] = {(void *)&L};
     return (int)cudaLaunchKernel(fn, dim3(grid), dim3(NT), args, 0, (cudaStream_t)stream);
@@ -68,9 +74,9 @@ int launch_cfl(int eq, const StageLaunch &L, int grid, void *stream)
     return (int)cudaLaunchKernel(fn, dim3(grid), dim3(NT), args, 0, (cudaStream_t)stream);
 }
 
-int stage_blocks_per_sm(int eq, int recon, int fp32)
+int stage_blocks_per_sm(int eq, int recon, int fp32, int scheme, int flux)
 {
-    const void *fn = pick_stage(eq, recon, fp32);
+    const void *fn = pick_stage(eq, recon, fp32, scheme, flux);
     if (!fn) return 0;
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, NT, 0) != cudaSuccess) return 0;

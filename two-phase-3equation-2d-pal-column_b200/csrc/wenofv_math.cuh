@@ -84,7 +84,9 @@ template <class R> __device__ __forceinline__ void weno_betas(R umm, R um, R u, 
 // One 5-point stencil prepared once and evaluated at several Gauss-Lobatto points: the
 // smoothness indicators (and WENO-Z's normalisation) depend on the stencil only, so they
 // are shared across points, which reproduces the per-point reference calls bit for bit.
-template <class R> struct Weno5 {
+// ZS: the scheme as a compile-time constant (0 WENO-JS, 1 WENO-Z) in the stage kernels, or -1
+// to take it from init's argument (the pointwise probes)
+template <class R, int ZS = -1> struct Weno5 {
     R umm, um, u, up, upp; // raw values (candidate polynomials use these)
     R g0, g1, g2;          // JS: (eps+beta_k)^2 [strict] or 1/(eps+beta_k)^2 [fast]; Z: 1 + tau/(beta_k+eps)
     int z;
@@ -100,12 +102,13 @@ template <class R> struct Weno5 {
     __device__ __forceinline__ void init(int scheme, R v0, R v1, R v2, R v3, R v4)
     {
         umm = v0; um = v1; u = v2; up = v3; upp = v4;
-        z = scheme;
+        const int sch = ZS < 0 ? scheme : ZS;
+        z = sch;
         if constexpr (SHARED) {
             R b0, b1, b2;
             weno_betas(v0, v1, v2, v3, v4, b0, b1, b2);
             R a0, a1, a2;
-            if (scheme == 1) {
+            if (sch == 1) {
                 const R umax = std_max(std_max(std_max(v0, v1), std_max(v4, v3)), v2);
                 const R umin = std_min(std_min(std_min(v0, v1), std_min(v4, v3)), v2);
                 const R sc = umax - umin + R(1e-20);
@@ -119,7 +122,7 @@ template <class R> struct Weno5 {
             const R a01 = a0 * a1;
             const R inv = R(1) / (a01 * a2);
             const R r0 = a1 * a2 * inv, r1 = a0 * a2 * inv, r2 = a01 * inv;
-            if (scheme == 1) {
+            if (sch == 1) {
                 const R tau = fabs(b0 - b2);
                 g0 = R(1) + tau * r0; g1 = R(1) + tau * r1; g2 = R(1) + tau * r2;
             } else {
@@ -127,7 +130,7 @@ template <class R> struct Weno5 {
             }
             return;
         }
-        if (scheme == 1) {
+        if (sch == 1) {
             // WENO-Z: normalise the stencil to [0,1], include/Utility.hpp:261-268
             const R umax = std_max(std_max(std_max(v0, v1), std_max(v4, v3)), v2);
             const R umin = std_min(std_min(std_min(v0, v1), std_min(v4, v3)), v2);
@@ -172,7 +175,7 @@ template <class R> struct Weno5 {
         weno_d<R, GP>(d0, d1, d2);
         weno_h<R, GP>(umm, um, u, up, upp, h0, h1, h2);
         R w0, w1, w2;
-        if (z) {
+        if ((ZS < 0 ? z : ZS) != 0) {
             w0 = d0 * g0; w1 = d1 * g1; w2 = d2 * g2;
         } else {
 #if WENOFV_STRICT
@@ -844,9 +847,12 @@ template <int EQ, class R> __device__ __forceinline__ void max_eigs(const EqPara
 // getRiemannFlux dispatch (include/Equations.hpp:329-343); flux 0 LLF, 1 HLLC.
 // For scalar advection both are the upwind (LLF with |a.n|) flux.
 // The face states come in FP64 and the flux goes out in FP64 in every form.
-template <int EQ, class R>
-__device__ __forceinline__ void riemann(const EqParams &P, int flux, const double *ULd, const double *URd, double *F, bool xdir)
+// FL: the flux as a compile-time constant (0 LLF, 1 HLLC) in the stage kernels, or -1 to take
+// it from the argument (the pointwise probes)
+template <int EQ, class R, int FL = -1>
+__device__ __forceinline__ void riemann(const EqParams &P, int flux_arg, const double *ULd, const double *URd, double *F, bool xdir)
 {
+    const int flux = FL < 0 ? flux_arg : FL;
     constexpr int NV = EqTraits<EQ>::NV;
     constexpr bool F32 = sizeof(R) < sizeof(double);
     R UL[NV], UR[NV], Fr[NV];

@@ -162,7 +162,9 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
 
     int sms = 0;
     WENOFV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device));
-    const int bps = strictf ? strict::stage_blocks_per_sm(eq->eq_kind, recon, fp32) : fast::stage_blocks_per_sm(eq->eq_kind, recon, fp32);
+    const int flx = eq->eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : cfg->riemann_flux;
+    const int bps = strictf ? strict::stage_blocks_per_sm(eq->eq_kind, recon, fp32, cfg->scheme, flx)
+                            : fast::stage_blocks_per_sm(eq->eq_kind, recon, fp32, cfg->scheme, flx);
     const int grid = (int)(k < (long)sms * (bps > 0 ? bps : 1) ? k : (long)sms * (bps > 0 ? bps : 1));
     for (int stage = 0; stage < stage_count(cfg->rk_method); stage++) {
         const Roles ro = stage_roles(cfg->rk_method, 0, stage);
@@ -180,8 +182,8 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
         L.final_stage = stage == stage_count(cfg->rk_method) - 1;
         L.rk1 = cfg->rk_method == 0;
         stage_coeffs(cfg->rk_method, stage, L.A, L.B, L.C);
-        const int lrc = strictf ? strict::launch_stage(eq->eq_kind, recon, 0, L, grid, stream)
-                                : fast::launch_stage(eq->eq_kind, recon, fp32, L, grid, stream);
+        const int lrc = strictf ? strict::launch_stage(eq->eq_kind, recon, 0, cfg->scheme, flx, L, grid, stream)
+                                : fast::launch_stage(eq->eq_kind, recon, fp32, cfg->scheme, flx, L, grid, stream);
         if (lrc) return cuda_fail((cudaError_t)lrc, "stage kernel launch");
     }
     if (flags) {

@@ -215,7 +215,7 @@ __device__ __forceinline__ void phase_eigen(StageSmem<EQ> &S, const InstDesc &D,
 // the deviations from the column's centre average (WENO is translation invariant), so that
 // FP32 rounds the small differences, not the large averages; the result is re-anchored in
 // FP64.
-template <int EQ, int RECON, class R>
+template <int EQ, int RECON, class R, int SCH>
 __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D, int r)
 {
     constexpr int NV = StageGeom<EQ>::NV;
@@ -239,7 +239,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
             }
         }
         const double c0 = DEV ? st[2] : 0.0;
-        Weno5<R> W;
+        Weno5<R, SCH> W;
         W.init(D.scheme, (R)(st[0] - c0), (R)(st[1] - c0), (R)(st[2] - c0), (R)(st[3] - c0), (R)(st[4] - c0));
         R o[4];
         W.eval4(o);
@@ -270,7 +270,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
             for (int j = 0; j < NV; j++) s += Lrow[j] * S.su[(r - 2 + m) & 7][j][p];
             pr[m] = DEV ? (R)(s - lc) : (R)s;
         }
-        Weno5<R> W;
+        Weno5<R, SCH> W;
         W.init(D.scheme, pr[0], pr[1], pr[2], pr[3], pr[4]);
         R cg[4];
         W.eval4(cg);
@@ -296,7 +296,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
 
 // ---- phase 2: x-direction sweep + limiter of row r (src/WENOFV.cpp:690-721, :836-880,
 //      limiter :1895-2000) -> face states (FP64 in every form) ------------------------------
-template <int EQ, int RECON, class R>
+template <int EQ, int RECON, class R, int SCH>
 __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D, InstState *st, int r, int i0, int TXe)
 {
     constexpr int NV = StageGeom<EQ>::NV, TX = StageGeom<EQ>::TX;
@@ -323,7 +323,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
         }
 #pragma unroll
         for (int gpj = 0; gpj < 4; gpj++) {
-            Weno5<R> W;
+            Weno5<R, SCH> W;
             W.init(D.scheme, (R)(S.sy[c + 1][gpj * NV + v] - cc), (R)(S.sy[c + 2][gpj * NV + v] - cc), (R)(S.sy[c + 3][gpj * NV + v] - cc),
                    (R)(S.sy[c + 4][gpj * NV + v] - cc), (R)(S.sy[c + 5][gpj * NV + v] - cc));
             if (gpj == 0 || gpj == 3) {
@@ -374,7 +374,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
                 for (int j = 0; j < NV; j++) s += Lrow[j] * S.sy[c + 1 + m][gpj * NV + j];
                 pr[m] = DEV ? (R)(s - lc) : (R)s;
             }
-            Weno5<R> W;
+            Weno5<R, SCH> W;
             W.init(D.scheme, pr[0], pr[1], pr[2], pr[3], pr[4]);
             R cg[4];
             const bool all4 = gpj == 0 || gpj == 3;
@@ -464,7 +464,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
 // x-faces of row r (when r is an interior row of the item) and y-faces between rows r-1
 // and r (when r-1 >= j0-1 and r <= j1).  Four consecutive lanes hold the four Gauss
 // points of one face; lane gp = 0 sums them in the reference's order.
-template <int EQ, class R>
+template <int EQ, class R, int FLX>
 __device__ __forceinline__ void phase_riemann(StageSmem<EQ> &S, const InstDesc &D, InstState *st, int r, int i0, int j0, int j1, int TXe)
 {
     constexpr int NV = StageGeom<EQ>::NV, TX = StageGeom<EQ>::TX;
@@ -490,7 +490,7 @@ __device__ __forceinline__ void phase_riemann(StageSmem<EQ> &S, const InstDesc &
 #pragma unroll
             for (int v = 0; v < NV; v++) { UL[v] = S.syt[(r - 1) & 1][f][gp * NV + v]; UR[v] = S.syb[f][gp * NV + v]; }
         }
-        riemann<EQ, R>(D.eq, D.flux, UL, UR, F, xf);
+        riemann<EQ, R, FLX>(D.eq, D.flux, UL, UR, F, xf);
         // gWeight = m_gweights_ref[gp] * (cell size) / 2.0 (src/WENOFV.cpp:1774, :1793)
         const double wq = xf ? gl_weight(gp) * dyr / 2.0 : gl_weight(gp) * S.sdxc[f] / 2.0;
         bool bad = false;
@@ -580,7 +580,9 @@ template <int RECON, class R> struct StageMinBlocks {
     static constexpr int value = sizeof(R) < sizeof(double) ? (RECON == 1 ? 5 : 4) : 3;
 };
 
-template <int EQ, int RECON, class R>
+// SCH, FLX: the scheme (0 WENO-JS, 1 WENO-Z) and flux (0 LLF, 1 HLLC) of every instance of the
+// launch, as compile-time constants (the engine groups instances by them)
+template <int EQ, int RECON, class R, int SCH, int FLX>
 __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_kernel(const StageLaunch L)
 {
     constexpr int TX = StageGeom<EQ>::TX;
@@ -624,11 +626,11 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
                 phase_eigen<EQ, RECON>(S, D, r, 0, NT);
                 __syncthreads();
             }
-            phase_ysweep<EQ, RECON, R>(S, D, r);
+            phase_ysweep<EQ, RECON, R, SCH>(S, D, r);
             __syncthreads();
-            phase_xsweep<EQ, RECON, R>(S, D, st, r, it.i0, TXe);
+            phase_xsweep<EQ, RECON, R, SCH>(S, D, st, r, it.i0, TXe);
             __syncthreads();
-            phase_riemann<EQ, R>(S, D, st, r, it.i0, it.j0, it.j1, TXe);
+            phase_riemann<EQ, R, FLX>(S, D, st, r, it.i0, it.j0, it.j1, TXe);
             // the last warp, idle in the second round of Riemann units, prepares the next
             // row's eigensystems (row r+1 is resident; se is not read until the next row)
             if (threadIdx.x >= NT - 32) phase_eigen<EQ, RECON>(S, D, r + 1, NT - 32, 32);

@@ -57,9 +57,10 @@ struct StageLaunch {
 #define WENOFV_DECLARE_LAUNCHERS(NS)                                                                     \
     namespace NS {                                                                                       \
     int stage_tx(int eq);                                                                                \
-    int launch_stage(int eq, int recon, int fp32, const StageLaunch &L, int grid, void *stream);        \
+    int launch_stage(int eq, int recon, int fp32, int scheme, int flux, const StageLaunch &L, int grid,  \
+                     void *stream);                                                                     \
     int launch_cfl(int eq, const StageLaunch &L, int grid, void *stream);                               \
-    int stage_blocks_per_sm(int eq, int recon, int fp32);                                                \
+    int stage_blocks_per_sm(int eq, int recon, int fp32, int scheme, int flux);                          \
     int probe_weno(int scheme, int fp32, const double *d_st, int n, double *d_out, void *stream);       \
     int probe_riemann(const EqParams &P, int flux, int fp32, const double *d_UL, const double *d_UR,   \
                       int n, int xdir, double *d_F, void *stream);                                       \
