@@ -52,6 +52,8 @@ OFV_CMP(>=)
 
 inline ofv_cnt sqrt(ofv_cnt a) { g_ofv_cnt.sqrt++; return ofv_cnt(std::sqrt(a.v)); }
 inline ofv_cnt fabs(ofv_cnt a) { g_ofv_cnt.abs++; return ofv_cnt(std::fabs(a.v)); }
+// pow(x, n) with a small integer n, as the restated path uses it: n - 1 multiplications
+inline ofv_cnt pow(ofv_cnt a, double n) { g_ofv_cnt.mul += (unsigned long long)(n - 1); return ofv_cnt(std::pow(a.v, n)); }
 inline bool ofv_isnan(ofv_cnt a) { return std::isnan(a.v); }
 
 #endif

@@ -10,6 +10,7 @@ leg of bench.py, and only as the checker.  The product library never loads it.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import json
 import os
@@ -52,7 +53,7 @@ class Problem:
     bc: int = BC_PERIOD
     rk: int = 2              # RKMETH
     cfl: float = 0.5         # CFL
-    scheme: int = 1          # SCHEME (0 WENO-JS, 1 WENO-Z)
+    scheme: int = 1          # SCHEME (0 WENO-JS, 1 WENO-Z, 2 WENOEXP)
     limiter: int = 0         # PPlimiter
     flux: int = 0            # RIEMANNFLUX (0 LLF, 1 HLLC)
     recon: int = 1           # RECONSTRUCTIONTYPE (0 conservative, 1 characteristic)
@@ -94,6 +95,9 @@ class Oracle:
         L.ofv_weno_js.argtypes = [_DP, C.c_int]
         L.ofv_weno_z.restype = C.c_double
         L.ofv_weno_z.argtypes = [_DP, C.c_int]
+        L.ofv_weno_exp.restype = C.c_double
+        L.ofv_weno_exp.argtypes = [_DP, C.c_int, C.c_double]
+        L.ofv_set_cube_rounded.argtypes = [C.c_int]
         for n in ("ofv_volume_frac", "ofv_pressure", "ofv_sound_speed"):
             getattr(L, n).restype = C.c_double
             getattr(L, n).argtypes = [EP, _DP]
@@ -113,9 +117,23 @@ class Oracle:
                                   C.c_void_p]
         self.L = L
 
+    @contextlib.contextmanager
+    def cube_rounded(self):
+        """WENOEXP's l^3 rounded once (the device kernels' form) instead of the C library's
+        pow(l, 3) (the reference's) inside the block.  The switch is process-wide."""
+        self.L.ofv_set_cube_rounded(1)
+        try:
+            yield self
+        finally:
+            self.L.ofv_set_cube_rounded(0)
+
     # pointwise -----------------------------------------------------------------
-    def weno(self, scheme: int, v, gp: int) -> float:
+    def weno(self, scheme: int, v, gp: int, dx: float = 0.0) -> float:
+        """One Gauss-point value: WENO-JS/Z on 5 values, WENOEXP (scheme 2) on 7 and dx."""
         a = np.ascontiguousarray(v, dtype=np.float64)
+        if scheme == 2:
+            assert a.size == 7
+            return self.L.ofv_weno_exp(a, gp, dx)
         return (self.L.ofv_weno_z if scheme == 1 else self.L.ofv_weno_js)(a, gp)
 
     def riemann(self, p: Problem, flux: int, UL, UR, nx: float, ny: float) -> np.ndarray:

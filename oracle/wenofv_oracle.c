@@ -13,8 +13,9 @@
  *      once per (column,row) and shared.
  *   2. Ghost-cell face states arrive in the reference by MPI exchange and a periodic copy
  *      (src/WENOFV.cpp:1558-1668, :1542-1556).  Here they are reconstructed directly from
- *      the 3-layer ghost-filled averages, which applies the same arithmetic to the same
- *      operands as the neighbouring interior cell.
+ *      4-layer ghost-filled averages (the 7-point WENOEXP stencil of a halo cell reaches
+ *      the 4th layer), which applies the same arithmetic to the same operands as the
+ *      neighbouring interior cell.
  */
 #include <math.h>
 #include <stdlib.h>
@@ -35,7 +36,9 @@ typedef double real_t;
 
 #include "wenofv_oracle.h"
 
-#define G 3 /* ghost layers, src/WENOFV.cpp:59 */
+#define G 3  /* ghost layers of the reference's grid, src/WENOFV.cpp:59 */
+#define GE 4 /* ghost layers of the oracle's work arrays: WENOEXP's 7-point stencils of the halo
+                cells reach one layer further than the reference's own stencils */
 
 /* std::min / std::max as used unqualified by the reference (MyMath.h:22 imports std). */
 static inline real_t std_min(real_t a, real_t b) { return (b < a) ? b : a; }
@@ -159,14 +162,98 @@ static real_t weno_z(real_t umm, real_t um, real_t u, real_t up, real_t upp, int
     return w0 * p0 + w1 * p1 + w2 * p2;
 }
 
-/* useWENO dispatch, src/WENOFV.cpp:1873-1893 (WENOEXP is out of scope) */
-static inline real_t weno(int scheme, const real_t *v, int gp)
+/* l^3 of WENOEXP's linear weights.  By default the C library's pow(l, 3), as the reference
+ * calls it (gcc keeps pow(x, 3) a library call without -ffast-math; glibc's pow is within
+ * 0.52 ulp, not always correctly rounded).  ofv_set_cube_rounded(1) selects l^3 rounded once
+ * instead -- the exact square x*x = p + e (e by fma), times x with the exact error of p*x --
+ * the form of the device kernels, so that they can be compared bit for bit. */
+static int g_cube_rn = 0;
+void ofv_set_cube_rounded(int on) { g_cube_rn = on; }
+static real_t cube_of(real_t l)
 {
+#ifndef OFV_COUNTING
+    if (g_cube_rn) {
+        const double x = l, p = x * x, e = fma(x, x, -p), hi = p * x, lo = fma(p, x, -hi);
+        return hi + (lo + e * x);
+    }
+#endif
+    return pow(l, 3);
+}
+
+/* WENOEXP (SCHEME 2), include/Utility.hpp:291-470: the linear weights are cubic polynomials
+ * in lambda^2 h^2 = dif5 / dif3 (from the 6 points on the side of the Gauss point, clipped at
+ * 1, or 0 where |dif3| < dx^4), the smoothness indicators are absolute values on the
+ * normalised stencil, and w_k = d_k (1 + 2 tau^2 / (beta_k^2 + 1e-16)). */
+static real_t weno_exp(const real_t *v7, int gp, double dx)
+{
+    real_t mmm = v7[0], mm = v7[1], m = v7[2], c = v7[3], p = v7[4], pp = v7[5], ppp = v7[6];
+    real_t dif5, dif3;
+    if (gp >= 2) {
+        dif5 = (-mm + 5.0 * m - 10.0 * c + 10.0 * p - 5.0 * pp + ppp);
+        dif3 = (mm - 11.0 * m + 28.0 * c - 28.0 * p + 11.0 * pp - ppp) / 6.0;
+    } else {
+        dif5 = (-mmm + 5.0 * mm - 10.0 * m + 10.0 * c - 5.0 * p + pp);
+        dif3 = (mmm - 11.0 * mm + 28.0 * m - 28.0 * c + 11.0 * p - pp) / 6.0;
+    }
+    real_t l2h2 = 0;
+    if (!(fabs(dif3) < pow(dx, 4))) {
+        l2h2 = dif5 / dif3;
+        if (fabs(l2h2) > 1) l2h2 = 1;
+    }
+    real_t h0, h1, h2, d0, d1, d2;
+    weno_h(gp, mm, m, c, p, pp, &h0, &h1, &h2); /* candidate values from the raw stencil */
+    const real_t l2 = pow(l2h2, 2), l3 = cube_of(l2h2);
+    if (gp == 0 || gp == 3) {
+        const real_t a = 0.3 - 0.057142858 * l2h2 + 0.0071428571 * l2 - 0.00077200577 * l3;
+        const real_t b = 0.6 + 0.078571429 * l2h2 - 0.0101190476 * l2 + 0.00112012987 * l3;
+        const real_t e = 0.1 - 0.021428571 * l2h2 + 0.0029761905 * l2 - 0.00034812410 * l3;
+        d0 = gp == 0 ? a : e; d1 = b; d2 = gp == 0 ? e : a;
+    } else {
+        const real_t a = 0.16108042 - 0.035187607 * l2h2 + 0.0049466098 * l2 - 0.00058211525 * l3;
+        const real_t b = 0.58636364 + 0.087692641 * l2h2 - 0.0120401515 * l2 + 0.00139436871 * l3;
+        const real_t e = 0.25255594 - 0.052505034 * l2h2 + 0.0070935417 * l2 - 0.00081225346 * l3;
+        d0 = gp == 1 ? a : e; d1 = b; d2 = gp == 1 ? e : a;
+    }
+    const real_t umax = std_max(std_max(std_max(mm, m), std_max(c, p)), pp);
+    const real_t umin = std_min(std_min(std_min(mm, m), std_min(c, p)), pp);
+    mm = (mm - umin) / (umax - umin + 1e-20);
+    m = (m - umin) / (umax - umin + 1e-20);
+    c = (c - umin) / (umax - umin + 1e-20);
+    p = (p - umin) / (umax - umin + 1e-20);
+    pp = (pp - umin) / (umax - umin + 1e-20);
+    const real_t beta0 = 1.0 * 1.0 / 2.0 * fabs(mm - 4 * m + 3 * c) + fabs(mm - 2 * m + c);
+    const real_t beta1 = 1.0 * 1.0 / 2.0 * fabs(m - p) + fabs(m - 2 * c + p);
+    const real_t beta2 = 1.0 * 1.0 / 2.0 * fabs(3 * c - 4 * p + pp) + fabs(c - 2 * p + pp);
+    const real_t tau = mm - 4.0 * m + 6.0 * c - 4.0 * p + pp;
+    const double epsilon = 1e-16;
+    real_t w0 = d0 * (1.0 + 2 * pow(tau, 2.0) / (pow(beta0, 2.0) + epsilon));
+    real_t w1 = d1 * (1.0 + 2 * pow(tau, 2.0) / (pow(beta1, 2.0) + epsilon));
+    real_t w2 = d2 * (1.0 + 2 * pow(tau, 2.0) / (pow(beta2, 2.0) + epsilon));
+    const real_t S = w0 + w1 + w2;
+    w0 /= S;
+    w1 /= S;
+    w2 /= S;
+    return w0 * h0 + w1 * h1 + w2 * h2;
+}
+
+/* useWENO dispatch, src/WENOFV.cpp:1873-1893, on a 7-point stencil v7 (the 5-point schemes
+ * use its middle 5) */
+static inline real_t weno7(int scheme, const real_t *v7, int gp, double dx)
+{
+    if (scheme == 2) return weno_exp(v7, gp, dx);
+    const real_t *v = v7 + 1;
     return scheme == 1 ? weno_z(v[0], v[1], v[2], v[3], v[4], gp) : weno_js(v[0], v[1], v[2], v[3], v[4], gp);
 }
 
+
 double ofv_weno_js(const double v[5], int gp) { return weno_js(v[0], v[1], v[2], v[3], v[4], gp); }
 double ofv_weno_z(const double v[5], int gp) { return weno_z(v[0], v[1], v[2], v[3], v[4], gp); }
+double ofv_weno_exp(const double v[7], int gp, double dx)
+{
+    real_t r[7];
+    for (int k = 0; k < 7; k++) r[k] = v[k];
+    return (double)weno_exp(r, gp, dx);
+}
 
 /* ------------------------------------------------------------------------------------ */
 /* Two-phase 3-equation model, linear acoustic EOS (include/Equations.hpp:52-483)         */
@@ -646,23 +733,24 @@ void ofv_metric(const ofv_problem *p, double *dxc, double *dxl, double *dy)
 
 typedef struct {
     const ofv_problem *p;
-    int nx, ny, nv, ex;          /* ex = nx + 2G (extended row length) */
-    real_t *E;                   /* ghost-extended averages [v][(j+G)*ex + i+G] */
-    real_t *Y;                   /* y-sweep [(j+1)*ex + i+G][gp*4+v], rows -1..ny */
+    int nx, ny, nv, ex, H;       /* ex = nx + 2GE (extended row length), H = stencil half-width */
+    real_t *E;                   /* ghost-extended averages [v][(j+GE)*ex + i+GE] */
+    real_t *Y;                   /* y-sweep [(j+1)*ex + i+GE][gp*4+v], rows -1..ny */
     real_t *FS;                  /* face states [(j+1)*(nx+2) + i+1][face*16 + v*4 + gp] */
     real_t *AX, *AY;             /* face averages: AX[(j*(nx+1) + i)*4+v], AY[(j*nx + i)*4+v] */
     double *dxc, *dxl, *dy, dX, dY;
 } ofv_ws;
 
-static inline real_t *Ecell(ofv_ws *w, int v, int i, int j) { return &w->E[(size_t)v * (w->ny + 2 * G) * w->ex + (size_t)(j + G) * w->ex + (i + G)]; }
-static inline real_t *Ycell(ofv_ws *w, int i, int j) { return &w->Y[((size_t)(j + 1) * w->ex + (i + G)) * 16]; }
+static inline real_t *Ecell(ofv_ws *w, int v, int i, int j) { return &w->E[(size_t)v * (w->ny + 2 * GE) * w->ex + (size_t)(j + GE) * w->ex + (i + GE)]; }
+static inline real_t *Ycell(ofv_ws *w, int i, int j) { return &w->Y[((size_t)(j + 1) * w->ex + (i + GE)) * 16]; }
 static inline real_t *Fcell(ofv_ws *w, int i, int j) { return &w->FS[((size_t)(j + 1) * (w->nx + 2) + (i + 1)) * 64]; }
 
 static void ws_init(ofv_ws *w, const ofv_problem *p)
 {
     w->p = p;
-    w->nx = p->nx; w->ny = p->ny; w->nv = ofv_nvar(&p->eq); w->ex = p->nx + 2 * G;
-    w->E = (real_t *)calloc((size_t)w->nv * w->ex * (p->ny + 2 * G), sizeof(real_t));
+    w->nx = p->nx; w->ny = p->ny; w->nv = ofv_nvar(&p->eq); w->ex = p->nx + 2 * GE;
+    w->H = p->scheme == 2 ? 3 : 2;
+    w->E = (real_t *)calloc((size_t)w->nv * w->ex * (p->ny + 2 * GE), sizeof(real_t));
     w->Y = (real_t *)calloc((size_t)w->ex * (p->ny + 2) * 16, sizeof(real_t));
     w->FS = (real_t *)calloc((size_t)(p->nx + 2) * (p->ny + 2) * 64, sizeof(real_t));
     w->AX = (real_t *)calloc((size_t)(p->nx + 1) * p->ny * 4, sizeof(real_t));
@@ -687,8 +775,8 @@ static void fill_ghosts(ofv_ws *w, const double *U)
 {
     const int nx = w->nx, ny = w->ny;
     for (int v = 0; v < w->nv; v++)
-        for (int j = -G; j < ny + G; j++)
-            for (int i = -G; i < nx + G; i++) {
+        for (int j = -GE; j < ny + GE; j++)
+            for (int i = -GE; i < nx + GE; i++) {
                 int si, sj;
                 if (w->p->bc == OFV_BC_OUTFLOW) {
                     si = i < 0 ? 0 : (i >= nx ? nx - 1 : i);
@@ -752,41 +840,41 @@ static void from_primitive(const ofv_eq *e, int recon, const real_t *P, real_t *
 static void y_sweep(ofv_ws *w, int i, int j)
 {
     const ofv_problem *p = w->p;
-    const int nv = w->nv;
+    const int nv = w->nv, m0 = 3 - w->H, m1 = 3 + w->H; /* stencil slots m0..m1 of 7 */
     real_t *out = Ycell(w, i, j);
     if (p->recon == 1 && nv > 1) {
-        real_t uc[4], L[16], R[16], pr[5][4], col[5][4], st[5], cg[4][4];
+        real_t uc[4], L[16], R[16], pr[7][4], col[7][4], st[7], cg[4][4];
         cell_avg(w, i, j, uc);
         eigen_L(&p->eq, uc, 0, 1, L);
         eigen_R(&p->eq, uc, 0, 1, R);
-        for (int m = 0; m < 5; m++) {
-            cell_avg(w, i, j - 2 + m, col[m]);
+        for (int m = m0; m <= m1; m++) {
+            cell_avg(w, i, j - 3 + m, col[m]);
             matvec(nv, L, col[m], pr[m]);
         }
         for (int gp = 0; gp < 4; gp++) {
             for (int k = 0; k < nv; k++) {
-                for (int m = 0; m < 5; m++) st[m] = pr[m][k];
-                cg[gp][k] = weno(p->scheme, st, gp);
+                for (int m = m0; m <= m1; m++) st[m] = pr[m][k];
+                cg[gp][k] = weno7(p->scheme, st, gp, w->dX);
             }
             real_t phys[4];
             matvec(nv, R, cg[gp], phys);
             for (int v = 0; v < nv; v++) out[gp * 4 + v] = phys[v];
         }
     } else if (p->recon >= 2 && nv > 1) {
-        real_t col[5][4], prim[5][4], st[5];
-        for (int m = 0; m < 5; m++) {
-            cell_avg(w, i, j - 2 + m, col[m]);
+        real_t col[7][4], prim[7][4], st[7];
+        for (int m = m0; m <= m1; m++) {
+            cell_avg(w, i, j - 3 + m, col[m]);
             to_primitive(&p->eq, p->recon, col[m], prim[m]);
         }
         for (int v = 0; v < nv; v++) {
-            for (int m = 0; m < 5; m++) st[m] = prim[m][v];
-            for (int gp = 0; gp < 4; gp++) out[gp * 4 + v] = weno(p->scheme, st, gp);
+            for (int m = m0; m <= m1; m++) st[m] = prim[m][v];
+            for (int gp = 0; gp < 4; gp++) out[gp * 4 + v] = weno7(p->scheme, st, gp, w->dX);
         }
     } else {
-        real_t st[5];
+        real_t st[7];
         for (int v = 0; v < nv; v++) {
-            for (int m = 0; m < 5; m++) st[m] = *Ecell(w, v, i, j - 2 + m);
-            for (int gp = 0; gp < 4; gp++) out[gp * 4 + v] = weno(p->scheme, st, gp);
+            for (int m = m0; m <= m1; m++) st[m] = *Ecell(w, v, i, j - 3 + m);
+            for (int gp = 0; gp < 4; gp++) out[gp * 4 + v] = weno7(p->scheme, st, gp, w->dX);
         }
     }
 }
@@ -851,31 +939,32 @@ static int x_sweep(ofv_ws *w, int i, int j)
     real_t *fs = Fcell(w, i, j);
     real_t uc[4];
     cell_avg(w, i, j, uc);
+    const int m0 = 3 - w->H, m1 = 3 + w->H; /* stencil slots m0..m1 of 7 */
     if (p->recon == 1 && nv > 1) {
-        real_t L[16], R[16], tc[5][4][4], st[5], c[4];
+        real_t L[16], R[16], tc[7][4][4], st[7], c[4];
         eigen_L(&p->eq, uc, 1, 0, L);
         eigen_R(&p->eq, uc, 1, 0, R);
-        for (int m = 0; m < 5; m++) {
-            const real_t *y = Ycell(w, i - 2 + m, j);
+        for (int m = m0; m <= m1; m++) {
+            const real_t *y = Ycell(w, i - 3 + m, j);
             for (int gp = 0; gp < 4; gp++) matvec(nv, L, y + gp * 4, tc[m][gp]);
         }
         for (int gpj = 0; gpj < 4; gpj++)
             for (int gpi = 0; gpi < 4; gpi++) {
                 if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
                 for (int k = 0; k < nv; k++) {
-                    for (int m = 0; m < 5; m++) st[m] = tc[m][gpj][k];
-                    c[k] = weno(p->scheme, st, gpi);
+                    for (int m = m0; m <= m1; m++) st[m] = tc[m][gpj][k];
+                    c[k] = weno7(p->scheme, st, gpi, w->dX);
                 }
                 matvec(nv, R, c, ugp[gpi][gpj]);
             }
     } else {
-        real_t st[5];
+        real_t st[7];
         for (int gpj = 0; gpj < 4; gpj++)
             for (int v = 0; v < nv; v++) {
-                for (int m = 0; m < 5; m++) st[m] = Ycell(w, i - 2 + m, j)[gpj * 4 + v];
+                for (int m = m0; m <= m1; m++) st[m] = Ycell(w, i - 3 + m, j)[gpj * 4 + v];
                 for (int gpi = 0; gpi < 4; gpi++) {
                     if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
-                    ugp[gpi][gpj][v] = weno(p->scheme, st, gpi);
+                    ugp[gpi][gpj][v] = weno7(p->scheme, st, gpi, w->dX);
                 }
             }
         if (p->recon >= 2 && nv > 1) /* the primitive values back to conservative ones */
@@ -908,9 +997,9 @@ static void reconstruct(ofv_ws *w, const double *U, double *theta_flags)
 #pragma omp parallel for schedule(static)
 #endif
     for (j = -1; j <= ny; j++)
-        for (int i = -G; i < nx + G; i++) {
-            /* halo rows only need columns -2..nx+1 (their cells need no x-halo) */
-            if ((j < 0 || j >= ny) && (i < -2 || i > nx + 1)) continue;
+        for (int i = -1 - w->H; i <= nx + w->H; i++) {
+            /* halo rows only need columns -H..nx-1+H (their cells need no x-halo) */
+            if ((j < 0 || j >= ny) && (i < -w->H || i > nx - 1 + w->H)) continue;
             y_sweep(w, i, j);
         }
 #ifdef _OPENMP

@@ -42,7 +42,7 @@ typedef struct {
     int bc;                /* OFV_BC_* */
     int rk;                /* RKMETH: 0 RK1, 1 RK2, 2 RK3 */
     double cfl;            /* CFL */
-    int scheme;            /* SCHEME: 0 WENO-JS, 1 WENO-Z */
+    int scheme;            /* SCHEME: 0 WENO-JS, 1 WENO-Z, 2 WENOEXP */
     int limiter;           /* PPlimiter */
     int flux;              /* RIEMANNFLUX: 0 LLF, 1 HLLC */
     int recon;             /* RECONSTRUCTIONTYPE: 0 conservative, 1 characteristic, 2 primitive
@@ -57,6 +57,11 @@ int ofv_nvar(const ofv_eq *eq);
 /* pointwise kernels */
 double ofv_weno_js(const double v[5], int gp);
 double ofv_weno_z(const double v[5], int gp);
+/* wenoExpthreconstruction (include/Utility.hpp:291-470) on a 7-point stencil, cell size dx */
+double ofv_weno_exp(const double v[7], int gp, double dx);
+/* 0 (default): WENOEXP's l^3 by the C library's pow, as the reference; 1: l^3 rounded once,
+ * the device kernels' form */
+void ofv_set_cube_rounded(int on);
 double ofv_volume_frac(const ofv_eq *eq, const double *U);
 double ofv_pressure(const ofv_eq *eq, const double *U);
 double ofv_sound_speed(const ofv_eq *eq, const double *U);

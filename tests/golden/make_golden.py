@@ -40,15 +40,25 @@ CASES = [
     ("sharp_z_prim_hllc_lim_rk3", 2, 40, 24, 1, 1, 2, 1, 2, 8, 0.0, False),
     ("smooth_js_prim2_llf_rk3", 0, 32, 16, 0, 0, 3, 0, 2, 5, 0.0, False),
     ("column_z_prim2_hllc_lim_rk3", 2, 48, 32, 1, 1, 3, 1, 2, 6, 0.0, True),
+    ("smooth_exp_cons_llf_rk3", 0, 32, 16, 2, 0, 0, 0, 2, 5, 0.0, False),
+    ("sharp_exp_char_hllc_lim_rk3", 2, 40, 24, 2, 1, 1, 1, 2, 8, 0.0, False),
+    ("column_exp_char_hllc_lim_rk3", 2, 48, 32, 2, 1, 1, 1, 2, 6, 0.0, True),
+    ("column_exp_prim_hllc_lim_rk3", 2, 48, 32, 2, 1, 2, 1, 2, 6, 0.0, True),
 ]
 
 PARAMS = {0: dict(rho10=1.2, rho20=1.0, sound1=1.0, sound2=1.0),
           2: dict(rho10=1000.0, rho20=1.0, sound1=70.0, sound2=70.0)}
 
 
-def main():
+def main(only=()):
+    """Regenerates every case, or only the named ones (the index keeps the others)."""
     index = {}
+    if only:
+        with open(os.path.join(OUT, "index.json")) as f:
+            index = json.load(f)
     for (name, tc, nx, ny, scheme, flux, recon, lim, rk, steps, t_end, column) in CASES:
+        if only and name not in only:
+            continue
         prm = dict(PARAMS[tc])
         U0 = None
         if column:
@@ -67,4 +77,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

@@ -36,7 +36,8 @@ def test_oracle_matches_reference_golden(name, oracle_lib):
 
 @pytest.mark.skipif(not reference_available(), reason="compiled reference not built (make -C oracle ref)")
 @pytest.mark.parametrize("scheme,flux,recon,lim,rk", [(1, 1, 1, 1, 2), (0, 0, 0, 1, 1), (1, 0, 0, 0, 0),
-                                                      (1, 1, 2, 1, 2), (0, 0, 2, 0, 1), (1, 1, 3, 1, 2), (0, 1, 3, 0, 2)])
+                                                      (1, 1, 2, 1, 2), (0, 0, 2, 0, 1), (1, 1, 3, 1, 2), (0, 1, 3, 0, 2),
+                                                      (2, 1, 1, 1, 2), (2, 0, 0, 0, 1), (2, 1, 2, 1, 2), (2, 1, 3, 0, 2)])
 def test_oracle_matches_live_reference(scheme, flux, recon, lim, rk, oracle_lib):
     U0, prm = cases.liquid_column(36, 20, seed=5)
     p = Problem(nx=36, ny=20, rk=rk, scheme=scheme, flux=flux, recon=recon, limiter=lim, ref_slabs=4,
@@ -59,6 +60,36 @@ def test_weno_reproduces_quadratics(oracle_lib):
     for scheme in (0, 1):
         for gp in range(4):
             assert abs(oracle_lib.weno(scheme, avg, gp) - f(xg[gp])) < 1e-9
+
+
+def test_weno_exp_reproduces_quadratics(oracle_lib):
+    # on the cell averages of a quadratic the third and fifth differences vanish (l2h2 = 0)
+    # and so does tau: the weights are the linear ones and the candidates are exact
+    rng = np.random.default_rng(3)
+    xg = np.array([-0.5, -np.sqrt(5) / 10, np.sqrt(5) / 10, 0.5])
+    for _ in range(20):
+        a, b, c = rng.standard_normal(3)
+        f = lambda x: a + b * x + c * x * x
+        avg = np.array([a + b * k + c * (k * k + 1.0 / 12.0) for k in range(-3, 4)])
+        for gp in range(4):
+            assert abs(oracle_lib.weno(2, avg, gp, 1.0) - f(xg[gp])) < 1e-9
+
+
+def test_weno_exp_cube_modes_agree(oracle_lib):
+    # the C library's pow(l, 3) and the once-rounded cube differ in the last bit for ~0.1 % of
+    # arguments; through the cubic's small coefficients that rarely reaches a linear weight
+    rng = np.random.default_rng(8)
+    st = rng.standard_normal((3000, 7))
+    a = np.array([[oracle_lib.weno(2, s, gp, 0.01) for gp in range(4)] for s in st])
+    with oracle_lib.cube_rounded():
+        b = np.array([[oracle_lib.weno(2, s, gp, 0.01) for gp in range(4)] for s in st])
+    assert np.abs(a - b).max() <= 4e-16 * np.abs(a).max()
+    for name in sorted(GOLD):  # and on the golden grids not a single bit
+        meta, g = GOLD[name], load_golden(name)
+        if meta["scheme"] != 2:
+            continue
+        with oracle_lib.cube_rounded():
+            assert np.array_equal(oracle_lib.rhs(problem_of(meta), g["U0"]), g["rhs"])
 
 
 def test_weno_flat_stencil(oracle_lib):
