@@ -86,7 +86,7 @@ typedef struct {
     int bc;                /* WENOFV_BC_* */
     int rk_method;         /* RKMETH: 0 RK1, 1 RK2, 2 RK3 */
     double cfl;            /* CFL */
-    int scheme;            /* SCHEME: 0 WENO-JS, 1 WENO-Z */
+    int scheme;            /* SCHEME: 0 WENO-JS, 1 WENO-Z, 2 WENOEXP (FP64 forms only) */
     int pp_limiter;        /* PPlimiter: 0 off, 1 on */
     int riemann_flux;      /* RIEMANNFLUX: 0 LLF, 1 HLLC */
     int reconstruction;    /* RECONSTRUCTIONTYPE: 0 conservative, 1 characteristic, 2 primitive
@@ -218,6 +218,9 @@ int wenofv_server_stats(wenofv_server *s, int64_t *admitted, int64_t *completed,
 /* WENO5threconstruction / WENO5Zthreconstruction (include/Utility.hpp:5-95, :193-290) at
  * the 4 Gauss-Lobatto points: stencils n x 5, out n x 4 */
 int wenofv_probe_weno(int scheme, int precision, const double *stencils, int n, double *out, int device);
+/* wenoExpthreconstruction (include/Utility.hpp:291-470) at the 4 Gauss-Lobatto points:
+ * stencils n x 7, cell size dx (the threshold is pow(dx, 4)), out n x 4; FP64 forms only */
+int wenofv_probe_weno_exp(int precision, const double *stencils, int n, double dx, double *out, int device);
 /* getRiemannFlux (include/Equations.hpp:329-483): UL, UR, F are n x nvar */
 int wenofv_probe_riemann(const wenofv_eq_params *eq, int flux, int precision, const double *UL,
                          const double *UR, int n, double nx, double ny, double *F, int device);

@@ -65,15 +65,17 @@ def test_batch_mixed_equations_and_tiling(wb):
     U3 = cases.advection_sine(150, 20)
     c3 = wb.make_config(150, 20, scheme=0, flux=0, recon=0, precision=wb.FP64_STRICT)
     e3 = wb.make_eq(kind=wb.EQ_LINEAR_ADV)
-    refs = [alone(wb, c, e, U, max_steps=5)[0] for c, e, U in ((c1, e1, U1), (c2, e2, U2), (c3, e3, U3))]
+    # and a WENOEXP column (7-point stencils: its own strip width and launch group)
+    c4, e4 = column_cfg(wb, 64, 48, prm, wb.FP64_STRICT, scheme=2)
+    refs = [alone(wb, c, e, U, max_steps=5)[0] for c, e, U in ((c1, e1, U1), (c2, e2, U2), (c3, e3, U3), (c4, e4, U1))]
     for rows, ctas in ((8, 1), (16, 0), (64, 2)):
-        b = wb.Batch([c1, c2, c3], [e1, e2, e3])
-        for k, U in enumerate((U1, U2, U3)):
+        b = wb.Batch([c1, c2, c3, c4], [e1, e2, e3, e4])
+        for k, U in enumerate((U1, U2, U3, U1)):
             b.upload(k, U)
         b.set_tiling(rows, ctas)
-        ns = b.advance([1e9] * 3, max_steps=5)
-        assert list(ns) == [5, 5, 5]
-        for k in range(3):
+        ns = b.advance([1e9] * 4, max_steps=5)
+        assert list(ns) == [5, 5, 5, 5]
+        for k in range(4):
             assert np.array_equal(b.download(k), refs[k])
         b.close()
 

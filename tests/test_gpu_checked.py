@@ -32,32 +32,36 @@ def child():
     assert wb.LIB_PATH == CHECKED
     o = Oracle()
     n_cases = 0
-    for nx, ny in [(1, 1), (3, 2), (8, 8), (12, 8), (27, 5), (26, 33), (130, 9)]:
+    o.L.ofv_set_cube_rounded(1)  # WENOEXP's l^3 as the device kernels form it
+    for nx, ny, scheme in [(1, 1, 1), (3, 2, 1), (8, 8, 1), (12, 8, 1), (27, 5, 1), (26, 33, 1), (130, 9, 1),
+                           (1, 1, 2), (3, 2, 2), (24, 8, 2), (25, 7, 2), (50, 33, 2)]:
         for recon in (0, 1, 2, 3):
             mild = dict(ratio=2.0, eps=0.05)
             U0, prm = cases.liquid_column(nx, ny, seed=nx + 7 * ny, **mild)
-            p = Problem(nx=nx, ny=ny, scheme=1, flux=1, recon=recon, limiter=1, **prm)
+            p = Problem(nx=nx, ny=ny, scheme=scheme, flux=1, recon=recon, limiter=1, **prm)
             V, *_ = o.advance(p, U0, t_end=1e9, max_steps=2)
             for prec in (wb.FP64_STRICT, wb.FP64, wb.FP32_BULK):
-                cfg = wb.make_config(nx, ny, scheme=1, flux=1, recon=recon, limiter=1, precision=prec)
+                if scheme == 2 and prec == wb.FP32_BULK:
+                    continue
+                cfg = wb.make_config(nx, ny, scheme=scheme, flux=1, recon=recon, limiter=1, precision=prec)
                 eq = wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"])
                 with wb.Solver(cfg, eq) as s:
                     s.upload(U0)
                     s.advance(1e9, max_steps=2)
                     flags, cell = s.status()
-                    assert flags == 0, (nx, ny, recon, prec, flags, cell)
+                    assert flags == 0, (nx, ny, scheme, recon, prec, flags, cell)
                     U = s.download()
                 if prec == wb.FP64_STRICT:
-                    assert np.array_equal(U, V), (nx, ny, recon)
+                    assert np.array_equal(U, V), (nx, ny, scheme, recon)
                 n_cases += 1
-    for nx, ny in [(5, 3), (40, 9)]:  # Euler, outflow
+    for nx, ny, scheme in [(5, 3, 1), (40, 9, 1), (5, 3, 2), (40, 9, 2)]:  # Euler, outflow
         U0, _ = cases.euler_quadrants(nx, ny, seed=3)
-        cfg = wb.make_config(nx, ny, bc=wb.BC_OUTFLOW, cfl=0.4, scheme=1, flux=1, recon=1, precision=wb.FP64_STRICT)
+        cfg = wb.make_config(nx, ny, bc=wb.BC_OUTFLOW, cfl=0.4, scheme=scheme, flux=1, recon=1, precision=wb.FP64_STRICT)
         with wb.Solver(cfg, wb.make_eq(kind=wb.EQ_EULER)) as s:
             s.upload(U0)
             s.advance(1e9, max_steps=2)
             assert s.status()[0] == 0
-            p = Problem(nx=nx, ny=ny, bc=BC_OUTFLOW, eq_kind=EQ_EULER, scheme=1, flux=1, recon=1, cfl=0.4)
+            p = Problem(nx=nx, ny=ny, bc=BC_OUTFLOW, eq_kind=EQ_EULER, scheme=scheme, flux=1, recon=1, cfl=0.4)
             assert np.array_equal(s.download(), o.advance(p, U0, t_end=1e9, max_steps=2)[0])
         n_cases += 1
     ens = cases.ensemble(5, seed=9, grids=[(1, 1), (26, 26), (27, 5), (64, 40)])

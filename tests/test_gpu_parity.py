@@ -4,6 +4,10 @@
   the reference's golden vectors bit for bit.
 * FP64 (contracted, reciprocal form) must agree with the oracle to 1e-11 of max |U| after
   a few steps (tolerances stated per test).
+* WENOEXP (SCHEME 2) forms l^3 rounded once where the reference calls the C library's
+  pow(l, 3); the oracle's cube_rounded() mode does the same, and FP64_STRICT must equal it
+  bit for bit.  (On the golden grids both cubes give the same bits, so WENOEXP also equals
+  the reference's golden vectors.)
 """
 from __future__ import annotations
 
@@ -54,6 +58,32 @@ def stencils(rng, n):
          np.where(rng.uniform(size=(n, 5)) < 0.5, 1e-6, 1000.0),           # jumps 1e-6 .. 1e3
          rng.standard_normal((n, 5)) * 1e-12]                              # tiny
     return np.concatenate(s)
+
+
+def exp_stencils(rng, n, dx):
+    x = np.arange(-3, 4) * dx
+    s = [rng.standard_normal((n, 7)),                                      # generic: |l2h2| clipped to 1 mostly
+         rng.uniform(0, 1, (n, 7)) * 1e3 + 1e3,                            # large offset
+         np.repeat(rng.standard_normal((n, 1)), 7, axis=1),                 # flat: dif3 = 0 -> l2h2 = 0
+         np.where(rng.uniform(size=(n, 7)) < 0.5, 1e-6, 1000.0),            # jumps
+         # smooth: quartics of the cell position (dif5 = 0, dif3 small, |l2h2| < 1)
+         np.polynomial.polynomial.polyval(x, rng.standard_normal((5, n))) ,
+         np.sin(x[None, :] * rng.uniform(1, 30, (n, 1)) + rng.uniform(0, 6, (n, 1))),
+         rng.standard_normal((n, 7)) * 1e-12]                               # tiny: |dif3| near dx^4
+    return np.concatenate(s)
+
+
+def test_weno_exp_probe(wb, oracle_lib):
+    dx = 1.0 / 64
+    st = exp_stencils(np.random.default_rng(5), 300, dx)
+    with oracle_lib.cube_rounded():
+        ref = np.array([[oracle_lib.weno(2, s, gp, dx) for gp in range(4)] for s in st])
+    assert np.array_equal(wb.probe_weno_exp(st, dx, precision=wb.FP64_STRICT), ref)
+    lib = np.array([[oracle_lib.weno(2, s, gp, dx) for gp in range(4)] for s in st])  # pow(l, 3)
+    assert np.abs(lib - ref).max() <= 1e-15 * np.abs(ref).max()
+    fast = wb.probe_weno_exp(st, dx, precision=wb.FP64)
+    scale = np.abs(st).max(axis=1, keepdims=True)
+    assert np.all(np.abs(fast - ref) <= 1e-13 * scale)
 
 
 @pytest.mark.parametrize("scheme", [0, 1])
@@ -214,27 +244,48 @@ def test_strict_matches_live_reference(wb):
 # ---- edge cases: ragged strips, short row runs, tiny and non-square grids --------------------
 @pytest.mark.parametrize("nx,ny", [(8, 8), (12, 8), (27, 5), (53, 70), (130, 9)])
 @pytest.mark.parametrize("recon,lim", [(0, 0), (1, 1), (2, 1), (3, 1)])
-def test_ragged_sizes_strict(wb, oracle_lib, nx, ny, recon, lim):
+@pytest.mark.parametrize("scheme", [1, 2])
+def test_ragged_sizes_strict(wb, oracle_lib, nx, ny, recon, lim, scheme):
     # without the limiter a density ratio of 1000 on these coarse grids drives the partial
     # densities negative (the oracle and the reference then produce NaN too), so that case
     # uses a mild column
     mild = dict(ratio=2.0, eps=0.05) if not lim else {}
     U0, prm = cases.liquid_column(nx, ny, seed=nx * 100 + ny, **mild)
-    p = Problem(nx=nx, ny=ny, scheme=1, flux=1, recon=recon, limiter=lim, **prm)
-    V, n, _, _ = oracle_lib.advance(p, U0, t_end=1e9, max_steps=3)
+    p = Problem(nx=nx, ny=ny, scheme=scheme, flux=1, recon=recon, limiter=lim, **prm)
+    with oracle_lib.cube_rounded():
+        V, n, _, _ = oracle_lib.advance(p, U0, t_end=1e9, max_steps=3)
+        R = oracle_lib.rhs(p, U0)
     with solver_for(wb, p, wb.FP64_STRICT) as s:
         s.upload(U0)
-        assert np.array_equal(s.rhs(), oracle_lib.rhs(p, U0))
+        assert np.array_equal(s.rhs(), R)
         s.advance(1e9, max_steps=3)
         assert np.array_equal(s.download(), V)
 
 
+@pytest.mark.parametrize("recon", [0, 1, 3])
+def test_weno_exp_column_fast(wb, oracle_lib, recon):
+    # lambda^2 h^2 = dif5 / dif3 is a ratio of high differences of nearly equal averages, so
+    # contraction moves it (and the linear weights) more than it moves WENO-Z's weights:
+    # after 5 steps the contracted build is within 1e-10 of max |U| (measured 4e-11 with
+    # PRIMITIVE2)
+    U0, prm = cases.liquid_column(96, 80, seed=13)
+    p = Problem(nx=96, ny=80, scheme=2, flux=1, recon=recon, limiter=1, ref_slabs=4, **prm)
+    with oracle_lib.cube_rounded():
+        V, *_ = oracle_lib.advance(p, U0, t_end=1e9, max_steps=5)
+    with solver_for(wb, p, wb.FP64) as s:
+        s.upload(U0)
+        s.advance(1e9, max_steps=5)
+        assert relerr(s.download(), V) <= 1e-10
+
+
 @pytest.mark.parametrize("recon", [0, 1])
 @pytest.mark.parametrize("flux", [0, 1])
-def test_euler_outflow_strict(wb, oracle_lib, recon, flux):
+@pytest.mark.parametrize("scheme", [1, 2])
+def test_euler_outflow_strict(wb, oracle_lib, recon, flux, scheme):
     U0, _ = cases.euler_quadrants(40, 30)
-    p = Problem(nx=40, ny=30, bc=BC_OUTFLOW, eq_kind=EQ_EULER, scheme=1, flux=flux, recon=recon, cfl=0.4)
-    V, n, t, _ = oracle_lib.advance(p, U0, t_end=0.01)
+    p = Problem(nx=40, ny=30, bc=BC_OUTFLOW, eq_kind=EQ_EULER, scheme=scheme, flux=flux, recon=recon, cfl=0.4)
+    with oracle_lib.cube_rounded():
+        V, n, t, _ = oracle_lib.advance(p, U0, t_end=0.01)
     with solver_for(wb, p, wb.FP64_STRICT) as s:
         s.upload(U0)
         t2, n2 = s.advance(0.01)
@@ -243,10 +294,12 @@ def test_euler_outflow_strict(wb, oracle_lib, recon, flux):
 
 
 @pytest.mark.parametrize("nx", [64, 130])
-def test_advection_strict(wb, oracle_lib, nx):
+@pytest.mark.parametrize("scheme", [0, 2])
+def test_advection_strict(wb, oracle_lib, nx, scheme):
     U0 = cases.advection_sine(nx, 32)
-    p = Problem(nx=nx, ny=32, eq_kind=EQ_LINEAR_ADV, scheme=0, flux=0, recon=0, cfl=0.5)
-    V, n, t, _ = oracle_lib.advance(p, U0, t_end=0.25)
+    p = Problem(nx=nx, ny=32, eq_kind=EQ_LINEAR_ADV, scheme=scheme, flux=0, recon=0, cfl=0.5)
+    with oracle_lib.cube_rounded():
+        V, n, t, _ = oracle_lib.advance(p, U0, t_end=0.25)
     with solver_for(wb, p, wb.FP64_STRICT) as s:
         s.upload(U0)
         t2, n2 = s.advance(0.25)

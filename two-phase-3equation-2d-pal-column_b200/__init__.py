@@ -35,7 +35,7 @@ EXPORTS = (
     "wenofv_batch_advance", "wenofv_batch_set_tiling", "wenofv_batch_stream", "wenofv_batch_autotune",
     "wenofv_server_create", "wenofv_server_destroy", "wenofv_server_submit", "wenofv_server_poll",
     "wenofv_server_clock", "wenofv_server_stats",
-    "wenofv_probe_weno", "wenofv_probe_riemann", "wenofv_probe_eigen", "wenofv_probe_fma_peak",
+    "wenofv_probe_weno", "wenofv_probe_weno_exp", "wenofv_probe_riemann", "wenofv_probe_eigen", "wenofv_probe_fma_peak",
 )
 
 
@@ -122,6 +122,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.wenofv_server_clock.argtypes = [P]
     L.wenofv_server_stats.argtypes = [P] + [C.POINTER(I64)] * 5
     L.wenofv_probe_weno.argtypes = [I, I, DP, I, DP, I]
+    L.wenofv_probe_weno_exp.argtypes = [I, DP, I, D, DP, I]
     L.wenofv_probe_riemann.argtypes = [C.POINTER(EqParams), I, I, DP, DP, I, D, D, DP, I]
     L.wenofv_probe_eigen.argtypes = [C.POINTER(EqParams), I, DP, I, D, D, DP, DP, I]
     L.wenofv_probe_fma_peak.argtypes = [I, I, DP]
@@ -356,6 +357,14 @@ def probe_weno(scheme: int, stencils: np.ndarray, precision=FP64, device=0) -> n
     s = np.ascontiguousarray(stencils, dtype=np.float64).reshape(-1, 5)
     out = np.empty((s.shape[0], 4))
     _check(L.wenofv_probe_weno(scheme, precision, _dp(s), s.shape[0], _dp(out), device), "wenofv_probe_weno")
+    return out
+
+
+def probe_weno_exp(stencils: np.ndarray, dx: float, precision=FP64, device=0) -> np.ndarray:
+    L = load()
+    s = np.ascontiguousarray(stencils, dtype=np.float64).reshape(-1, 7)
+    out = np.empty((s.shape[0], 4))
+    _check(L.wenofv_probe_weno_exp(precision, _dp(s), s.shape[0], dx, _dp(out), device), "wenofv_probe_weno_exp")
     return out
 
 

@@ -2,6 +2,7 @@
 // batches and device probes; the serving entry points are in wenofv_server.cu).
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -211,6 +212,26 @@ int wenofv_probe_weno(int scheme, int precision, const double *stencils, int n, 
     const int rc = precision == WENOFV_FP64_STRICT ? strict::probe_weno(scheme, 0, s, n, o, nullptr)
                                                    : fast::probe_weno(scheme, precision == WENOFV_FP32_BULK, s, n, o, nullptr);
     if (rc) return cuda_fail((cudaError_t)rc, "probe_weno");
+    WENOFV_CUDA(cudaMemcpy(out, o, (size_t)4 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    return WENOFV_OK;
+}
+
+int wenofv_probe_weno_exp(int precision, const double *stencils, int n, double dx, double *out, int device)
+{
+    if (n < 0 || (n > 0 && (!stencils || !out)) || precision == WENOFV_FP32_BULK) {
+        set_error("bad arguments (WENOEXP has no FP32 form)");
+        return WENOFV_EINVAL;
+    }
+    if (n == 0) return WENOFV_OK;
+    WENOFV_CUDA(cudaSetDevice(device));
+    DevBufs B;
+    double *s = B.alloc((size_t)7 * n), *o = B.alloc((size_t)4 * n);
+    if (!s || !o) { set_error("device allocation failed"); return WENOFV_ENOMEM; }
+    WENOFV_CUDA(cudaMemcpy(s, stencils, (size_t)7 * n * sizeof(double), cudaMemcpyHostToDevice));
+    const double dx4 = std::pow(dx, 4); // as the engine forms it for a grid
+    const int rc = precision == WENOFV_FP64_STRICT ? strict::probe_weno_exp(s, n, dx4, o, nullptr)
+                                                   : fast::probe_weno_exp(s, n, dx4, o, nullptr);
+    if (rc) return cuda_fail((cudaError_t)rc, "probe_weno_exp");
     WENOFV_CUDA(cudaMemcpy(out, o, (size_t)4 * n * sizeof(double), cudaMemcpyDeviceToHost));
     return WENOFV_OK;
 }

@@ -39,8 +39,12 @@ int validate(const wenofv_config *c, const wenofv_eq_params *e)
     if (!(c->xr > c->xl) || !(c->yr > c->yl)) { set_error("empty domain"); return WENOFV_EINVAL; }
     if (c->rk_method < 0 || c->rk_method > 2) { set_error("RKMETH must be 0, 1 or 2"); return WENOFV_EINVAL; }
     if (!(c->cfl > 0)) { set_error("CFL must be positive"); return WENOFV_EINVAL; }
-    if (c->scheme == 2) { set_error("SCHEME 2 (WENOEXP) is not supported"); return WENOFV_ENOTSUP; }
-    if (c->scheme < 0 || c->scheme > 1) { set_error("SCHEME must be 0 or 1"); return WENOFV_EINVAL; }
+    if (c->scheme < 0 || c->scheme > 2) { set_error("SCHEME must be 0, 1 or 2"); return WENOFV_EINVAL; }
+    if (c->scheme == 2 && c->precision == WENOFV_FP32_BULK) {
+        // lambda^2 h^2 is a ratio of 5th to 3rd differences, which FP32 rounds to noise on smooth data
+        set_error("SCHEME 2 (WENOEXP) runs in FP64 only");
+        return WENOFV_ENOTSUP;
+    }
     if (c->reconstruction >= 4 && c->reconstruction <= 5) { set_error("RECONSTRUCTIONTYPE %d is not supported", c->reconstruction); return WENOFV_ENOTSUP; }
     if (c->reconstruction < 0 || c->reconstruction > 3) { set_error("RECONSTRUCTIONTYPE must be 0, 1, 2 or 3"); return WENOFV_EINVAL; }
     if (c->reconstruction >= 2 && e && e->eq_kind != WENOFV_EQ_TWO_PHASE) {
@@ -198,6 +202,7 @@ int Engine::alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params
     d.eq_kind = e.eq_kind;
     d.cfl = c.cfl;
     d.dX = (c.xr - c.xl) / c.nx;
+    d.dx4 = std::pow(d.dX, 4); // the reference's pow(m_deltaX, 4), include/Utility.hpp:313
     d.dY = (c.yr - c.yl) / c.ny;
     d.eq = EqParams{e.eq_kind, e.rho10, e.rho20, e.sound1, e.sound2, e.preb, e.gamma, e.adv_u, e.adv_v};
     WENOFV_CUDA(cudaMemcpyAsync(d_desc_ + i, &d, sizeof(InstDesc), cudaMemcpyHostToDevice, stream));
@@ -344,7 +349,7 @@ int Engine::build_work()
         groups_[it->second].inst.push_back(i);
     }
     for (Group &g : groups_) {
-        const int tx = g.ns_strict ? strict::stage_tx(g.eq) : fast::stage_tx(g.eq);
+        const int tx = g.ns_strict ? strict::stage_tx(g.eq, g.scheme) : fast::stage_tx(g.eq, g.scheme);
         const int bps = std::max(1, g.ns_strict ? strict::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux)
                                                 : fast::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux));
         const int slots = sms_ * (ctas_per_sm_ > 0 ? std::min(ctas_per_sm_, bps) : bps);
@@ -429,7 +434,8 @@ int Engine::launch_cfl_all()
         L.fin_ids = g.d_fin;
         L.nfin = (int)g.inst.size();
         L.counter = g.d_counter;
-        const int rc = g.ns_strict ? strict::launch_cfl(g.eq, L, g.grid, stream) : fast::launch_cfl(g.eq, L, g.grid, stream);
+        const int rc = g.ns_strict ? strict::launch_cfl(g.eq, g.scheme, L, g.grid, stream)
+                                   : fast::launch_cfl(g.eq, g.scheme, L, g.grid, stream);
         if (rc) return cuda_fail((cudaError_t)rc, "cfl kernel launch");
     }
     return WENOFV_OK;

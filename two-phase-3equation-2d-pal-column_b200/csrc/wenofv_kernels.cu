@@ -21,15 +21,29 @@ namespace fast {
 #define WENOFV_HAS_FP32 1
 #endif
 
-int stage_tx(int eq) { return eq == EQ_LINEAR_ADV ? StageGeom<EQ_LINEAR_ADV>::TX : StageGeom<EQ_TWO_PHASE>::TX; }
+// strip width of the work items: 5-point stencils (H = 2) or WENOEXP's 7-point ones (H = 3)
+int stage_tx(int eq, int scheme)
+{
+    if (scheme == 2) return eq == EQ_LINEAR_ADV ? StageGeom<EQ_LINEAR_ADV, 3>::TX : StageGeom<EQ_TWO_PHASE, 3>::TX;
+    return eq == EQ_LINEAR_ADV ? StageGeom<EQ_LINEAR_ADV, 2>::TX : StageGeom<EQ_TWO_PHASE, 2>::TX;
+}
 
 template <int EQ, int RECON, class R, int SCH, int FLX> static const void *stage_fn()
 {
     return (const void *)stage_kernel<EQ, RECON, R, SCH, FLX>;
 }
 // the scheme and flux of a launch group as template arguments (scalar advection has one flux)
+// (WENOEXP, scheme 2, only in FP64)
 template <int EQ, int RECON, class R> static const void *pick_sf(int scheme, int flux)
 {
+    if constexpr (sizeof(R) == sizeof(double)) {
+        if (scheme == 2) {
+            if (EQ == EQ_LINEAR_ADV) return stage_fn<EQ, RECON, R, 2, 0>();
+            return flux ? stage_fn<EQ, RECON, R, 2, 1>() : stage_fn<EQ, RECON, R, 2, 0>();
+        }
+    } else {
+        if (scheme == 2) return nullptr;
+    }
     if (EQ == EQ_LINEAR_ADV) return scheme ? stage_fn<EQ, RECON, R, 1, 0>() : stage_fn<EQ, RECON, R, 0, 0>();
     if (scheme) return flux ? stage_fn<EQ, RECON, R, 1, 1>() : stage_fn<EQ, RECON, R, 1, 0>();
     return flux ? stage_fn<EQ, RECON, R, 0, 1>() : stage_fn<EQ, RECON, R, 0, 0>();
@@ -48,7 +62,7 @@ template <class R> static const void *pick_eq(int eq, int recon, int scheme, int
 
 static const void *pick_stage(int eq, int recon, int fp32, int scheme, int flux)
 {
-    if (scheme < 0 || scheme > 1 || flux < 0 || flux > 1) return nullptr;
+    if (scheme < 0 || scheme > 2 || flux < 0 || flux > 1) return nullptr;
 #if WENOFV_HAS_FP32
     if (fp32) return pick_eq<float>(eq, recon, scheme, flux);
 #else
@@ -65,11 +79,16 @@ int launch_stage(int eq, int recon, int fp32, int scheme, int flux, const StageL
     return (int)cudaLaunchKernel(fn, dim3(grid), dim3(NT), args, 0, (cudaStream_t)stream);
 }
 
-int launch_cfl(int eq, const StageLaunch &L, int grid, void *stream)
+template <int H> static const void *cfl_fn(int eq)
 {
-    const void *fn = eq == EQ_TWO_PHASE ? (const void *)cfl_kernel<EQ_TWO_PHASE>
-                     : eq == EQ_EULER   ? (const void *)cfl_kernel<EQ_EULER>
-                                        : (const void *)cfl_kernel<EQ_LINEAR_ADV>;
+    return eq == EQ_TWO_PHASE ? (const void *)cfl_kernel<EQ_TWO_PHASE, StageGeom<EQ_TWO_PHASE, H>::TX>
+         : eq == EQ_EULER     ? (const void *)cfl_kernel<EQ_EULER, StageGeom<EQ_EULER, H>::TX>
+                              : (const void *)cfl_kernel<EQ_LINEAR_ADV, StageGeom<EQ_LINEAR_ADV, H>::TX>;
+}
+
+int launch_cfl(int eq, int scheme, const StageLaunch &L, int grid, void *stream)
+{
+    const void *fn = scheme == 2 ? cfl_fn<3>(eq) : cfl_fn<2>(eq);
     void *args[] = {(void *)&L};
     return (int)cudaLaunchKernel(fn, dim3(grid), dim3(NT), args, 0, (cudaStream_t)stream);
 }
@@ -94,6 +113,15 @@ template <class R> __global__ void probe_weno_kernel(int scheme, const double *s
     out[4 * k + 1] = (double)W.template eval<1>();
     out[4 * k + 2] = (double)W.template eval<2>();
     out[4 * k + 3] = (double)W.template eval<3>();
+}
+
+__global__ void probe_weno_exp_kernel(const double *st, int n, double dx4, double *out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    WenoExp W;
+    W.init(st + 7 * k, dx4);
+    W.eval4(out + 4 * k);
 }
 
 template <int EQ, class R>
@@ -135,6 +163,14 @@ int probe_weno(int scheme, int fp32, const double *d_st, int n, double *d_out, v
     else
 #endif
         probe_weno_kernel<double><<<g, b, 0, (cudaStream_t)stream>>>(scheme, d_st, n, d_out);
+    return (int)cudaGetLastError();
+}
+
+int probe_weno_exp(const double *d_st, int n, double dx4, double *d_out, void *stream)
+{
+    const int b = 128, g = (n + b - 1) / b;
+    if (n <= 0) return 0;
+    probe_weno_exp_kernel<<<g, b, 0, (cudaStream_t)stream>>>(d_st, n, dx4, d_out);
     return (int)cudaGetLastError();
 }
 

@@ -234,6 +234,105 @@ template <class R, int ZS = -1> struct Weno5 {
     }
 };
 
+// x^3 rounded once: the exact square p + e (e = fma(x, x, -p)) times x, as hi + lo with
+// the exact product error of p x, so only the final sum rounds (error ~2^-104 before it)
+__device__ __forceinline__ double cube_rn(double x)
+{
+    const double p = x * x;
+    const double e = fma(x, x, -p);
+    const double hi = p * x;
+    const double lo = fma(p, x, -hi);
+    return hi + (lo + e * x);
+}
+
+// WENOEXP (SCHEME 2, include/Utility.hpp:291-470) on a 7-point stencil.  The linear weights
+// are cubics in lambda^2 h^2 = dif5 / dif3, from the 6 points on the Gauss point's side
+// (gp 0, 1: v0..v5; gp 2, 3: v1..v6), clipped to 1 and set to 0 where |dif3| < dx^4; the
+// candidates are WENO5's, from the raw values; the smoothness indicators and tau use the
+// stencil normalised to [0, 1] and w_k = d_k (1 + 2 tau^2 / (beta_k^2 + 1e-16)).  The
+// factors 1 + 2 tau^2 / (beta_k^2 + 1e-16) depend on the stencil only and are formed once.
+// The reference's pow(l, 3) is the C library's (within 0.52 ulp of l^3); here it is l^3
+// rounded once (cube_rn), so the linear weights can differ from the reference's in the last
+// bit where the C library's pow is not correctly rounded.  FP64 only.
+struct WenoExp {
+    double umm, um, u, up, upp; // raw centre-5 values
+    double f0, f1, f2;          // 1 + 2 tau^2 / (beta_k^2 + eps)
+    double lam[2];              // lambda^2 h^2 of the left (gp 0, 1) and right (gp 2, 3) side
+
+    static __device__ __forceinline__ double side(double a, double b, double c, double d, double e, double f, double dx4)
+    {
+        const double dif5 = (-a + 5.0 * b - 10.0 * c + 10.0 * d - 5.0 * e + f);
+        const double dif3 = (a - 11.0 * b + 28.0 * c - 28.0 * d + 11.0 * e - f) / 6.0;
+        double l = 0.0;
+        if (!(fabs(dif3) < dx4)) {
+            l = dif5 / dif3;
+            if (fabs(l) > 1) l = 1;
+        }
+        return l;
+    }
+
+    __device__ __forceinline__ void init(const double *v, double dx4)
+    {
+        umm = v[1]; um = v[2]; u = v[3]; up = v[4]; upp = v[5];
+        lam[0] = side(v[0], v[1], v[2], v[3], v[4], v[5], dx4);
+        lam[1] = side(v[1], v[2], v[3], v[4], v[5], v[6], dx4);
+        const double umax = std_max(std_max(std_max(umm, um), std_max(u, up)), upp);
+        const double umin = std_min(std_min(std_min(umm, um), std_min(u, up)), upp);
+        double n0, n1, n2, n3, n4;
+#if WENOFV_STRICT
+        n0 = (umm - umin) / (umax - umin + 1e-20);
+        n1 = (um - umin) / (umax - umin + 1e-20);
+        n2 = (u - umin) / (umax - umin + 1e-20);
+        n3 = (up - umin) / (umax - umin + 1e-20);
+        n4 = (upp - umin) / (umax - umin + 1e-20);
+#else
+        const double inv = 1.0 / (umax - umin + 1e-20);
+        n0 = (umm - umin) * inv; n1 = (um - umin) * inv; n2 = (u - umin) * inv;
+        n3 = (up - umin) * inv; n4 = (upp - umin) * inv;
+#endif
+        // theta * 1.0 / 2.0 with theta = 1 is the exact 0.5
+        const double b0 = 0.5 * fabs(n0 - 4 * n1 + 3 * n2) + fabs(n0 - 2 * n1 + n2);
+        const double b1 = 0.5 * fabs(n1 - n3) + fabs(n1 - 2 * n2 + n3);
+        const double b2 = 0.5 * fabs(3 * n2 - 4 * n3 + n4) + fabs(n2 - 2 * n3 + n4);
+        const double tau = n0 - 4.0 * n1 + 6.0 * n2 - 4.0 * n3 + n4;
+        const double t2 = 2 * (tau * tau); // pow(x, 2.0) is x * x
+        f0 = 1.0 + t2 / (b0 * b0 + 1e-16);
+        f1 = 1.0 + t2 / (b1 * b1 + 1e-16);
+        f2 = 1.0 + t2 / (b2 * b2 + 1e-16);
+    }
+
+    template <int GP> __device__ __forceinline__ double eval() const
+    {
+        const double l = lam[GP >= 2 ? 1 : 0], l2 = l * l, l3 = cube_rn(l);
+        const double a = (GP == 0 || GP == 3) ? 0.3 - 0.057142858 * l + 0.0071428571 * l2 - 0.00077200577 * l3
+                                               : 0.16108042 - 0.035187607 * l + 0.0049466098 * l2 - 0.00058211525 * l3;
+        const double b = (GP == 0 || GP == 3) ? 0.6 + 0.078571429 * l - 0.0101190476 * l2 + 0.00112012987 * l3
+                                               : 0.58636364 + 0.087692641 * l - 0.0120401515 * l2 + 0.00139436871 * l3;
+        const double c = (GP == 0 || GP == 3) ? 0.1 - 0.021428571 * l + 0.0029761905 * l2 - 0.00034812410 * l3
+                                               : 0.25255594 - 0.052505034 * l + 0.0070935417 * l2 - 0.00081225346 * l3;
+        // gp 0, 1: (d0, d1, d2) = (a, b, c); gp 2, 3 mirror them
+        const double d0 = GP < 2 ? a : c, d1 = b, d2 = GP < 2 ? c : a;
+        double h0, h1, h2;
+        weno_h<double, GP>(umm, um, u, up, upp, h0, h1, h2);
+        double w0 = d0 * f0, w1 = d1 * f1, w2 = d2 * f2;
+        const double S = w0 + w1 + w2;
+#if WENOFV_STRICT
+        w0 /= S; w1 /= S; w2 /= S;
+        return w0 * h0 + w1 * h1 + w2 * h2;
+#else
+        return (w0 * h0 + w1 * h1 + w2 * h2) / S;
+#endif
+    }
+    __device__ __forceinline__ void eval4(double *o) const
+    {
+        o[0] = eval<0>(); o[1] = eval<1>(); o[2] = eval<2>(); o[3] = eval<3>();
+    }
+    __device__ __forceinline__ void eval03(double &o0, double &o3) const
+    {
+        o0 = eval<0>(); o3 = eval<3>();
+    }
+};
+
 // ------------------------------------------------------------------------------------
 // equations
 // ------------------------------------------------------------------------------------

@@ -21,6 +21,7 @@
 // contents, but two calls whose work overlaps on the GPU race on it and corrupt each other.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
 #include <mutex>
 
@@ -92,7 +93,7 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
         set_error("the no-allocation step needs 2*nx + ny <= %d", NOALLOC_METRIC_DOUBLES);
         return WENOFV_EINVAL;
     }
-    const int tx = strictf ? strict::stage_tx(eq->eq_kind) : fast::stage_tx(eq->eq_kind);
+    const int tx = strictf ? strict::stage_tx(eq->eq_kind, cfg->scheme) : fast::stage_tx(eq->eq_kind, cfg->scheme);
     const long nwork = (long)((cfg->nx + tx - 1) / tx) * ((cfg->ny + NOALLOC_ROWS - 1) / NOALLOC_ROWS);
     if (nwork > NOALLOC_MAX_WORK) { set_error("the no-allocation step takes at most %d work items", NOALLOC_MAX_WORK); return WENOFV_EINVAL; }
 
@@ -122,6 +123,7 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
     d.eq_kind = eq->eq_kind;
     d.cfl = cfg->cfl;
     d.dX = (cfg->xr - cfg->xl) / cfg->nx;
+    d.dx4 = std::pow(d.dX, 4); // the reference's pow(m_deltaX, 4), include/Utility.hpp:313
     d.dY = (cfg->yr - cfg->yl) / cfg->ny;
     d.eq = EqParams{eq->eq_kind, eq->rho10, eq->rho20, eq->sound1, eq->sound2, eq->preb, eq->gamma, eq->adv_u, eq->adv_v};
 

@@ -7,18 +7,19 @@
 // max-wavespeed reduction.  Nothing but the cell averages touches HBM.
 //
 // A work item is a strip of TX columns and a run of rows of one instance.  The CTA streams
-// through the rows: iteration r loads row r+3 (cp.async into an 8-row ring), sweeps row r
-// in y, reconstructs the face states of row r in x, solves the Riemann problems of row r's
-// x-faces and of the y-faces between rows r-1 and r, and updates row r-1.  The y-sweep of a
-// column is shared by the 7 cells whose stencils contain it (the reference recomputes it
-// per cell, src/WENOFV.cpp:670-687 and :796-833, with identical operands).
+// through the rows: iteration r loads row r+H+1 (cp.async into an 8-row ring; H = 2 for the
+// 5-point WENO-JS/Z, 3 for the 7-point WENOEXP), sweeps row r in y, reconstructs the face
+// states of row r in x, solves the Riemann problems of row r's x-faces and of the y-faces
+// between rows r-1 and r, and updates row r-1.  The y-sweep of a column is shared by the 7
+// cells whose stencils contain it (the reference recomputes it per cell,
+// src/WENOFV.cpp:670-687 and :796-833, with identical operands).
 //
 // Thread mapping (NT = 128 threads): a unit of the y-sweep is (position, variable), of the
 // x-sweep (cell, variable), of the Riemann phase (face, Gauss point) and of the update
 // (cell, variable); groups of NV (or 4) consecutive lanes belong to the same position, cell
 // or face, so characteristic projections, the limiter's theta and the GL quadrature sums
-// exchange values by warp shuffles.  TX = NT/NV - 6 makes the y-sweep exactly one unit per
-// thread.
+// exchange values by warp shuffles.  TX = NT/NV - 2(H+1) makes the y-sweep exactly one unit
+// per thread.
 #pragma once
 #include "wenofv_math.cuh"
 
@@ -37,7 +38,24 @@ namespace fast {
 #endif
 
 constexpr int NT = 128;
-constexpr int G = 3; // ghost layers / stencil half-width, src/WENOFV.cpp:59
+
+// the reconstruction of one stencil at the Gauss-Lobatto points, by scheme: the 5-point
+// WENO-JS/Z (half-width H = 2) or the 7-point WENOEXP (H = 3, FP64 only)
+template <class R, int SCH> struct StencilRecon {
+    static constexpr int H = 2, NS = 5;
+    Weno5<R, SCH> W;
+    __device__ __forceinline__ void init(const R *v, int scheme, double) { W.init(scheme, v[0], v[1], v[2], v[3], v[4]); }
+    __device__ __forceinline__ void eval4(R *o) const { W.eval4(o); }
+    __device__ __forceinline__ void eval03(R &o0, R &o3) const { W.eval03(o0, o3); }
+};
+template <class R> struct StencilRecon<R, 2> {
+    static_assert(sizeof(R) == sizeof(double), "WENOEXP runs in FP64");
+    static constexpr int H = 3, NS = 7;
+    WenoExp W;
+    __device__ __forceinline__ void init(const R *v, int, double dx4) { W.init(v, dx4); }
+    __device__ __forceinline__ void eval4(R *o) const { W.eval4(o); }
+    __device__ __forceinline__ void eval03(R &o0, R &o3) const { W.eval03(o0, o3); }
+};
 
 __device__ __forceinline__ int map_index(int k, int n, int bc)
 {
@@ -120,15 +138,20 @@ __device__ __forceinline__ double block_min(double v, double *s_red)
     return m;
 }
 
-template <int EQ> struct StageGeom {
+// strip geometry for stencil half-width H: a cell's face states need the y-sweep at the
+// H positions on each side of it and its neighbours', so the strip carries GH = H + 1
+// halo positions on each side (GH = 3 is the reference's ghost layer count,
+// src/WENOFV.cpp:59)
+template <int EQ, int H> struct StageGeom {
     static constexpr int NV = EqTraits<EQ>::NV;
-    static constexpr int TX = NT / NV - 2 * G; // interior columns per strip
-    static constexpr int P = TX + 2 * G;       // y-sweep positions per row
+    static constexpr int GH = H + 1;
+    static constexpr int TX = NT / NV - 2 * GH; // interior columns per strip
+    static constexpr int P = TX + 2 * GH;       // y-sweep positions per row
 };
 
 // shared memory of one CTA (doubles)
-template <int EQ> struct StageSmem {
-    static constexpr int NV = StageGeom<EQ>::NV, TX = StageGeom<EQ>::TX, P = StageGeom<EQ>::P;
+template <int EQ, int H> struct StageSmem {
+    static constexpr int NV = StageGeom<EQ, H>::NV, TX = StageGeom<EQ, H>::TX, P = StageGeom<EQ, H>::P;
     // Strides are padded so that the lanes of a half-warp (8-byte accesses are served 16
     // lanes at a time) hit distinct bank pairs: rows of 4 variables at P+4 doubles
     // (variable v of 4 neighbouring positions: banks 8v + 2p), positions and cells at an odd
@@ -155,20 +178,20 @@ template <int EQ> struct StageSmem {
 };
 
 // one row of NV x P stage values into shared memory (ghost fill = index map), cp.async 8 B
-template <int EQ>
-__device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ>::PS], const double *buf, const InstDesc &D, int row, int i0,
-                                         InstState *st)
+template <int EQ, int H>
+__device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
+                                         int i0, InstState *st)
 {
-    constexpr int P = StageGeom<EQ>::P, NV = StageGeom<EQ>::NV;
+    constexpr int P = StageGeom<EQ, H>::P, NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
     const int jj = map_index(row, D.ny, D.bc);
     const size_t plane = (size_t)D.ny * D.pitch;
 #pragma unroll
     for (int e = threadIdx.x; e < NV * P; e += NT) {
         const int v = e / P, p = e - v * P;
-        const int ii = map_index(i0 - G + p, D.nx, D.bc);
+        const int ii = map_index(i0 - GH + p, D.nx, D.bc);
 #if WENOFV_CHECK_BOUNDS
         if (jj < 0 || jj >= D.ny || ii < 0 || ii >= D.nx) { // record and skip the access
-            flag_error(st, 16u /* WENOFV_FLAG_BOUNDS */, (long long)row * D.nx + (i0 - G + p));
+            flag_error(st, 16u /* WENOFV_FLAG_BOUNDS */, (long long)row * D.nx + (i0 - GH + p));
             continue;
         }
 #else
@@ -189,10 +212,10 @@ template <bool DEV, class R> __device__ __forceinline__ double anchor(double c, 
 // ---- phase 0: the per-cell eigensystem data (L/R rows, wave speeds) of row r at the
 // strip's P positions, computed once per cell by one thread each (threads t0 .. t0+n-1)
 // instead of by every lane that needs it.  Identical arithmetic to the per-lane form.
-template <int EQ, int RECON>
-__device__ __forceinline__ void phase_eigen(StageSmem<EQ> &S, const InstDesc &D, int r, int t0, int n)
+template <int EQ, int RECON, int H>
+__device__ __forceinline__ void phase_eigen(StageSmem<EQ, H> &S, const InstDesc &D, int r, int t0, int n)
 {
-    constexpr int NV = StageGeom<EQ>::NV, P = StageGeom<EQ>::P;
+    constexpr int NV = StageGeom<EQ, H>::NV, P = StageGeom<EQ, H>::P;
     if constexpr (NV > 1) {
         if (!(RECON == 1 || D.limiter)) return;
         for (int p = (int)threadIdx.x - t0; p < P; p += n) {
@@ -216,31 +239,36 @@ __device__ __forceinline__ void phase_eigen(StageSmem<EQ> &S, const InstDesc &D,
 // FP32 rounds the small differences, not the large averages; the result is re-anchored in
 // FP64.
 template <int EQ, int RECON, class R, int SCH>
-__device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D, int r)
+__device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>::H> &S, const InstDesc &D, int r)
 {
-    constexpr int NV = StageGeom<EQ>::NV;
+    using SR = StencilRecon<R, SCH>;
+    constexpr int H = SR::H, NS = SR::NS;
+    constexpr int NV = StageGeom<EQ, H>::NV;
     constexpr bool DEV = sizeof(R) < sizeof(double); // deviation form
     const int t = threadIdx.x;
     const int p = t / NV, v = t - p * NV;
     if (RECON != 1 || NV == 1) {
         // conservative: the averages; primitive (RECONSTRUCTIONTYPE 2, 3): the primitive
-        // variables of each of the 5 cells (src/WENOFV.cpp:944-979)
-        double st[5];
+        // variables of each of the NS cells (src/WENOFV.cpp:944-979)
+        double st[NS];
 #pragma unroll
-        for (int m = 0; m < 5; m++) {
+        for (int m = 0; m < NS; m++) {
             if constexpr (RECON >= 2 && NV == 4) {
                 double U4[4], W4[4];
 #pragma unroll
-                for (int j = 0; j < 4; j++) U4[j] = S.su[(r - 2 + m) & 7][j][p];
+                for (int j = 0; j < 4; j++) U4[j] = S.su[(r - H + m) & 7][j][p];
                 tp_to_primitive(D.eq, RECON, U4, W4);
                 st[m] = W4[v];
             } else {
-                st[m] = S.su[(r - 2 + m) & 7][v][p];
+                st[m] = S.su[(r - H + m) & 7][v][p];
             }
         }
-        const double c0 = DEV ? st[2] : 0.0;
-        Weno5<R, SCH> W;
-        W.init(D.scheme, (R)(st[0] - c0), (R)(st[1] - c0), (R)(st[2] - c0), (R)(st[3] - c0), (R)(st[4] - c0));
+        const double c0 = DEV ? st[H] : 0.0;
+        R sv[NS];
+#pragma unroll
+        for (int m = 0; m < NS; m++) sv[m] = (R)(st[m] - c0);
+        SR W;
+        W.init(sv, D.scheme, D.dx4);
         R o[4];
         W.eval4(o);
 #pragma unroll
@@ -252,7 +280,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
         // of L against FP32 rows of R (|R L - I| ~ 3e-4) would mix the large partial density
         // into the small momenta.
         double Uc[NV], Lrow[NV], Rrow[NV];
-        R pr[5];
+        R pr[NS];
 #pragma unroll
         for (int j = 0; j < NV; j++) Uc[j] = S.su[r & 7][j][p];
         eigen_rows_of<EQ>(D.eq, S.se[p], false, v, Lrow, Rrow);
@@ -264,14 +292,14 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
             for (int j = 0; j < NV; j++) lc += Lrow[j] * Uc[j];
         }
 #pragma unroll
-        for (int m = 0; m < 5; m++) {
+        for (int m = 0; m < NS; m++) {
             double s = 0.0;
 #pragma unroll
-            for (int j = 0; j < NV; j++) s += Lrow[j] * S.su[(r - 2 + m) & 7][j][p];
+            for (int j = 0; j < NV; j++) s += Lrow[j] * S.su[(r - H + m) & 7][j][p];
             pr[m] = DEV ? (R)(s - lc) : (R)s;
         }
-        Weno5<R, SCH> W;
-        W.init(D.scheme, pr[0], pr[1], pr[2], pr[3], pr[4]);
+        SR W;
+        W.init(pr, D.scheme, D.dx4);
         R cg[4];
         W.eval4(cg);
         const int lane = t & 31, gbase = lane & ~(NV - 1);
@@ -297,9 +325,12 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ> &S, const InstDesc &D
 // ---- phase 2: x-direction sweep + limiter of row r (src/WENOFV.cpp:690-721, :836-880,
 //      limiter :1895-2000) -> face states (FP64 in every form) ------------------------------
 template <int EQ, int RECON, class R, int SCH>
-__device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D, InstState *st, int r, int i0, int TXe)
+__device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>::H> &S, const InstDesc &D, InstState *st, int r,
+                                             int i0, int TXe)
 {
-    constexpr int NV = StageGeom<EQ>::NV, TX = StageGeom<EQ>::TX;
+    using SR = StencilRecon<R, SCH>;
+    constexpr int H = SR::H, NS = SR::NS;
+    constexpr int NV = StageGeom<EQ, H>::NV, TX = StageGeom<EQ, H>::TX, GH = StageGeom<EQ, H>::GH;
     constexpr bool DEV = sizeof(R) < sizeof(double);
     const int t = threadIdx.x;
     const int cu = t / NV, v = t - cu * NV;
@@ -314,18 +345,21 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
             if constexpr (RECON >= 2 && NV == 4) {
                 double U4[4], W4[4];
 #pragma unroll
-                for (int j = 0; j < 4; j++) U4[j] = S.su[r & 7][j][c + G];
+                for (int j = 0; j < 4; j++) U4[j] = S.su[r & 7][j][c + GH];
                 tp_to_primitive(D.eq, RECON, U4, W4);
                 cc = W4[v];
             } else {
-                cc = S.su[r & 7][v][c + G];
+                cc = S.su[r & 7][v][c + GH];
             }
         }
 #pragma unroll
         for (int gpj = 0; gpj < 4; gpj++) {
-            Weno5<R, SCH> W;
-            W.init(D.scheme, (R)(S.sy[c + 1][gpj * NV + v] - cc), (R)(S.sy[c + 2][gpj * NV + v] - cc), (R)(S.sy[c + 3][gpj * NV + v] - cc),
-                   (R)(S.sy[c + 4][gpj * NV + v] - cc), (R)(S.sy[c + 5][gpj * NV + v] - cc));
+            // the stencil of cell c: positions c+GH-H .. c+GH+H = c+1 .. c+1+2H
+            R sv[NS];
+#pragma unroll
+            for (int m = 0; m < NS; m++) sv[m] = (R)(S.sy[c + 1 + m][gpj * NV + v] - cc);
+            SR W;
+            W.init(sv, D.scheme, D.dx4);
             if (gpj == 0 || gpj == 3) {
                 R o[4];
                 W.eval4(o);
@@ -355,8 +389,8 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
     } else {
         double Uc[NV], Lrow[NV], Rrow[NV]; // FP64 in every form, as in the y-sweep
 #pragma unroll
-        for (int j = 0; j < NV; j++) Uc[j] = S.su[r & 7][j][c + G];
-        eigen_rows_of<EQ>(D.eq, S.se[c + G], true, v, Lrow, Rrow);
+        for (int j = 0; j < NV; j++) Uc[j] = S.su[r & 7][j][c + GH];
+        eigen_rows_of<EQ>(D.eq, S.se[c + GH], true, v, Lrow, Rrow);
         double lc = 0.0; // L Uc of the deviation form, as in the y-sweep
         if constexpr (DEV) {
 #pragma unroll
@@ -366,16 +400,16 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
         // that point's characteristic values are live (not all twelve)
 #pragma unroll
         for (int gpj = 0; gpj < 4; gpj++) {
-            R pr[5];
+            R pr[NS];
 #pragma unroll
-            for (int m = 0; m < 5; m++) {
+            for (int m = 0; m < NS; m++) {
                 double s = 0.0;
 #pragma unroll
                 for (int j = 0; j < NV; j++) s += Lrow[j] * S.sy[c + 1 + m][gpj * NV + j];
                 pr[m] = DEV ? (R)(s - lc) : (R)s;
             }
-            Weno5<R, SCH> W;
-            W.init(D.scheme, pr[0], pr[1], pr[2], pr[3], pr[4]);
+            SR W;
+            W.init(pr, D.scheme, D.dx4);
             R cg[4];
             const bool all4 = gpj == 0 || gpj == 3;
             if (all4) W.eval4(cg);
@@ -403,8 +437,8 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
     if (NLIM > 0 && D.limiter) {
         double ub[NV];
 #pragma unroll
-        for (int j = 0; j < NV; j++) ub[j] = S.su[r & 7][j][c + G];
-        const double mu1 = S.smu[c + G][0], mu2 = S.smu[c + G][1];
+        for (int j = 0; j < NV; j++) ub[j] = S.su[r & 7][j][c + GH];
+        const double mu1 = S.smu[c + GH][0], mu2 = S.smu[c + GH][1];
         double th = 1.0;
         if (v < NLIM) {
             const double uave = ub[v];
@@ -464,10 +498,11 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ> &S, const InstDesc &D
 // x-faces of row r (when r is an interior row of the item) and y-faces between rows r-1
 // and r (when r-1 >= j0-1 and r <= j1).  Four consecutive lanes hold the four Gauss
 // points of one face; lane gp = 0 sums them in the reference's order.
-template <int EQ, class R, int FLX>
-__device__ __forceinline__ void phase_riemann(StageSmem<EQ> &S, const InstDesc &D, InstState *st, int r, int i0, int j0, int j1, int TXe)
+template <int EQ, class R, int FLX, int H>
+__device__ __forceinline__ void phase_riemann(StageSmem<EQ, H> &S, const InstDesc &D, InstState *st, int r, int i0, int j0, int j1,
+                                              int TXe)
 {
-    constexpr int NV = StageGeom<EQ>::NV, TX = StageGeom<EQ>::TX;
+    constexpr int NV = StageGeom<EQ, H>::NV, TX = StageGeom<EQ, H>::TX;
     const int nxf = (r >= j0 && r < j1) ? (TX + 1) * 4 : 0;
     const int nyf = (r >= j0 && r <= j1) ? TX * 4 : 0;
     const int total = nxf + nyf;
@@ -517,11 +552,11 @@ __device__ __forceinline__ void phase_riemann(StageSmem<EQ> &S, const InstDesc &
 
 // ---- phase 4: RHS scatter (src/WENOFV.cpp:1802-1827) + SSP-RK combination (:376-473)
 //      of row q = r-1, and on the final stage the per-cell CFL step (:486-514) ---------
-template <int EQ>
-__device__ __forceinline__ double phase_update(StageSmem<EQ> &S, const InstDesc &D, InstState *st, const StageLaunch &L,
+template <int EQ, int H>
+__device__ __forceinline__ double phase_update(StageSmem<EQ, H> &S, const InstDesc &D, InstState *st, const StageLaunch &L,
                                                int q, int i0, int TXe, double dt, double cmin)
 {
-    constexpr int NV = StageGeom<EQ>::NV;
+    constexpr int NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
     const int t = threadIdx.x;
     const int cu = t / NV, v = t - cu * NV;
     const bool act = cu < TXe;
@@ -539,8 +574,8 @@ __device__ __forceinline__ double phase_update(StageSmem<EQ> &S, const InstDesc 
     const double idy = 1.0 / dyq, idxc = S.sidxc[c], idxl = S.sidxl[c];
     rhs = ((aL * idxl - aR * idxc) + (aB - aT) * idxc) * idy;
 #endif
-    const double U = S.su[q & 7][v][c + G];
-    const double Un = L.first_stage ? U : S.sun[q & 1][v][c + G];
+    const double U = S.su[q & 7][v][c + GH];
+    const double Un = L.first_stage ? U : S.sun[q & 1][v][c + GH];
     double Unew;
     if (L.rk1) Unew = U + dt * rhs;
     else Unew = L.A * Un + L.B * U + L.C * dt * rhs;
@@ -580,13 +615,14 @@ template <int RECON, class R> struct StageMinBlocks {
     static constexpr int value = sizeof(R) < sizeof(double) ? (RECON == 1 ? 5 : 4) : 3;
 };
 
-// SCH, FLX: the scheme (0 WENO-JS, 1 WENO-Z) and flux (0 LLF, 1 HLLC) of every instance of the
-// launch, as compile-time constants (the engine groups instances by them)
+// SCH, FLX: the scheme (0 WENO-JS, 1 WENO-Z, 2 WENOEXP) and flux (0 LLF, 1 HLLC) of every
+// instance of the launch, as compile-time constants (the engine groups instances by them)
 template <int EQ, int RECON, class R, int SCH, int FLX>
 __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_kernel(const StageLaunch L)
 {
-    constexpr int TX = StageGeom<EQ>::TX;
-    __shared__ StageSmem<EQ> S;
+    constexpr int H = StencilRecon<R, SCH>::H;
+    constexpr int TX = StageGeom<EQ, H>::TX;
+    __shared__ StageSmem<EQ, H> S;
     for (int w = blockIdx.x; w < L.nwork; w += gridDim.x) {
         const WorkItem it = L.work[w];
         const InstDesc &D = L.inst[it.inst];
@@ -611,31 +647,33 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
         }
         const double *bin = D.buf[L.bin];
         const double *bun = D.buf[L.bun];
+        // rows j0-1-H .. j0-1+H, the stencils of the first iteration's row
 #pragma unroll 1
-        for (int m = 0; m < 5; m++) load_row<EQ>(S.su[(it.j0 - G + m) & 7], bin, D, it.j0 - G + m, it.i0, st);
+        for (int m = 0; m <= 2 * H; m++) load_row<EQ, H>(S.su[(it.j0 - 1 - H + m) & 7], bin, D, it.j0 - 1 - H + m, it.i0, st);
         cp_async_commit();
         double cmin = __longlong_as_double(0x7ff0000000000000LL);
 #pragma unroll 1
         for (int r = it.j0 - 1; r <= it.j1; r++) {
             cp_async_wait_all();
             __syncthreads();
-            if (r + 3 <= it.j1 + 2) load_row<EQ>(S.su[(r + 3) & 7], bin, D, r + 3, it.i0, st);
-            if (!L.first_stage && r >= it.j0 && r < it.j1) load_row<EQ>(S.sun[r & 1], bun, D, r, it.i0, st);
+            // row r+H+1 into the slot of row r-H-1 (8 slots: rows r-H .. r+H in use, one in flight)
+            if (r + H + 1 <= it.j1 + H) load_row<EQ, H>(S.su[(r + H + 1) & 7], bin, D, r + H + 1, it.i0, st);
+            if (!L.first_stage && r >= it.j0 && r < it.j1) load_row<EQ, H>(S.sun[r & 1], bun, D, r, it.i0, st);
             cp_async_commit();
             if (r == it.j0 - 1) { // eigensystems of the first row; later rows come from phase 3
-                phase_eigen<EQ, RECON>(S, D, r, 0, NT);
+                phase_eigen<EQ, RECON, H>(S, D, r, 0, NT);
                 __syncthreads();
             }
             phase_ysweep<EQ, RECON, R, SCH>(S, D, r);
             __syncthreads();
             phase_xsweep<EQ, RECON, R, SCH>(S, D, st, r, it.i0, TXe);
             __syncthreads();
-            phase_riemann<EQ, R, FLX>(S, D, st, r, it.i0, it.j0, it.j1, TXe);
+            phase_riemann<EQ, R, FLX, H>(S, D, st, r, it.i0, it.j0, it.j1, TXe);
             // the last warp, idle in the second round of Riemann units, prepares the next
             // row's eigensystems (row r+1 is resident; se is not read until the next row)
-            if (threadIdx.x >= NT - 32) phase_eigen<EQ, RECON>(S, D, r + 1, NT - 32, 32);
+            if (threadIdx.x >= NT - 32) phase_eigen<EQ, RECON, H>(S, D, r + 1, NT - 32, 32);
             __syncthreads();
-            if (r - 1 >= it.j0) cmin = phase_update<EQ>(S, D, st, L, r - 1, it.i0, TXe, dt, cmin);
+            if (r - 1 >= it.j0) cmin = phase_update<EQ, H>(S, D, st, L, r - 1, it.i0, TXe, dt, cmin);
         }
         if (L.final_stage && !L.rhs_out) {
             const double m = block_min(cmin, S.sred);
@@ -647,8 +685,9 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
 }
 
 // calculateDeltaT of the current state (src/WENOFV.cpp:474-540) for every instance of the
-// launch, then the loop bookkeeping (FIN_INIT) by the last CTA.
-template <int EQ>
+// launch, then the loop bookkeeping (FIN_INIT) by the last CTA.  TXW: the strip width of the
+// launch's work items.
+template <int EQ, int TXW>
 __global__ void __launch_bounds__(NT) cfl_kernel(const StageLaunch L)
 {
     constexpr int NV = EqTraits<EQ>::NV;
@@ -661,7 +700,7 @@ __global__ void __launch_bounds__(NT) cfl_kernel(const StageLaunch L)
         if (st->done) continue;
         const double *U = D.buf[st->cur_buf];
         const size_t plane = (size_t)D.ny * D.pitch;
-        const int width = min(StageGeom<EQ>::TX, D.nx - it.i0);
+        const int width = min(TXW, D.nx - it.i0);
         double cmin = __longlong_as_double(0x7ff0000000000000LL);
         for (int e = threadIdx.x; e < width * (it.j1 - it.j0); e += NT) {
             const int j = it.j0 + e / width, i = it.i0 + e % width;

@@ -20,6 +20,7 @@ struct InstDesc {
     int nx, ny, pitch, bc;
     int scheme, flux, limiter, recon, eq_kind, pad;
     double cfl, dX, dY;
+    double dx4; // pow(dX, 4) as the host C library rounds it: WENOEXP's smoothness threshold
     EqParams eq;
 };
 
@@ -56,12 +57,13 @@ struct StageLaunch {
 // host launchers exported by each build of wenofv_kernels.cu
 #define WENOFV_DECLARE_LAUNCHERS(NS)                                                                     \
     namespace NS {                                                                                       \
-    int stage_tx(int eq);                                                                                \
+    int stage_tx(int eq, int scheme);                                                                    \
     int launch_stage(int eq, int recon, int fp32, int scheme, int flux, const StageLaunch &L, int grid,  \
                      void *stream);                                                                     \
-    int launch_cfl(int eq, const StageLaunch &L, int grid, void *stream);                               \
+    int launch_cfl(int eq, int scheme, const StageLaunch &L, int grid, void *stream);                   \
     int stage_blocks_per_sm(int eq, int recon, int fp32, int scheme, int flux);                          \
     int probe_weno(int scheme, int fp32, const double *d_st, int n, double *d_out, void *stream);       \
+    int probe_weno_exp(const double *d_st, int n, double dx4, double *d_out, void *stream);             \
     int probe_riemann(const EqParams &P, int flux, int fp32, const double *d_UL, const double *d_UR,   \
                       int n, int xdir, double *d_F, void *stream);                                       \
     int probe_eigen(const EqParams &P, int fp32, const double *d_U, int n, int xdir, double *d_L,       \
