@@ -56,7 +56,7 @@ int main()
     const char *eqn[] = {"two_phase", "linear_advection", "euler"};
     for (int eqk = 0; eqk < 3; eqk++)
         for (int recon = 0; recon < 2; recon++)
-            for (int scheme = 0; scheme < 2; scheme++)
+            for (int scheme = 0; scheme < 3; scheme++)
                 for (int flux = 0; flux < 2; flux++)
                     for (int lim = 0; lim < 2; lim++) {
                         if (eqk == OFV_EQ_LINEAR_ADV && (recon || flux || lim)) continue;

@@ -253,7 +253,10 @@ __device__ __forceinline__ double cube_rn(double x)
 // factors 1 + 2 tau^2 / (beta_k^2 + 1e-16) depend on the stencil only and are formed once.
 // The reference's pow(l, 3) is the C library's (within 0.52 ulp of l^3); here it is l^3
 // rounded once (cube_rn), so the linear weights can differ from the reference's in the last
-// bit where the C library's pow is not correctly rounded.  FP64 only.
+// bit where the C library's pow is not correctly rounded.  FP64 only.  The contracted build
+// shares divisions as Weno5 does: one for both sides' dif5 / dif3, one for the three
+// factors and one for the normalisations of all Gauss points evaluated together (10
+// divisions per stencil in the reference's order, 4 here).
 struct WenoExp {
     double umm, um, u, up, upp; // raw centre-5 values
     double f0, f1, f2;          // 1 + 2 tau^2 / (beta_k^2 + eps)
@@ -274,8 +277,25 @@ struct WenoExp {
     __device__ __forceinline__ void init(const double *v, double dx4)
     {
         umm = v[1]; um = v[2]; u = v[3]; up = v[4]; upp = v[5];
+#if WENOFV_STRICT
         lam[0] = side(v[0], v[1], v[2], v[3], v[4], v[5], dx4);
         lam[1] = side(v[1], v[2], v[3], v[4], v[5], v[6], dx4);
+#else
+        // 6 dif3 compared against 6 dx^4; lambda^2 h^2 = 6 dif5 / (6 dif3) with one division
+        const double a5 = -v[0] + 5.0 * v[1] - 10.0 * v[2] + 10.0 * v[3] - 5.0 * v[4] + v[5];
+        const double a3 = v[0] - 11.0 * v[1] + 28.0 * v[2] - 28.0 * v[3] + 11.0 * v[4] - v[5];
+        const double b5 = -v[1] + 5.0 * v[2] - 10.0 * v[3] + 10.0 * v[4] - 5.0 * v[5] + v[6];
+        const double b3 = v[1] - 11.0 * v[2] + 28.0 * v[3] - 28.0 * v[4] + 11.0 * v[5] - v[6];
+        const double th = 6.0 * dx4;
+        const bool za = fabs(a3) < th, zb = fabs(b3) < th;
+        const double qa = za ? 1.0 : a3, qb = zb ? 1.0 : b3;
+        const double inv3 = 6.0 / (qa * qb);
+        double la = za ? 0.0 : a5 * qb * inv3, lb = zb ? 0.0 : b5 * qa * inv3;
+        if (fabs(la) > 1) la = 1;
+        if (fabs(lb) > 1) lb = 1;
+        lam[0] = la;
+        lam[1] = lb;
+#endif
         const double umax = std_max(std_max(std_max(umm, um), std_max(u, up)), upp);
         const double umin = std_min(std_min(std_min(umm, um), std_min(u, up)), upp);
         double n0, n1, n2, n3, n4;
@@ -296,12 +316,23 @@ struct WenoExp {
         const double b2 = 0.5 * fabs(3 * n2 - 4 * n3 + n4) + fabs(n2 - 2 * n3 + n4);
         const double tau = n0 - 4.0 * n1 + 6.0 * n2 - 4.0 * n3 + n4;
         const double t2 = 2 * (tau * tau); // pow(x, 2.0) is x * x
+#if WENOFV_STRICT
         f0 = 1.0 + t2 / (b0 * b0 + 1e-16);
         f1 = 1.0 + t2 / (b1 * b1 + 1e-16);
         f2 = 1.0 + t2 / (b2 * b2 + 1e-16);
+#else
+        // beta_k^2 + 1e-16 lies in [1e-16, ~40]: the product of the three stays far from
+        // underflow and overflow
+        const double a0 = b0 * b0 + 1e-16, a1 = b1 * b1 + 1e-16, a2 = b2 * b2 + 1e-16;
+        const double a01 = a0 * a1, tq = t2 / (a01 * a2);
+        f0 = 1.0 + a1 * a2 * tq;
+        f1 = 1.0 + a0 * a2 * tq;
+        f2 = 1.0 + a01 * tq;
+#endif
     }
 
-    template <int GP> __device__ __forceinline__ double eval() const
+    // numerator and denominator of the value at GP
+    template <int GP> __device__ __forceinline__ double num_den(double &S) const
     {
         const double l = lam[GP >= 2 ? 1 : 0], l2 = l * l, l3 = cube_rn(l);
         const double a = (GP == 0 || GP == 3) ? 0.3 - 0.057142858 * l + 0.0071428571 * l2 - 0.00077200577 * l3
@@ -315,21 +346,41 @@ struct WenoExp {
         double h0, h1, h2;
         weno_h<double, GP>(umm, um, u, up, upp, h0, h1, h2);
         double w0 = d0 * f0, w1 = d1 * f1, w2 = d2 * f2;
-        const double S = w0 + w1 + w2;
+        S = w0 + w1 + w2;
 #if WENOFV_STRICT
         w0 /= S; w1 /= S; w2 /= S;
         return w0 * h0 + w1 * h1 + w2 * h2;
 #else
-        return (w0 * h0 + w1 * h1 + w2 * h2) / S;
+        return w0 * h0 + w1 * h1 + w2 * h2;
 #endif
     }
+    // S = sum of w_k lies in [~0.05, ~1e19]: products of four stay in range
     __device__ __forceinline__ void eval4(double *o) const
     {
-        o[0] = eval<0>(); o[1] = eval<1>(); o[2] = eval<2>(); o[3] = eval<3>();
+        double q0, q1, q2, q3;
+        const double n0 = num_den<0>(q0), n1 = num_den<1>(q1), n2 = num_den<2>(q2), n3 = num_den<3>(q3);
+#if WENOFV_STRICT
+        o[0] = n0; o[1] = n1; o[2] = n2; o[3] = n3;
+#else
+        const double q01 = q0 * q1, q23 = q2 * q3;
+        const double inv = 1.0 / (q01 * q23);
+        o[0] = n0 * (q1 * q23) * inv;
+        o[1] = n1 * (q0 * q23) * inv;
+        o[2] = n2 * (q01 * q3) * inv;
+        o[3] = n3 * (q01 * q2) * inv;
+#endif
     }
     __device__ __forceinline__ void eval03(double &o0, double &o3) const
     {
-        o0 = eval<0>(); o3 = eval<3>();
+        double q0, q3;
+        const double n0 = num_den<0>(q0), n3 = num_den<3>(q3);
+#if WENOFV_STRICT
+        o0 = n0; o3 = n3;
+#else
+        const double inv = 1.0 / (q0 * q3);
+        o0 = n0 * q3 * inv;
+        o3 = n3 * q0 * inv;
+#endif
     }
 };
 
