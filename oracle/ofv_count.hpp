@@ -3,14 +3,14 @@
 // TEST INFRASTRUCTURE ONLY.  When wenofv_oracle.c is compiled as C++ with -DOFV_COUNTING,
 // every arithmetic scalar of the restated path is an ofv_cnt: each +, -, *, /, sqrt, fabs
 // and comparison increments a global counter.  Division and sqrt count as one flop each
-// (the convention of the roofline table); comparisons and fabs are counted separately and
-// are not flops.
+// (the convention of the roofline table), and so do exp, log and tanh (PRIMITIVE3's THINC
+// profile); comparisons and fabs are counted separately and are not flops.
 #ifndef OFV_COUNT_HPP
 #define OFV_COUNT_HPP
 #include <cmath>
 
 struct ofv_counters {
-    unsigned long long add, mul, div, sqrt, cmp, abs;
+    unsigned long long add, mul, div, sqrt, cmp, abs, tr;
 };
 extern ofv_counters g_ofv_cnt;
 
@@ -55,5 +55,8 @@ inline ofv_cnt fabs(ofv_cnt a) { g_ofv_cnt.abs++; return ofv_cnt(std::fabs(a.v))
 // pow(x, n) with a small integer n, as the restated path uses it: n - 1 multiplications
 inline ofv_cnt pow(ofv_cnt a, double n) { g_ofv_cnt.mul += (unsigned long long)(n - 1); return ofv_cnt(std::pow(a.v, n)); }
 inline bool ofv_isnan(ofv_cnt a) { return std::isnan(a.v); }
+inline ofv_cnt exp(ofv_cnt a) { g_ofv_cnt.tr++; return ofv_cnt(std::exp(a.v)); }
+inline ofv_cnt log(ofv_cnt a) { g_ofv_cnt.tr++; return ofv_cnt(std::log(a.v)); }
+inline ofv_cnt tanh(ofv_cnt a) { g_ofv_cnt.tr++; return ofv_cnt(std::tanh(a.v)); }
 
 #endif

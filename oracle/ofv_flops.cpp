@@ -37,7 +37,7 @@ static void init_state(const ofv_problem &p, std::vector<double> &U)
         }
 }
 
-static double total(const ofv_counters &c) { return (double)(c.add + c.mul + c.div + c.sqrt); }
+static double total(const ofv_counters &c) { return (double)(c.add + c.mul + c.div + c.sqrt + c.tr); }
 
 static double count_rhs(ofv_problem p, int n, ofv_counters *out)
 {

@@ -56,7 +56,7 @@ class Problem:
     scheme: int = 1          # SCHEME (0 WENO-JS, 1 WENO-Z, 2 WENOEXP)
     limiter: int = 0         # PPlimiter
     flux: int = 0            # RIEMANNFLUX (0 LLF, 1 HLLC)
-    recon: int = 1           # RECONSTRUCTIONTYPE (0 conservative, 1 characteristic)
+    recon: int = 1           # RECONSTRUCTIONTYPE (0 conservative, 1 characteristic, 2-4 primitive)
     ref_slabs: int = 0       # 4 = the reference's 4-slab grid metric
     threads: int = 0
     eq_kind: int = EQ_TWO_PHASE
@@ -97,6 +97,8 @@ class Oracle:
         L.ofv_weno_z.argtypes = [_DP, C.c_int]
         L.ofv_weno_exp.restype = C.c_double
         L.ofv_weno_exp.argtypes = [_DP, C.c_int, C.c_double]
+        L.ofv_weno_exp_thinc.restype = C.c_double
+        L.ofv_weno_exp_thinc.argtypes = [_DP, C.c_int, C.c_double]
         L.ofv_set_cube_rounded.argtypes = [C.c_int]
         for n in ("ofv_volume_frac", "ofv_pressure", "ofv_sound_speed"):
             getattr(L, n).restype = C.c_double
@@ -129,8 +131,12 @@ class Oracle:
 
     # pointwise -----------------------------------------------------------------
     def weno(self, scheme: int, v, gp: int, dx: float = 0.0) -> float:
-        """One Gauss-point value: WENO-JS/Z on 5 values, WENOEXP (scheme 2) on 7 and dx."""
+        """One Gauss-point value: WENO-JS/Z on 5 values, WENOEXP (scheme 2) on 7 and dx, and
+        PRIMITIVE3's WENOEXP/THINC z1 kernel (scheme "thinc") on 7 and dx."""
         a = np.ascontiguousarray(v, dtype=np.float64)
+        if scheme == "thinc":
+            assert a.size == 7
+            return self.L.ofv_weno_exp_thinc(a, gp, dx)
         if scheme == 2:
             assert a.size == 7
             return self.L.ofv_weno_exp(a, gp, dx)

@@ -180,6 +180,24 @@ static real_t cube_of(real_t l)
     return pow(l, 3);
 }
 
+/* WENOEXP's linear weights at Gauss point gp, cubics in l2h2 (include/Utility.hpp:362-392,
+ * the same in :553-583) */
+static void exp_linear_weights(int gp, real_t l2h2, real_t *d0, real_t *d1, real_t *d2)
+{
+    const real_t l2 = pow(l2h2, 2), l3 = cube_of(l2h2);
+    if (gp == 0 || gp == 3) {
+        const real_t a = 0.3 - 0.057142858 * l2h2 + 0.0071428571 * l2 - 0.00077200577 * l3;
+        const real_t b = 0.6 + 0.078571429 * l2h2 - 0.0101190476 * l2 + 0.00112012987 * l3;
+        const real_t e = 0.1 - 0.021428571 * l2h2 + 0.0029761905 * l2 - 0.00034812410 * l3;
+        *d0 = gp == 0 ? a : e; *d1 = b; *d2 = gp == 0 ? e : a;
+    } else {
+        const real_t a = 0.16108042 - 0.035187607 * l2h2 + 0.0049466098 * l2 - 0.00058211525 * l3;
+        const real_t b = 0.58636364 + 0.087692641 * l2h2 - 0.0120401515 * l2 + 0.00139436871 * l3;
+        const real_t e = 0.25255594 - 0.052505034 * l2h2 + 0.0070935417 * l2 - 0.00081225346 * l3;
+        *d0 = gp == 1 ? a : e; *d1 = b; *d2 = gp == 1 ? e : a;
+    }
+}
+
 /* WENOEXP (SCHEME 2), include/Utility.hpp:291-470: the linear weights are cubic polynomials
  * in lambda^2 h^2 = dif5 / dif3 (from the 6 points on the side of the Gauss point, clipped at
  * 1, or 0 where |dif3| < dx^4), the smoothness indicators are absolute values on the
@@ -202,18 +220,7 @@ static real_t weno_exp(const real_t *v7, int gp, double dx)
     }
     real_t h0, h1, h2, d0, d1, d2;
     weno_h(gp, mm, m, c, p, pp, &h0, &h1, &h2); /* candidate values from the raw stencil */
-    const real_t l2 = pow(l2h2, 2), l3 = cube_of(l2h2);
-    if (gp == 0 || gp == 3) {
-        const real_t a = 0.3 - 0.057142858 * l2h2 + 0.0071428571 * l2 - 0.00077200577 * l3;
-        const real_t b = 0.6 + 0.078571429 * l2h2 - 0.0101190476 * l2 + 0.00112012987 * l3;
-        const real_t e = 0.1 - 0.021428571 * l2h2 + 0.0029761905 * l2 - 0.00034812410 * l3;
-        d0 = gp == 0 ? a : e; d1 = b; d2 = gp == 0 ? e : a;
-    } else {
-        const real_t a = 0.16108042 - 0.035187607 * l2h2 + 0.0049466098 * l2 - 0.00058211525 * l3;
-        const real_t b = 0.58636364 + 0.087692641 * l2h2 - 0.0120401515 * l2 + 0.00139436871 * l3;
-        const real_t e = 0.25255594 - 0.052505034 * l2h2 + 0.0070935417 * l2 - 0.00081225346 * l3;
-        d0 = gp == 1 ? a : e; d1 = b; d2 = gp == 1 ? e : a;
-    }
+    exp_linear_weights(gp, l2h2, &d0, &d1, &d2);
     const real_t umax = std_max(std_max(std_max(mm, m), std_max(c, p)), pp);
     const real_t umin = std_min(std_min(std_min(mm, m), std_min(c, p)), pp);
     mm = (mm - umin) / (umax - umin + 1e-20);
@@ -236,6 +243,67 @@ static real_t weno_exp(const real_t *v7, int gp, double dx)
     return w0 * h0 + w1 * h1 + w2 * h2;
 }
 
+/* Gauss-Lobatto points of the reference interval (GaussLobatto_ref(4),
+ * third_party/scTools/GaussQuadratureInRef.hpp:250-259) */
+static const double GLOB_X[4] = {-1, -0.447213595499957939281834733746, 0.447213595499957939281834733746, 1};
+
+/* wenoExpWithThincReconstruction, include/Utility.hpp:473-688: PRIMITIVE3's reconstruction of
+ * z1.  Where the centre value is a mixture (1e-6 < u < 1 - 1e-6) a THINC profile (a tanh of
+ * steepness 1.5 through the cell, from its two neighbours); elsewhere WENOEXP's linear weights
+ * (l2h2 unclipped) with WENO-Z's smoothness indicators on the normalised stencil and
+ * w_k = d_k (1 + |beta0 - beta2| / (beta_k + 1e-16)).  The THINC branch's unused A
+ * (:668) is left out. */
+static real_t weno_exp_thinc(const real_t *v7, int gp, double dx)
+{
+    real_t mmm = v7[0], mm = v7[1], m = v7[2], c = v7[3], p = v7[4], pp = v7[5], ppp = v7[6];
+    real_t dif5, dif3;
+    if (gp >= 2) {
+        dif5 = (-mm + 5.0 * m - 10.0 * c + 10.0 * p - 5.0 * pp + ppp);
+        dif3 = (mm - 11.0 * m + 28.0 * c - 28.0 * p + 11.0 * pp - ppp) / 6.0;
+    } else {
+        dif5 = (-mmm + 5.0 * mm - 10.0 * m + 10.0 * c - 5.0 * p + pp);
+        dif3 = (mmm - 11.0 * mm + 28.0 * m - 28.0 * c + 11.0 * p - pp) / 6.0;
+    }
+    real_t l2h2 = 0;
+    if (!(fabs(dif3) < pow(dx, 4))) l2h2 = dif5 / dif3;
+    const int thinc = (1e-6 < c) & (c < 1 - 1e-6);
+    if (!thinc) {
+        real_t h0, h1, h2, d0, d1, d2;
+        weno_h(gp, mm, m, c, p, pp, &h0, &h1, &h2);
+        exp_linear_weights(gp, l2h2, &d0, &d1, &d2);
+        const real_t umax = std_max(std_max(std_max(mm, m), std_max(c, p)), pp);
+        const real_t umin = std_min(std_min(std_min(mm, m), std_min(c, p)), pp);
+        mm = (mm - umin) / (umax - umin + 1e-20);
+        m = (m - umin) / (umax - umin + 1e-20);
+        c = (c - umin) / (umax - umin + 1e-20);
+        p = (p - umin) / (umax - umin + 1e-20);
+        pp = (pp - umin) / (umax - umin + 1e-20);
+        const real_t beta0 = 0.25 * pow(mm - 4 * m + 3 * c, 2) + 13.0 / 12.0 * pow(mm - 2 * m + c, 2);
+        const real_t beta1 = 0.25 * pow(m - p, 2) + 13.0 / 12.0 * pow(m - 2 * c + p, 2);
+        const real_t beta2 = 0.25 * pow(3 * c - 4 * p + pp, 2) + 13.0 / 12.0 * pow(c - 2 * p + pp, 2);
+        const double eps = 1.0e-16;
+        const real_t tau = fabs(beta0 - beta2);
+        real_t w0 = d0 * (1 + tau / (beta0 + eps));
+        real_t w1 = d1 * (1 + tau / (beta1 + eps));
+        real_t w2 = d2 * (1 + tau / (beta2 + eps));
+        const real_t S = w0 + w1 + w2;
+        w0 /= S;
+        w1 /= S;
+        w2 /= S;
+        return w0 * h0 + w1 * h1 + w2 * h2;
+    }
+    const real_t Qmin = std_min(m, p);
+    const real_t Qmax = std_max(m, p) - Qmin;
+    const real_t theta = (p - c >= 0) ? 1 : -1; /* sc_math::Sign, third_party/scTools/MyMath.h:47-50 */
+    const double beta = 1.5;
+    const real_t C = (c - Qmin + 1e-20) / (Qmax + 1e-20);
+    const real_t B = exp(theta * beta * (2.0 * C - 1.0));
+    const real_t xc = (exp(beta) - B) / (B - exp(-beta));
+    const real_t xcc = log(xc) / (2.0 * beta);
+    if ((c - m) * (p - c) < 0) return c;
+    return 0.5 * Qmax * (1 + theta * tanh(beta * ((GLOB_X[gp] + 1) / 2 - xcc))) + Qmin;
+}
+
 /* useWENO dispatch, src/WENOFV.cpp:1873-1893, on a 7-point stencil v7 (the 5-point schemes
  * use its middle 5) */
 static inline real_t weno7(int scheme, const real_t *v7, int gp, double dx)
@@ -243,6 +311,13 @@ static inline real_t weno7(int scheme, const real_t *v7, int gp, double dx)
     if (scheme == 2) return weno_exp(v7, gp, dx);
     const real_t *v = v7 + 1;
     return scheme == 1 ? weno_z(v[0], v[1], v[2], v[3], v[4], gp) : weno_js(v[0], v[1], v[2], v[3], v[4], gp);
+}
+/* variable k of a primitive reconstruction: PRIMITIVE3 (src/WENOFV.cpp:1293-1331) takes z1
+ * through wenoExpWithThincReconstruction and the others through WENO-Z, whatever SCHEME is */
+static inline real_t weno7_var(int scheme, int recon, int k, const real_t *v7, int gp, double dx)
+{
+    if (recon == 4) return k == 0 ? weno_exp_thinc(v7, gp, dx) : weno_z(v7[1], v7[2], v7[3], v7[4], v7[5], gp);
+    return weno7(scheme, v7, gp, dx);
 }
 
 
@@ -253,6 +328,12 @@ double ofv_weno_exp(const double v[7], int gp, double dx)
     real_t r[7];
     for (int k = 0; k < 7; k++) r[k] = v[k];
     return (double)weno_exp(r, gp, dx);
+}
+double ofv_weno_exp_thinc(const double v[7], int gp, double dx)
+{
+    real_t r[7];
+    for (int k = 0; k < 7; k++) r[k] = v[k];
+    return (double)weno_exp_thinc(r, gp, dx);
 }
 
 /* ------------------------------------------------------------------------------------ */
@@ -749,7 +830,7 @@ static void ws_init(ofv_ws *w, const ofv_problem *p)
 {
     w->p = p;
     w->nx = p->nx; w->ny = p->ny; w->nv = ofv_nvar(&p->eq); w->ex = p->nx + 2 * GE;
-    w->H = p->scheme == 2 ? 3 : 2;
+    w->H = (p->scheme == 2 || p->recon == 4) ? 3 : 2;
     w->E = (real_t *)calloc((size_t)w->nv * w->ex * (p->ny + 2 * GE), sizeof(real_t));
     w->Y = (real_t *)calloc((size_t)w->ex * (p->ny + 2) * 16, sizeof(real_t));
     w->FS = (real_t *)calloc((size_t)(p->nx + 2) * (p->ny + 2) * 64, sizeof(real_t));
@@ -868,7 +949,7 @@ static void y_sweep(ofv_ws *w, int i, int j)
         }
         for (int v = 0; v < nv; v++) {
             for (int m = m0; m <= m1; m++) st[m] = prim[m][v];
-            for (int gp = 0; gp < 4; gp++) out[gp * 4 + v] = weno7(p->scheme, st, gp, w->dX);
+            for (int gp = 0; gp < 4; gp++) out[gp * 4 + v] = weno7_var(p->scheme, p->recon, v, st, gp, w->dX);
         }
     } else {
         real_t st[7];
@@ -964,7 +1045,7 @@ static int x_sweep(ofv_ws *w, int i, int j)
                 for (int m = m0; m <= m1; m++) st[m] = Ycell(w, i - 3 + m, j)[gpj * 4 + v];
                 for (int gpi = 0; gpi < 4; gpi++) {
                     if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
-                    ugp[gpi][gpj][v] = weno7(p->scheme, st, gpi, w->dX);
+                    ugp[gpi][gpj][v] = weno7_var(p->scheme, p->recon, v, st, gpi, w->dX);
                 }
             }
         if (p->recon >= 2 && nv > 1) /* the primitive values back to conservative ones */

@@ -59,6 +59,8 @@ double ofv_weno_js(const double v[5], int gp);
 double ofv_weno_z(const double v[5], int gp);
 /* wenoExpthreconstruction (include/Utility.hpp:291-470) on a 7-point stencil, cell size dx */
 double ofv_weno_exp(const double v[7], int gp, double dx);
+/* wenoExpWithThincReconstruction (include/Utility.hpp:473-688), PRIMITIVE3's z1 kernel */
+double ofv_weno_exp_thinc(const double v[7], int gp, double dx);
 /* 0 (default): WENOEXP's l^3 by the C library's pow, as the reference; 1: l^3 rounded once,
  * the device kernels' form */
 void ofv_set_cube_rounded(int on);

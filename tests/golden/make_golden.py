@@ -44,6 +44,9 @@ CASES = [
     ("sharp_exp_char_hllc_lim_rk3", 2, 40, 24, 2, 1, 1, 1, 2, 8, 0.0, False),
     ("column_exp_char_hllc_lim_rk3", 2, 48, 32, 2, 1, 1, 1, 2, 6, 0.0, True),
     ("column_exp_prim_hllc_lim_rk3", 2, 48, 32, 2, 1, 2, 1, 2, 6, 0.0, True),
+    ("smooth_prim3_llf_rk3", 0, 32, 16, 1, 0, 4, 0, 2, 5, 0.0, False),
+    ("sharp_prim3_hllc_lim_rk3", 2, 40, 24, 1, 1, 4, 1, 2, 8, 0.0, False),
+    ("column_prim3_hllc_lim_rk3", 2, 48, 32, 0, 1, 4, 1, 2, 6, 0.0, True),
 ]
 
 PARAMS = {0: dict(rho10=1.2, rho20=1.0, sound1=1.0, sound2=1.0),

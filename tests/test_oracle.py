@@ -37,7 +37,8 @@ def test_oracle_matches_reference_golden(name, oracle_lib):
 @pytest.mark.skipif(not reference_available(), reason="compiled reference not built (make -C oracle ref)")
 @pytest.mark.parametrize("scheme,flux,recon,lim,rk", [(1, 1, 1, 1, 2), (0, 0, 0, 1, 1), (1, 0, 0, 0, 0),
                                                       (1, 1, 2, 1, 2), (0, 0, 2, 0, 1), (1, 1, 3, 1, 2), (0, 1, 3, 0, 2),
-                                                      (2, 1, 1, 1, 2), (2, 0, 0, 0, 1), (2, 1, 2, 1, 2), (2, 1, 3, 0, 2)])
+                                                      (2, 1, 1, 1, 2), (2, 0, 0, 0, 1), (2, 1, 2, 1, 2), (2, 1, 3, 0, 2),
+                                                      (1, 1, 4, 1, 2), (0, 0, 4, 0, 1), (2, 1, 4, 1, 0)])
 def test_oracle_matches_live_reference(scheme, flux, recon, lim, rk, oracle_lib):
     U0, prm = cases.liquid_column(36, 20, seed=5)
     p = Problem(nx=36, ny=20, rk=rk, scheme=scheme, flux=flux, recon=recon, limiter=lim, ref_slabs=4,
@@ -90,6 +91,28 @@ def test_weno_exp_cube_modes_agree(oracle_lib):
             continue
         with oracle_lib.cube_rounded():
             assert np.array_equal(oracle_lib.rhs(problem_of(meta), g["U0"]), g["rhs"])
+
+
+def test_thinc_profile(oracle_lib):
+    # PRIMITIVE3's z1 kernel: in a mixed cell between monotone neighbours the THINC tanh
+    # profile stays within the neighbours' range and is monotone over the Gauss points; at a
+    # local extremum it returns the cell value; in a pure cell it is WENO (exact on a flat
+    # stencil)
+    rng = np.random.default_rng(4)
+    for _ in range(200):
+        lo, hi = np.sort(rng.uniform(0, 1, 2))
+        c = rng.uniform(max(lo, 2e-6), min(hi, 1 - 2e-6)) if hi - lo > 1e-3 else 0.5
+        if not (lo < c < hi):
+            continue
+        for up in (True, False):
+            v = np.array([lo, lo, lo, c, hi, hi, hi]) if up else np.array([hi, hi, hi, c, lo, lo, lo])
+            g = [oracle_lib.weno("thinc", v, gp, 0.01) for gp in range(4)]
+            assert all(min(lo, hi) - 1e-12 <= x <= max(lo, hi) + 1e-12 for x in g)
+            assert all(np.diff(g) >= -1e-15) if up else all(np.diff(g) <= 1e-15)
+    v = np.array([0.1, 0.2, 0.3, 0.5, 0.2, 0.1, 0.0])  # extremum at the centre
+    assert all(oracle_lib.weno("thinc", v, gp, 0.01) == 0.5 for gp in range(4))
+    flat = np.full(7, 1.0)  # a pure liquid cell: no THINC
+    assert all(oracle_lib.weno("thinc", flat, gp, 0.01) == pytest.approx(1.0, rel=1e-15) for gp in range(4))
 
 
 def test_weno_flat_stencil(oracle_lib):
