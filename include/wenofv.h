@@ -3,7 +3,7 @@
  *
  * The library replaces the hot path of the reference solver's CWENOFV class
  * (infinity-07/two-phase-3equation-2D-pal-column): the ghost-cell fill, the
- * dimension-by-dimension WENO-JS/WENO-Z reconstruction at Gauss-Lobatto points, the
+ * dimension-by-dimension WENO-JS/WENO-Z/WENOEXP reconstruction at Gauss-Lobatto points, the
  * bound-preserving theta limiter, the LLF/HLLC Riemann fluxes with Gauss-Lobatto face
  * quadrature, the SSP-RK stage combination and the CFL max-wavespeed reduction.  The whole
  * domain stays resident in one GPU's HBM; the reference's 4-rank MPI x-slab
@@ -90,8 +90,10 @@ typedef struct {
     int pp_limiter;        /* PPlimiter: 0 off, 1 on */
     int riemann_flux;      /* RIEMANNFLUX: 0 LLF, 1 HLLC */
     int reconstruction;    /* RECONSTRUCTIONTYPE: 0 conservative, 1 characteristic, 2 primitive
-                              (z1, rho1, u, v), 3 primitive2 (z1, p, u, v); 2-3 for the two-phase
-                              model (src/WENOFV.cpp:884-1204); 4 (THINC) is not supported */
+                              (z1, rho1, u, v), 3 primitive2 (z1, p, u, v), 4 primitive3 (z1 by
+                              WENOEXP/THINC, p, u, v by WENO-Z whatever SCHEME is; FP64 forms
+                              only); 2-4 for the two-phase model (src/WENOFV.cpp:884-1372);
+                              5 (ThincOnlyForZ1, not dispatched by the reference) is not supported */
     int ref_slabs;         /* 0: uniform cell sizes; P > 0: cell sizes exactly as the
                               reference's P-slab grid generator rounds them (src/WENOFV.cpp:89-123) */
     int precision;         /* WENOFV_FP64, WENOFV_FP64_STRICT, WENOFV_FP32_BULK */

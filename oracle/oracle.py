@@ -100,6 +100,7 @@ class Oracle:
         L.ofv_weno_exp_thinc.restype = C.c_double
         L.ofv_weno_exp_thinc.argtypes = [_DP, C.c_int, C.c_double]
         L.ofv_set_cube_rounded.argtypes = [C.c_int]
+        L.ofv_set_thinc_ulp.argtypes = [C.c_int]
         for n in ("ofv_volume_frac", "ofv_pressure", "ofv_sound_speed"):
             getattr(L, n).restype = C.c_double
             getattr(L, n).argtypes = [EP, _DP]
@@ -128,6 +129,17 @@ class Oracle:
             yield self
         finally:
             self.L.ofv_set_cube_rounded(0)
+
+    @contextlib.contextmanager
+    def thinc_ulp(self):
+        """PRIMITIVE3's THINC exp/log/tanh each moved one ulp up inside the block: the
+        difference to the default run measures how far the reference's own result moves
+        with the last bit of its math library.  The switch is process-wide."""
+        self.L.ofv_set_thinc_ulp(1)
+        try:
+            yield self
+        finally:
+            self.L.ofv_set_thinc_ulp(0)
 
     # pointwise -----------------------------------------------------------------
     def weno(self, scheme: int, v, gp: int, dx: float = 0.0) -> float:

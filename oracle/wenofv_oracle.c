@@ -243,6 +243,34 @@ static real_t weno_exp(const real_t *v7, int gp, double dx)
     return w0 * h0 + w1 * h1 + w2 * h2;
 }
 
+/* exp, log and tanh of the THINC profile: the C library's, or (ofv_set_thinc_ulp(1), a
+ * sensitivity probe for tests) each result moved one ulp up.  exp at exactly +-1.5 stays
+ * exact there: those are the degenerate profiles (C = 0 or 1) whose xc is exactly 0 or inf
+ * because B equals the compile-time constant exp(+-beta). */
+static int g_thinc_ulp = 0;
+void ofv_set_thinc_ulp(int on) { g_thinc_ulp = on; }
+static real_t thinc_exp(real_t x)
+{
+#ifndef OFV_COUNTING
+    if (g_thinc_ulp && x != 1.5 && x != -1.5) return nextafter(exp(x), INFINITY);
+#endif
+    return exp(x);
+}
+static real_t thinc_log(real_t x)
+{
+#ifndef OFV_COUNTING
+    if (g_thinc_ulp) return nextafter(log(x), INFINITY);
+#endif
+    return log(x);
+}
+static real_t thinc_tanh(real_t x)
+{
+#ifndef OFV_COUNTING
+    if (g_thinc_ulp) return nextafter(tanh(x), INFINITY);
+#endif
+    return tanh(x);
+}
+
 /* Gauss-Lobatto points of the reference interval (GaussLobatto_ref(4),
  * third_party/scTools/GaussQuadratureInRef.hpp:250-259) */
 static const double GLOB_X[4] = {-1, -0.447213595499957939281834733746, 0.447213595499957939281834733746, 1};
@@ -297,11 +325,11 @@ static real_t weno_exp_thinc(const real_t *v7, int gp, double dx)
     const real_t theta = (p - c >= 0) ? 1 : -1; /* sc_math::Sign, third_party/scTools/MyMath.h:47-50 */
     const double beta = 1.5;
     const real_t C = (c - Qmin + 1e-20) / (Qmax + 1e-20);
-    const real_t B = exp(theta * beta * (2.0 * C - 1.0));
+    const real_t B = thinc_exp(theta * beta * (2.0 * C - 1.0));
     const real_t xc = (exp(beta) - B) / (B - exp(-beta));
-    const real_t xcc = log(xc) / (2.0 * beta);
+    const real_t xcc = thinc_log(xc) / (2.0 * beta);
     if ((c - m) * (p - c) < 0) return c;
-    return 0.5 * Qmax * (1 + theta * tanh(beta * ((GLOB_X[gp] + 1) / 2 - xcc))) + Qmin;
+    return 0.5 * Qmax * (1 + theta * thinc_tanh(beta * ((GLOB_X[gp] + 1) / 2 - xcc))) + Qmin;
 }
 
 /* useWENO dispatch, src/WENOFV.cpp:1873-1893, on a 7-point stencil v7 (the 5-point schemes

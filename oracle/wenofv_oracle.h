@@ -64,6 +64,9 @@ double ofv_weno_exp_thinc(const double v[7], int gp, double dx);
 /* 0 (default): WENOEXP's l^3 by the C library's pow, as the reference; 1: l^3 rounded once,
  * the device kernels' form */
 void ofv_set_cube_rounded(int on);
+/* 0 (default): THINC's exp, log and tanh as the C library returns them; 1: each moved one
+ * ulp up (a probe of how much the result depends on the last bit of the math library) */
+void ofv_set_thinc_ulp(int on);
 double ofv_volume_frac(const ofv_eq *eq, const double *U);
 double ofv_pressure(const ofv_eq *eq, const double *U);
 double ofv_sound_speed(const ofv_eq *eq, const double *U);

@@ -44,7 +44,7 @@ def test_default_config_is_shipped_settings(wb):
 
 
 @pytest.mark.parametrize("field,value,code", [
-    ("nx", 0, 1), ("rk_method", 3, 1), ("cfl", 0.0, 1), ("scheme", 3, 1), ("reconstruction", 4, 6), ("reconstruction", 6, 1),
+    ("nx", 0, 1), ("rk_method", 3, 1), ("cfl", 0.0, 1), ("scheme", 3, 1), ("reconstruction", 5, 6), ("reconstruction", 6, 1),
     ("riemann_flux", 4, 1), ("bc", 1, 6), ("precision", 9, 1), ("ref_slabs", 3, 1),
 ])
 def test_invalid_options_rejected(wb, field, value, code):
@@ -65,9 +65,12 @@ def test_invalid_equation_rejected(wb):
     assert L.wenofv_create(C.byref(wb.make_config(8, 8)), C.byref(wb.make_eq(kind=2, gamma=1.0)), C.byref(h)) == wb.EINVAL
     # primitive variables are defined for the two-phase model only
     assert L.wenofv_create(C.byref(wb.make_config(8, 8, recon=2)), C.byref(wb.make_eq(kind=2)), C.byref(h)) == wb.ENOTSUP
-    # WENOEXP has no FP32-bulk form
+    # WENOEXP and PRIMITIVE3 have no FP32-bulk form; PRIMITIVE3 is two-phase only
     c = wb.make_config(8, 8, scheme=2, precision=wb.FP32_BULK)
     assert L.wenofv_create(C.byref(c), C.byref(wb.make_eq()), C.byref(h)) == wb.ENOTSUP
+    c = wb.make_config(8, 8, recon=4, precision=wb.FP32_BULK)
+    assert L.wenofv_create(C.byref(c), C.byref(wb.make_eq()), C.byref(h)) == wb.ENOTSUP
+    assert L.wenofv_create(C.byref(wb.make_config(8, 8, recon=4)), C.byref(wb.make_eq(kind=2)), C.byref(h)) == wb.ENOTSUP
 
 
 def test_null_arguments(wb):

@@ -35,13 +35,13 @@ def child():
     o.L.ofv_set_cube_rounded(1)  # WENOEXP's l^3 as the device kernels form it
     for nx, ny, scheme in [(1, 1, 1), (3, 2, 1), (8, 8, 1), (12, 8, 1), (27, 5, 1), (26, 33, 1), (130, 9, 1),
                            (1, 1, 2), (3, 2, 2), (24, 8, 2), (25, 7, 2), (50, 33, 2)]:
-        for recon in (0, 1, 2, 3):
+        for recon in (0, 1, 2, 3, 4):
             mild = dict(ratio=2.0, eps=0.05)
             U0, prm = cases.liquid_column(nx, ny, seed=nx + 7 * ny, **mild)
             p = Problem(nx=nx, ny=ny, scheme=scheme, flux=1, recon=recon, limiter=1, **prm)
             V, *_ = o.advance(p, U0, t_end=1e9, max_steps=2)
             for prec in (wb.FP64_STRICT, wb.FP64, wb.FP32_BULK):
-                if scheme == 2 and prec == wb.FP32_BULK:
+                if (scheme == 2 or recon == 4) and prec == wb.FP32_BULK:
                     continue
                 cfg = wb.make_config(nx, ny, scheme=scheme, flux=1, recon=recon, limiter=1, precision=prec)
                 eq = wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"])
@@ -51,7 +51,13 @@ def child():
                     flags, cell = s.status()
                     assert flags == 0, (nx, ny, scheme, recon, prec, flags, cell)
                     U = s.download()
-                if prec == wb.FP64_STRICT:
+                if prec == wb.FP64_STRICT and recon == 4:  # THINC: CUDA's exp/log/tanh
+                    o.L.ofv_set_thinc_ulp(1)
+                    W, *_ = o.advance(p, U0, t_end=1e9, max_steps=2)
+                    o.L.ofv_set_thinc_ulp(0)
+                    tol = 16 * np.abs(W - V).max() + 1e-14 * np.abs(V).max()
+                    assert np.abs(U - V).max() <= tol, (nx, ny, scheme, recon)
+                elif prec == wb.FP64_STRICT:
                     assert np.array_equal(U, V), (nx, ny, scheme, recon)
                 n_cases += 1
     for nx, ny, scheme in [(5, 3, 1), (40, 9, 1), (5, 3, 2), (40, 9, 2)]:  # Euler, outflow

@@ -45,8 +45,16 @@ int validate(const wenofv_config *c, const wenofv_eq_params *e)
         set_error("SCHEME 2 (WENOEXP) runs in FP64 only");
         return WENOFV_ENOTSUP;
     }
-    if (c->reconstruction >= 4 && c->reconstruction <= 5) { set_error("RECONSTRUCTIONTYPE %d is not supported", c->reconstruction); return WENOFV_ENOTSUP; }
-    if (c->reconstruction < 0 || c->reconstruction > 3) { set_error("RECONSTRUCTIONTYPE must be 0, 1, 2 or 3"); return WENOFV_EINVAL; }
+    if (c->reconstruction == 5) {
+        // ThincOnlyForZ1: the reference's dispatch has no branch for it (src/WENOFV.cpp:593-598)
+        set_error("RECONSTRUCTIONTYPE 5 is not supported");
+        return WENOFV_ENOTSUP;
+    }
+    if (c->reconstruction < 0 || c->reconstruction > 4) { set_error("RECONSTRUCTIONTYPE must be 0 .. 4"); return WENOFV_EINVAL; }
+    if (c->reconstruction == 4 && c->precision == WENOFV_FP32_BULK) {
+        set_error("RECONSTRUCTIONTYPE 4 (PRIMITIVE3) runs in FP64 only");
+        return WENOFV_ENOTSUP;
+    }
     if (c->reconstruction >= 2 && e && e->eq_kind != WENOFV_EQ_TWO_PHASE) {
         set_error("RECONSTRUCTIONTYPE %d (primitive variables) is defined for the two-phase model only", c->reconstruction);
         return WENOFV_ENOTSUP;
@@ -334,7 +342,9 @@ int Engine::build_work()
         if (!live_[i]) continue;
         const int strict = cfg_[i].precision == WENOFV_FP64_STRICT;
         const int fp32 = cfg_[i].precision == WENOFV_FP32_BULK;
-        const int sch = desc_[i].scheme, flx = desc_[i].eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : desc_[i].flux;
+        // PRIMITIVE3 reconstructs on WENOEXP's 7-point geometry whatever SCHEME is
+        const int sch = desc_[i].recon == 4 ? 2 : desc_[i].scheme;
+        const int flx = desc_[i].eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : desc_[i].flux;
         const long key = ((long)strict << 32) | ((long)fp32 << 24) | (desc_[i].eq_kind << 16) | (desc_[i].recon << 8) |
                          (sch << 4) | flx;
         auto it = key2g.find(key);

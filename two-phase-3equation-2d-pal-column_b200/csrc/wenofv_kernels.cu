@@ -36,24 +36,34 @@ template <int EQ, int RECON, class R, int SCH, int FLX> static const void *stage
 // (WENOEXP, scheme 2, only in FP64)
 template <int EQ, int RECON, class R> static const void *pick_sf(int scheme, int flux)
 {
-    if constexpr (sizeof(R) == sizeof(double)) {
-        if (scheme == 2) {
-            if (EQ == EQ_LINEAR_ADV) return stage_fn<EQ, RECON, R, 2, 0>();
+    if constexpr (RECON == 4) { // PRIMITIVE3: FP64, on the 7-point geometry (scheme 2) whatever SCHEME is
+        if constexpr (EQ == EQ_TWO_PHASE && sizeof(R) == sizeof(double)) {
+            if (scheme != 2) return nullptr;
             return flux ? stage_fn<EQ, RECON, R, 2, 1>() : stage_fn<EQ, RECON, R, 2, 0>();
+        } else {
+            return nullptr;
         }
     } else {
-        if (scheme == 2) return nullptr;
+        if constexpr (sizeof(R) == sizeof(double)) {
+            if (scheme == 2) {
+                if (EQ == EQ_LINEAR_ADV) return stage_fn<EQ, RECON, R, 2, 0>();
+                return flux ? stage_fn<EQ, RECON, R, 2, 1>() : stage_fn<EQ, RECON, R, 2, 0>();
+            }
+        } else {
+            if (scheme == 2) return nullptr;
+        }
+        if (EQ == EQ_LINEAR_ADV) return scheme ? stage_fn<EQ, RECON, R, 1, 0>() : stage_fn<EQ, RECON, R, 0, 0>();
+        if (scheme) return flux ? stage_fn<EQ, RECON, R, 1, 1>() : stage_fn<EQ, RECON, R, 1, 0>();
+        return flux ? stage_fn<EQ, RECON, R, 0, 1>() : stage_fn<EQ, RECON, R, 0, 0>();
     }
-    if (EQ == EQ_LINEAR_ADV) return scheme ? stage_fn<EQ, RECON, R, 1, 0>() : stage_fn<EQ, RECON, R, 0, 0>();
-    if (scheme) return flux ? stage_fn<EQ, RECON, R, 1, 1>() : stage_fn<EQ, RECON, R, 1, 0>();
-    return flux ? stage_fn<EQ, RECON, R, 0, 1>() : stage_fn<EQ, RECON, R, 0, 0>();
 }
 template <class R> static const void *pick_eq(int eq, int recon, int scheme, int flux)
 {
     switch (eq) {
     case EQ_TWO_PHASE:
         return recon == 1 ? pick_sf<EQ_TWO_PHASE, 1, R>(scheme, flux) : recon == 2 ? pick_sf<EQ_TWO_PHASE, 2, R>(scheme, flux)
-             : recon == 3 ? pick_sf<EQ_TWO_PHASE, 3, R>(scheme, flux) : pick_sf<EQ_TWO_PHASE, 0, R>(scheme, flux);
+             : recon == 3 ? pick_sf<EQ_TWO_PHASE, 3, R>(scheme, flux) : recon == 4 ? pick_sf<EQ_TWO_PHASE, 4, R>(scheme, flux)
+                          : pick_sf<EQ_TWO_PHASE, 0, R>(scheme, flux);
     case EQ_EULER: return recon ? pick_sf<EQ_EULER, 1, R>(scheme, flux) : pick_sf<EQ_EULER, 0, R>(scheme, flux);
     case EQ_LINEAR_ADV: return pick_sf<EQ_LINEAR_ADV, 0, R>(scheme, flux);
     default: return nullptr;

@@ -384,6 +384,158 @@ struct WenoExp {
     }
 };
 
+// wenoExpWithThincReconstruction (include/Utility.hpp:473-688): PRIMITIVE3's reconstruction
+// of z1 on a 7-point stencil.  A mixed centre (1e-6 < u < 1 - 1e-6) takes the THINC profile
+// 0.5 Qmax (1 + theta tanh(1.5 ((x_gp + 1) / 2 - xcc))) + Qmin from its two neighbours (the
+// cell value at a local extremum); any other cell WENOEXP's linear weights (lambda^2 h^2
+// unclipped here) with WENO-Z's smoothness indicators on the normalised stencil and
+// w_k = d_k (1 + |beta0 - beta2| / (beta_k + 1e-16)).  exp(1.5) and exp(-1.5), which gcc
+// folds at compile time, are the correctly rounded constants; the exp, log and tanh of the
+// profile are CUDA's, within an ulp or two of the C library's, so THINC cells do not agree
+// with the reference bit for bit.  The profile itself amplifies such last-bit differences
+// (xc = (e^beta - B) / (B - e^-beta) cancels as C nears 0 or 1): moving the C library's
+// results by one ulp moves the reference's own RHS by up to ~1e-9 of max |U|.  FP64 only.
+struct ExpThinc {
+    double umm, um, u, up, upp;
+    double f0, f1, f2, lam[2];    // WENO branch
+    double qmin, qmax, theta, xcc; // THINC branch
+    bool thinc, ext;
+
+    __device__ __forceinline__ void init(const double *v, double dx4)
+    {
+        umm = v[1]; um = v[2]; u = v[3]; up = v[4]; upp = v[5];
+        thinc = (1e-6 < u) & (u < 1 - 1e-6);
+        if (thinc) {
+            constexpr double beta = 1.5, e_beta = 0x1.1ed3fe64fc541p+2, e_mbeta = 0x1.c8f87724b5c1dp-3; // e^1.5, e^-1.5
+            qmin = std_min(um, up);
+            qmax = std_max(um, up) - qmin;
+            theta = (up - u >= 0) ? 1.0 : -1.0; // sc_math::Sign, third_party/scTools/MyMath.h:47-50
+            const double C = (u - qmin + 1e-20) / (qmax + 1e-20);
+            const double arg = theta * beta * (2.0 * C - 1.0);
+            // at exactly +-1.5 (C = 0 or 1) the reference's B is its compile-time exp(+-beta),
+            // so that xc is exactly 0 or inf (the profile saturates) rather than +-tiny
+            const double B = arg == beta ? e_beta : (arg == -beta ? e_mbeta : exp(arg));
+            const double xc = (e_beta - B) / (B - e_mbeta);
+            xcc = log(xc) / (2.0 * beta);
+            ext = (u - um) * (up - u) < 0;
+            return;
+        }
+#if WENOFV_STRICT
+        for (int s = 0; s < 2; s++) {
+            const double *w = v + s;
+            const double dif5 = (-w[0] + 5.0 * w[1] - 10.0 * w[2] + 10.0 * w[3] - 5.0 * w[4] + w[5]);
+            const double dif3 = (w[0] - 11.0 * w[1] + 28.0 * w[2] - 28.0 * w[3] + 11.0 * w[4] - w[5]) / 6.0;
+            lam[s] = fabs(dif3) < dx4 ? 0.0 : dif5 / dif3;
+        }
+#else
+        const double a5 = -v[0] + 5.0 * v[1] - 10.0 * v[2] + 10.0 * v[3] - 5.0 * v[4] + v[5];
+        const double a3 = v[0] - 11.0 * v[1] + 28.0 * v[2] - 28.0 * v[3] + 11.0 * v[4] - v[5];
+        const double b5 = -v[1] + 5.0 * v[2] - 10.0 * v[3] + 10.0 * v[4] - 5.0 * v[5] + v[6];
+        const double b3 = v[1] - 11.0 * v[2] + 28.0 * v[3] - 28.0 * v[4] + 11.0 * v[5] - v[6];
+        const double th = 6.0 * dx4;
+        const bool za = fabs(a3) < th, zb = fabs(b3) < th;
+        const double qa = za ? 1.0 : a3, qb = zb ? 1.0 : b3;
+        const double inv3 = 6.0 / (qa * qb);
+        lam[0] = za ? 0.0 : a5 * qb * inv3;
+        lam[1] = zb ? 0.0 : b5 * qa * inv3;
+#endif
+        const double umax = std_max(std_max(std_max(umm, um), std_max(u, up)), upp);
+        const double umin = std_min(std_min(std_min(umm, um), std_min(u, up)), upp);
+        double n0, n1, n2, n3, n4;
+#if WENOFV_STRICT
+        n0 = (umm - umin) / (umax - umin + 1e-20);
+        n1 = (um - umin) / (umax - umin + 1e-20);
+        n2 = (u - umin) / (umax - umin + 1e-20);
+        n3 = (up - umin) / (umax - umin + 1e-20);
+        n4 = (upp - umin) / (umax - umin + 1e-20);
+#else
+        const double inv = 1.0 / (umax - umin + 1e-20);
+        n0 = (umm - umin) * inv; n1 = (um - umin) * inv; n2 = (u - umin) * inv;
+        n3 = (up - umin) * inv; n4 = (upp - umin) * inv;
+#endif
+        double b0, b1, b2;
+        weno_betas(n0, n1, n2, n3, n4, b0, b1, b2);
+        const double tau = fabs(b0 - b2);
+#if WENOFV_STRICT
+        f0 = 1 + tau / (b0 + 1e-16);
+        f1 = 1 + tau / (b1 + 1e-16);
+        f2 = 1 + tau / (b2 + 1e-16);
+#else
+        // beta_k + 1e-16 in [1e-16, ~80]: the product of the three stays in range
+        const double a0 = b0 + 1e-16, a1 = b1 + 1e-16, a2 = b2 + 1e-16;
+        const double a01 = a0 * a1, tq = tau / (a01 * a2);
+        f0 = 1 + a1 * a2 * tq;
+        f1 = 1 + a0 * a2 * tq;
+        f2 = 1 + a01 * tq;
+#endif
+    }
+
+    template <int GP> __device__ __forceinline__ double thinc_at() const
+    {
+        // (x + 1) / 2 of the reference-interval Gauss-Lobatto points (GaussLobatto_ref(4),
+        // third_party/scTools/GaussQuadratureInRef.hpp:250-259)
+        constexpr double x = GP == 0 ? -1.0 : GP == 1 ? -0.447213595499957939281834733746
+                           : GP == 2 ? 0.447213595499957939281834733746 : 1.0;
+        if (ext) return u;
+        return 0.5 * qmax * (1 + theta * tanh(1.5 * ((x + 1) / 2 - xcc))) + qmin;
+    }
+    // numerator and denominator of the WENO value at GP (strict: the value, S unused)
+    template <int GP> __device__ __forceinline__ double num_den(double &S) const
+    {
+        const double l = lam[GP >= 2 ? 1 : 0], l2 = l * l, l3 = cube_rn(l);
+        const double a = (GP == 0 || GP == 3) ? 0.3 - 0.057142858 * l + 0.0071428571 * l2 - 0.00077200577 * l3
+                                               : 0.16108042 - 0.035187607 * l + 0.0049466098 * l2 - 0.00058211525 * l3;
+        const double b = (GP == 0 || GP == 3) ? 0.6 + 0.078571429 * l - 0.0101190476 * l2 + 0.00112012987 * l3
+                                               : 0.58636364 + 0.087692641 * l - 0.0120401515 * l2 + 0.00139436871 * l3;
+        const double c = (GP == 0 || GP == 3) ? 0.1 - 0.021428571 * l + 0.0029761905 * l2 - 0.00034812410 * l3
+                                               : 0.25255594 - 0.052505034 * l + 0.0070935417 * l2 - 0.00081225346 * l3;
+        const double d0 = GP < 2 ? a : c, d1 = b, d2 = GP < 2 ? c : a;
+        double h0, h1, h2;
+        weno_h<double, GP>(umm, um, u, up, upp, h0, h1, h2);
+        double w0 = d0 * f0, w1 = d1 * f1, w2 = d2 * f2;
+        S = w0 + w1 + w2;
+#if WENOFV_STRICT
+        w0 /= S; w1 /= S; w2 /= S;
+#endif
+        return w0 * h0 + w1 * h1 + w2 * h2;
+    }
+    __device__ __forceinline__ void eval4(double *o) const
+    {
+        if (thinc) {
+            o[0] = thinc_at<0>(); o[1] = thinc_at<1>(); o[2] = thinc_at<2>(); o[3] = thinc_at<3>();
+            return;
+        }
+        double q0, q1, q2, q3;
+        const double n0 = num_den<0>(q0), n1 = num_den<1>(q1), n2 = num_den<2>(q2), n3 = num_den<3>(q3);
+#if WENOFV_STRICT
+        o[0] = n0; o[1] = n1; o[2] = n2; o[3] = n3;
+#else
+        const double q01 = q0 * q1, q23 = q2 * q3; // S in [~0.05, ~1e18]
+        const double inv = 1.0 / (q01 * q23);
+        o[0] = n0 * (q1 * q23) * inv;
+        o[1] = n1 * (q0 * q23) * inv;
+        o[2] = n2 * (q01 * q3) * inv;
+        o[3] = n3 * (q01 * q2) * inv;
+#endif
+    }
+    __device__ __forceinline__ void eval03(double &o0, double &o3) const
+    {
+        if (thinc) {
+            o0 = thinc_at<0>(); o3 = thinc_at<3>();
+            return;
+        }
+        double q0, q3;
+        const double n0 = num_den<0>(q0), n3 = num_den<3>(q3);
+#if WENOFV_STRICT
+        o0 = n0; o3 = n3;
+#else
+        const double inv = 1.0 / (q0 * q3);
+        o0 = n0 * q3 * inv;
+        o3 = n3 * q0 * inv;
+#endif
+    }
+};
+
 // ------------------------------------------------------------------------------------
 // equations
 // ------------------------------------------------------------------------------------

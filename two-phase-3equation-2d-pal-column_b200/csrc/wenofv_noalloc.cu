@@ -83,6 +83,7 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
     if (pitch < cfg->nx) { set_error("pitch (%d) must be at least nx (%d)", pitch, cfg->nx); return WENOFV_EINVAL; }
     const int nv = nvar_of(eq->eq_kind);
     const int recon = eq->eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : cfg->reconstruction;
+    const int sch = recon == 4 ? 2 : cfg->scheme; // PRIMITIVE3: the 7-point geometry
     const int strictf = cfg->precision == WENOFV_FP64_STRICT, fp32 = cfg->precision == WENOFV_FP32_BULK;
     const size_t state = (size_t)nv * cfg->ny * pitch;
     if (state > NOALLOC_STATE_DOUBLES) {
@@ -93,7 +94,7 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
         set_error("the no-allocation step needs 2*nx + ny <= %d", NOALLOC_METRIC_DOUBLES);
         return WENOFV_EINVAL;
     }
-    const int tx = strictf ? strict::stage_tx(eq->eq_kind, cfg->scheme) : fast::stage_tx(eq->eq_kind, cfg->scheme);
+    const int tx = strictf ? strict::stage_tx(eq->eq_kind, sch) : fast::stage_tx(eq->eq_kind, sch);
     const long nwork = (long)((cfg->nx + tx - 1) / tx) * ((cfg->ny + NOALLOC_ROWS - 1) / NOALLOC_ROWS);
     if (nwork > NOALLOC_MAX_WORK) { set_error("the no-allocation step takes at most %d work items", NOALLOC_MAX_WORK); return WENOFV_EINVAL; }
 
@@ -165,8 +166,8 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
     int sms = 0;
     WENOFV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device));
     const int flx = eq->eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : cfg->riemann_flux;
-    const int bps = strictf ? strict::stage_blocks_per_sm(eq->eq_kind, recon, fp32, cfg->scheme, flx)
-                            : fast::stage_blocks_per_sm(eq->eq_kind, recon, fp32, cfg->scheme, flx);
+    const int bps = strictf ? strict::stage_blocks_per_sm(eq->eq_kind, recon, fp32, sch, flx)
+                            : fast::stage_blocks_per_sm(eq->eq_kind, recon, fp32, sch, flx);
     const int grid = (int)(k < (long)sms * (bps > 0 ? bps : 1) ? k : (long)sms * (bps > 0 ? bps : 1));
     for (int stage = 0; stage < stage_count(cfg->rk_method); stage++) {
         const Roles ro = stage_roles(cfg->rk_method, 0, stage);
@@ -184,8 +185,8 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
         L.final_stage = stage == stage_count(cfg->rk_method) - 1;
         L.rk1 = cfg->rk_method == 0;
         stage_coeffs(cfg->rk_method, stage, L.A, L.B, L.C);
-        const int lrc = strictf ? strict::launch_stage(eq->eq_kind, recon, 0, cfg->scheme, flx, L, grid, stream)
-                                : fast::launch_stage(eq->eq_kind, recon, fp32, cfg->scheme, flx, L, grid, stream);
+        const int lrc = strictf ? strict::launch_stage(eq->eq_kind, recon, 0, sch, flx, L, grid, stream)
+                                : fast::launch_stage(eq->eq_kind, recon, fp32, sch, flx, L, grid, stream);
         if (lrc) return cuda_fail((cudaError_t)lrc, "stage kernel launch");
     }
     if (flags) {

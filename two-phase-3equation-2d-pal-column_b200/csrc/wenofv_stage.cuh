@@ -44,7 +44,7 @@ constexpr int NT = 128;
 template <class R, int SCH> struct StencilRecon {
     static constexpr int H = 2, NS = 5;
     Weno5<R, SCH> W;
-    __device__ __forceinline__ void init(const R *v, int scheme, double) { W.init(scheme, v[0], v[1], v[2], v[3], v[4]); }
+    __device__ __forceinline__ void init(const R *v, int scheme, int, double) { W.init(scheme, v[0], v[1], v[2], v[3], v[4]); }
     __device__ __forceinline__ void eval4(R *o) const { W.eval4(o); }
     __device__ __forceinline__ void eval03(R &o0, R &o3) const { W.eval03(o0, o3); }
 };
@@ -52,9 +52,40 @@ template <class R> struct StencilRecon<R, 2> {
     static_assert(sizeof(R) == sizeof(double), "WENOEXP runs in FP64");
     static constexpr int H = 3, NS = 7;
     WenoExp W;
-    __device__ __forceinline__ void init(const R *v, int, double dx4) { W.init(v, dx4); }
+    __device__ __forceinline__ void init(const R *v, int, int, double dx4) { W.init(v, dx4); }
     __device__ __forceinline__ void eval4(R *o) const { W.eval4(o); }
     __device__ __forceinline__ void eval03(R &o0, R &o3) const { W.eval03(o0, o3); }
+};
+// PRIMITIVE3 (RECONSTRUCTIONTYPE 4, src/WENOFV.cpp:1293-1331): z1 (variable 0) through the
+// WENOEXP/THINC kernel, the pressure and the velocities through WENO-Z on the middle 5
+// points, whatever SCHEME is.  FP64 only.
+struct Prim3Recon {
+    static constexpr int H = 3, NS = 7;
+    ExpThinc E;
+    Weno5<double, 1> W;
+    bool z;
+    __device__ __forceinline__ void init(const double *v, int, int var, double dx4)
+    {
+        z = var == 0;
+        if (z) E.init(v, dx4);
+        else W.init(1, v[1], v[2], v[3], v[4], v[5]);
+    }
+    __device__ __forceinline__ void eval4(double *o) const
+    {
+        if (z) E.eval4(o);
+        else W.eval4(o);
+    }
+    __device__ __forceinline__ void eval03(double &o0, double &o3) const
+    {
+        if (z) E.eval03(o0, o3);
+        else W.eval03(o0, o3);
+    }
+};
+// the per-variable reconstruction of a non-characteristic sweep
+template <class R, int SCH, int RECON> struct ReconSel { using type = StencilRecon<R, SCH>; };
+template <class R, int SCH> struct ReconSel<R, SCH, 4> {
+    static_assert(SCH == 2 && sizeof(R) == sizeof(double), "PRIMITIVE3 runs in FP64 on the 7-point geometry");
+    using type = Prim3Recon;
 };
 
 __device__ __forceinline__ int map_index(int k, int n, int bc)
@@ -241,7 +272,7 @@ __device__ __forceinline__ void phase_eigen(StageSmem<EQ, H> &S, const InstDesc 
 template <int EQ, int RECON, class R, int SCH>
 __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>::H> &S, const InstDesc &D, int r)
 {
-    using SR = StencilRecon<R, SCH>;
+    using SR = typename ReconSel<R, SCH, RECON>::type;
     constexpr int H = SR::H, NS = SR::NS;
     constexpr int NV = StageGeom<EQ, H>::NV;
     constexpr bool DEV = sizeof(R) < sizeof(double); // deviation form
@@ -268,7 +299,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
 #pragma unroll
         for (int m = 0; m < NS; m++) sv[m] = (R)(st[m] - c0);
         SR W;
-        W.init(sv, D.scheme, D.dx4);
+        W.init(sv, D.scheme, v, D.dx4);
         R o[4];
         W.eval4(o);
 #pragma unroll
@@ -299,7 +330,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
             pr[m] = DEV ? (R)(s - lc) : (R)s;
         }
         SR W;
-        W.init(pr, D.scheme, D.dx4);
+        W.init(pr, D.scheme, v, D.dx4);
         R cg[4];
         W.eval4(cg);
         const int lane = t & 31, gbase = lane & ~(NV - 1);
@@ -328,7 +359,7 @@ template <int EQ, int RECON, class R, int SCH>
 __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>::H> &S, const InstDesc &D, InstState *st, int r,
                                              int i0, int TXe)
 {
-    using SR = StencilRecon<R, SCH>;
+    using SR = typename ReconSel<R, SCH, RECON>::type;
     constexpr int H = SR::H, NS = SR::NS;
     constexpr int NV = StageGeom<EQ, H>::NV, TX = StageGeom<EQ, H>::TX, GH = StageGeom<EQ, H>::GH;
     constexpr bool DEV = sizeof(R) < sizeof(double);
@@ -359,7 +390,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
 #pragma unroll
             for (int m = 0; m < NS; m++) sv[m] = (R)(S.sy[c + 1 + m][gpj * NV + v] - cc);
             SR W;
-            W.init(sv, D.scheme, D.dx4);
+            W.init(sv, D.scheme, v, D.dx4);
             if (gpj == 0 || gpj == 3) {
                 R o[4];
                 W.eval4(o);
@@ -409,7 +440,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
                 pr[m] = DEV ? (R)(s - lc) : (R)s;
             }
             SR W;
-            W.init(pr, D.scheme, D.dx4);
+            W.init(pr, D.scheme, v, D.dx4);
             R cg[4];
             const bool all4 = gpj == 0 || gpj == 3;
             if (all4) W.eval4(cg);
