@@ -44,10 +44,12 @@ import cases  # noqa: E402
 FLOP_KEYS = {
     "column1024": ("two_phase", 1, 1, 1, 1),    # characteristic, WENO-Z, HLLC, limiter
     "column1024_exp": ("two_phase", 1, 2, 1, 1),  # the same with WENOEXP (7-point stencils)
+    "column1024_prim3": ("two_phase", 4, 1, 1, 1),  # PRIMITIVE3: z1 by WENOEXP/THINC, p, u, v by WENO-Z
     "euler512": ("euler", 0, 1, 1, 0),          # conservative, WENO-Z, HLLC
     "advection128": ("linear_advection", 0, 0, 0, 0),
 }
-BYTES_PER_CELL_STAGE = {"column1024": 96.0, "column1024_exp": 96.0, "euler512": 96.0, "advection128": 24.0}
+BYTES_PER_CELL_STAGE = {"column1024": 96.0, "column1024_exp": 96.0, "column1024_prim3": 96.0, "euler512": 96.0,
+                        "advection128": 24.0}
 
 
 def flops_per_cell_stage(name: str) -> float:
@@ -63,16 +65,18 @@ def flops_per_cell_stage(name: str) -> float:
 
 def workload(name: str, wb, form: int):
     """(U0, config, eq, description dict) of a named workload"""
-    if name in ("column1024", "column1024_exp"):
+    if name in ("column1024", "column1024_exp", "column1024_prim3"):
         sch = 2 if name == "column1024_exp" else 1
+        rec = 4 if name == "column1024_prim3" else 1
         U0, prm = cases.liquid_column(1024, 1024, seed=3)
-        cfg = wb.make_config(1024, 1024, rk=2, cfl=0.5, scheme=sch, limiter=1, flux=1, recon=1, precision=form)
+        cfg = wb.make_config(1024, 1024, rk=2, cfl=0.5, scheme=sch, limiter=1, flux=1, recon=rec, precision=form)
         eq = wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"])
-        desc = dict(workload="liquid_column_1024_ref_eos" + ("_wenoexp" if sch == 2 else ""), grid="1024x1024",
+        desc = dict(workload="liquid_column_1024_ref_eos" + {"column1024": "", "column1024_exp": "_wenoexp",
+                                                             "column1024_prim3": "_primitive3"}[name], grid="1024x1024",
                     equation="two-phase 3-equation, linear EOS "
                     "linearised from stiffened gas (g1=4.4, pinf1=6e3, g2=1.4, pinf2=0) at p=1, density ratio 1000",
-                    bc="periodic", scheme="WENOEXP" if sch == 2 else "WENO-Z", flux="HLLC",
-                    reconstruction="characteristic", limiter=True,
+                    bc="periodic", scheme="WENOEXP" if sch == 2 else ("WENOEXP/THINC (z1), WENO-Z" if rec == 4 else "WENO-Z"),
+                    flux="HLLC", reconstruction="primitive3 (z1, p, u, v)" if rec == 4 else "characteristic", limiter=True,
                     rk="SSP-RK3", cfl=0.5, ic="disk r=0.2 tanh-smoothed over 2 cells, eps=1e-6, seeded periodic "
                     "Gaussian velocity field amplitude 1e-2 (seed 3)")
     elif name == "euler512":
@@ -102,13 +106,14 @@ def cpu_baseline(name: str, steps: int, warmup: int, sample_n: int = 256):
 
     ncores = os.cpu_count() or 1
     sch = "2" if name == "column1024_exp" else "1"
-    if name in ("column1024", "column1024_exp") and O.reference_available():
+    rec = "4" if name == "column1024_prim3" else "1"
+    if name in ("column1024", "column1024_exp", "column1024_prim3") and O.reference_available():
         U0, prm = cases.liquid_column(sample_n, sample_n, seed=3)
         nproc = max(1, ncores // 4)
         with tempfile.TemporaryDirectory() as d:
             U0.tofile(os.path.join(d, "u0.bin"))
             args = [O.REF_BIN, "--testcase", "2", "--nx", str(sample_n), "--ny", str(sample_n), "--rk", "2",
-                    "--cfl", "0.5", "--scheme", sch, "--limiter", "1", "--flux", "1", "--recon", "1",
+                    "--cfl", "0.5", "--scheme", sch, "--limiter", "1", "--flux", "1", "--recon", rec,
                     "--rho10", O._f(prm["rho10"]), "--rho20", O._f(prm["rho20"]), "--sound1", O._f(prm["sound1"]),
                     "--sound2", O._f(prm["sound2"]), "--u0", os.path.join(d, "u0.bin"), "--steps", str(steps),
                     "--warmup", str(warmup), "--time"]
@@ -154,7 +159,7 @@ def cpu_baseline(name: str, steps: int, warmup: int, sample_n: int = 256):
                       threads=ncores)
     else:
         U0, prm = cases.liquid_column(sample_n, sample_n, seed=3)
-        p = O.Problem(nx=sample_n, ny=sample_n, rk=2, cfl=0.5, scheme=int(sch), flux=1, recon=1, limiter=1,
+        p = O.Problem(nx=sample_n, ny=sample_n, rk=2, cfl=0.5, scheme=int(sch), flux=1, recon=int(rec), limiter=1,
                       threads=ncores, **prm)
     orc = O.Oracle()
     dt = orc.compute_dt(p, U0)
@@ -319,7 +324,7 @@ def run_ours(args, rank, world, dist):
     # FP32-bulk beside FP64: the same steps from the same state, device-timed the same way,
     # and the error of its result against the FP64 one
     fp32 = None
-    if form == wb.FP64 and args.workload not in ("advection128", "column1024_exp") and not args.no_fp32:
+    if form == wb.FP64 and args.workload not in ("advection128", "column1024_exp", "column1024_prim3") and not args.no_fp32:
         fp32 = compare_fp32(args, wb, cfg, eq, U0, dt, U_dev_end, ncells, nstages, flush, barrier, dist, world, local)
 
     # end to end through the public API with host arrays (pinned host memory)

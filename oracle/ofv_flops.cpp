@@ -55,11 +55,13 @@ int main()
 {
     const char *eqn[] = {"two_phase", "linear_advection", "euler"};
     for (int eqk = 0; eqk < 3; eqk++)
-        for (int recon = 0; recon < 2; recon++)
+        for (int recon = 0; recon < 5; recon++)
             for (int scheme = 0; scheme < 3; scheme++)
                 for (int flux = 0; flux < 2; flux++)
                     for (int lim = 0; lim < 2; lim++) {
                         if (eqk == OFV_EQ_LINEAR_ADV && (recon || flux || lim)) continue;
+                        if (recon >= 2 && eqk != OFV_EQ_TWO_PHASE) continue; // primitive forms: two-phase only
+                        if (recon == 4 && scheme != 1) continue;               // PRIMITIVE3 ignores SCHEME
                         ofv_problem p{};
                         p.xl = 0; p.xr = 1; p.yl = 0; p.yr = 1;
                         p.bc = OFV_BC_PERIOD; p.rk = 2; p.cfl = 0.5;

@@ -86,7 +86,8 @@ def test_initial_averages_equal_reference(host_bin, tmp_path, testcase):
                                          (2, ("RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=1", "PPlimiter=1")),
                                          (2, ("RECONSTRUCTIONTYPE=0", "RIEMANNFLUX=1", "PPlimiter=1", "STEPMODE=1")),
                                          (2, ("RECONSTRUCTIONTYPE=2", "RIEMANNFLUX=1", "PPlimiter=1")),
-                                         (0, ("RECONSTRUCTIONTYPE=3", "RIEMANNFLUX=0", "PPlimiter=0"))])
+                                         (0, ("RECONSTRUCTIONTYPE=3", "RIEMANNFLUX=0", "PPlimiter=0")),
+                                         (2, ("SCHEME=2", "RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=1", "PPlimiter=1"))])
 def test_host_run_equals_reference(host_bin, tmp_path, testcase, kv):
     nx, ny, tend = 32, 32, 0.01
     out = str(tmp_path / "u.bin")
@@ -97,7 +98,8 @@ def test_host_run_equals_reference(host_bin, tmp_path, testcase, kv):
     opts = dict(x.split("=") for x in kv if not x.startswith("STEPMODE"))
     r10, r20, c1, c2 = CASE_PARAMS[testcase]
     p = Problem(nx=nx, ny=ny, rho10=r10, rho20=r20, sound1=c1, sound2=c2, recon=int(opts["RECONSTRUCTIONTYPE"]),
-                flux=int(opts["RIEMANNFLUX"]), limiter=int(opts["PPlimiter"]), scheme=1, rk=2, cfl=0.5)
+                flux=int(opts["RIEMANNFLUX"]), limiter=int(opts["PPlimiter"]), scheme=int(opts.get("SCHEME", 1)),
+                rk=2, cfl=0.5)
     ref = run_reference(p, testcase=testcase, t_end=tend)
     assert np.array_equal(mine, ref.U)
 
