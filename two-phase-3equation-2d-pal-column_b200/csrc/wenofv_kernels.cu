@@ -81,12 +81,33 @@ static const void *pick_stage(int eq, int recon, int fp32, int scheme, int flux)
     return pick_eq<double>(eq, recon, scheme, flux);
 }
 
+// dynamic shared memory of a stage kernel (the primitive ring; the same for both geometries)
+static int stage_dyn_bytes(int eq, int recon)
+{
+    static_assert(StageDynSmem<EQ_TWO_PHASE, 2, 2>::value == StageDynSmem<EQ_TWO_PHASE, 2, 3>::value, "ring size");
+    return (eq == EQ_TWO_PHASE && recon >= 2) ? StageDynSmem<EQ_TWO_PHASE, 2, 2>::value : 0;
+}
+// static plus dynamic shared memory passes the default 48 KB: opt in (not during a stream
+// capture, where the engine has already done it through stage_blocks_per_sm)
+static cudaError_t allow_dyn(const void *fn, int dyn)
+{
+    if (dyn <= 0) return cudaSuccess;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+}
+
 int launch_stage(int eq, int recon, int fp32, int scheme, int flux, const StageLaunch &L, int grid, void *stream)
 {
     const void *fn = pick_stage(eq, recon, fp32, scheme, flux);
     if (!fn) return (int)cudaErrorInvalidValue;
+    const int dyn = stage_dyn_bytes(eq, recon);
+    if (dyn > 0) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaError_t e = cudaStreamIsCapturing((cudaStream_t)stream, &cs);
+        if (e != cudaSuccess) return (int)e;
+        if (cs == cudaStreamCaptureStatusNone && (e = allow_dyn(fn, dyn)) != cudaSuccess) return (int)e;
+    }
     void *args[] = {(void *)&L};
-    return (int)cudaLaunchKernel(fn, dim3(grid), dim3(NT), args, 0, (cudaStream_t)stream);
+    return (int)cudaLaunchKernel(fn, dim3(grid), dim3(NT), args, (size_t)dyn, (cudaStream_t)stream);
 }
 
 template <int H> static const void *cfl_fn(int eq)
@@ -107,8 +128,10 @@ int stage_blocks_per_sm(int eq, int recon, int fp32, int scheme, int flux)
 {
     const void *fn = pick_stage(eq, recon, fp32, scheme, flux);
     if (!fn) return 0;
+    const int dyn = stage_dyn_bytes(eq, recon);
+    if (allow_dyn(fn, dyn) != cudaSuccess) return 0;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, NT, 0) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, NT, (size_t)dyn) != cudaSuccess) return 0;
     return n;
 }
 

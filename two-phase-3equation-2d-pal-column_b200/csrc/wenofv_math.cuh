@@ -398,7 +398,7 @@ struct WenoExp {
 struct ExpThinc {
     double umm, um, u, up, upp;
     double f0, f1, f2, lam[2];    // WENO branch
-    double qmin, qmax, theta, xcc; // THINC branch
+    double qmin, qmax, theta, xcc; // THINC branch (contracted build: xcc holds xc)
     bool thinc, ext;
 
     __device__ __forceinline__ void init(const double *v, double dx4)
@@ -416,7 +416,11 @@ struct ExpThinc {
             // so that xc is exactly 0 or inf (the profile saturates) rather than +-tiny
             const double B = arg == beta ? e_beta : (arg == -beta ? e_mbeta : exp(arg));
             const double xc = (e_beta - B) / (B - e_mbeta);
+#if WENOFV_STRICT
             xcc = log(xc) / (2.0 * beta);
+#else
+            xcc = xc; // the profile from xc itself (thinc_at)
+#endif
             ext = (u - um) * (up - u) < 0;
             return;
         }
@@ -472,12 +476,23 @@ struct ExpThinc {
 
     template <int GP> __device__ __forceinline__ double thinc_at() const
     {
+        if (ext) return u;
+#if WENOFV_STRICT
         // (x + 1) / 2 of the reference-interval Gauss-Lobatto points (GaussLobatto_ref(4),
         // third_party/scTools/GaussQuadratureInRef.hpp:250-259)
         constexpr double x = GP == 0 ? -1.0 : GP == 1 ? -0.447213595499957939281834733746
                            : GP == 2 ? 0.447213595499957939281834733746 : 1.0;
-        if (ext) return u;
         return 0.5 * qmax * (1 + theta * tanh(1.5 * ((x + 1) / 2 - xcc))) + qmin;
+#else
+        // with xcc = log(xc) / (2 beta): tanh(beta ((x + 1) / 2 - xcc)) = (K - xc) / (K + xc),
+        // K = e^(beta (x + 1)), so the profile needs neither log nor tanh (xc = 0 gives 1;
+        // xc = inf, the other saturated end, gives -1)
+        constexpr double K = GP == 0 ? 1.0 : GP == 1 ? 0x1.254dd7e1a7f2ep+1 /* e^(1.5 (1 - 1/sqrt 5)) */
+                           : GP == 2 ? 0x1.187ebf9c17648p+3 /* e^(1.5 (1 + 1/sqrt 5)) */ : 0x1.415e5bf6fb106p+4 /* e^3 */;
+        const double xc = xcc;
+        const double th = isinf(xc) ? -1.0 : (K - xc) / (K + xc);
+        return 0.5 * qmax * (1 + theta * th) + qmin;
+#endif
     }
     // numerator and denominator of the WENO value at GP (strict: the value, S unused)
     template <int GP> __device__ __forceinline__ double num_den(double &S) const

@@ -269,28 +269,51 @@ __device__ __forceinline__ void phase_eigen(StageSmem<EQ, H> &S, const InstDesc 
 // the deviations from the column's centre average (WENO is translation invariant), so that
 // FP32 rounds the small differences, not the large averages; the result is re-anchored in
 // FP64.
+// bytes of dynamic shared memory of a stage kernel: the primitive-variable ring of the
+// primitive reconstructions (8 rows of the 4 primitives at the strip's positions)
+template <int EQ, int RECON, int H> struct StageDynSmem {
+    static constexpr int value = (RECON >= 2 && EqTraits<EQ>::NV == 4) ? 8 * 4 * StageSmem<EQ, H>::PS * (int)sizeof(double) : 0;
+};
+
 template <int EQ, int RECON, class R, int SCH>
-__device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>::H> &S, const InstDesc &D, int r)
+__device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>::H> &S, const InstDesc &D, int r, double *ring_raw,
+                                             bool first)
 {
     using SR = typename ReconSel<R, SCH, RECON>::type;
     constexpr int H = SR::H, NS = SR::NS;
     constexpr int NV = StageGeom<EQ, H>::NV;
     constexpr bool DEV = sizeof(R) < sizeof(double); // deviation form
     const int t = threadIdx.x;
-    const int p = t / NV, v = t - p * NV;
+    // PRIMITIVE3 reconstructs z1 with another kernel than p, u, v: one warp per variable (the
+    // strip's 32 positions on its lanes, the z1 warp rotating with the row) instead of the 4
+    // variables of a position on 4 lanes, so that the two kernels do not diverge in a warp
+    const int p = RECON == 4 ? (t & 31) : t / NV;
+    const int v = RECON == 4 ? (((t >> 5) + r) & 3) : t - p * NV;
+    static_assert(RECON != 4 || (NV == 4 && StageGeom<EQ, H>::P == 32 && NT == 128), "variable-major y-sweep");
     if (RECON != 1 || NV == 1) {
-        // conservative: the averages; primitive (RECONSTRUCTIONTYPE 2, 3): the primitive
-        // variables of each of the NS cells (src/WENOFV.cpp:944-979)
+        // conservative: the averages; primitive (RECONSTRUCTIONTYPE 2-4): the primitive
+        // variables of each of the NS cells (src/WENOFV.cpp:944-979).  Each (position,
+        // variable) thread keeps the primitive values of its own column in a ring of 8 rows
+        // (only it reads and writes its entries), so a row is converted once, when it enters
+        // the stencil (all NS rows at the first row of a work item).
         double st[NS];
 #pragma unroll
         for (int m = 0; m < NS; m++) {
             if constexpr (RECON >= 2 && NV == 4) {
-                double U4[4], W4[4];
+                auto ring = reinterpret_cast<double (*)[4][StageSmem<EQ, H>::PS]>(ring_raw);
+                const int row = r - H + m;
+                if (first || m == NS - 1) {
+                    double U4[4], W4[4];
 #pragma unroll
-                for (int j = 0; j < 4; j++) U4[j] = S.su[(r - H + m) & 7][j][p];
-                tp_to_primitive(D.eq, RECON, U4, W4);
-                st[m] = W4[v];
+                    for (int j = 0; j < 4; j++) U4[j] = S.su[row & 7][j][p];
+                    tp_to_primitive(D.eq, RECON, U4, W4);
+                    st[m] = W4[v];
+                    ring[row & 7][v][p] = st[m];
+                } else {
+                    st[m] = ring[row & 7][v][p];
+                }
             } else {
+                (void)ring_raw; (void)first;
                 st[m] = S.su[(r - H + m) & 7][v][p];
             }
         }
@@ -357,7 +380,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
 //      limiter :1895-2000) -> face states (FP64 in every form) ------------------------------
 template <int EQ, int RECON, class R, int SCH>
 __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>::H> &S, const InstDesc &D, InstState *st, int r,
-                                             int i0, int TXe)
+                                             int i0, int TXe, const double *ring_raw)
 {
     using SR = typename ReconSel<R, SCH, RECON>::type;
     constexpr int H = SR::H, NS = SR::NS;
@@ -370,19 +393,53 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
     const int lane = t & 31, gbase = lane & ~(NV - 1);
     double fv[4][4]; // face values [gpi][gpj] of variable v (boundary points only)
 
-    if (RECON != 1 || NV == 1) {
-        double cc = 0.0; // deviation anchor: the cell's own (primitive) average
-        if constexpr (DEV) {
-            if constexpr (RECON >= 2 && NV == 4) {
-                double U4[4], W4[4];
+    if constexpr (RECON >= 2 && NV == 4) {
+        // primitive reconstructions (src/WENOFV.cpp:981-1025, :1137-1189, :1302-1354): lane v
+        // of the cell reconstructs all 4 primitive variables at y Gauss point gj = v, so that
+        // PRIMITIVE3's z1 kernel and WENO-Z do not diverge across the cell's lanes, converts
+        // its points back to conserved variables, and shuffles hand every lane its variable
+        // at the 12 boundary points.  Lanes 1 and 2 also evaluate the inner points (unused)
+        // to keep the lanes converged.
+        auto ring = reinterpret_cast<const double (*)[4][StageSmem<EQ, H>::PS]>(ring_raw);
+        const int gj = v;
+        double pv[4][4]; // [gpi][variable] at (gpi, gj)
 #pragma unroll
-                for (int j = 0; j < 4; j++) U4[j] = S.su[r & 7][j][c + GH];
-                tp_to_primitive(D.eq, RECON, U4, W4);
-                cc = W4[v];
-            } else {
-                cc = S.su[r & 7][v][c + GH];
-            }
+        for (int k = 0; k < 4; k++) {
+            const double ck = DEV ? ring[r & 7][k][c + GH] : 0.0; // deviation anchor: the primitive average
+            R sv[NS];
+#pragma unroll
+            for (int m = 0; m < NS; m++) sv[m] = (R)(S.sy[c + 1 + m][gj * NV + k] - ck);
+            SR W;
+            W.init(sv, D.scheme, k, D.dx4);
+            R o[4];
+            W.eval4(o);
+#pragma unroll
+            for (int gpi = 0; gpi < 4; gpi++) pv[gpi][k] = anchor<DEV>(ck, o[gpi]);
         }
+#pragma unroll
+        for (int gpi = 0; gpi < 4; gpi++) {
+            double U4[4];
+            tp_from_primitive(D.eq, RECON, pv[gpi], U4);
+#pragma unroll
+            for (int k = 0; k < 4; k++) pv[gpi][k] = U4[k];
+        }
+#pragma unroll
+        for (int gpj = 0; gpj < 4; gpj++)
+#pragma unroll
+            for (int gpi = 0; gpi < 4; gpi++) {
+                if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
+                double x = 0.0;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const double y = __shfl_sync(0xffffffffu, pv[gpi][k], gbase + gpj);
+                    if (k == v) x = y;
+                }
+                fv[gpi][gpj] = x;
+            }
+    } else if (RECON != 1 || NV == 1) {
+        (void)ring_raw;
+        double cc = 0.0; // deviation anchor: the cell's own average
+        if constexpr (DEV) cc = S.su[r & 7][v][c + GH];
 #pragma unroll
         for (int gpj = 0; gpj < 4; gpj++) {
             // the stencil of cell c: positions c+GH-H .. c+GH+H = c+1 .. c+1+2H
@@ -402,20 +459,6 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
                 fv[0][gpj] = anchor<DEV>(cc, o0);
                 fv[3][gpj] = anchor<DEV>(cc, o3);
             }
-        }
-        if constexpr (RECON >= 2 && NV == 4) {
-            // the primitive face values back to conserved ones (src/WENOFV.cpp:1002-1025, :1178-1189)
-#pragma unroll
-            for (int gpj = 0; gpj < 4; gpj++)
-#pragma unroll
-                for (int gpi = 0; gpi < 4; gpi++) {
-                    if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
-                    double W4[4], U4[4];
-#pragma unroll
-                    for (int k = 0; k < 4; k++) W4[k] = __shfl_sync(0xffffffffu, fv[gpi][gpj], gbase + k);
-                    tp_from_primitive(D.eq, RECON, W4, U4);
-                    fv[gpi][gpj] = U4[v];
-                }
         }
     } else {
         double Uc[NV], Lrow[NV], Rrow[NV]; // FP64 in every form, as in the y-sweep
@@ -654,6 +697,7 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
     constexpr int H = StencilRecon<R, SCH>::H;
     constexpr int TX = StageGeom<EQ, H>::TX;
     __shared__ StageSmem<EQ, H> S;
+    extern __shared__ __align__(16) double stage_dyn_smem[]; // StageDynSmem bytes: the primitive ring
     for (int w = blockIdx.x; w < L.nwork; w += gridDim.x) {
         const WorkItem it = L.work[w];
         const InstDesc &D = L.inst[it.inst];
@@ -695,9 +739,9 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
                 phase_eigen<EQ, RECON, H>(S, D, r, 0, NT);
                 __syncthreads();
             }
-            phase_ysweep<EQ, RECON, R, SCH>(S, D, r);
+            phase_ysweep<EQ, RECON, R, SCH>(S, D, r, stage_dyn_smem, r == it.j0 - 1);
             __syncthreads();
-            phase_xsweep<EQ, RECON, R, SCH>(S, D, st, r, it.i0, TXe);
+            phase_xsweep<EQ, RECON, R, SCH>(S, D, st, r, it.i0, TXe, stage_dyn_smem);
             __syncthreads();
             phase_riemann<EQ, R, FLX, H>(S, D, st, r, it.i0, it.j0, it.j1, TXe);
             // the last warp, idle in the second round of Riemann units, prepares the next
