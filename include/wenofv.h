@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define WENOFV_ABI_VERSION 1
+#define WENOFV_ABI_VERSION 2 /* 2: wenofv_eq_params gained the stiffened-gas fields */
 
 /* status codes (the reference prints, waits on std::cin and exits instead:
  * src/WENOFV.cpp:34-38, :521-531, :1927-1932, :2287-2292; include/Equations.hpp:345-359) */
@@ -42,7 +42,7 @@ enum {
 };
 
 /* equation kinds; TWO_PHASE is TwoPhaseEquation (include/Equations.hpp:52-1044) */
-enum { WENOFV_EQ_TWO_PHASE = 0, WENOFV_EQ_LINEAR_ADV = 1, WENOFV_EQ_EULER = 2 };
+enum { WENOFV_EQ_TWO_PHASE = 0, WENOFV_EQ_LINEAR_ADV = 1, WENOFV_EQ_EULER = 2, WENOFV_EQ_TWO_PHASE_SG = 3 };
 /* boundary kinds; PERIOD keeps the number of BOUNDARYTYPE::PERIOD (include/Equations.hpp:27);
  * OUTFLOW (zero-gradient) has no counterpart in the reference */
 enum { WENOFV_BC_PERIOD = 0, WENOFV_BC_OUTFLOW = 5 };
@@ -76,6 +76,12 @@ typedef struct {
     double rho10, rho20, sound1, sound2, preb;
     double gamma;        /* Euler ratio of specific heats */
     double adv_u, adv_v; /* linear advection velocity */
+    /* WENOFV_EQ_TWO_PHASE_SG (an extension): stiffened-gas phases on their isentropes through
+     * (preb, rho10) and (preb, rho20), p_k = (preb + pinf_k) (rho_k / rho_k0)^gamma_k - pinf_k;
+     * sound1/sound2 are ignored (the library uses the linearised c_k^2 = gamma_k (preb +
+     * pinf_k) / rho_k0 for the first guess of the pressure equilibrium); FP64 forms and
+     * RECONSTRUCTIONTYPE 0-1 only */
+    double gamma1, pinf1, gamma2, pinf2;
 } wenofv_eq_params;
 
 /* Solver options: the settings.cfg keys (config/settings.cfg:11-24, read at

@@ -52,8 +52,15 @@ OFV_CMP(>=)
 
 inline ofv_cnt sqrt(ofv_cnt a) { g_ofv_cnt.sqrt++; return ofv_cnt(std::sqrt(a.v)); }
 inline ofv_cnt fabs(ofv_cnt a) { g_ofv_cnt.abs++; return ofv_cnt(std::fabs(a.v)); }
-// pow(x, n) with a small integer n, as the restated path uses it: n - 1 multiplications
-inline ofv_cnt pow(ofv_cnt a, double n) { g_ofv_cnt.mul += (unsigned long long)(n - 1); return ofv_cnt(std::pow(a.v, n)); }
+// pow(x, n): with a small integer n (the WENO kernels) n - 1 multiplications, otherwise (the
+// stiffened-gas isentropes) one transcendental
+inline ofv_cnt pow(ofv_cnt a, double n)
+{
+    if (n >= 1 && n <= 8 && n == (double)(int)n) g_ofv_cnt.mul += (unsigned long long)(n - 1);
+    else g_ofv_cnt.tr++;
+    return ofv_cnt(std::pow(a.v, n));
+}
+inline ofv_cnt pow(ofv_cnt a, ofv_cnt n) { return pow(a, n.v); }
 inline bool ofv_isnan(ofv_cnt a) { return std::isnan(a.v); }
 inline ofv_cnt exp(ofv_cnt a) { g_ofv_cnt.tr++; return ofv_cnt(std::exp(a.v)); }
 inline ofv_cnt log(ofv_cnt a) { g_ofv_cnt.tr++; return ofv_cnt(std::log(a.v)); }

@@ -24,14 +24,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "wenofv_ref")
 
-EQ_TWO_PHASE, EQ_LINEAR_ADV, EQ_EULER = 0, 1, 2
+EQ_TWO_PHASE, EQ_LINEAR_ADV, EQ_EULER, EQ_TWO_PHASE_SG = 0, 1, 2, 3
 BC_PERIOD, BC_OUTFLOW = 0, 5
 
 
 class _Eq(C.Structure):
     _fields_ = [("kind", C.c_int), ("rho10", C.c_double), ("rho20", C.c_double),
                 ("sound1", C.c_double), ("sound2", C.c_double), ("preb", C.c_double),
-                ("gamma", C.c_double), ("adv_u", C.c_double), ("adv_v", C.c_double)]
+                ("gamma", C.c_double), ("adv_u", C.c_double), ("adv_v", C.c_double),
+                ("gamma1", C.c_double), ("pinf1", C.c_double), ("gamma2", C.c_double), ("pinf2", C.c_double)]
 
 
 class _Problem(C.Structure):
@@ -68,6 +69,11 @@ class Problem:
     gamma: float = 1.4
     adv_u: float = 1.0
     adv_v: float = 1.0
+    # stiffened-gas phases (EQ_TWO_PHASE_SG): isentropes through (preb, rho10) and (preb, rho20)
+    gamma1: float = 4.4
+    pinf1: float = 6.0e3
+    gamma2: float = 1.4
+    pinf2: float = 0.0
 
     @property
     def nvar(self) -> int:
@@ -75,7 +81,7 @@ class Problem:
 
     def to_c(self) -> _Problem:
         e = _Eq(self.eq_kind, self.rho10, self.rho20, self.sound1, self.sound2, self.preb,
-                self.gamma, self.adv_u, self.adv_v)
+                self.gamma, self.adv_u, self.adv_v, self.gamma1, self.pinf1, self.gamma2, self.pinf2)
         return _Problem(self.nx, self.ny, self.xl, self.xr, self.yl, self.yr, self.bc, self.rk,
                         self.cfl, self.scheme, self.limiter, self.flux, self.recon, self.ref_slabs,
                         self.threads, e)
@@ -170,6 +176,13 @@ class Oracle:
         self.L.ofv_eigen_R(C.byref(e), u, nx, ny, R)
         n = p.nvar
         return L[: n * n].reshape(n, n), R[: n * n].reshape(n, n)
+
+    def thermo(self, p: Problem, U):
+        """(volume fraction, pressure less preb, sound speed) of one state"""
+        e = p.to_c().eq
+        u = np.ascontiguousarray(U, dtype=np.float64)
+        return (self.L.ofv_volume_frac(C.byref(e), u), self.L.ofv_pressure(C.byref(e), u),
+                self.L.ofv_sound_speed(C.byref(e), u))
 
     def max_eig(self, p: Problem, U, nx: float, ny: float) -> float:
         e = p.to_c().eq

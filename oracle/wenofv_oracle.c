@@ -369,9 +369,70 @@ double ofv_weno_exp_thinc(const double v[7], int gp, double dx)
 /* U = (z1 rho1, z2 rho2, rho u, rho v)                                                   */
 /* ------------------------------------------------------------------------------------ */
 
+/* Stiffened-gas phases on their isentropes (OFV_EQ_TWO_PHASE_SG; an extension, not in the
+ * reference): p_k(rho) = (preb + pi_k) (rho / rho_k0)^gamma_k - pi_k, whose expansion at preb
+ * is the reference's linear model with c_k^2 = gamma_k (preb + pi_k) / rho_k0.  Pressure
+ * equilibrium z1rho1 / rho_1(p) + z2rho2 / rho_2(p) = 1 is solved for p by Newton steps from
+ * the linear model's state (kept above -min(pi_k), where both densities exist), until a step
+ * is below 1e-14 (|p| + max(pi_k) + |preb|), at most SG_NEWTON; z1 = z1rho1 / rho_1(p).
+ * Phase sound speeds c_k^2 = gamma_k (p + pi_k) / rho_k. */
+#define SG_NEWTON 12
+static real_t tp_volume_frac(const ofv_eq *e, const real_t *U);
+static real_t tp_pressure_z(const ofv_eq *e, const real_t *U, real_t z1);
+static void sg_linearised(const ofv_eq *e, ofv_eq *lin)
+{
+    *lin = *e;
+    lin->kind = OFV_EQ_TWO_PHASE;
+    lin->sound1 = sqrt(e->gamma1 * (e->preb + e->pinf1) / e->rho10);
+    lin->sound2 = sqrt(e->gamma2 * (e->preb + e->pinf2) / e->rho20);
+}
+static void sg_solve(const ofv_eq *e, const real_t *U, real_t *z1_out, real_t *p_out)
+{
+    ofv_eq lin;
+    sg_linearised(e, &lin);
+    const real_t m1 = U[0], m2 = U[1];
+    const double pref = e->preb, g1 = e->gamma1, g2 = e->gamma2, pi1 = e->pinf1, pi2 = e->pinf2;
+    const double a1 = 1.0 / (pref + pi1), a2 = 1.0 / (pref + pi2), ig1 = 1.0 / g1, ig2 = 1.0 / g2;
+    const double lo = -(pi1 < pi2 ? pi1 : pi2);
+    const double scale = (pi1 > pi2 ? pi1 : pi2) + fabs(pref);
+    real_t p = pref + tp_pressure_z(&lin, U, tp_volume_frac(&lin, U));
+    if (!(p > lo)) p = 0.5 * (pref + lo);
+    for (int it = 0; it < SG_NEWTON; it++) {
+        const real_t r1 = e->rho10 * pow((p + pi1) * a1, ig1);
+        const real_t r2 = e->rho20 * pow((p + pi2) * a2, ig2);
+        const real_t h = m1 / r1 + m2 / r2 - 1.0;
+        const real_t dh = -(m1 / (r1 * (g1 * (p + pi1))) + m2 / (r2 * (g2 * (p + pi2))));
+        real_t pn = p - h / dh;
+        if (!(pn > lo)) pn = 0.5 * (p + lo);
+        const real_t dp = pn - p;
+        p = pn;
+        if (fabs(dp) <= 1e-14 * (fabs(p) + scale)) break;
+    }
+    *z1_out = m1 / (e->rho10 * pow((p + pi1) * a1, ig1));
+    *p_out = p;
+}
+/* the phase sound speeds squared (constant in the linear model) */
+static void tp_phase_c2(const ofv_eq *e, const real_t *U, real_t z1, real_t *c1_2, real_t *c2_2)
+{
+    if (e->kind == OFV_EQ_TWO_PHASE_SG) {
+        real_t zz, p;
+        sg_solve(e, U, &zz, &p);
+        *c1_2 = e->gamma1 * (p + e->pinf1) * z1 / U[0];
+        *c2_2 = e->gamma2 * (p + e->pinf2) * (1.0 - z1) / U[1];
+        return;
+    }
+    *c1_2 = (real_t)e->sound1 * e->sound1;
+    *c2_2 = (real_t)e->sound2 * e->sound2;
+}
+
 /* getVolumeFrac, include/Equations.hpp:84-99 */
 static real_t tp_volume_frac(const ofv_eq *e, const real_t *U)
 {
+    if (e->kind == OFV_EQ_TWO_PHASE_SG) {
+        real_t z1, p;
+        sg_solve(e, U, &z1, &p);
+        return z1;
+    }
     const real_t z1rho1 = U[0], z2rho2 = U[1];
     const real_t c1_2 = (real_t)e->sound1 * e->sound1;
     const real_t c2_2 = (real_t)e->sound2 * e->sound2;
@@ -384,6 +445,11 @@ static real_t tp_volume_frac(const ofv_eq *e, const real_t *U)
 /* getPressure, include/Equations.hpp:101-124: the dominant phase's pressure (g_preb dropped) */
 static real_t tp_pressure_z(const ofv_eq *e, const real_t *U, real_t z1)
 {
+    if (e->kind == OFV_EQ_TWO_PHASE_SG) { /* the equilibrium pressure, less g_preb as in the linear model */
+        real_t zz, p;
+        sg_solve(e, U, &zz, &p);
+        return p - e->preb;
+    }
     const real_t z2 = 1.0 - z1;
     const real_t c1_2 = (real_t)e->sound1 * e->sound1;
     const real_t c2_2 = (real_t)e->sound2 * e->sound2;
@@ -397,6 +463,12 @@ static real_t tp_pressure_z(const ofv_eq *e, const real_t *U, real_t z1)
 /* getSoundSpeed (Wood), include/Equations.hpp:126-146 */
 static real_t tp_sound_z(const ofv_eq *e, const real_t *U, real_t z1)
 {
+    if (e->kind == OFV_EQ_TWO_PHASE_SG) { /* Wood: 1 / (rho c^2) = sum_k z_k / (gamma_k (p + pi_k)) */
+        real_t zz, p;
+        sg_solve(e, U, &zz, &p);
+        const real_t rho = U[0] + U[1];
+        return 1.0 / sqrt(rho * (z1 / (e->gamma1 * (p + e->pinf1)) + (1.0 - z1) / (e->gamma2 * (p + e->pinf2))));
+    }
     const real_t z2 = 1.0 - z1;
     const real_t rho = U[0] + U[1];
     const real_t rho1 = U[0] / z1;
@@ -609,7 +681,7 @@ static void eu_hllc_flux(const ofv_eq *e, const real_t *UL, const real_t *UR, re
  * equation HLLC reduces to the upwind flux, which is the LLF flux with |a.n|. */
 static void riemann(const ofv_eq *e, int flux, const real_t *UL, const real_t *UR, real_t *F, double nx, double ny)
 {
-    if (flux == 1 && e->kind == OFV_EQ_TWO_PHASE)
+    if (flux == 1 && (e->kind == OFV_EQ_TWO_PHASE || e->kind == OFV_EQ_TWO_PHASE_SG))
         tp_hllc_flux(e, UL, UR, F, nx, ny);
     else if (flux == 1 && e->kind == OFV_EQ_EULER)
         eu_hllc_flux(e, UL, UR, F, nx, ny);
@@ -630,8 +702,8 @@ static void tp_eigen_R(const ofv_eq *e, const real_t *U, double nx, double ny, r
     const real_t z1 = tp_volume_frac(e, U);
     const real_t z2 = 1.0 - z1;
     const real_t c = tp_sound_z(e, U, z1);
-    const real_t c1_2 = (real_t)e->sound1 * e->sound1;
-    const real_t c2_2 = (real_t)e->sound2 * e->sound2;
+    real_t c1_2, c2_2;
+    tp_phase_c2(e, U, z1, &c1_2, &c2_2);
     const real_t zrho1 = z1rho1 * c1_2 / (z1 * z1);
     const real_t zrho2 = z2rho2 * c2_2 / (z2 * z2);
     const real_t sc1_2 = c1_2 / z1 - c1_2 / z1 * zrho1 / (zrho1 + zrho2);
@@ -667,8 +739,8 @@ static void tp_eigen_L(const ofv_eq *e, const real_t *U, double nx, double ny, r
     const real_t z2 = 1.0 - z1;
     const real_t c = tp_sound_z(e, U, z1);
     const real_t c2 = c * c; /* pow(c, 2) */
-    const real_t c1_2 = (real_t)e->sound1 * e->sound1;
-    const real_t c2_2 = (real_t)e->sound2 * e->sound2;
+    real_t c1_2, c2_2;
+    tp_phase_c2(e, U, z1, &c1_2, &c2_2);
     const real_t zrho1 = z1rho1 * c1_2 / (z1 * z1);
     const real_t zrho2 = z2rho2 * c2_2 / (z2 * z2);
     const real_t sc1_2 = c1_2 / z1 - c1_2 / z1 * zrho1 / (zrho1 + zrho2);
@@ -726,13 +798,13 @@ static void eu_eigen(const ofv_eq *e, const real_t *U, double nx, double ny, rea
 static void eigen_L(const ofv_eq *e, const real_t *U, double nx, double ny, real_t *M)
 {
     if (e->kind == OFV_EQ_EULER) eu_eigen(e, U, nx, ny, M, NULL);
-    else if (e->kind == OFV_EQ_TWO_PHASE) tp_eigen_L(e, U, nx, ny, M);
+    else if (e->kind == OFV_EQ_TWO_PHASE || e->kind == OFV_EQ_TWO_PHASE_SG) tp_eigen_L(e, U, nx, ny, M);
     else M[0] = 1.0;
 }
 static void eigen_R(const ofv_eq *e, const real_t *U, double nx, double ny, real_t *M)
 {
     if (e->kind == OFV_EQ_EULER) eu_eigen(e, U, nx, ny, NULL, M);
-    else if (e->kind == OFV_EQ_TWO_PHASE) tp_eigen_R(e, U, nx, ny, M);
+    else if (e->kind == OFV_EQ_TWO_PHASE || e->kind == OFV_EQ_TWO_PHASE_SG) tp_eigen_R(e, U, nx, ny, M);
     else M[0] = 1.0;
 }
 
@@ -994,7 +1066,7 @@ static int pp_limit(ofv_ws *w, const real_t *ubar, real_t *fs)
 {
     const ofv_eq *e = &w->p->eq;
     const int nv = w->nv;
-    const int nlim = e->kind == OFV_EQ_TWO_PHASE ? 2 : (e->kind == OFV_EQ_EULER ? 1 : 0);
+    const int nlim = (e->kind == OFV_EQ_TWO_PHASE || e->kind == OFV_EQ_TWO_PHASE_SG) ? 2 : (e->kind == OFV_EQ_EULER ? 1 : 0);
     if (nlim == 0) return 0;
     const double zeps = 1e-12, omega1 = 0.1, omegaR = 1.0 - 2 * omega1;
     const real_t a1 = max_eig(e, ubar, 1, 0);

@@ -22,7 +22,7 @@ extern "C" {
 #endif
 
 /* Equation kinds (same numbering as include/wenofv.h). */
-enum { OFV_EQ_TWO_PHASE = 0, OFV_EQ_LINEAR_ADV = 1, OFV_EQ_EULER = 2 };
+enum { OFV_EQ_TWO_PHASE = 0, OFV_EQ_LINEAR_ADV = 1, OFV_EQ_EULER = 2, OFV_EQ_TWO_PHASE_SG = 3 };
 /* Boundary kinds: PERIOD = 0 as include/Equations.hpp:27; OUTFLOW is an extension. */
 enum { OFV_BC_PERIOD = 0, OFV_BC_OUTFLOW = 5 };
 
@@ -34,6 +34,9 @@ typedef struct {
     double gamma;
     /* linear advection velocity */
     double adv_u, adv_v;
+    /* stiffened-gas phases (OFV_EQ_TWO_PHASE_SG, an extension): p_k(rho) on the isentrope
+     * through (preb, rho_k0), rho10 and rho20 being the densities at preb */
+    double gamma1, pinf1, gamma2, pinf2;
 } ofv_eq;
 
 typedef struct {

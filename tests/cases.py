@@ -122,6 +122,29 @@ def liquid_column(nx, ny, seed=3, ratio=1000.0, radius=0.2, eps=1e-6, amp=1e-2, 
     return cell_average(f, nx, ny), prm
 
 
+def sg_params(ratio=1000.0, g1=4.4, pinf1=6e3, g2=1.4, pinf2=0.0, p0=1.0, rho2=1.0):
+    """stiffened-gas parameters (eq kind 3): phase k on its isentrope through (p0, rho_k0)"""
+    return dict(rho10=ratio * rho2, rho20=rho2, preb=p0, gamma1=g1, pinf1=pinf1, gamma2=g2, pinf2=pinf2)
+
+
+def sg_column(nx, ny, seed=3, ratio=1000.0, radius=0.2, eps=1e-6, amp=1e-2, p0=1.0):
+    """the liquid column of liquid_column with stiffened-gas phases at the uniform pressure
+    p0, where the phase densities are rho10 and rho20 themselves"""
+    prm = sg_params(ratio=ratio, p0=p0)
+    rng = np.random.default_rng(seed)
+    fu, fv = periodic_field(rng), periodic_field(rng)
+    h = max(1.0 / nx, 1.0 / ny)
+
+    def f(x, y):
+        r = np.hypot(x - 0.5, y - 0.5)
+        z1 = eps + (1 - 2 * eps) * 0.5 * (1 - np.tanh((r - radius) / (2 * h)))
+        a1, a2 = z1 * prm["rho10"], (1 - z1) * prm["rho20"]
+        rho = a1 + a2
+        return np.stack([a1, a2, rho * amp * fu(x, y), rho * amp * fv(x, y)])
+
+    return cell_average(f, nx, ny), prm
+
+
 def point_column(nx, ny, seed=3, ratio=1000.0, radius=0.2, eps=1e-6, amp=1e-2, p0=1.0):
     """the liquid column sampled at cell centres with a one-mode-ring velocity field: the
     same physics as liquid_column, cheap enough to build thousands of grids for serving"""

@@ -25,13 +25,13 @@ def test_library_exports_every_symbol(wb):
     L = wb.load()
     for name in declared_functions():
         assert hasattr(L, name), name
-    assert L.wenofv_abi_version() == 1
+    assert L.wenofv_abi_version() == 2
 
 
 def test_struct_layouts(wb):
-    # wenofv_eq_params: int (+4 pad) + 8 doubles; wenofv_config: 2 ints, 4 doubles, 2 ints,
+    # wenofv_eq_params: int (+4 pad) + 12 doubles; wenofv_config: 2 ints, 4 doubles, 2 ints,
     # double, 7 ints (+4 pad)
-    assert C.sizeof(wb.EqParams) == 72
+    assert C.sizeof(wb.EqParams) == 104
     assert C.sizeof(wb.Config) == 88
 
 
@@ -71,6 +71,12 @@ def test_invalid_equation_rejected(wb):
     c = wb.make_config(8, 8, recon=4, precision=wb.FP32_BULK)
     assert L.wenofv_create(C.byref(c), C.byref(wb.make_eq()), C.byref(h)) == wb.ENOTSUP
     assert L.wenofv_create(C.byref(wb.make_config(8, 8, recon=4)), C.byref(wb.make_eq(kind=2)), C.byref(h)) == wb.ENOTSUP
+    # the stiffened-gas model: FP64 forms, RECONSTRUCTIONTYPE 0-1, valid phase parameters
+    sg = wb.make_eq(kind=wb.EQ_TWO_PHASE_SG, rho10=1000.0, rho20=1.0, preb=1.0)
+    assert L.wenofv_create(C.byref(wb.make_config(8, 8, precision=wb.FP32_BULK)), C.byref(sg), C.byref(h)) == wb.ENOTSUP
+    assert L.wenofv_create(C.byref(wb.make_config(8, 8, recon=3)), C.byref(sg), C.byref(h)) == wb.ENOTSUP
+    bad = wb.make_eq(kind=wb.EQ_TWO_PHASE_SG, rho10=1000.0, rho20=1.0, preb=1.0, gamma2=1.0)
+    assert L.wenofv_create(C.byref(wb.make_config(8, 8)), C.byref(bad), C.byref(h)) == wb.EINVAL
 
 
 def test_null_arguments(wb):

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from conftest import golden_cases, load_golden
-from oracle import EQ_EULER, EQ_LINEAR_ADV, BC_OUTFLOW, Oracle, Problem, reference_available, run_reference
+from oracle import EQ_EULER, EQ_LINEAR_ADV, EQ_TWO_PHASE_SG, BC_OUTFLOW, Oracle, Problem, reference_available, run_reference
 import cases
 
 GOLD = golden_cases()
@@ -204,3 +204,67 @@ def test_oracle_reproduces_smooth_known_answer():
     V, k, t, _ = Oracle().advance(p, U0, t_end=0.05)
     got = T.smooth_accuracy(V, n, 0.05)
     assert np.allclose(got, T.SMOOTH_KNOWN[1][1], rtol=1e-12, atol=0), got
+
+
+# ---- the stiffened-gas extension (not in the reference: checked by its own properties) -------
+def sg_states(rng, n):
+    """states in pressure equilibrium at known (z1, p): liquid-rich cells at p in [0.2, 26] (the gas
+    needs p > 0), gas-rich ones at p in 1 +- 0.15"""
+    z1 = np.where(np.arange(n) % 2 == 0, 10 ** rng.uniform(-8, -0.3, n), 1 - 10 ** rng.uniform(-8, -0.3, n))
+    p = np.where(z1 > 0.5, rng.uniform(0.2, 26.0, n), 1 + 0.15 * rng.uniform(-1, 1, n))
+    r1 = 1000 * ((p + 6000) / 6001) ** (1 / 4.4)
+    r2 = p ** (1 / 1.4)
+    rho = z1 * r1 + (1 - z1) * r2
+    U = np.stack([z1 * r1, (1 - z1) * r2, rho * rng.uniform(-0.1, 0.1, n), rho * rng.uniform(-0.1, 0.1, n)], axis=1)
+    return U, z1, p
+
+
+def test_sg_equilibrium_recovers_the_state(oracle_lib):
+    U, z1, p = sg_states(np.random.default_rng(6), 1500)
+    prm = cases.sg_params()
+    pr = Problem(nx=8, ny=8, eq_kind=EQ_TWO_PHASE_SG, **prm)
+    for k in range(len(U)):
+        z, pg, c = oracle_lib.thermo(pr, U[k])
+        zmin = min(z1[k], 1 - z1[k])
+        assert abs(z - z1[k]) <= 1e-15 / zmin + 1e-13 * zmin, (k, z, z1[k])
+        assert abs(pg + 1 - p[k]) <= 1e-11 * (abs(p[k]) + 6000 * (z1[k] > 0.5))
+        # Wood's sound speed lies between the phase sound speeds
+        c1 = np.sqrt(4.4 * (p[k] + 6000) / (U[k, 0] / z1[k]))
+        c2 = np.sqrt(1.4 * p[k] / (U[k, 1] / (1 - z1[k])))
+        assert c <= max(c1, c2) * (1 + 1e-12)
+
+
+def test_sg_linearises_to_the_reference_model(oracle_lib):
+    # near the reference pressure the stiffened-gas model is the reference's linear model with
+    # c_k^2 = gamma_k (preb + pinf_k) / rho_k0 (preb dropped): pressures agree to second order
+    prm = cases.sg_params()
+    sg = Problem(nx=8, ny=8, eq_kind=EQ_TWO_PHASE_SG, **prm)
+    lin = Problem(nx=8, ny=8, **cases.column_params())
+    for dp in (1e-3, 1e-2):
+        for z1 in (1e-6, 0.3, 0.7, 1 - 1e-6):
+            p = 1 + dp
+            r1, r2 = 1000 * ((p + 6000) / 6001) ** (1 / 4.4), p ** (1 / 1.4)
+            U = np.array([z1 * r1, (1 - z1) * r2, 0.0, 0.0])
+            psg = oracle_lib.thermo(sg, U)[1]
+            # both are gauge pressures: zero at rho_k = rho_k0
+            plin = oracle_lib.thermo(lin, U)[1]
+            assert abs(psg - plin) <= 2 * dp * dp, (dp, z1, psg, plin)
+
+
+@pytest.mark.parametrize("recon,flux", [(1, 1), (0, 1), (1, 0)])
+def test_sg_column_conserves_and_stays_positive(oracle_lib, recon, flux):
+    U0, prm = cases.sg_column(40, 40, seed=5)
+    p = Problem(nx=40, ny=40, eq_kind=EQ_TWO_PHASE_SG, scheme=1, flux=flux, recon=recon, limiter=1, **prm)
+    U, n, t, _ = oracle_lib.advance(p, U0, t_end=1e9, max_steps=15)
+    assert np.isfinite(U).all() and (U[0] > 0).all() and (U[1] > 0).all()
+    m0, m1 = U0.sum(axis=(1, 2)), U.sum(axis=(1, 2))
+    assert np.all(np.abs(m1 - m0) <= 1e-13 * np.abs(U0).sum(axis=(1, 2)))
+
+
+def test_sg_eigenvectors_are_inverse(oracle_lib):
+    U, _, _ = sg_states(np.random.default_rng(9), 200)
+    p = Problem(nx=8, ny=8, eq_kind=EQ_TWO_PHASE_SG, **cases.sg_params())
+    for k in range(len(U)):
+        for normal in ((1.0, 0.0), (0.0, 1.0)):
+            L, R = oracle_lib.eigen(p, U[k], *normal)
+            assert np.abs(R @ L - np.eye(4)).max() <= 1e-6

@@ -185,7 +185,7 @@ int wenofv_batch_autotune(wenofv_batch *b, int *rows_per_item, int *ctas_per_sm,
 // ---- probes ---------------------------------------------------------------------------------
 static EqParams to_params(const wenofv_eq_params *e)
 {
-    return EqParams{e->eq_kind, e->rho10, e->rho20, e->sound1, e->sound2, e->preb, e->gamma, e->adv_u, e->adv_v};
+    return eq_params_of(*e);
 }
 
 struct DevBufs {

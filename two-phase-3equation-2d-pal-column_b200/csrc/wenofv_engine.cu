@@ -32,6 +32,17 @@ int cuda_fail(cudaError_t e, const char *what)
 
 int nvar_of(int k) { return k == WENOFV_EQ_LINEAR_ADV ? 1 : 4; }
 
+EqParams eq_params_of(const wenofv_eq_params &e)
+{
+    EqParams P{e.eq_kind, e.rho10, e.rho20, e.sound1, e.sound2, e.preb, e.gamma, e.adv_u, e.adv_v,
+               e.gamma1, e.pinf1, e.gamma2, e.pinf2};
+    if (e.eq_kind == WENOFV_EQ_TWO_PHASE_SG) { // the linearised sound speeds: the first guess of the equilibrium
+        P.sound1 = std::sqrt(e.gamma1 * (e.preb + e.pinf1) / e.rho10);
+        P.sound2 = std::sqrt(e.gamma2 * (e.preb + e.pinf2) / e.rho20);
+    }
+    return P;
+}
+
 int validate(const wenofv_config *c, const wenofv_eq_params *e)
 {
     if (!c || !e) { set_error("null config or equation"); return WENOFV_EINVAL; }
@@ -67,7 +78,19 @@ int validate(const wenofv_config *c, const wenofv_eq_params *e)
         set_error("ELEMNUMX (%d) must be divisible by the slab count (%d)", c->nx, c->ref_slabs);
         return WENOFV_EINVAL;
     }
-    if (e->eq_kind < 0 || e->eq_kind > 2) { set_error("unknown equation kind %d", e->eq_kind); return WENOFV_EINVAL; }
+    if (e->eq_kind < 0 || e->eq_kind > 3) { set_error("unknown equation kind %d", e->eq_kind); return WENOFV_EINVAL; }
+    if (e->eq_kind == WENOFV_EQ_TWO_PHASE_SG) {
+        if (!(e->gamma1 > 1.0 && e->gamma2 > 1.0 && e->pinf1 >= 0.0 && e->pinf2 >= 0.0 && e->rho10 > 0.0 && e->rho20 > 0.0 &&
+              e->preb + e->pinf1 > 0.0 && e->preb + e->pinf2 > 0.0)) {
+            set_error("stiffened gas needs gamma_k > 1, pinf_k >= 0, rho_k0 > 0 and preb + pinf_k > 0");
+            return WENOFV_EINVAL;
+        }
+        if (c->reconstruction > 1) {
+            set_error("the stiffened-gas model has RECONSTRUCTIONTYPE 0 and 1 only");
+            return WENOFV_ENOTSUP;
+        }
+        if (c->precision == WENOFV_FP32_BULK) { set_error("the stiffened-gas model runs in FP64 only"); return WENOFV_ENOTSUP; }
+    }
     if (e->eq_kind == WENOFV_EQ_TWO_PHASE && !(e->sound1 > 0 && e->sound2 > 0)) { set_error("sound speeds must be positive"); return WENOFV_EINVAL; }
     if (e->eq_kind == WENOFV_EQ_EULER && !(e->gamma > 1.0)) { set_error("gamma must exceed 1"); return WENOFV_EINVAL; }
     if ((size_t)c->nx * c->ny > (size_t)1 << 31) { set_error("grid too large"); return WENOFV_EINVAL; }
@@ -212,7 +235,7 @@ int Engine::alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params
     d.dX = (c.xr - c.xl) / c.nx;
     d.dx4 = std::pow(d.dX, 4); // the reference's pow(m_deltaX, 4), include/Utility.hpp:313
     d.dY = (c.yr - c.yl) / c.ny;
-    d.eq = EqParams{e.eq_kind, e.rho10, e.rho20, e.sound1, e.sound2, e.preb, e.gamma, e.adv_u, e.adv_v};
+    d.eq = eq_params_of(e);
     WENOFV_CUDA(cudaMemcpyAsync(d_desc_ + i, &d, sizeof(InstDesc), cudaMemcpyHostToDevice, stream));
     WENOFV_CUDA(cudaStreamSynchronize(stream)); // the metric staging above is a host local
     cfg_[i] = c;

@@ -24,6 +24,9 @@ int cuda_fail(cudaError_t e, const char *what);
 
 int validate(const wenofv_config *cfg, const wenofv_eq_params *eq);
 int nvar_of(int eq_kind);
+// the device-side equation parameters (for the stiffened-gas model with the linearised sound
+// speeds of its first guess)
+EqParams eq_params_of(const wenofv_eq_params &e);
 // the reference's grid metric (src/WENOFV.cpp:89-123), see wenofv_create
 void grid_metric(const wenofv_config &c, double *dxc, double *dxl, double *dy);
 

@@ -66,6 +66,13 @@ template <class R> static const void *pick_eq(int eq, int recon, int scheme, int
                           : pick_sf<EQ_TWO_PHASE, 0, R>(scheme, flux);
     case EQ_EULER: return recon ? pick_sf<EQ_EULER, 1, R>(scheme, flux) : pick_sf<EQ_EULER, 0, R>(scheme, flux);
     case EQ_LINEAR_ADV: return pick_sf<EQ_LINEAR_ADV, 0, R>(scheme, flux);
+    case EQ_TWO_PHASE_SG: // FP64, conservative or characteristic reconstruction
+        if constexpr (sizeof(R) == sizeof(double)) {
+            if (recon > 1) return nullptr;
+            return recon ? pick_sf<EQ_TWO_PHASE_SG, 1, R>(scheme, flux) : pick_sf<EQ_TWO_PHASE_SG, 0, R>(scheme, flux);
+        } else {
+            return nullptr;
+        }
     default: return nullptr;
     }
 }
@@ -112,9 +119,10 @@ int launch_stage(int eq, int recon, int fp32, int scheme, int flux, const StageL
 
 template <int H> static const void *cfl_fn(int eq)
 {
-    return eq == EQ_TWO_PHASE ? (const void *)cfl_kernel<EQ_TWO_PHASE, StageGeom<EQ_TWO_PHASE, H>::TX>
-         : eq == EQ_EULER     ? (const void *)cfl_kernel<EQ_EULER, StageGeom<EQ_EULER, H>::TX>
-                              : (const void *)cfl_kernel<EQ_LINEAR_ADV, StageGeom<EQ_LINEAR_ADV, H>::TX>;
+    return eq == EQ_TWO_PHASE      ? (const void *)cfl_kernel<EQ_TWO_PHASE, StageGeom<EQ_TWO_PHASE, H>::TX>
+         : eq == EQ_EULER          ? (const void *)cfl_kernel<EQ_EULER, StageGeom<EQ_EULER, H>::TX>
+         : eq == EQ_TWO_PHASE_SG   ? (const void *)cfl_kernel<EQ_TWO_PHASE_SG, StageGeom<EQ_TWO_PHASE_SG, H>::TX>
+                                   : (const void *)cfl_kernel<EQ_LINEAR_ADV, StageGeom<EQ_LINEAR_ADV, H>::TX>;
 }
 
 int launch_cfl(int eq, int scheme, const StageLaunch &L, int grid, void *stream)
@@ -212,6 +220,11 @@ int probe_riemann(const EqParams &P, int flux, int fp32, const double *d_UL, con
     const int b = 128, g = (n + b - 1) / b;
     if (n <= 0) return 0;
     cudaStream_t s = (cudaStream_t)stream;
+    if (P.kind == EQ_TWO_PHASE_SG) { // FP64 only
+        if (fp32) return (int)cudaErrorInvalidValue;
+        probe_riemann_kernel<EQ_TWO_PHASE_SG, double><<<g, b, 0, s>>>(P, flux, d_UL, d_UR, n, xdir, d_F);
+        return (int)cudaGetLastError();
+    }
 #if WENOFV_HAS_FP32
     if (fp32) {
         if (P.kind == EQ_TWO_PHASE) probe_riemann_kernel<EQ_TWO_PHASE, float><<<g, b, 0, s>>>(P, flux, d_UL, d_UR, n, xdir, d_F);
@@ -231,6 +244,11 @@ int probe_eigen(const EqParams &P, int fp32, const double *d_U, int n, int xdir,
     const int b = 128, g = (n + b - 1) / b;
     if (n <= 0) return 0;
     cudaStream_t s = (cudaStream_t)stream;
+    if (P.kind == EQ_TWO_PHASE_SG) { // FP64 only
+        if (fp32) return (int)cudaErrorInvalidValue;
+        probe_eigen_kernel<EQ_TWO_PHASE_SG, double><<<g, b, 0, s>>>(P, d_U, n, xdir, d_L, d_R);
+        return (int)cudaGetLastError();
+    }
 #if WENOFV_HAS_FP32
     if (fp32) {
         if (P.kind == EQ_TWO_PHASE) probe_eigen_kernel<EQ_TWO_PHASE, float><<<g, b, 0, s>>>(P, d_U, n, xdir, d_L, d_R);

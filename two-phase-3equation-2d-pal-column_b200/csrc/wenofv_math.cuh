@@ -615,6 +615,31 @@ struct TwoPhaseK {
         const double pre1 = c1_2 * (z1rho1 + z1rho1 * Dn / N - rho10);
         p = (z1 < z2) ? pre2 : pre1;
     }
+    // the strict order of tp_state: getVolumeFrac, then getPressure
+    __device__ __forceinline__ void state(double z1rho1, double z2rho2, double &z1, double &p) const
+    {
+        z1 = volume_frac(z1rho1, z2rho2);
+        p = pressure(z1rho1, z2rho2, z1);
+    }
+    // the volume fraction of the eigensystem (the pressure is not needed there)
+    __device__ __forceinline__ void eigen_state(double z1rho1, double z2rho2, double &z1, double &p) const
+    {
+#if WENOFV_STRICT
+        z1 = volume_frac(z1rho1, z2rho2);
+        p = 0.0;
+#else
+        recover(z1rho1, z2rho2, z1, p);
+#endif
+    }
+    template <class R> __device__ __forceinline__ R sound_p(R z1rho1, R z2rho2, R z1, R z2, double) const
+    {
+        return sound<R>(z1rho1, z2rho2, z1, z2);
+    }
+    template <class R> __device__ __forceinline__ void phase_c2(R, R, R, R, double, R &a, R &b) const
+    {
+        a = R(c1_2);
+        b = R(c2_2);
+    }
     // z2 comes in as 1 - z1 rounded from FP64: in FP32, 1 - (float)z1 loses z2 near pure phase 1
     template <class R> __device__ __forceinline__ R sound(R z1rho1, R z2rho2, R z1, R z2) const
     {
@@ -633,6 +658,82 @@ struct TwoPhaseK {
     }
 };
 
+// Stiffened-gas phases on their isentropes (EQ_TWO_PHASE_SG; an extension, not in the
+// reference): p_k(rho) = (pref + pi_k) (rho / rho_k0)^gamma_k - pi_k, whose expansion at pref
+// is the linear model with c_k^2 = gamma_k (pref + pi_k) / rho_k0 (P.sound1/2 hold those).
+// Pressure equilibrium z1rho1 / rho_1(p) + z2rho2 / rho_2(p) = 1 is solved for p by Newton
+// steps from the linear model's state, kept above -min(pi_k) where both densities exist,
+// until a step is below 1e-14 (|p| + max(pi_k) + |pref|), at most SG_NEWTON; then
+// z1 = z1rho1 / rho_1(p).  The flux pressure is p - pref, as the linear model drops g_preb.
+// The phase sound speeds are c_k^2 = gamma_k (p + pi_k) z_k / z_krho_k.  FP64 only; pow is
+// CUDA's, so the results agree with the C library's to a few ulp, not bit for bit.
+constexpr int SG_NEWTON = 12;
+struct StiffK {
+    TwoPhaseK lin;
+    double g1, g2, pi1, pi2, pref, rho10, rho20, a1, a2, ig1, ig2, lo, scale;
+    __device__ __forceinline__ explicit StiffK(const EqParams &p) : lin(p)
+    {
+        g1 = p.gamma1; g2 = p.gamma2; pi1 = p.pinf1; pi2 = p.pinf2; pref = p.preb;
+        rho10 = p.rho10; rho20 = p.rho20;
+        a1 = 1.0 / (pref + pi1); a2 = 1.0 / (pref + pi2);
+        ig1 = 1.0 / g1; ig2 = 1.0 / g2;
+        lo = -(pi1 < pi2 ? pi1 : pi2);
+        scale = (pi1 > pi2 ? pi1 : pi2) + fabs(pref);
+    }
+    // (z1, p - pref) of the state
+    __device__ __forceinline__ void solve(double m1, double m2, double &z1, double &pg) const
+    {
+        double p = pref + lin.pressure(m1, m2, lin.volume_frac(m1, m2));
+        if (!(p > lo)) p = 0.5 * (pref + lo);
+        for (int it = 0; it < SG_NEWTON; it++) {
+            const double r1 = rho10 * pow((p + pi1) * a1, ig1);
+            const double r2 = rho20 * pow((p + pi2) * a2, ig2);
+            const double h = m1 / r1 + m2 / r2 - 1.0;
+            const double dh = -(m1 / (r1 * (g1 * (p + pi1))) + m2 / (r2 * (g2 * (p + pi2))));
+            double pn = p - h / dh;
+            if (!(pn > lo)) pn = 0.5 * (p + lo);
+            const double dp = pn - p;
+            p = pn;
+            if (fabs(dp) <= 1e-14 * (fabs(p) + scale)) break;
+        }
+        z1 = m1 / (rho10 * pow((p + pi1) * a1, ig1));
+        pg = p - pref;
+    }
+    __device__ __forceinline__ double volume_frac(double m1, double m2) const
+    {
+        double z1, pg;
+        solve(m1, m2, z1, pg);
+        return z1;
+    }
+    __device__ __forceinline__ void state(double m1, double m2, double &z1, double &pg) const { solve(m1, m2, z1, pg); }
+    __device__ __forceinline__ void eigen_state(double m1, double m2, double &z1, double &pg) const { solve(m1, m2, z1, pg); }
+    __device__ __forceinline__ void recover(double m1, double m2, double &z1, double &pg) const { solve(m1, m2, z1, pg); }
+    __device__ __forceinline__ void recover_rho(double m1, double m2, double rho, double &irho, double &z1, double &pg) const
+    {
+        solve(m1, m2, z1, pg);
+        irho = 1.0 / rho;
+    }
+    // Wood: 1 / (rho c^2) = z1 / (gamma_1 (p + pi_1)) + z2 / (gamma_2 (p + pi_2))
+    template <class R> __device__ __forceinline__ R sound_p(R m1, R m2, R z1, R z2, double pg) const
+    {
+        static_assert(sizeof(R) == sizeof(double), "the stiffened-gas model runs in FP64");
+        const double p = pg + pref;
+        const double rho = m1 + m2;
+        return 1.0 / sqrt(rho * (z1 / (g1 * (p + pi1)) + z2 / (g2 * (p + pi2))));
+    }
+    template <class R> __device__ __forceinline__ void phase_c2(R m1, R m2, R z1, R z2, double pg, R &c1_2, R &c2_2) const
+    {
+        const double p = pg + pref;
+        c1_2 = g1 * (p + pi1) * z1 / m1;
+        c2_2 = g2 * (p + pi2) * z2 / m2;
+    }
+};
+
+// the two-phase equation kinds and their thermodynamics
+template <int EQ> struct IsTwoPhase { static constexpr bool value = EQ == EQ_TWO_PHASE || EQ == EQ_TWO_PHASE_SG; };
+template <int EQ> struct TPKOf { using type = TwoPhaseK; };
+template <> struct TPKOf<EQ_TWO_PHASE_SG> { using type = StiffK; };
+
 // Primitive quantities of one state, computed once and reused by every consumer (the
 // reference recomputes getVolumeFrac per call; the values are identical).
 template <class R> struct TPState {
@@ -642,16 +743,16 @@ template <class R> struct TPState {
 
 // The state comes in FP64 in every form: the volume fraction and the pressure are
 // recovered from the FP64 values.
-template <class R>
-__device__ __forceinline__ void tp_state(const TwoPhaseK &K, const double *U, TPState<R> &s)
+template <class R, class KT>
+__device__ __forceinline__ void tp_state(const KT &K, const double *U, TPState<R> &s)
 {
     s.z1rho1 = (R)U[0]; s.z2rho2 = (R)U[1]; s.rhou = (R)U[2]; s.rhov = (R)U[3];
     s.rho = s.z1rho1 + s.z2rho2;
 #if WENOFV_STRICT
     s.u = s.rhou / s.rho;
     s.v = s.rhov / s.rho;
-    const double z1 = K.volume_frac(U[0], U[1]);
-    s.pd = K.pressure(U[0], U[1], z1);
+    double z1;
+    K.state(U[0], U[1], z1, s.pd);
 #else
     double z1;
     if constexpr (sizeof(R) == sizeof(double)) {
@@ -667,7 +768,7 @@ __device__ __forceinline__ void tp_state(const TwoPhaseK &K, const double *U, TP
     }
 #endif
     s.pre = (R)s.pd;
-    s.c = K.sound<R>(s.z1rho1, s.z2rho2, (R)z1, (R)(1.0 - z1));
+    s.c = K.template sound_p<R>(s.z1rho1, s.z2rho2, (R)z1, (R)(1.0 - z1), s.pd);
 }
 
 // getMaxEigenValue, include/Equations.hpp:149-156 (u from U[2]/(U[0]+U[1]) as there)
@@ -861,7 +962,7 @@ template <class R> struct TPEigen {
     R z1rho1, z2rho2, rho, u, v, c, c2, sc1_2, sc2_2;
     R i2c2, i2c, irc2, idsc, irho, pad; // reciprocals of the contracted build; pad: odd size in smem
 };
-template <class R> __device__ __forceinline__ void tp_eigen_prep(const TwoPhaseK &K, const double *U, TPEigen<R> &e)
+template <class R, class KT> __device__ __forceinline__ void tp_eigen_prep(const KT &K, const double *U, TPEigen<R> &e)
 {
     e.z1rho1 = (R)U[0]; e.z2rho2 = (R)U[1];
     e.rho = e.z1rho1 + e.z2rho2;
@@ -873,17 +974,14 @@ template <class R> __device__ __forceinline__ void tp_eigen_prep(const TwoPhaseK
     e.u = (R)U[2] * e.irho;
     e.v = (R)U[3] * e.irho;
 #endif
-#if WENOFV_STRICT
-    const double z1d = K.volume_frac(U[0], U[1]);
-#else
-    double z1d, pdummy;
-    K.recover(U[0], U[1], z1d, pdummy);
-#endif
+    double z1d, pd;
+    K.eigen_state(U[0], U[1], z1d, pd);
     const R z1 = (R)z1d;
     const R z2 = (R)(1.0 - z1d);
-    e.c = K.sound<R>(e.z1rho1, e.z2rho2, z1, z2);
+    e.c = K.template sound_p<R>(e.z1rho1, e.z2rho2, z1, z2, pd);
     e.c2 = e.c * e.c;
-    const R c1_2 = R(K.c1_2), c2_2 = R(K.c2_2);
+    R c1_2, c2_2;
+    K.template phase_c2<R>(e.z1rho1, e.z2rho2, z1, z2, pd, c1_2, c2_2);
     if constexpr (sizeof(R) < sizeof(double)) {
         // FP32: the same quantities without the cancellation 1 - zrho1/(zrho1+zrho2) and
         // without dividing by z_k^2 (exact algebra: multiply zrho_k through by z1^2 z2^2)
@@ -1144,13 +1242,13 @@ template <> struct EqTraits<EQ_LINEAR_ADV> { static constexpr int NV = 1; };
 // getMaxEigenValue (include/Equations.hpp:149-156) for the CFL and the limiter's mu
 template <int EQ, class R> __device__ __forceinline__ void max_eigs(const EqParams &P, const double *U, R &ax, R &ay)
 {
-    if (EQ == EQ_TWO_PHASE) {
-        TwoPhaseK K(P);
+    if constexpr (IsTwoPhase<EQ>::value) {
+        const typename TPKOf<EQ>::type K(P);
         TPState<R> s;
         tp_state<R>(K, U, s);
         ax = tp_max_eig(s, 1.0, 0.0);
         ay = tp_max_eig(s, 0.0, 1.0);
-    } else if (EQ == EQ_EULER) {
+    } else if constexpr (EQ == EQ_EULER) {
         EUState<R> s;
         eu_state<R>(P.gamma, U, s);
         ax = fabs(s.u * R(1.0) + s.v * R(0.0)) + s.c;
@@ -1175,8 +1273,8 @@ __device__ __forceinline__ void riemann(const EqParams &P, int flux_arg, const d
     R UL[NV], UR[NV], Fr[NV];
 #pragma unroll
     for (int v = 0; v < NV; v++) { UL[v] = (R)ULd[v]; UR[v] = (R)URd[v]; }
-    if constexpr (EQ == EQ_TWO_PHASE) {
-        TwoPhaseK K(P);
+    if constexpr (IsTwoPhase<EQ>::value) {
+        const typename TPKOf<EQ>::type K(P);
         TPState<R> l, r;
         tp_state<R>(K, ULd, l);
         tp_state<R>(K, URd, r);
@@ -1198,7 +1296,7 @@ __device__ __forceinline__ void riemann(const EqParams &P, int flux_arg, const d
         const R ws = std_max(fabs(an), fabs(an));
         Fr[0] = R(0.5) * (an * UL[0] + an * UR[0] - ws * (UR[0] - UL[0]));
     }
-    if constexpr (!(F32 && EQ == EQ_TWO_PHASE)) { // the FP32 two-phase fluxes write F themselves
+    if constexpr (!(F32 && IsTwoPhase<EQ>::value)) { // the FP32 two-phase fluxes write F themselves
 #pragma unroll
         for (int v = 0; v < NV; v++) F[v] = (double)Fr[v];
     }
@@ -1208,13 +1306,13 @@ __device__ __forceinline__ void riemann(const EqParams &P, int flux_arg, const d
 template <int EQ, class R>
 __device__ __forceinline__ void eigen_rows(const EqParams &P, const double *U, bool xdir, int k, R *Lrow, R *Rrow)
 {
-    if (EQ == EQ_TWO_PHASE) {
-        TwoPhaseK K(P);
+    if constexpr (IsTwoPhase<EQ>::value) {
+        const typename TPKOf<EQ>::type K(P);
         TPEigen<R> e;
         tp_eigen_prep<R>(K, U, e);
         tp_L_row<R>(e, xdir, k, Lrow);
         tp_R_row<R>(e, xdir, k, Rrow);
-    } else if (EQ == EQ_EULER) {
+    } else if constexpr (EQ == EQ_EULER) {
         EUState<R> s;
         eu_state<R>(P.gamma, U, s);
         eu_L_row<R>(P.gamma, s, xdir, k, Lrow);
@@ -1266,8 +1364,8 @@ template <> struct CellEigen<EQ_EULER> { using type = EUState<double>; };
 
 template <int EQ> __device__ __forceinline__ void cell_eigen(const EqParams &P, const double *U, typename CellEigen<EQ>::type &e)
 {
-    if constexpr (EQ == EQ_TWO_PHASE) {
-        TwoPhaseK K(P);
+    if constexpr (IsTwoPhase<EQ>::value) {
+        const typename TPKOf<EQ>::type K(P);
         tp_eigen_prep<double>(K, U, e);
     } else if constexpr (EQ == EQ_EULER) {
         eu_state<double>(P.gamma, U, e);
@@ -1277,7 +1375,7 @@ template <int EQ>
 __device__ __forceinline__ void eigen_rows_of(const EqParams &P, const typename CellEigen<EQ>::type &e, bool xdir, int k,
                                               double *Lrow, double *Rrow)
 {
-    if constexpr (EQ == EQ_TWO_PHASE) {
+    if constexpr (IsTwoPhase<EQ>::value) {
         tp_L_row<double>(e, xdir, k, Lrow);
         tp_R_row<double>(e, xdir, k, Rrow);
     } else if constexpr (EQ == EQ_EULER) {
@@ -1298,7 +1396,7 @@ template <int EQ> __device__ __forceinline__ void max_eigs_of(const typename Cel
 // number of leading variables the bound-preserving limiter acts on: the two partial
 // densities of the two-phase model (src/WENOFV.cpp:1964), the density for Euler, none for
 // scalar advection
-template <int EQ> struct LimitedVars { static constexpr int N = EQ == EQ_TWO_PHASE ? 2 : (EQ == EQ_EULER ? 1 : 0); };
+template <int EQ> struct LimitedVars { static constexpr int N = IsTwoPhase<EQ>::value ? 2 : (EQ == EQ_EULER ? 1 : 0); };
 
 // Gauss-Lobatto 4-point weights as written at third_party/scTools/GaussQuadratureInRef.hpp:252-262
 __device__ __forceinline__ double gl_weight(int gp)

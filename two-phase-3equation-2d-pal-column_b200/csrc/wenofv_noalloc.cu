@@ -126,7 +126,7 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
     d.dX = (cfg->xr - cfg->xl) / cfg->nx;
     d.dx4 = std::pow(d.dX, 4); // the reference's pow(m_deltaX, 4), include/Utility.hpp:313
     d.dY = (cfg->yr - cfg->yl) / cfg->ny;
-    d.eq = EqParams{eq->eq_kind, eq->rho10, eq->rho20, eq->sound1, eq->sound2, eq->preb, eq->gamma, eq->adv_u, eq->adv_v};
+    d.eq = eq_params_of(*eq);
 
     InstState st;
     std::memset(&st, 0, sizeof st);
