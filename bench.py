@@ -45,11 +45,12 @@ FLOP_KEYS = {
     "column1024": ("two_phase", 1, 1, 1, 1),    # characteristic, WENO-Z, HLLC, limiter
     "column1024_exp": ("two_phase", 1, 2, 1, 1),  # the same with WENOEXP (7-point stencils)
     "column1024_prim3": ("two_phase", 4, 1, 1, 1),  # PRIMITIVE3: z1 by WENOEXP/THINC, p, u, v by WENO-Z
+    "column1024_sg": ("two_phase_sg", 1, 1, 1, 1),  # the column with stiffened-gas phases
     "euler512": ("euler", 0, 1, 1, 0),          # conservative, WENO-Z, HLLC
     "advection128": ("linear_advection", 0, 0, 0, 0),
 }
-BYTES_PER_CELL_STAGE = {"column1024": 96.0, "column1024_exp": 96.0, "column1024_prim3": 96.0, "euler512": 96.0,
-                        "advection128": 24.0}
+BYTES_PER_CELL_STAGE = {"column1024": 96.0, "column1024_exp": 96.0, "column1024_prim3": 96.0, "column1024_sg": 96.0,
+                        "euler512": 96.0, "advection128": 24.0}
 
 
 def flops_per_cell_stage(name: str) -> float:
@@ -78,6 +79,17 @@ def workload(name: str, wb, form: int):
                     bc="periodic", scheme="WENOEXP" if sch == 2 else ("WENOEXP/THINC (z1), WENO-Z" if rec == 4 else "WENO-Z"),
                     flux="HLLC", reconstruction="primitive3 (z1, p, u, v)" if rec == 4 else "characteristic", limiter=True,
                     rk="SSP-RK3", cfl=0.5, ic="disk r=0.2 tanh-smoothed over 2 cells, eps=1e-6, seeded periodic "
+                    "Gaussian velocity field amplitude 1e-2 (seed 3)")
+    elif name == "column1024_sg":
+        U0, prm = cases.sg_column(1024, 1024, seed=3)
+        cfg = wb.make_config(1024, 1024, rk=2, cfl=0.5, scheme=1, limiter=1, flux=1, recon=1, precision=form)
+        eq = wb.make_eq(kind=wb.EQ_TWO_PHASE_SG, rho10=prm["rho10"], rho20=prm["rho20"], preb=prm["preb"],
+                        gamma1=prm["gamma1"], pinf1=prm["pinf1"], gamma2=prm["gamma2"], pinf2=prm["pinf2"])
+        desc = dict(workload="liquid_column_1024_stiffened_gas", grid="1024x1024",
+                    equation="two-phase 3-equation, stiffened-gas phases on their isentropes (g1=4.4, pinf1=6e3; "
+                    "g2=1.4, pinf2=0) through p=1, density ratio 1000, Newton pressure equilibrium",
+                    bc="periodic", scheme="WENO-Z", flux="HLLC", reconstruction="characteristic", limiter=True,
+                    rk="SSP-RK3", cfl=0.5, ic="disk r=0.2 tanh-smoothed over 2 cells, eps=1e-6, p=1, seeded periodic "
                     "Gaussian velocity field amplitude 1e-2 (seed 3)")
     elif name == "euler512":
         U0, _ = cases.euler_quadrants(512, 512, seed=2)
@@ -152,6 +164,10 @@ def cpu_baseline(name: str, steps: int, warmup: int, sample_n: int = 256):
         U0, _ = cases.euler_quadrants(sample_n, sample_n, seed=2)
         p = O.Problem(nx=sample_n, ny=sample_n, bc=O.BC_OUTFLOW, eq_kind=O.EQ_EULER, rk=2, cfl=0.4, scheme=1,
                       flux=1, recon=0, threads=ncores)
+    elif name == "column1024_sg":
+        U0, prm = cases.sg_column(sample_n, sample_n, seed=3)
+        p = O.Problem(nx=sample_n, ny=sample_n, eq_kind=O.EQ_TWO_PHASE_SG, rk=2, cfl=0.5, scheme=1, flux=1, recon=1,
+                      limiter=1, threads=ncores, **prm)
     elif name == "advection128":
         sample_n = 128
         U0 = cases.advection_sine(128, 128)
@@ -324,7 +340,8 @@ def run_ours(args, rank, world, dist):
     # FP32-bulk beside FP64: the same steps from the same state, device-timed the same way,
     # and the error of its result against the FP64 one
     fp32 = None
-    if form == wb.FP64 and args.workload not in ("advection128", "column1024_exp", "column1024_prim3") and not args.no_fp32:
+    if form == wb.FP64 and args.workload not in ("advection128", "column1024_exp", "column1024_prim3", "column1024_sg") \
+            and not args.no_fp32:
         fp32 = compare_fp32(args, wb, cfg, eq, U0, dt, U_dev_end, ncells, nstages, flush, barrier, dist, world, local)
 
     # end to end through the public API with host arrays (pinned host memory)

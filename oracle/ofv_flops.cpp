@@ -53,8 +53,8 @@ static double count_rhs(ofv_problem p, int n, ofv_counters *out)
 
 int main()
 {
-    const char *eqn[] = {"two_phase", "linear_advection", "euler"};
-    for (int eqk = 0; eqk < 3; eqk++)
+    const char *eqn[] = {"two_phase", "linear_advection", "euler", "two_phase_sg"};
+    for (int eqk = 0; eqk < 4; eqk++)
         for (int recon = 0; recon < 5; recon++)
             for (int scheme = 0; scheme < 3; scheme++)
                 for (int flux = 0; flux < 2; flux++)
@@ -70,6 +70,10 @@ int main()
                         p.eq.kind = eqk;
                         p.eq.rho10 = 1000; p.eq.rho20 = 1; p.eq.sound1 = 70; p.eq.sound2 = 70;
                         p.eq.gamma = 1.4; p.eq.adv_u = 1; p.eq.adv_v = 1;
+                        if (eqk == OFV_EQ_TWO_PHASE_SG) { // at the reference pressure (rho_k = rho_k0)
+                            p.eq.preb = 1.0;
+                            p.eq.gamma1 = 4.4; p.eq.pinf1 = 6000; p.eq.gamma2 = 1.4; p.eq.pinf2 = 0;
+                        }
                         const double c1 = count_rhs(p, 32, nullptr), c2 = count_rhs(p, 64, nullptr);
                         ofv_counters k3;
                         const double c3 = count_rhs(p, 128, &k3);

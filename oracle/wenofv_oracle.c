@@ -386,7 +386,32 @@ static void sg_linearised(const ofv_eq *e, ofv_eq *lin)
     lin->sound1 = sqrt(e->gamma1 * (e->preb + e->pinf1) / e->rho10);
     lin->sound2 = sqrt(e->gamma2 * (e->preb + e->pinf2) / e->rho20);
 }
+/* the last solve of each thread, so that the volume fraction, pressure, sound speed and phase
+ * sound speeds of one state (asked for one by one, as the reference's functions are) cost
+ * one solve; the result does not depend on the cache */
+#ifdef OFV_COUNTING
+#define OFV_TLS thread_local
+#else
+#define OFV_TLS __thread
+#endif
+static OFV_TLS double sg_key[9], sg_val[2];
+static OFV_TLS int sg_valid = 0;
+static void sg_solve_uncached(const ofv_eq *e, const real_t *U, real_t *z1_out, real_t *p_out);
 static void sg_solve(const ofv_eq *e, const real_t *U, real_t *z1_out, real_t *p_out)
+{
+    const double key[9] = {(double)U[0], (double)U[1], e->rho10, e->rho20, e->preb, e->gamma1, e->pinf1, e->gamma2, e->pinf2};
+    if (sg_valid && memcmp(key, sg_key, sizeof key) == 0) {
+        *z1_out = sg_val[0];
+        *p_out = sg_val[1];
+        return;
+    }
+    sg_solve_uncached(e, U, z1_out, p_out);
+    memcpy(sg_key, key, sizeof key);
+    sg_val[0] = (double)*z1_out;
+    sg_val[1] = (double)*p_out;
+    sg_valid = 1;
+}
+static void sg_solve_uncached(const ofv_eq *e, const real_t *U, real_t *z1_out, real_t *p_out)
 {
     ofv_eq lin;
     sg_linearised(e, &lin);
