@@ -7,7 +7,9 @@ the tolerances are stated instead of bit equality:
 
 * pointwise fluxes and eigenvectors: FP64_STRICT within 1e-12 of the state's scale, FP64
   within 1e-11;
-* a few RK steps of a 64x48 column: FP64_STRICT within 1e-12 of max |U|, FP64 within 1e-10;
+* a few RK steps of a 64x48 column: FP64_STRICT within 1e-12 of max |U|, FP64 within 1e-10,
+  the CFL time step within 100 times those (the equilibrium pressure carries the liquid's
+  density rounding times rho_1 c_1^2, which the gas of a mixed cell feels relative to p ~ 1);
 * conservation to roundoff and positive partial densities on a 256^2 column.
 """
 from __future__ import annotations
@@ -67,7 +69,9 @@ def test_sg_column_against_oracle(wb, oracle_lib, recon, flux):
         cfg = wb.make_config(nx, ny, scheme=1, flux=flux, recon=recon, limiter=1, precision=prec)
         with wb.Solver(cfg, eq) as s:
             s.upload(U0)
-            assert abs(s.compute_dt() - dts[0]) <= 1e-13 * dts[0]
+            # a relative 1e-16 in the liquid's density is 1e-16 rho_1 c_1^2 ~ 3e-12 in the pressure,
+            # which the gas of a mixed cell feels relative to p ~ 1
+            assert abs(s.compute_dt() - dts[0]) <= 100 * tol * dts[0]
             t2, n2 = s.advance(1e9, max_steps=5)
             assert n2 == n and abs(t2 - t) <= 1e-12 * t
             U = s.download()

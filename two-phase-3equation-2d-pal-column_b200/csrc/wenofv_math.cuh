@@ -680,14 +680,26 @@ struct StiffK {
         lo = -(pi1 < pi2 ? pi1 : pi2);
         scale = (pi1 > pi2 ? pi1 : pi2) + fabs(pref);
     }
+    // x^(1/gamma) of the isentropes: pow in the strict build; exp(log(x) / gamma) in the
+    // contracted one (x is near 1, so the error stays at a few ulp, without pow's extended
+    // precision cost)
+    static __device__ __forceinline__ double root(double x, double ig)
+    {
+#if WENOFV_STRICT
+        return pow(x, ig);
+#else
+        return exp(ig * log(x));
+#endif
+    }
     // (z1, p - pref) of the state
     __device__ __forceinline__ void solve(double m1, double m2, double &z1, double &pg) const
     {
         double p = pref + lin.pressure(m1, m2, lin.volume_frac(m1, m2));
         if (!(p > lo)) p = 0.5 * (pref + lo);
+        double r1 = 0.0;
         for (int it = 0; it < SG_NEWTON; it++) {
-            const double r1 = rho10 * pow((p + pi1) * a1, ig1);
-            const double r2 = rho20 * pow((p + pi2) * a2, ig2);
+            r1 = rho10 * root((p + pi1) * a1, ig1);
+            const double r2 = rho20 * root((p + pi2) * a2, ig2);
             const double h = m1 / r1 + m2 / r2 - 1.0;
             const double dh = -(m1 / (r1 * (g1 * (p + pi1))) + m2 / (r2 * (g2 * (p + pi2))));
             double pn = p - h / dh;
@@ -696,7 +708,13 @@ struct StiffK {
             p = pn;
             if (fabs(dp) <= 1e-14 * (fabs(p) + scale)) break;
         }
+#if WENOFV_STRICT
         z1 = m1 / (rho10 * pow((p + pi1) * a1, ig1));
+#else
+        // rho_1 of the last step: its p moved by at most 1e-14 (|p| + max pi_k) since, which
+        // changes rho_1 = rho10 x^(1/gamma_1) by at most that over gamma_1 (p + pi_1)
+        z1 = m1 / r1;
+#endif
         pg = p - pref;
     }
     __device__ __forceinline__ double volume_frac(double m1, double m2) const
