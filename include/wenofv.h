@@ -82,6 +82,10 @@ typedef struct {
      * pinf_k) / rho_k0 for the first guess of the pressure equilibrium); FP64 forms and
      * RECONSTRUCTIONTYPE 0-1 only */
     double gamma1, pinf1, gamma2, pinf2;
+    /* gravity of the two-phase kinds, assembleSourceTerm's g_g0 (src/WENOFV.cpp:1831-1872):
+     * the y-momentum RHS gains -rho g; 9.81 for DAMBREAK/RTI, 2 pi for STANDING_WAVE, 0 for
+     * the periodic test cases */
+    double gravity;
 } wenofv_eq_params;
 
 /* Solver options: the settings.cfg keys (config/settings.cfg:11-24, read at

@@ -32,7 +32,8 @@ class _Eq(C.Structure):
     _fields_ = [("kind", C.c_int), ("rho10", C.c_double), ("rho20", C.c_double),
                 ("sound1", C.c_double), ("sound2", C.c_double), ("preb", C.c_double),
                 ("gamma", C.c_double), ("adv_u", C.c_double), ("adv_v", C.c_double),
-                ("gamma1", C.c_double), ("pinf1", C.c_double), ("gamma2", C.c_double), ("pinf2", C.c_double)]
+                ("gamma1", C.c_double), ("pinf1", C.c_double), ("gamma2", C.c_double), ("pinf2", C.c_double),
+                ("gravity", C.c_double)]
 
 
 class _Problem(C.Structure):
@@ -74,6 +75,7 @@ class Problem:
     pinf1: float = 6.0e3
     gamma2: float = 1.4
     pinf2: float = 0.0
+    gravity: float = 0.0     # assembleSourceTerm's g_g0 (two-phase kinds)
 
     @property
     def nvar(self) -> int:
@@ -81,7 +83,7 @@ class Problem:
 
     def to_c(self) -> _Problem:
         e = _Eq(self.eq_kind, self.rho10, self.rho20, self.sound1, self.sound2, self.preb,
-                self.gamma, self.adv_u, self.adv_v, self.gamma1, self.pinf1, self.gamma2, self.pinf2)
+                self.gamma, self.adv_u, self.adv_v, self.gamma1, self.pinf1, self.gamma2, self.pinf2, self.gravity)
         return _Problem(self.nx, self.ny, self.xl, self.xr, self.yl, self.yr, self.bc, self.rk,
                         self.cfl, self.scheme, self.limiter, self.flux, self.recon, self.ref_slabs,
                         self.threads, e)
@@ -248,7 +250,7 @@ def reference_available() -> bool:
 
 def run_reference(p: Problem, testcase: int = 0, U0: np.ndarray | None = None, steps: int = 0,
                   t_end: float = 0.0, want_rhs: bool = False, time: bool = False,
-                  timeout: float = 600.0, warmup: int = 0) -> RefResult:
+                  timeout: float = 600.0, warmup: int = 0, source_case: int = -1) -> RefResult:
     """Run the unmodified reference (4 slab ranks) on the two-phase system.
 
     ``testcase`` selects the reference's own test case (its domain, boundary and, when
@@ -279,6 +281,8 @@ def run_reference(p: Problem, testcase: int = 0, U0: np.ndarray | None = None, s
             args += ["--time"]
         if warmup:
             args += ["--warmup", str(warmup)]
+        if source_case >= 0:  # the test case of assembleSourceTerm (its gravity)
+            args += ["--source-case", str(source_case)]
         cp = subprocess.run(args, capture_output=True, text=True, timeout=timeout)
         if cp.returncode != 0:
             raise RuntimeError(f"reference failed ({cp.returncode}): {cp.stderr[-2000:]}")

@@ -15,6 +15,10 @@
 //                   [--rhs FILE]       one assembleRHS of the initial state, SoA FP64
 //                   [--faces FILE]     face states after that assembleRHS [cell][B,T,L,R][v][gp]
 //                   [--out FILE] [--dts FILE] [--time]
+//                   [--source-case N]  after initialisation, the test case that assembleSourceTerm
+//                                      sees (DAMBREAK/RTI: g = 9.81, STANDING_WAVE: 2 pi), so that
+//                                      its gravity runs on a periodic case's grid and boundaries
+//                                      (the walls of those cases are not implemented)
 #include <mpi.h>
 
 #include <atomic>
@@ -42,6 +46,7 @@ struct Args {
     long steps = -1, warmup = 0;
     double tend = -1;
     bool time = false;
+    int source_case = -1;
 };
 
 struct Shared {
@@ -80,6 +85,7 @@ void rank_main(int rank, const Args &a, Shared &sh, const std::vector<double> &u
     if (a.rho20 > 0) equation->g_rho20 = a.rho20;
     if (a.sound1 > 0) equation->g_sound1 = a.sound1;
     if (a.sound2 > 0) equation->g_sound2 = a.sound2;
+    if (a.source_case >= 0) solver.m_testcase = (TESTCASETYPE)a.source_case;
 
     const int nx = sh.nx, ny = sh.ny, nv = solver.m_varNum;
     const int x0 = solver.m_procIndexX * solver.m_elemNumX;
@@ -173,6 +179,7 @@ int main(int argc, char **argv)
         else if (s == "--warmup") { a.warmup = std::atol(val); k++; }
         else if (s == "--tend") { a.tend = std::atof(val); k++; }
         else if (s == "--time") { a.time = true; }
+        else if (s == "--source-case") { a.source_case = std::atoi(val); k++; }
         else { std::fprintf(stderr, "unknown argument %s\n", s.c_str()); return 2; }
     }
     if (a.steps < 0 && a.tend <= 0) a.steps = 0;

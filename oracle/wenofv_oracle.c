@@ -1301,6 +1301,12 @@ static void rhs_ws(ofv_ws *w, const double *U, double *rhs, double *theta_flags)
                 r += -aR / w->dxc[i] / w->dy[j];
                 r += aB / w->dxc[i] / w->dy[j];
                 r -= aT / w->dxc[i] / w->dy[j];
+                if (v == 3 && p->eq.gravity != 0.0 && (p->eq.kind == OFV_EQ_TWO_PHASE || p->eq.kind == OFV_EQ_TWO_PHASE_SG)) {
+                    /* assembleSourceTerm, src/WENOFV.cpp:1843-1853 */
+                    const size_t k = (size_t)j * nx + i;
+                    const real_t rho = (real_t)U[k] + (real_t)U[(size_t)nx * ny + k];
+                    r -= rho * p->eq.gravity;
+                }
                 rhs[(size_t)v * nx * ny + (size_t)j * nx + i] = (double)r;
             }
 }

@@ -37,6 +37,9 @@ typedef struct {
     /* stiffened-gas phases (OFV_EQ_TWO_PHASE_SG, an extension): p_k(rho) on the isentrope
      * through (preb, rho_k0), rho10 and rho20 being the densities at preb */
     double gamma1, pinf1, gamma2, pinf2;
+    /* assembleSourceTerm's g_g0 (src/WENOFV.cpp:1831-1872): rhs[rho v] -= rho g for the two-phase
+     * kinds; 9.81 for DAMBREAK/RTI, 2 pi for STANDING_WAVE, 0 otherwise */
+    double gravity;
 } ofv_eq;
 
 typedef struct {

@@ -48,6 +48,9 @@ CASES = [
     ("sharp_prim3_hllc_lim_rk3", 2, 40, 24, 1, 1, 4, 1, 2, 8, 0.0, False),
     ("column_prim3_hllc_lim_rk3", 2, 48, 32, 0, 1, 4, 1, 2, 6, 0.0, True),
 ]
+# cases with the gravity source of assembleSourceTerm: name -> (the test case it sees, g_g0)
+GRAVITY = {"column_gravity_z_char_hllc_lim_rk3": (6, 9.81)}
+CASES.append(("column_gravity_z_char_hllc_lim_rk3", 2, 48, 32, 1, 1, 1, 1, 2, 6, 0.0, True))
 
 PARAMS = {0: dict(rho10=1.2, rho20=1.0, sound1=1.0, sound2=1.0),
           2: dict(rho10=1000.0, rho20=1.0, sound1=70.0, sound2=70.0)}
@@ -67,12 +70,13 @@ def main(only=()):
         if column:
             U0, cp = cases.liquid_column(nx, ny, seed=11)
             prm = dict(rho10=cp["rho10"], rho20=cp["rho20"], sound1=cp["sound1"], sound2=cp["sound2"])
+        source_case, g = GRAVITY.get(name, (-1, 0.0))
         p = Problem(nx=nx, ny=ny, rk=rk, cfl=0.5, scheme=scheme, flux=flux, recon=recon,
-                    limiter=lim, ref_slabs=4, **prm)
-        r = run_reference(p, testcase=tc, U0=U0, steps=steps, t_end=t_end, want_rhs=True)
+                    limiter=lim, ref_slabs=4, gravity=g, **prm)
+        r = run_reference(p, testcase=tc, U0=U0, steps=steps, t_end=t_end, want_rhs=True, source_case=source_case)
         np.savez_compressed(os.path.join(OUT, name + ".npz"), U0=r.U0, rhs=r.rhs, U=r.U, dts=r.dts)
         index[name] = dict(testcase=tc, nx=nx, ny=ny, scheme=scheme, flux=flux, recon=recon,
-                           limiter=lim, rk=rk, steps=steps, t_end=t_end, cfl=0.5, ref_slabs=4,
+                           limiter=lim, rk=rk, steps=steps, t_end=t_end, cfl=0.5, ref_slabs=4, gravity=g,
                            nsteps_taken=int(len(r.dts)), **prm)
         print(name, "steps", len(r.dts), "|U|max", float(np.abs(r.U).max()))
     with open(os.path.join(OUT, "index.json"), "w") as f:

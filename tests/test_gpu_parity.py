@@ -56,14 +56,15 @@ def solver_for(wb, p: Problem, precision):
                          scheme=p.scheme, limiter=p.limiter, flux=p.flux, recon=p.recon,
                          ref_slabs=p.ref_slabs, precision=precision)
     eq = wb.make_eq(kind=p.eq_kind, rho10=p.rho10, rho20=p.rho20, sound1=p.sound1, sound2=p.sound2,
-                    gamma=p.gamma, adv_u=p.adv_u, adv_v=p.adv_v)
+                    gamma=p.gamma, adv_u=p.adv_u, adv_v=p.adv_v, gravity=p.gravity)
     return wb.Solver(cfg, eq)
 
 
 def problem_of(meta) -> Problem:
     return Problem(nx=meta["nx"], ny=meta["ny"], rk=meta["rk"], cfl=meta["cfl"], scheme=meta["scheme"],
                    flux=meta["flux"], recon=meta["recon"], limiter=meta["limiter"], ref_slabs=meta["ref_slabs"],
-                   rho10=meta["rho10"], rho20=meta["rho20"], sound1=meta["sound1"], sound2=meta["sound2"])
+                   rho10=meta["rho10"], rho20=meta["rho20"], sound1=meta["sound1"], sound2=meta["sound2"],
+                   gravity=meta.get("gravity", 0.0))
 
 
 # ---- pointwise kernels ------------------------------------------------------------------------

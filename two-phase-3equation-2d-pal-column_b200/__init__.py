@@ -44,7 +44,8 @@ class EqParams(C.Structure):
     _fields_ = [("eq_kind", C.c_int), ("rho10", C.c_double), ("rho20", C.c_double),
                 ("sound1", C.c_double), ("sound2", C.c_double), ("preb", C.c_double),
                 ("gamma", C.c_double), ("adv_u", C.c_double), ("adv_v", C.c_double),
-                ("gamma1", C.c_double), ("pinf1", C.c_double), ("gamma2", C.c_double), ("pinf2", C.c_double)]
+                ("gamma1", C.c_double), ("pinf1", C.c_double), ("gamma2", C.c_double), ("pinf2", C.c_double),
+                ("gravity", C.c_double)]
 
 
 class Config(C.Structure):
@@ -150,10 +151,10 @@ def make_config(nx: int, ny: int, *, xl=0.0, xr=1.0, yl=0.0, yr=1.0, bc=BC_PERIO
 
 
 def make_eq(kind=EQ_TWO_PHASE, rho10=1.2, rho20=1.0, sound1=1.0, sound2=1.0, preb=0.0, gamma=1.4,
-            adv_u=1.0, adv_v=1.0, gamma1=4.4, pinf1=6.0e3, gamma2=1.4, pinf2=0.0) -> EqParams:
+            adv_u=1.0, adv_v=1.0, gamma1=4.4, pinf1=6.0e3, gamma2=1.4, pinf2=0.0, gravity=0.0) -> EqParams:
     """kind EQ_TWO_PHASE_SG: stiffened-gas phases (gamma_k, pinf_k) on their isentropes through
     (preb, rho10) and (preb, rho20); sound1/sound2 are ignored"""
-    return EqParams(kind, rho10, rho20, sound1, sound2, preb, gamma, adv_u, adv_v, gamma1, pinf1, gamma2, pinf2)
+    return EqParams(kind, rho10, rho20, sound1, sound2, preb, gamma, adv_u, adv_v, gamma1, pinf1, gamma2, pinf2, gravity)
 
 
 def nvar(eq: EqParams) -> int:

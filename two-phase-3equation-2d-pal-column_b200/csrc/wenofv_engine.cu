@@ -35,7 +35,7 @@ int nvar_of(int k) { return k == WENOFV_EQ_LINEAR_ADV ? 1 : 4; }
 EqParams eq_params_of(const wenofv_eq_params &e)
 {
     EqParams P{e.eq_kind, e.rho10, e.rho20, e.sound1, e.sound2, e.preb, e.gamma, e.adv_u, e.adv_v,
-               e.gamma1, e.pinf1, e.gamma2, e.pinf2};
+               e.gamma1, e.pinf1, e.gamma2, e.pinf2, e.gravity};
     if (e.eq_kind == WENOFV_EQ_TWO_PHASE_SG) { // the linearised sound speeds: the first guess of the equilibrium
         P.sound1 = std::sqrt(e.gamma1 * (e.preb + e.pinf1) / e.rho10);
         P.sound2 = std::sqrt(e.gamma2 * (e.preb + e.pinf2) / e.rho20);
@@ -79,6 +79,10 @@ int validate(const wenofv_config *c, const wenofv_eq_params *e)
         return WENOFV_EINVAL;
     }
     if (e->eq_kind < 0 || e->eq_kind > 3) { set_error("unknown equation kind %d", e->eq_kind); return WENOFV_EINVAL; }
+    if (!(e->gravity == e->gravity) || (e->gravity != 0.0 && e->eq_kind != WENOFV_EQ_TWO_PHASE && e->eq_kind != WENOFV_EQ_TWO_PHASE_SG)) {
+        set_error("gravity is a finite source of the two-phase kinds");
+        return WENOFV_EINVAL;
+    }
     if (e->eq_kind == WENOFV_EQ_TWO_PHASE_SG) {
         if (!(e->gamma1 > 1.0 && e->gamma2 > 1.0 && e->pinf1 >= 0.0 && e->pinf2 >= 0.0 && e->rho10 > 0.0 && e->rho20 > 0.0 &&
               e->preb + e->pinf1 > 0.0 && e->preb + e->pinf2 > 0.0)) {

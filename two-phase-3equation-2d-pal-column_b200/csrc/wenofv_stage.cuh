@@ -648,6 +648,12 @@ __device__ __forceinline__ double phase_update(StageSmem<EQ, H> &S, const InstDe
     const double idy = 1.0 / dyq, idxc = S.sidxc[c], idxl = S.sidxl[c];
     rhs = ((aL * idxl - aR * idxc) + (aB - aT) * idxc) * idy;
 #endif
+    if constexpr (IsTwoPhase<EQ>::value) { // assembleSourceTerm, src/WENOFV.cpp:1831-1872
+        if (v == 3 && D.eq.gravity != 0.0) {
+            const double rho = S.su[q & 7][0][c + GH] + S.su[q & 7][1][c + GH];
+            rhs -= rho * D.eq.gravity;
+        }
+    }
     const double U = S.su[q & 7][v][c + GH];
     const double Un = L.first_stage ? U : S.sun[q & 1][v][c + GH];
     double Unew;

@@ -9,6 +9,7 @@ struct EqParams {
     int kind; // 0 two-phase, 1 linear advection, 2 Euler, 3 two-phase stiffened gas (include/wenofv.h)
     double rho10, rho20, sound1, sound2, preb, gamma, adv_u, adv_v;
     double gamma1, pinf1, gamma2, pinf2;
+    double gravity; // two-phase kinds: rhs[rho v] -= rho g
 };
 
 enum { EQ_TWO_PHASE = 0, EQ_LINEAR_ADV = 1, EQ_EULER = 2, EQ_TWO_PHASE_SG = 3 };
