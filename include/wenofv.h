@@ -43,9 +43,20 @@ enum {
 
 /* equation kinds; TWO_PHASE is TwoPhaseEquation (include/Equations.hpp:52-1044) */
 enum { WENOFV_EQ_TWO_PHASE = 0, WENOFV_EQ_LINEAR_ADV = 1, WENOFV_EQ_EULER = 2, WENOFV_EQ_TWO_PHASE_SG = 3 };
-/* boundary kinds; PERIOD keeps the number of BOUNDARYTYPE::PERIOD (include/Equations.hpp:27);
- * OUTFLOW (zero-gradient) has no counterpart in the reference */
-enum { WENOFV_BC_PERIOD = 0, WENOFV_BC_OUTFLOW = 5 };
+/* boundary kinds with the numbers of BOUNDARYTYPE (include/Equations.hpp:25-32): PERIOD;
+ * NEUMANN ("reflective, slip") and FREESLIP: mirror ghost cells with the normal momentum
+ * negated; NOSLIP: mirror ghost cells with both momenta negated.  The reference declares the
+ * wall kinds but does not implement them (src/WENOFV.cpp:2254-2292), so their ghost rule is
+ * this library's; NEUMANN2 (boundary from the initial data) is not supported.  OUTFLOW
+ * (zero-gradient) has no counterpart in the reference. */
+enum {
+    WENOFV_BC_PERIOD = 0,
+    WENOFV_BC_NEUMANN = 1,
+    WENOFV_BC_NOSLIP = 2,
+    WENOFV_BC_NEUMANN2 = 3,
+    WENOFV_BC_FREESLIP = 4,
+    WENOFV_BC_OUTFLOW = 5
+};
 /* arithmetic forms */
 enum {
     WENOFV_FP64 = 0,        /* FP64 with fused multiply-add contraction */

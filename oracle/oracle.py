@@ -25,7 +25,7 @@ LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "wenofv_ref")
 
 EQ_TWO_PHASE, EQ_LINEAR_ADV, EQ_EULER, EQ_TWO_PHASE_SG = 0, 1, 2, 3
-BC_PERIOD, BC_OUTFLOW = 0, 5
+BC_PERIOD, BC_NEUMANN, BC_NOSLIP, BC_NEUMANN2, BC_FREESLIP, BC_OUTFLOW = 0, 1, 2, 3, 4, 5
 
 
 class _Eq(C.Structure):

@@ -976,7 +976,19 @@ static void ws_free(ofv_ws *w)
 
 /* Ghost fill.  PERIOD reproduces the ring exchange plus the periodic y copy over the full
  * extended x range (src/WENOFV.cpp:2175-2269), i.e. a 2-D periodic wrap including corners.
- * OUTFLOW (extension) is a zero-gradient copy of the nearest interior cell. */
+ * OUTFLOW (extension) is a zero-gradient copy of the nearest interior cell.  The walls
+ * NEUMANN / FREESLIP (the normal momentum negated) and NOSLIP (both momenta negated), which
+ * the reference declares but does not implement, mirror the interior across the boundary
+ * (again for grids narrower than the halo), a sign change per reflection. */
+static int mirror(int k, int n, int *flips)
+{
+    *flips = 0;
+    for (int it = 0; it < 64 && (k < 0 || k >= n); it++) {
+        k = k < 0 ? -1 - k : 2 * n - 1 - k;
+        (*flips)++;
+    }
+    return k < 0 ? 0 : (k >= n ? n - 1 : k);
+}
 static void fill_ghosts(ofv_ws *w, const double *U)
 {
     const int nx = w->nx, ny = w->ny;
@@ -984,14 +996,28 @@ static void fill_ghosts(ofv_ws *w, const double *U)
         for (int j = -GE; j < ny + GE; j++)
             for (int i = -GE; i < nx + GE; i++) {
                 int si, sj;
-                if (w->p->bc == OFV_BC_OUTFLOW) {
+                double sign = 1.0;
+                const int bc = w->p->bc;
+                if (bc == OFV_BC_OUTFLOW) {
                     si = i < 0 ? 0 : (i >= nx ? nx - 1 : i);
                     sj = j < 0 ? 0 : (j >= ny ? ny - 1 : j);
+                } else if (bc == OFV_BC_NEUMANN || bc == OFV_BC_NOSLIP || bc == OFV_BC_FREESLIP) {
+                    int fx, fy;
+                    si = mirror(i, nx, &fx);
+                    sj = mirror(j, ny, &fy);
+                    const int kind = w->p->eq.kind;
+                    const int mx = kind == OFV_EQ_EULER ? 1 : 2, my = mx + 1;
+                    int nflip = 0;
+                    if (kind != OFV_EQ_LINEAR_ADV) {
+                        if (v == mx) nflip = fx + (bc == OFV_BC_NOSLIP ? fy : 0);
+                        else if (v == my) nflip = fy + (bc == OFV_BC_NOSLIP ? fx : 0);
+                    }
+                    if (nflip & 1) sign = -1.0;
                 } else { /* a true modulo: grids narrower than the 3 ghost layers wrap more than once */
                     si = ((i % nx) + nx) % nx;
                     sj = ((j % ny) + ny) % ny;
                 }
-                *Ecell(w, v, i, j) = U[(size_t)v * nx * ny + (size_t)sj * nx + si];
+                *Ecell(w, v, i, j) = sign * U[(size_t)v * nx * ny + (size_t)sj * nx + si];
             }
 }
 

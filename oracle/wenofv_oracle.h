@@ -24,7 +24,7 @@ extern "C" {
 /* Equation kinds (same numbering as include/wenofv.h). */
 enum { OFV_EQ_TWO_PHASE = 0, OFV_EQ_LINEAR_ADV = 1, OFV_EQ_EULER = 2, OFV_EQ_TWO_PHASE_SG = 3 };
 /* Boundary kinds: PERIOD = 0 as include/Equations.hpp:27; OUTFLOW is an extension. */
-enum { OFV_BC_PERIOD = 0, OFV_BC_OUTFLOW = 5 };
+enum { OFV_BC_PERIOD = 0, OFV_BC_NEUMANN = 1, OFV_BC_NOSLIP = 2, OFV_BC_FREESLIP = 4, OFV_BC_OUTFLOW = 5 };
 
 typedef struct {
     int kind;

@@ -60,6 +60,19 @@ def child():
                 elif prec == wb.FP64_STRICT:
                     assert np.array_equal(U, V), (nx, ny, scheme, recon)
                 n_cases += 1
+    for nx, ny, bc in [(1, 1, 1), (3, 2, 2), (26, 9, 4), (25, 33, 1)]:  # walls, two-phase with gravity
+        U0, prm = cases.liquid_column(nx, ny, seed=nx + ny, ratio=2.0, eps=0.05)
+        for scheme in (1, 2):
+            p = Problem(nx=nx, ny=ny, bc=bc, scheme=scheme, flux=1, recon=1, limiter=1, gravity=9.81, **prm)
+            V, *_ = o.advance(p, U0, t_end=1e9, max_steps=2)
+            cfg = wb.make_config(nx, ny, bc=bc, scheme=scheme, flux=1, recon=1, limiter=1, precision=wb.FP64_STRICT)
+            eq = wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"], gravity=9.81)
+            with wb.Solver(cfg, eq) as s:
+                s.upload(U0)
+                s.advance(1e9, max_steps=2)
+                assert s.status()[0] == 0, (nx, ny, bc, scheme)
+                assert np.array_equal(s.download(), V), (nx, ny, bc, scheme)
+            n_cases += 1
     for nx, ny, scheme in [(5, 3, 1), (40, 9, 1), (5, 3, 2), (40, 9, 2)]:  # Euler, outflow
         U0, _ = cases.euler_quadrants(nx, ny, seed=3)
         cfg = wb.make_config(nx, ny, bc=wb.BC_OUTFLOW, cfl=0.4, scheme=scheme, flux=1, recon=1, precision=wb.FP64_STRICT)

@@ -20,7 +20,8 @@ import numpy as np
 import pytest
 
 from conftest import golden_cases, load_golden
-from oracle import BC_OUTFLOW, EQ_EULER, EQ_LINEAR_ADV, Problem, reference_available, run_reference
+from oracle import (BC_FREESLIP, BC_NEUMANN, BC_NOSLIP, BC_OUTFLOW, EQ_EULER, EQ_LINEAR_ADV, EQ_TWO_PHASE_SG, Problem,
+                    reference_available, run_reference)
 import cases
 
 pytestmark = pytest.mark.gpu
@@ -346,6 +347,37 @@ def test_euler_outflow_strict(wb, oracle_lib, recon, flux, scheme):
         t2, n2 = s.advance(0.01)
         assert n2 == n and t2 == t
         assert np.array_equal(s.download(), V)
+
+
+@pytest.mark.parametrize("bc", [BC_NEUMANN, BC_NOSLIP, BC_FREESLIP])
+@pytest.mark.parametrize("nx,ny", [(3, 2), (8, 8), (27, 5), (53, 70)])
+def test_walls_strict(wb, oracle_lib, bc, nx, ny):
+    # mirror ghost cells with momentum signs (several reflections on grids narrower than the
+    # halo): two-phase with gravity (WENO-Z and WENOEXP), Euler, scalar advection and the
+    # stiffened gas
+    mild = dict(ratio=2.0, eps=0.05) if min(nx, ny) < 8 else {}
+    U0, prm = cases.liquid_column(nx, ny, seed=nx * 10 + ny, **mild)
+    E0, _ = cases.euler_quadrants(nx, ny, seed=4)
+    runs = [(Problem(nx=nx, ny=ny, bc=bc, scheme=1, flux=1, recon=1, limiter=1, gravity=9.81, **prm), U0),
+            (Problem(nx=nx, ny=ny, bc=bc, scheme=2, flux=0, recon=0, limiter=1, **prm), U0),
+            (Problem(nx=nx, ny=ny, bc=bc, eq_kind=EQ_EULER, scheme=1, flux=1, recon=1, cfl=0.4), E0),
+            (Problem(nx=nx, ny=ny, bc=bc, eq_kind=EQ_LINEAR_ADV, scheme=0, flux=0, recon=0), cases.advection_sine(nx, ny))]
+    for p, X0 in runs:
+        with oracle_lib.cube_rounded():
+            V, *_ = oracle_lib.advance(p, X0, t_end=1e9, max_steps=3)
+        with solver_for(wb, p, wb.FP64_STRICT) as s:
+            s.upload(X0)
+            s.advance(1e9, max_steps=3)
+            assert np.array_equal(s.download(), V), (p.eq_kind, p.scheme)
+    S0, sprm = cases.sg_column(nx, ny, seed=nx + ny, **mild)
+    p = Problem(nx=nx, ny=ny, bc=bc, eq_kind=EQ_TWO_PHASE_SG, scheme=1, flux=1, recon=1, limiter=1, **sprm)
+    V, *_ = oracle_lib.advance(p, S0, t_end=1e9, max_steps=3)
+    cfg = wb.make_config(nx, ny, bc=bc, scheme=1, flux=1, recon=1, limiter=1, precision=wb.FP64_STRICT)
+    eq = wb.make_eq(kind=wb.EQ_TWO_PHASE_SG, **{k: sprm[k] for k in ("rho10", "rho20", "preb", "gamma1", "pinf1", "gamma2", "pinf2")})
+    with wb.Solver(cfg, eq) as s:
+        s.upload(S0)
+        s.advance(1e9, max_steps=3)
+        assert np.abs(s.download() - V).max() <= 1e-12 * np.abs(V).max()
 
 
 @pytest.mark.parametrize("nx", [64, 130])

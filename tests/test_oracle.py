@@ -8,7 +8,8 @@ import numpy as np
 import pytest
 
 from conftest import golden_cases, load_golden
-from oracle import EQ_EULER, EQ_LINEAR_ADV, EQ_TWO_PHASE_SG, BC_OUTFLOW, Oracle, Problem, reference_available, run_reference
+from oracle import (EQ_EULER, EQ_LINEAR_ADV, EQ_TWO_PHASE_SG, BC_FREESLIP, BC_NEUMANN, BC_NOSLIP, BC_OUTFLOW, Oracle,
+                    Problem, reference_available, run_reference)
 import cases
 
 GOLD = golden_cases()
@@ -283,3 +284,35 @@ def test_sg_eigenvectors_are_inverse(oracle_lib):
         for normal in ((1.0, 0.0), (0.0, 1.0)):
             L, R = oracle_lib.eigen(p, U[k], *normal)
             assert np.abs(R @ L - np.eye(4)).max() <= 1e-6
+
+
+# ---- wall boundaries (declared by the reference, not implemented there) ----------------------
+@pytest.mark.parametrize("bc", [BC_NEUMANN, BC_NOSLIP, BC_FREESLIP])
+def test_walls_conserve_mass_and_energy(oracle_lib, bc):
+    # mirror ghost cells: no mass (or Euler energy) crosses a wall, up to the rounding of the
+    # left- and right-biased reconstructions at the wall face
+    U0, prm = cases.liquid_column(40, 36, seed=5)
+    p = Problem(nx=40, ny=36, bc=bc, scheme=1, flux=1, recon=1, limiter=1, gravity=9.81, **prm)
+    U, n, _, _ = oracle_lib.advance(p, U0, t_end=1e9, max_steps=12)
+    assert np.isfinite(U).all() and (U[0] > 0).all() and (U[1] > 0).all()
+    for v in (0, 1):
+        assert abs(U[v].sum() - U0[v].sum()) <= 1e-12 * U0[v].sum()
+    E0, _ = cases.euler_quadrants(32, 32, seed=4)
+    pe = Problem(nx=32, ny=32, bc=bc, eq_kind=EQ_EULER, scheme=1, flux=1, recon=0, cfl=0.4)
+    E, *_ = oracle_lib.advance(pe, E0, t_end=1e9, max_steps=12)
+    for v in (0, 3):
+        assert abs(E[v].sum() - E0[v].sum()) <= 1e-12 * E0[v].sum()
+
+
+def test_wall_mirror_symmetry(oracle_lib):
+    # a state symmetric about x = 1/2 (x-momentum antisymmetric) stays so between walls
+    U0, prm = cases.liquid_column(32, 24, seed=2, amp=0.0)
+    rng = np.random.default_rng(3)
+    bump = rng.uniform(-1, 1, (24, 16))
+    vel = np.concatenate([bump, -bump[:, ::-1]], axis=1) * 1e-2
+    U0[2] = (U0[0] + U0[1]) * vel
+    U0[3] = 0.0
+    p = Problem(nx=32, ny=24, bc=BC_NEUMANN, scheme=1, flux=1, recon=0, limiter=1, **prm)
+    U, *_ = oracle_lib.advance(p, U0, t_end=1e9, max_steps=10)
+    assert np.allclose(U[0], U[0][:, ::-1], rtol=1e-10, atol=0)
+    assert np.abs(U[2] + U[2][:, ::-1]).max() <= 1e-9 * np.abs(U[2]).max()

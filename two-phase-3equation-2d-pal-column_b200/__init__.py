@@ -20,7 +20,7 @@ LIB_PATH = os.environ.get("WENOFV_LIB") or os.path.join(HERE, "lib", "libwenofv_
 
 OK, EINVAL, ENOMEM, ENUMERIC, ETIMEDOUT, ECUDA, ENOTSUP, EBUSY, ENOTFOUND = range(9)
 EQ_TWO_PHASE, EQ_LINEAR_ADV, EQ_EULER, EQ_TWO_PHASE_SG = 0, 1, 2, 3
-BC_PERIOD, BC_OUTFLOW = 0, 5
+BC_PERIOD, BC_NEUMANN, BC_NOSLIP, BC_NEUMANN2, BC_FREESLIP, BC_OUTFLOW = 0, 1, 2, 3, 4, 5
 FP64, FP64_STRICT, FP32_BULK = 0, 1, 2
 LAYOUT_SOA, LAYOUT_REF_AOS = 0, 1
 FLAG_NAN_DT, FLAG_BAD_THETA, FLAG_NAN_FLUX, FLAG_NAN_STATE, FLAG_BOUNDS = 1, 2, 4, 8, 16

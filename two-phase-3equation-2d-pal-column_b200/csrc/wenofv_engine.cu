@@ -72,7 +72,8 @@ int validate(const wenofv_config *c, const wenofv_eq_params *e)
     }
     if (c->riemann_flux < 0 || c->riemann_flux > 1) { set_error("RIEMANNFLUX must be 0 or 1"); return WENOFV_EINVAL; }
     if (c->pp_limiter < 0 || c->pp_limiter > 1) { set_error("PPlimiter must be 0 or 1"); return WENOFV_EINVAL; }
-    if (c->bc != WENOFV_BC_PERIOD && c->bc != WENOFV_BC_OUTFLOW) { set_error("boundary kind %d is not supported", c->bc); return WENOFV_ENOTSUP; }
+    if (c->bc == WENOFV_BC_NEUMANN2) { set_error("NEUMANN2 (boundary from the initial data) is not supported"); return WENOFV_ENOTSUP; }
+    if (c->bc < 0 || c->bc > 5) { set_error("boundary kind %d is not supported", c->bc); return WENOFV_ENOTSUP; }
     if (c->precision < 0 || c->precision > 2) { set_error("unknown precision %d", c->precision); return WENOFV_EINVAL; }
     if (c->ref_slabs < 0 || (c->ref_slabs > 0 && c->nx % c->ref_slabs != 0)) {
         set_error("ELEMNUMX (%d) must be divisible by the slab count (%d)", c->nx, c->ref_slabs);

@@ -88,11 +88,41 @@ template <class R, int SCH> struct ReconSel<R, SCH, 4> {
     using type = Prim3Recon;
 };
 
+// walls (NEUMANN 1, NOSLIP 2, FREESLIP 4): the mirror image across the boundary, reflected
+// again for grids narrower than the halo; flips counts the reflections (bounded: each one
+// lands at least one cell nearer to [0, n))
+__device__ __forceinline__ int mirror_index(int k, int n, int &flips)
+{
+    flips = 0;
+    for (int it = 0; it < 64 && (k < 0 || k >= n); it++) {
+        k = k < 0 ? -1 - k : 2 * n - 1 - k;
+        flips++;
+    }
+    return k < 0 ? 0 : (k >= n ? n - 1 : k);
+}
+__device__ __forceinline__ bool is_wall(int bc) { return bc == 1 || bc == 2 || bc == 4; }
+
 __device__ __forceinline__ int map_index(int k, int n, int bc)
 {
     if (bc == 5) return k < 0 ? 0 : (k >= n ? n - 1 : k); // outflow: zero-gradient copy
+    if (is_wall(bc)) {
+        int f;
+        return mirror_index(k, n, f);
+    }
     k %= n;
     return k < 0 ? k + n : k; // periodic wrap (2-D, corners included)
+}
+
+// the sign of variable v in a wall ghost cell reflected fx times in x and fy times in y:
+// the normal momentum changes sign at each reflection, the tangential one too for NOSLIP
+template <int EQ> __device__ __forceinline__ double wall_sign(int v, int fx, int fy, int bc)
+{
+    constexpr int MX = EQ == EQ_EULER ? 1 : 2, MY = MX + 1; // momentum components
+    if (EQ == EQ_LINEAR_ADV) return 1.0;
+    int n = 0;
+    if (v == MX) n = fx + (bc == 2 ? fy : 0);
+    else if (v == MY) n = fy + (bc == 2 ? fx : 0);
+    return (n & 1) ? -1.0 : 1.0;
 }
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
@@ -216,6 +246,9 @@ __device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ, H>::PS], co
     constexpr int P = StageGeom<EQ, H>::P, NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
     const int jj = map_index(row, D.ny, D.bc);
     const size_t plane = (size_t)D.ny * D.pitch;
+    const bool wall = is_wall(D.bc);
+    int fy = 0;
+    if (wall) mirror_index(row, D.ny, fy);
 #pragma unroll
     for (int e = threadIdx.x; e < NV * P; e += NT) {
         const int v = e / P, p = e - v * P;
@@ -228,6 +261,14 @@ __device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ, H>::PS], co
 #else
         (void)st;
 #endif
+        if (wall) {
+            int fx;
+            mirror_index(i0 - GH + p, D.nx, fx);
+            if (fx | fy) { // a wall ghost cell: a plain load with the momentum signs
+                dst[v][p] = wall_sign<EQ>(v, fx, fy, D.bc) * buf[v * plane + (size_t)jj * D.pitch + ii];
+                continue;
+            }
+        }
         cp_async8(&dst[v][p], buf + v * plane + (size_t)jj * D.pitch + ii);
     }
 }
