@@ -377,7 +377,8 @@ def test_walls_strict(wb, oracle_lib, bc, nx, ny):
     with wb.Solver(cfg, eq) as s:
         s.upload(S0)
         s.advance(1e9, max_steps=3)
-        assert np.abs(s.download() - V).max() <= 1e-12 * np.abs(V).max()
+        # pow differs by ulps between CUDA and the C library; coarse walled grids amplify it
+        assert np.abs(s.download() - V).max() <= 1e-11 * np.abs(V).max()
 
 
 @pytest.mark.parametrize("nx", [64, 130])
