@@ -7,10 +7,13 @@
 // sound speed, fluxes, eigenvectors) runs on the GPU inside libwenofv_b200; params()
 // hands the parameters to it as the C-ABI POD.
 //
-// setEquationParameters covers the periodic test cases the reference can run
-// (SMOOTH, VORTEX, SHARP: include/Equations.hpp:490-689).  The others need the
-// reference's unimplemented non-periodic boundary conditions and a gravity source; they
-// throw std::invalid_argument, like an unknown case does in the reference (:975).
+// setEquationParameters covers the periodic test cases the reference can run (SMOOTH,
+// VORTEX, SHARP: include/Equations.hpp:490-689) and the wall cases it declares but cannot
+// run, because it stops on their boundary kind (src/WENOFV.cpp:2286-2292): DAMBREAK,
+// DAMBREAK2, DAMBREAK3, RTI and STANDING_WAVE (include/Equations.hpp:747-973), with the
+// library's NEUMANN walls and the gravity of assembleSourceTerm (src/WENOFV.cpp:1831-1872).
+// ZALESAK needs NEUMANN2 (boundary from the initial data), which the library does not
+// provide; it throws std::invalid_argument, like an unknown case does in the reference (:975).
 #pragma once
 #include <cmath>
 #include <stdexcept>
@@ -50,14 +53,16 @@ public:
     double g_sound1 = 1.0, g_sound2 = 1.0;
     double g_u0 = 1.0, g_v0 = 1.0, g_preb = 0.0;
     double g_epsa = 1e-8;
+    double g_g0 = 0.0; // assembleSourceTerm's gravity of the case
 
     int getVarNum() const { return 4; }
 
-    // the parameter sets of the periodic cases (include/Equations.hpp:490-689)
+    // the parameter sets of the test cases (include/Equations.hpp:490-973)
     void setEquationParameters(TESTCASETYPE type)
     {
         testcase = type;
         boundaryCondition = PERIOD;
+        g_g0 = 0.0;
         switch (type) {
         case SMOOTH:
             set_box(0.0, 1.0, 0.0, 1.0);
@@ -74,9 +79,39 @@ public:
             outputTimes = {0, 1.0};
             set_phase(1000.0, 1.0, 70.0, 70.0, 1.0, 1.0, 1e-8);
             break;
+        case STANDING_WAVE: // (:747-789)
+            set_box(0.0, 0.5, 0.0, 0.5);
+            outputTimes = {3.0};
+            set_phase(1000.0, 1.0, 100.0, 100.0, 0.0, 0.0, 1e-6, 1e4);
+            walls(2 * M_PI);
+            break;
+        case RTI: // (:791-829)
+            set_box(0.0, 1.0, 0.0, 4.0);
+            outputTimes = {0.0, 0.1, 0.2, 0.3, 0.4, 0.5, 0.6, 0.7, 0.8, 0.9, 1.0};
+            set_phase(1.225, 0.1694, 100.0, 100.0, 0.0, 0.0, 1.0e-8, 10000.0);
+            walls(9.81);
+            break;
+        case DAMBREAK: // (:831-877)
+            set_box(0.0, 1.61, 0.0, 0.805);
+            outputTimes = {0.0, 0.1599, 0.2766, 0.3733, 0.4499, 0.5733, 0.8623, 1.0233, 1.1666};
+            set_phase(1000.0, 1.0, 100.0, 100.0, 0.0, 0.0, 1e-6, 1e4);
+            walls(9.81);
+            break;
+        case DAMBREAK2: // (:879-925)
+            set_box(0.0, 1.61, 0.0, 0.6);
+            outputTimes = {1.5};
+            set_phase(1000.0, 1.0, 100.0, 100.0, 0.0, 0.0, 1e-5, 1e4);
+            walls(9.81);
+            break;
+        case DAMBREAK3: // (:927-973)
+            set_box(0.0, 0.8, 0.0, 0.6);
+            outputTimes = {1.5};
+            set_phase(1000.0, 1.0, 100.0, 100.0, 0.0, 0.0, 1e-5, 1e4);
+            walls(9.81);
+            break;
         default:
             throw std::invalid_argument(std::string("test case ") + TESTCASETYPE_STRINGS[type] +
-                                        " needs non-periodic boundaries and gravity, which the CUDA backend does not provide");
+                                        " needs the NEUMANN2 boundary (from the initial data), which the CUDA backend does not provide");
         }
     }
 
@@ -97,13 +132,30 @@ public:
             const double xc = (xL + xR) / 2.0, yc = (yL + yR) / 2.0;
             return (std::fabs(x - xc) < r && std::fabs(y - yc) < r) ? 1 - g_epsa : g_epsa;
         }
+        case STANDING_WAVE: { // liquid below y = 0.25 + 0.025 cos(2 pi x) (:764-773)
+            const double hs = 0.25, A = 0.025, kn = 2 * M_PI;
+            return (y <= hs + A * std::cos(kn * x)) ? 1.0 - g_epsa : g_epsa;
+        }
+        case RTI: { // the heavy phase above y = 2 + 0.05 cos(2 pi x) (:814-820)
+            const double yi = 2.0 + 0.05 * std::cos(2.0 * M_PI * x);
+            return (y >= yi) ? 1.0 - g_epsa : g_epsa;
+        }
+        case DAMBREAK:  // a water block of L0 x H0 at the right (:855-861)
+        case DAMBREAK2: // (:903-909)
+        case DAMBREAK3: { // at the left (:951-957)
+            const double H0 = testcase == DAMBREAK ? 0.3 : (testcase == DAMBREAK2 ? 0.6 : 0.4);
+            const double L0 = testcase == DAMBREAK3 ? 0.2 : 0.6;
+            if (testcase == DAMBREAK3)
+                return (x >= xL && x <= xL + L0 && y >= yL && y <= yL + H0) ? 1.0 - g_epsa : g_epsa;
+            return (x >= xR - L0 && x <= xR && y >= yL && y <= yL + H0) ? 1.0 - g_epsa : g_epsa;
+        }
         default:
             return g_epsa;
         }
     }
 
     // getU0 (include/Equations.hpp:979-1002): partial densities from the phase pressures
-    // (uniform g_preb in every periodic case) and momenta from the uniform velocity
+    // (uniform g_preb in every case built here) and momenta from the uniform velocity
     void getU0(double xP, double yP, double *U) const
     {
         const double z_1 = z1_0(xP, yP);
@@ -142,15 +194,21 @@ public:
         p.sound2 = g_sound2;
         p.preb = g_preb;
         p.gamma = 1.4;
+        p.gravity = g_g0;
         return p;
     }
 
 private:
     void set_box(double xl, double xr, double yl, double yr) { xL = xl; xR = xr; yL = yl; yR = yr; }
-    void set_phase(double rho10, double rho20, double c1, double c2, double u0, double v0, double epsa)
+    void set_phase(double rho10, double rho20, double c1, double c2, double u0, double v0, double epsa, double preb = 0.0)
     {
         g_rho10 = rho10; g_rho20 = rho20; g_sound1 = c1; g_sound2 = c2;
-        g_u0 = u0; g_v0 = v0; g_preb = 0.0; g_epsa = epsa;
+        g_u0 = u0; g_v0 = v0; g_preb = preb; g_epsa = epsa;
+    }
+    void walls(double g)
+    {
+        boundaryCondition = NEUMANN;
+        g_g0 = g;
     }
     static double wrap(double v, double lo, double hi)
     {

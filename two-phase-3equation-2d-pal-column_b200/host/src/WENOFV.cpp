@@ -129,7 +129,7 @@ wenofv_config CWENOFV::config() const
     c.xr = equation->xR;
     c.yl = equation->yL;
     c.yr = equation->yR;
-    c.bc = WENOFV_BC_PERIOD;
+    c.bc = (int)equation->boundaryCondition; // BOUNDARYTYPE and WENOFV_BC_* share their numbers
     c.rk_method = (int)m_rkMeth;
     c.cfl = m_cfl;
     c.scheme = (int)m_scheme;
