@@ -238,39 +238,65 @@ template <int EQ, int H> struct StageSmem {
     int s_last;
 };
 
+// periodic wrap or outflow clamp (the ghost fill of the non-wall kinds)
+__device__ __forceinline__ int map_index_po(int k, int n, int bc)
+{
+    if (bc == 5) return k < 0 ? 0 : (k >= n ? n - 1 : k);
+    k %= n;
+    return k < 0 ? k + n : k;
+}
+
+// the wall form of load_row: ghost cells are plain loads with the momentum signs (kept out
+// of line, so that the periodic and outflow loads keep their own register allocation)
+template <int EQ, int H>
+__device__ __noinline__ void load_row_walls(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
+                                            int i0, InstState *st)
+{
+    constexpr int P = StageGeom<EQ, H>::P, NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
+    const size_t plane = (size_t)D.ny * D.pitch;
+    (void)st;
+    int fy;
+    const int jj = mirror_index(row, D.ny, fy);
+    for (int e = threadIdx.x; e < NV * P; e += NT) {
+        const int v = e / P, p = e - v * P;
+        int fx;
+        const int ii = mirror_index(i0 - GH + p, D.nx, fx);
+#if WENOFV_CHECK_BOUNDS
+        if (jj < 0 || jj >= D.ny || ii < 0 || ii >= D.nx) {
+            flag_error(st, 16u /* WENOFV_FLAG_BOUNDS */, (long long)row * D.nx + (i0 - GH + p));
+            continue;
+        }
+#endif
+        if (fx | fy) dst[v][p] = wall_sign<EQ>(v, fx, fy, D.bc) * buf[v * plane + (size_t)jj * D.pitch + ii];
+        else cp_async8(&dst[v][p], buf + v * plane + (size_t)jj * D.pitch + ii);
+    }
+}
+
 // one row of NV x P stage values into shared memory (ghost fill = index map), cp.async 8 B
 template <int EQ, int H>
 __device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
                                          int i0, InstState *st)
 {
     constexpr int P = StageGeom<EQ, H>::P, NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
-    const int jj = map_index(row, D.ny, D.bc);
     const size_t plane = (size_t)D.ny * D.pitch;
-    const bool wall = is_wall(D.bc);
-    int fy = 0;
-    if (wall) mirror_index(row, D.ny, fy);
+    (void)st;
+    if (!is_wall(D.bc)) {
+        const int jj = map_index_po(row, D.ny, D.bc);
 #pragma unroll
-    for (int e = threadIdx.x; e < NV * P; e += NT) {
-        const int v = e / P, p = e - v * P;
-        const int ii = map_index(i0 - GH + p, D.nx, D.bc);
+        for (int e = threadIdx.x; e < NV * P; e += NT) {
+            const int v = e / P, p = e - v * P;
+            const int ii = map_index_po(i0 - GH + p, D.nx, D.bc);
 #if WENOFV_CHECK_BOUNDS
-        if (jj < 0 || jj >= D.ny || ii < 0 || ii >= D.nx) { // record and skip the access
-            flag_error(st, 16u /* WENOFV_FLAG_BOUNDS */, (long long)row * D.nx + (i0 - GH + p));
-            continue;
-        }
-#else
-        (void)st;
-#endif
-        if (wall) {
-            int fx;
-            mirror_index(i0 - GH + p, D.nx, fx);
-            if (fx | fy) { // a wall ghost cell: a plain load with the momentum signs
-                dst[v][p] = wall_sign<EQ>(v, fx, fy, D.bc) * buf[v * plane + (size_t)jj * D.pitch + ii];
+            if (jj < 0 || jj >= D.ny || ii < 0 || ii >= D.nx) { // record and skip the access
+                flag_error(st, 16u /* WENOFV_FLAG_BOUNDS */, (long long)row * D.nx + (i0 - GH + p));
                 continue;
             }
+#endif
+            cp_async8(&dst[v][p], buf + v * plane + (size_t)jj * D.pitch + ii);
         }
-        cp_async8(&dst[v][p], buf + v * plane + (size_t)jj * D.pitch + ii);
+        return;
     }
+    load_row_walls<EQ, H>(dst, buf, D, row, i0, st);
 }
 
 // value of a reconstruction: in the deviation form the anchor plus the FP32 deviation, in
