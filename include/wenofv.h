@@ -47,8 +47,11 @@ enum { WENOFV_EQ_TWO_PHASE = 0, WENOFV_EQ_LINEAR_ADV = 1, WENOFV_EQ_EULER = 2, W
  * NEUMANN ("reflective, slip") and FREESLIP: mirror ghost cells with the normal momentum
  * negated; NOSLIP: mirror ghost cells with both momenta negated.  The reference declares the
  * wall kinds but does not implement them (src/WENOFV.cpp:2254-2292), so their ghost rule is
- * this library's; NEUMANN2 (boundary from the initial data) is not supported.  OUTFLOW
- * (zero-gradient) has no counterpart in the reference. */
+ * this library's.  NEUMANN2 ("boundary from the initial data", also declared and not
+ * implemented) takes every ghost cell from a fixed frame of averages that the caller sets
+ * with wenofv_set_frame / wenofv_batch_set_frame before the first step; the serving API and
+ * wenofv_step_noalloc reject it.  OUTFLOW (zero-gradient) has no counterpart in the
+ * reference. */
 enum {
     WENOFV_BC_PERIOD = 0,
     WENOFV_BC_NEUMANN = 1,
@@ -140,6 +143,12 @@ void wenofv_destroy(wenofv_ctx *ctx);
 int wenofv_upload(wenofv_ctx *ctx, const double *U, int layout);
 /* reads the interior cell averages (what getWorldUh gathers, src/WENOFV.cpp:2059-2117) */
 int wenofv_download(wenofv_ctx *ctx, double *U, int layout);
+/* NEUMANN2 only: the fixed ghost averages, host SoA [v][ny+8][nx+8] with cell (i, j) at
+ * [v][j+4][i+4]; the entries of the interior are not read.  Copied synchronously, held for
+ * every later stage.  Replaces the ghost fill of BOUNDARYTYPE NEUMANN2, which the reference
+ * declares (include/Equations.hpp:30, set for ZALESAK at :696) but whose branch of
+ * setBoundaryAverages2 (src/WENOFV.cpp:2254-2292) it never wrote. */
+int wenofv_set_frame(wenofv_ctx *ctx, const double *frame);
 
 /* CWENOFV::calculateDeltaT (src/WENOFV.cpp:474-540): min over cells of
  * CFL / (lambda_x/dx + lambda_y/dy), starting from 1.0; WENOFV_ENUMERIC on a NaN */
@@ -204,6 +213,8 @@ int wenofv_batch_create(int n, const wenofv_config *cfgs, const wenofv_eq_params
 void wenofv_batch_destroy(wenofv_batch *b);
 int wenofv_batch_upload(wenofv_batch *b, int i, const double *U, int layout);
 int wenofv_batch_download(wenofv_batch *b, int i, double *U, int layout);
+/* wenofv_set_frame for instance i of a batch */
+int wenofv_batch_set_frame(wenofv_batch *b, int i, const double *frame);
 /* advances instance k from t=0 to t_end[k]; nsteps[k] receives its step count */
 int wenofv_batch_advance(wenofv_batch *b, const double *t_end, int64_t max_steps, int64_t *nsteps);
 /* rows per work item and CTAs per SM of the persistent stage kernel (0 = automatic) */

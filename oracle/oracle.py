@@ -40,7 +40,8 @@ class _Problem(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("xl", C.c_double), ("xr", C.c_double),
                 ("yl", C.c_double), ("yr", C.c_double), ("bc", C.c_int), ("rk", C.c_int),
                 ("cfl", C.c_double), ("scheme", C.c_int), ("limiter", C.c_int), ("flux", C.c_int),
-                ("recon", C.c_int), ("ref_slabs", C.c_int), ("threads", C.c_int), ("eq", _Eq)]
+                ("recon", C.c_int), ("ref_slabs", C.c_int), ("threads", C.c_int), ("eq", _Eq),
+                ("frame", C.c_void_p)]
 
 
 @dataclass
@@ -76,6 +77,8 @@ class Problem:
     gamma2: float = 1.4
     pinf2: float = 0.0
     gravity: float = 0.0     # assembleSourceTerm's g_g0 (two-phase kinds)
+    # NEUMANN2: fixed ghost averages [nvar][ny+8][nx+8], interior at offset (4, 4)
+    frame: np.ndarray | None = None
 
     @property
     def nvar(self) -> int:
@@ -84,9 +87,18 @@ class Problem:
     def to_c(self) -> _Problem:
         e = _Eq(self.eq_kind, self.rho10, self.rho20, self.sound1, self.sound2, self.preb,
                 self.gamma, self.adv_u, self.adv_v, self.gamma1, self.pinf1, self.gamma2, self.pinf2, self.gravity)
+        fp = None
+        if self.bc == BC_NEUMANN2:
+            if self.frame is None:
+                raise ValueError("NEUMANN2 needs a frame of ghost averages")
+            fr = np.ascontiguousarray(self.frame, dtype=np.float64)
+            if fr.shape != (self.nvar, self.ny + 8, self.nx + 8):
+                raise ValueError(f"frame shape {fr.shape} != {(self.nvar, self.ny + 8, self.nx + 8)}")
+            self._frame_keep = fr  # the C struct holds a raw pointer into it
+            fp = fr.ctypes.data
         return _Problem(self.nx, self.ny, self.xl, self.xr, self.yl, self.yr, self.bc, self.rk,
                         self.cfl, self.scheme, self.limiter, self.flux, self.recon, self.ref_slabs,
-                        self.threads, e)
+                        self.threads, e, fp)
 
 
 _DP = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")

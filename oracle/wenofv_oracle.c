@@ -979,7 +979,9 @@ static void ws_free(ofv_ws *w)
  * OUTFLOW (extension) is a zero-gradient copy of the nearest interior cell.  The walls
  * NEUMANN / FREESLIP (the normal momentum negated) and NOSLIP (both momenta negated), which
  * the reference declares but does not implement, mirror the interior across the boundary
- * (again for grids narrower than the halo), a sign change per reflection. */
+ * (again for grids narrower than the halo), a sign change per reflection.  NEUMANN2, also
+ * declared and not implemented there, reads each ghost cell from a fixed frame of averages
+ * (the initial data around the domain), the same for every stage. */
 static int mirror(int k, int n, int *flips)
 {
     *flips = 0;
@@ -1013,6 +1015,14 @@ static void fill_ghosts(ofv_ws *w, const double *U)
                         else if (v == my) nflip = fy + (bc == OFV_BC_NOSLIP ? fx : 0);
                     }
                     if (nflip & 1) sign = -1.0;
+                } else if (bc == OFV_BC_NEUMANN2) {
+                    if (i < 0 || i >= nx || j < 0 || j >= ny) {
+                        const size_t fw = (size_t)nx + 8, fplane = fw * ((size_t)ny + 8);
+                        *Ecell(w, v, i, j) = w->p->frame[v * fplane + (size_t)(j + 4) * fw + (size_t)(i + 4)];
+                        continue;
+                    }
+                    si = i;
+                    sj = j;
                 } else { /* a true modulo: grids narrower than the 3 ghost layers wrap more than once */
                     si = ((i % nx) + nx) % nx;
                     sj = ((j % ny) + ny) % ny;

@@ -24,7 +24,7 @@ extern "C" {
 /* Equation kinds (same numbering as include/wenofv.h). */
 enum { OFV_EQ_TWO_PHASE = 0, OFV_EQ_LINEAR_ADV = 1, OFV_EQ_EULER = 2, OFV_EQ_TWO_PHASE_SG = 3 };
 /* Boundary kinds: PERIOD = 0 as include/Equations.hpp:27; OUTFLOW is an extension. */
-enum { OFV_BC_PERIOD = 0, OFV_BC_NEUMANN = 1, OFV_BC_NOSLIP = 2, OFV_BC_FREESLIP = 4, OFV_BC_OUTFLOW = 5 };
+enum { OFV_BC_PERIOD = 0, OFV_BC_NEUMANN = 1, OFV_BC_NOSLIP = 2, OFV_BC_NEUMANN2 = 3, OFV_BC_FREESLIP = 4, OFV_BC_OUTFLOW = 5 };
 
 typedef struct {
     int kind;
@@ -56,6 +56,10 @@ typedef struct {
     int ref_slabs;         /* 0: uniform cell sizes; P>0: the reference's P-slab x metric */
     int threads;           /* OpenMP threads (0 = library default) */
     ofv_eq eq;
+    /* NEUMANN2 (BOUNDARYTYPE 3, "boundary from the initial data", include/Equations.hpp:30):
+     * fixed ghost averages, SoA [v][ny+8][nx+8] with the interior at offset (4, 4); the
+     * interior entries are not read.  Unused by the other kinds. */
+    const double *frame;
 } ofv_problem;
 
 int ofv_nvar(const ofv_eq *eq);

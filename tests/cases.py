@@ -182,3 +182,12 @@ def ensemble(n, seed=4, grids=None):
         U0, prm = liquid_column(nx, ny, seed=1000 + k, ratio=ratio, radius=r, eps=eps)
         out.append((U0, dict(prm, nx=nx, ny=ny, scheme=scheme, radius=r, ratio=ratio, eps=eps)))
     return out
+
+
+def periodic_frame(U):
+    """NEUMANN2 ghost frame [nv][ny+8][nx+8] holding the periodic wrap of U, cell (i, j) at
+    [v][j+4][i+4] (the interior entries are U itself; the solvers do not read them)."""
+    nv, ny, nx = U.shape
+    jj = np.arange(-4, ny + 4) % ny
+    ii = np.arange(-4, nx + 4) % nx
+    return np.ascontiguousarray(U[:, jj][:, :, ii])

@@ -45,7 +45,7 @@ def test_default_config_is_shipped_settings(wb):
 
 @pytest.mark.parametrize("field,value,code", [
     ("nx", 0, 1), ("rk_method", 3, 1), ("cfl", 0.0, 1), ("scheme", 3, 1), ("reconstruction", 5, 6), ("reconstruction", 6, 1),
-    ("riemann_flux", 4, 1), ("bc", 3, 6), ("bc", 7, 6), ("precision", 9, 1), ("ref_slabs", 3, 1),
+    ("riemann_flux", 4, 1), ("bc", -1, 6), ("bc", 7, 6), ("precision", 9, 1), ("ref_slabs", 3, 1),
 ])
 def test_invalid_options_rejected(wb, field, value, code):
     L = wb.load()

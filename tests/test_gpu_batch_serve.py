@@ -155,6 +155,11 @@ def test_server_rejects_and_isolates_failures(wb):
         srv.submit(cfg, eq, U0, 0.01)  # over the budget
     assert e.value.code == wb.ENOMEM
     U1, prm = cases.liquid_column(16, 16, seed=2)
+    c0, e0 = column_cfg(wb, 16, 16, prm, wb.FP64)
+    c0.bc = wb.BC_NEUMANN2
+    with pytest.raises(wb.WenofvError) as e:
+        srv.submit(c0, e0, U1, 0.01)  # a request carries no ghost frame
+    assert e.value.code == wb.ENOTSUP
     c1, e1 = column_cfg(wb, 16, 16, prm, wb.FP64)
     U1[1, 3, 3] = np.nan  # a failing request does not disturb the others
     bad = srv.submit(c1, e1, U1, 1e9, max_steps=3)

@@ -4,7 +4,7 @@ compute-sanitizer is not available, so the library is also built with every glob
 the stage kernel checked against its buffer before the access: a violation sets
 WENOFV_FLAG_BOUNDS (and the call returns WENOFV_ENUMERIC) instead of touching the memory.
 A child process loads that build and runs tiny and ragged grids through every
-reconstruction, both boundary kinds, the three arithmetic forms and a batch. No flag may be
+reconstruction, the boundary kinds (NEUMANN2's frame included), the three arithmetic forms and a batch. No flag may be
 raised, and FP64_STRICT must still equal the oracle bit for bit.
 """
 from __future__ import annotations
@@ -25,7 +25,7 @@ def child():
     sys.path.insert(0, HERE)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from conftest import import_package
-    from oracle import BC_OUTFLOW, EQ_EULER, Oracle, Problem
+    from oracle import BC_NEUMANN2, BC_OUTFLOW, EQ_EULER, Oracle, Problem
     import cases
 
     wb = import_package()
@@ -73,6 +73,21 @@ def child():
                 assert s.status()[0] == 0, (nx, ny, bc, scheme)
                 assert np.array_equal(s.download(), V), (nx, ny, bc, scheme)
             n_cases += 1
+    for nx, ny, scheme in [(1, 1, 1), (3, 2, 2), (26, 9, 1), (25, 33, 2)]:  # NEUMANN2 ghost frame
+        U0, prm = cases.liquid_column(nx, ny, seed=nx + ny, ratio=2.0, eps=0.05)
+        F0, _ = cases.liquid_column(nx, ny, seed=nx + ny + 1, ratio=2.0, eps=0.05)
+        p = Problem(nx=nx, ny=ny, bc=BC_NEUMANN2, frame=cases.periodic_frame(F0), scheme=scheme, flux=1, recon=1,
+                    limiter=1, **prm)
+        V, *_ = o.advance(p, U0, t_end=1e9, max_steps=2)
+        cfg = wb.make_config(nx, ny, bc=BC_NEUMANN2, scheme=scheme, flux=1, recon=1, limiter=1, precision=wb.FP64_STRICT)
+        eq = wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"])
+        with wb.Solver(cfg, eq) as s:
+            s.set_frame(p.frame)
+            s.upload(U0)
+            s.advance(1e9, max_steps=2)
+            assert s.status()[0] == 0, (nx, ny, scheme)
+            assert np.array_equal(s.download(), V), (nx, ny, scheme)
+        n_cases += 1
     for nx, ny, scheme in [(5, 3, 1), (40, 9, 1), (5, 3, 2), (40, 9, 2)]:  # Euler, outflow
         U0, _ = cases.euler_quadrants(nx, ny, seed=3)
         cfg = wb.make_config(nx, ny, bc=wb.BC_OUTFLOW, cfl=0.4, scheme=scheme, flux=1, recon=1, precision=wb.FP64_STRICT)

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from conftest import golden_cases, load_golden
-from oracle import (EQ_EULER, EQ_LINEAR_ADV, EQ_TWO_PHASE_SG, BC_FREESLIP, BC_NEUMANN, BC_NOSLIP, BC_OUTFLOW, Oracle,
+from oracle import (EQ_EULER, EQ_LINEAR_ADV, EQ_TWO_PHASE_SG, BC_FREESLIP, BC_NEUMANN, BC_NEUMANN2, BC_NOSLIP, BC_OUTFLOW, Oracle,
                     Problem, reference_available, run_reference)
 import cases
 
@@ -316,3 +316,41 @@ def test_wall_mirror_symmetry(oracle_lib):
     U, *_ = oracle_lib.advance(p, U0, t_end=1e9, max_steps=10)
     assert np.allclose(U[0], U[0][:, ::-1], rtol=1e-10, atol=0)
     assert np.abs(U[2] + U[2][:, ::-1]).max() <= 1e-9 * np.abs(U[2]).max()
+
+
+@pytest.mark.parametrize("scheme,recon", [(1, 1), (2, 0), (0, 3)])
+def test_neumann2_frame_of_periodic_wrap_is_periodic(oracle_lib, scheme, recon):
+    # NEUMANN2 reads its ghosts from a fixed frame.  With the frame set to the periodic wrap of
+    # the state, one forward-Euler stage (RKMETH 0, whose only stage sees that state) must equal
+    # the periodic solve bit for bit, on a grid narrower than the halo too
+    for nx, ny in [(20, 14), (3, 5)]:
+        mild = dict(ratio=2.0, eps=0.05) if min(nx, ny) < 8 else {}
+        U0, prm = cases.liquid_column(nx, ny, seed=nx + ny, **mild)
+        per = Problem(nx=nx, ny=ny, rk=0, scheme=scheme, flux=1, recon=recon, limiter=1, gravity=9.81, **prm)
+        fix = Problem(nx=nx, ny=ny, rk=0, scheme=scheme, flux=1, recon=recon, limiter=1, gravity=9.81, bc=BC_NEUMANN2,
+                      frame=cases.periodic_frame(U0), **prm)
+        assert np.array_equal(oracle_lib.rhs(fix, U0), oracle_lib.rhs(per, U0))
+        A, *_ = oracle_lib.advance(per, U0, t_end=1e9, max_steps=1)
+        B, *_ = oracle_lib.advance(fix, U0, t_end=1e9, max_steps=1)
+        assert np.array_equal(A, B)
+
+
+def test_neumann2_keeps_a_uniform_state(oracle_lib):
+    # a uniform moving state inside a frame of the same state is a steady solution
+    nx, ny = 24, 16
+    U0, prm = cases.liquid_column(nx, ny, seed=1)
+    c = U0[:, 0, 0].copy()
+    U = np.broadcast_to(c[:, None, None], U0.shape).copy()
+    p = Problem(nx=nx, ny=ny, bc=BC_NEUMANN2, frame=cases.periodic_frame(U), scheme=1, flux=1, recon=1, limiter=1, **prm)
+    V, n, *_ = oracle_lib.advance(p, U, t_end=1e9, max_steps=5)
+    assert n == 5
+    # up to rounding: the characteristic projection and the Gauss-point sums of a constant
+    # are exact only to a few ulps per stage
+    assert np.abs(V - U).max() <= 1e-10 * np.abs(U).max()
+
+
+def test_neumann2_needs_a_frame():
+    with pytest.raises(ValueError):
+        Problem(nx=8, ny=8, bc=BC_NEUMANN2).to_c()
+    with pytest.raises(ValueError):
+        Problem(nx=8, ny=8, bc=BC_NEUMANN2, frame=np.zeros((4, 8, 8))).to_c()

@@ -28,10 +28,10 @@ FLAG_NAN_DT, FLAG_BAD_THETA, FLAG_NAN_FLUX, FLAG_NAN_STATE, FLAG_BOUNDS = 1, 2, 
 # every entry point declared in include/wenofv.h
 EXPORTS = (
     "wenofv_abi_version", "wenofv_strerror", "wenofv_last_error", "wenofv_default_config",
-    "wenofv_create", "wenofv_destroy", "wenofv_upload", "wenofv_download", "wenofv_compute_dt",
+    "wenofv_create", "wenofv_destroy", "wenofv_upload", "wenofv_set_frame", "wenofv_download", "wenofv_compute_dt",
     "wenofv_step", "wenofv_rhs", "wenofv_advance", "wenofv_status", "wenofv_synchronize",
     "wenofv_stream", "wenofv_device_state", "wenofv_step_noalloc", "wenofv_init_testcase", "wenofv_accuracy",
-    "wenofv_batch_create", "wenofv_batch_destroy", "wenofv_batch_upload", "wenofv_batch_download",
+    "wenofv_batch_create", "wenofv_batch_destroy", "wenofv_batch_upload", "wenofv_batch_set_frame", "wenofv_batch_download",
     "wenofv_batch_advance", "wenofv_batch_set_tiling", "wenofv_batch_stream", "wenofv_batch_autotune",
     "wenofv_server_create", "wenofv_server_destroy", "wenofv_server_submit", "wenofv_server_poll",
     "wenofv_server_clock", "wenofv_server_stats",
@@ -99,6 +99,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.wenofv_destroy.argtypes = [P]
     L.wenofv_upload.argtypes = [P, DP, I]
     L.wenofv_download.argtypes = [P, DP, I]
+    L.wenofv_set_frame.argtypes = [P, DP]
+    L.wenofv_batch_set_frame.argtypes = [P, I, DP]
     L.wenofv_compute_dt.argtypes = [P, DP]
     L.wenofv_step.argtypes = [P, D]
     L.wenofv_rhs.argtypes = [P, DP, I]
@@ -194,6 +196,13 @@ class Solver:
         a = np.ascontiguousarray(U, dtype=np.float64)
         _check(self.L.wenofv_upload(self.h, _dp(a), layout), "wenofv_upload")
 
+    def set_frame(self, frame: np.ndarray):
+        """NEUMANN2 ghost averages, [nv][ny+8][nx+8] with cell (i, j) at [v][j+4][i+4]."""
+        a = np.ascontiguousarray(frame, dtype=np.float64)
+        if a.shape != (self.nv, self.cfg.ny + 8, self.cfg.nx + 8):
+            raise ValueError(f"frame shape {a.shape} != {(self.nv, self.cfg.ny + 8, self.cfg.nx + 8)}")
+        _check(self.L.wenofv_set_frame(self.h, _dp(a)), "wenofv_set_frame")
+
     def download(self, layout=LAYOUT_SOA) -> np.ndarray:
         out = np.empty(self.shape if layout == LAYOUT_SOA else (self.cfg.nx, self.cfg.ny, self.nv))
         _check(self.L.wenofv_download(self.h, _dp(out), layout), "wenofv_download")
@@ -283,6 +292,13 @@ class Batch:
     def upload(self, i, U):
         a = np.ascontiguousarray(U, dtype=np.float64)
         _check(self.L.wenofv_batch_upload(self.h, i, _dp(a), LAYOUT_SOA), "wenofv_batch_upload")
+
+    def set_frame(self, i, frame: np.ndarray):
+        nv, ny, nx = self.shape(i)
+        a = np.ascontiguousarray(frame, dtype=np.float64)
+        if a.shape != (nv, ny + 8, nx + 8):
+            raise ValueError(f"frame shape {a.shape} != {(nv, ny + 8, nx + 8)}")
+        _check(self.L.wenofv_batch_set_frame(self.h, i, _dp(a)), "wenofv_batch_set_frame")
 
     def download(self, i) -> np.ndarray:
         out = np.empty(self.shape(i))

@@ -92,6 +92,11 @@ int wenofv_upload(wenofv_ctx *ctx, const double *U, int layout)
     if (!ctx) { set_error("null context"); return WENOFV_EINVAL; }
     return ctx->eng.upload(0, U, layout);
 }
+int wenofv_set_frame(wenofv_ctx *ctx, const double *frame)
+{
+    if (!ctx) { set_error("null context"); return WENOFV_EINVAL; }
+    return ctx->eng.set_frame(0, frame);
+}
 int wenofv_download(wenofv_ctx *ctx, double *U, int layout)
 {
     if (!ctx) { set_error("null context"); return WENOFV_EINVAL; }
@@ -154,6 +159,11 @@ int wenofv_batch_upload(wenofv_batch *b, int i, const double *U, int layout)
 {
     if (!b) { set_error("null batch"); return WENOFV_EINVAL; }
     return b->eng.upload(i, U, layout);
+}
+int wenofv_batch_set_frame(wenofv_batch *b, int i, const double *frame)
+{
+    if (!b) { set_error("null batch"); return WENOFV_EINVAL; }
+    return b->eng.set_frame(i, frame);
 }
 int wenofv_batch_download(wenofv_batch *b, int i, double *U, int layout)
 {

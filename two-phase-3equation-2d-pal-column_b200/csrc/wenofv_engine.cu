@@ -72,7 +72,6 @@ int validate(const wenofv_config *c, const wenofv_eq_params *e)
     }
     if (c->riemann_flux < 0 || c->riemann_flux > 1) { set_error("RIEMANNFLUX must be 0 or 1"); return WENOFV_EINVAL; }
     if (c->pp_limiter < 0 || c->pp_limiter > 1) { set_error("PPlimiter must be 0 or 1"); return WENOFV_EINVAL; }
-    if (c->bc == WENOFV_BC_NEUMANN2) { set_error("NEUMANN2 (boundary from the initial data) is not supported"); return WENOFV_ENOTSUP; }
     if (c->bc < 0 || c->bc > 5) { set_error("boundary kind %d is not supported", c->bc); return WENOFV_ENOTSUP; }
     if (c->precision < 0 || c->precision > 2) { set_error("unknown precision %d", c->precision); return WENOFV_EINVAL; }
     if (c->ref_slabs < 0 || (c->ref_slabs > 0 && c->nx % c->ref_slabs != 0)) {
@@ -203,6 +202,8 @@ int Engine::init_slots(int capacity, int dev, int rk_method)
     desc_.assign(cap_, InstDesc{});
     dmem_.assign(cap_, nullptr);
     dmetric_.assign(cap_, nullptr);
+    dframe_.assign(cap_, nullptr);
+    frame_set_.assign(cap_, 0);
     live_.assign(cap_, 0);
     WENOFV_CUDA(cudaMalloc(&d_desc_, cap_ * sizeof(InstDesc)));
     WENOFV_CUDA(cudaMemset(d_desc_, 0, cap_ * sizeof(InstDesc)));
@@ -213,6 +214,36 @@ int Engine::init_slots(int capacity, int dev, int rk_method)
         h_state_[i].done = 1; // an empty slot is never stepped
     }
     return push_state();
+}
+
+// NEUMANN2's fixed ghost frame: every variable on the grid widened by 4 cells on each side
+// (the widest halo, WENOEXP's), SoA [v][ny+8][nx+8]; the interior entries are never read
+static size_t frame_bytes(const wenofv_config &c, const wenofv_eq_params &e)
+{
+    return (size_t)nvar_of(e.eq_kind) * ((size_t)c.ny + 8) * ((size_t)c.nx + 8) * sizeof(double);
+}
+
+int Engine::set_frame(int i, const double *frame)
+{
+    if (!live(i)) { set_error("instance %d is not live", i); return WENOFV_EINVAL; }
+    if (cfg_[i].bc != WENOFV_BC_NEUMANN2) { set_error("a ghost frame belongs to the NEUMANN2 boundary only"); return WENOFV_EINVAL; }
+    if (!frame) { set_error("null frame"); return WENOFV_EINVAL; }
+    WENOFV_CUDA(cudaSetDevice(device));
+    // synchronous: the caller may reuse its array on return, and later stages read the copy
+    WENOFV_CUDA(cudaMemcpyAsync(dframe_[i], frame, frame_bytes(cfg_[i], eq_[i]), cudaMemcpyHostToDevice, stream));
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    frame_set_[i] = 1;
+    return WENOFV_OK;
+}
+
+int Engine::check_frames() const
+{
+    for (int i = 0; i < n; i++)
+        if (live_[i] && cfg_[i].bc == WENOFV_BC_NEUMANN2 && !frame_set_[i]) {
+            set_error("instance %d has the NEUMANN2 boundary but no ghost frame (wenofv_set_frame)", i);
+            return WENOFV_EINVAL;
+        }
+    return WENOFV_OK;
 }
 
 int Engine::alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params &e)
@@ -241,6 +272,11 @@ int Engine::alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params
     d.dx4 = std::pow(d.dX, 4); // the reference's pow(m_deltaX, 4), include/Utility.hpp:313
     d.dY = (c.yr - c.yl) / c.ny;
     d.eq = eq_params_of(e);
+    frame_set_[i] = 0;
+    if (c.bc == WENOFV_BC_NEUMANN2) {
+        WENOFV_CUDA(cudaMalloc(&dframe_[i], frame_bytes(c, e)));
+        d.frame = dframe_[i];
+    }
     WENOFV_CUDA(cudaMemcpyAsync(d_desc_ + i, &d, sizeof(InstDesc), cudaMemcpyHostToDevice, stream));
     WENOFV_CUDA(cudaStreamSynchronize(stream)); // the metric staging above is a host local
     cfg_[i] = c;
@@ -256,8 +292,11 @@ void Engine::free_instance(int i)
     if (i < 0 || i >= cap_) return;
     if (dmem_[i]) cudaFree(dmem_[i]);
     if (dmetric_[i]) cudaFree(dmetric_[i]);
+    if (dframe_[i]) cudaFree(dframe_[i]);
     dmem_[i] = nullptr;
     dmetric_[i] = nullptr;
+    dframe_[i] = nullptr;
+    frame_set_[i] = 0;
     if (live_[i]) work_dirty_ = true;
     live_[i] = 0;
     if (h_state_) {
@@ -591,6 +630,7 @@ int Engine::compute_dt(double *dt_out)
 int Engine::step(double dt)
 {
     Range nvtx_range("wenofv::step");
+    if (const int fr = check_frames()) return fr;
     WENOFV_CUDA(cudaSetDevice(device));
     for (int i = 0; i < n; i++) {
         h_state_[i] = fresh_state(cur_);
@@ -609,6 +649,7 @@ int Engine::rhs(double *out, int layout)
 {
     Range nvtx_range("wenofv::rhs");
     if (n != 1) { set_error("rhs is defined for a single instance"); return WENOFV_EINVAL; }
+    if (const int fr = check_frames()) return fr;
     WENOFV_CUDA(cudaSetDevice(device));
     const InstDesc &d = desc_[0];
     const int nv = nvar_of(d.eq_kind);
@@ -682,6 +723,7 @@ int Engine::normalize_buffers()
 int Engine::advance(const double *t0, const double *t_end, int64_t max_steps, double *t_out, int64_t *nsteps)
 {
     Range nvtx_range("wenofv::advance");
+    if (const int fr = check_frames()) return fr;
     WENOFV_CUDA(cudaSetDevice(device));
     // every instance's state into buffer 0, where the captured step pairs start
     for (int i = 0; i < n; i++) h_state_[i].cur_buf = cur_;

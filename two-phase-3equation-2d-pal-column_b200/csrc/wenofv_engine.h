@@ -53,6 +53,7 @@ public:
     int set_tiling(int rows, int ctas_per_sm);
     int autotune(int *rows, int *ctas_per_sm, double *best_ms);
     int device_state(int i, double **U, int *pitch);
+    int set_frame(int i, const double *frame); // NEUMANN2 ghost averages, SoA [v][ny+8][nx+8]
     int init_testcase(int i, const wenofv_testcase *tc);                      // wenofv_init.cu
     int accuracy(int i, const wenofv_testcase *tc, double t, double *norms); // wenofv_init.cu
 
@@ -89,6 +90,7 @@ private:
     int alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params &e);
     void free_instance(int i);
     int launch_stage_all(int parity, int stage, double *rhs_out);
+    int check_frames() const;
     int ensure_stage(size_t bytes);
     int launch_cfl_all();
     int pull_state();
@@ -102,6 +104,8 @@ private:
     std::vector<InstDesc> desc_;
     std::vector<double *> dmem_;    // per instance: 3 state buffers
     std::vector<double *> dmetric_; // per instance: dxc, dxl, dy
+    std::vector<double *> dframe_;  // per NEUMANN2 instance: its ghost frame
+    std::vector<char> frame_set_;
     std::vector<char> live_;
     std::vector<Group> groups_;
     InstDesc *d_desc_ = nullptr;

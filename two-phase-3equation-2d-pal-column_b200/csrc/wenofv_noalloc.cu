@@ -78,6 +78,7 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
 {
     int rc = validate(cfg, eq);
     if (rc) return rc;
+    if (cfg->bc == WENOFV_BC_NEUMANN2) { set_error("NEUMANN2 needs a ghost frame: use a context (wenofv_set_frame)"); return WENOFV_ENOTSUP; }
     if (!d_U || !d_U_next || d_U == d_U_next) { set_error("need distinct device input and output states"); return WENOFV_EINVAL; }
     if (!(dt >= 0.0)) { set_error("dt must be a non-negative number"); return WENOFV_EINVAL; }
     if (pitch < cfg->nx) { set_error("pitch (%d) must be at least nx (%d)", pitch, cfg->nx); return WENOFV_EINVAL; }

@@ -219,6 +219,7 @@ int wenofv_server_submit(wenofv_server *s, const wenofv_config *cfg, const wenof
     int rc = validate(cfg, eq);
     if (rc) return rc;
     if (cfg->rk_method != 2 || cfg->device != s->device) { set_error("the server runs SSP-RK3 on its own device"); return WENOFV_ENOTSUP; }
+    if (cfg->bc == WENOFV_BC_NEUMANN2) { set_error("the server takes no NEUMANN2 requests (they need a ghost frame)"); return WENOFV_ENOTSUP; }
     if (!(t_end > 0)) { set_error("t_end must be positive"); return WENOFV_EINVAL; }
     const size_t bytes = Engine::bytes_needed(*cfg, *eq);
     if (bytes > s->budget) { set_error("request needs %zu bytes, over the HBM budget", bytes); return WENOFV_ENOMEM; }

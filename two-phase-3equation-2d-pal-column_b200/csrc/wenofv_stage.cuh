@@ -272,6 +272,40 @@ __device__ __noinline__ void load_row_walls(double (*dst)[StageSmem<EQ, H>::PS],
     }
 }
 
+// the NEUMANN2 form of load_row: interior cells stream in by cp.async, ghost cells are plain
+// loads of the instance's fixed frame [v][ny+8][nx+8] (interior at (4, 4)).  Rows stay in
+// [-GH, ny+GH) with GH <= 4; columns past nx+4 only occur in a strip's unused tail and are
+// clamped into the frame.
+template <int EQ, int H>
+__device__ __noinline__ void load_row_frame(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
+                                            int i0, InstState *st)
+{
+    constexpr int P = StageGeom<EQ, H>::P, NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
+    static_assert(GH <= 4, "the frame holds 4 ghost layers");
+    const size_t plane = (size_t)D.ny * D.pitch;
+    const int fw = D.nx + 8;
+    const size_t fplane = (size_t)(D.ny + 8) * fw;
+    const int fr = min(max(row, -4), D.ny + 3) + 4;
+    const bool ghost_row = row < 0 || row >= D.ny;
+    (void)st;
+    for (int e = threadIdx.x; e < NV * P; e += NT) {
+        const int v = e / P, p = e - v * P;
+        const int col = i0 - GH + p;
+        if (ghost_row || col < 0 || col >= D.nx) {
+            const int fc = min(max(col, -4), D.nx + 3) + 4;
+#if WENOFV_CHECK_BOUNDS
+            if (row < -4 || row >= D.ny + 4 || col < -4) { // the clamps above only hide a strip's tail
+                flag_error(st, 16u /* WENOFV_FLAG_BOUNDS */, (long long)row * D.nx + col);
+                continue;
+            }
+#endif
+            dst[v][p] = D.frame[v * fplane + (size_t)fr * fw + fc];
+        } else {
+            cp_async8(&dst[v][p], buf + v * plane + (size_t)row * D.pitch + col);
+        }
+    }
+}
+
 // one row of NV x P stage values into shared memory (ghost fill = index map), cp.async 8 B
 template <int EQ, int H>
 __device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
@@ -280,7 +314,7 @@ __device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ, H>::PS], co
     constexpr int P = StageGeom<EQ, H>::P, NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
     const size_t plane = (size_t)D.ny * D.pitch;
     (void)st;
-    if (!is_wall(D.bc)) {
+    if (D.bc == 0 || D.bc == 5) {
         const int jj = map_index_po(row, D.ny, D.bc);
 #pragma unroll
         for (int e = threadIdx.x; e < NV * P; e += NT) {
@@ -294,6 +328,10 @@ __device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ, H>::PS], co
 #endif
             cp_async8(&dst[v][p], buf + v * plane + (size_t)jj * D.pitch + ii);
         }
+        return;
+    }
+    if (D.bc == 3) {
+        load_row_frame<EQ, H>(dst, buf, D, row, i0, st);
         return;
     }
     load_row_walls<EQ, H>(dst, buf, D, row, i0, st);

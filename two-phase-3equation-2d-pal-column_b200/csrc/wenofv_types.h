@@ -24,6 +24,7 @@ struct InstDesc {
     double cfl, dX, dY;
     double dx4; // pow(dX, 4) as the host C library rounds it: WENOEXP's smoothness threshold
     EqParams eq;
+    const double *frame; // NEUMANN2: fixed ghost averages [v][ny+8][nx+8], interior at (4, 4)
 };
 
 // mutable per-instance state of the device-side time loop
