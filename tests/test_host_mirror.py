@@ -45,8 +45,8 @@ def to_soa(raw, nx, ny):
 
 
 def test_host_builds_and_rejects_unsupported(host_bin, tmp_path):
-    cp = run_host(host_bin, "TESTCASE=8", dump_ic=str(tmp_path / "x.bin"))
-    assert cp.returncode == 1 and "NEUMANN2" in cp.stderr
+    cp = run_host(host_bin, "TESTCASE=9", dump_ic=str(tmp_path / "x.bin"))
+    assert cp.returncode == 1
     cp = run_host(host_bin, "BACKEND=CPU", dump_ic=str(tmp_path / "x.bin"))
     assert cp.returncode == 1 and "CUDA backend only" in cp.stderr
     cp = run_host(host_bin, "ELEMNUMX=30", dump_ic=str(tmp_path / "x.bin"))
@@ -239,6 +239,44 @@ def test_host_wall_cases_equal_oracle(host_bin, oracle_lib, tmp_path, testcase):
     (xl, xr, yl, yr), (r10, r20, c1, c2), g = WALL_CASES[testcase]
     p = Problem(nx=nx, ny=ny, xl=xl, xr=xr, yl=yl, yr=yr, bc=1, rho10=r10, rho20=r20, sound1=c1, sound2=c2,
                 gravity=g, scheme=1, recon=1, flux=1, limiter=1, ref_slabs=4, rk=2, cfl=0.5)
+    V, n, t, _ = oracle_lib.advance(p, U0, t_end=tend)
+    assert n > 0 and abs(t - tend) <= 1e-10
+    assert np.array_equal(mine, V)
+
+
+def test_host_zalesak_frame(host_bin, tmp_path):
+    # ZALESAK selects NEUMANN2: the host mirror writes the ghost frame of its initial data
+    # (the disc far from the edges, solid-body rotation u = pi (0.5 - y), v = pi (x - 0.5))
+    nx, ny = 16, 12
+    ic = str(tmp_path / "ic.bin")
+    assert run_host(host_bin, "TESTCASE=8", f"ELEMNUMX={nx}", f"ELEMNUMY={ny}", "REFSLABS=4", dump_ic=ic).returncode == 0
+    F = np.fromfile(ic + ".frame").reshape(4, ny + 8, nx + 8)
+    assert np.all(F[:, 4:-4, 4:-4] == 0.0)  # the interior is not part of the frame
+    ghost = np.ones((ny + 8, nx + 8), bool)
+    ghost[4:-4, 4:-4] = False
+    rho = F[0] + F[1]
+    assert np.allclose(F[0][ghost], 1000.0 * 1e-8) and np.allclose(F[1][ghost], 1.0 - 1e-8)
+    yc = (np.arange(-4, ny + 4) + 0.5) / ny
+    xc = (np.arange(-4, nx + 4) + 0.5) / nx
+    assert np.allclose(F[2][ghost], (rho * np.pi * (0.5 - yc)[:, None])[ghost], rtol=1e-12, atol=1e-12)
+    assert np.allclose(F[3][ghost], (rho * np.pi * (xc - 0.5)[None, :])[ghost], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.gpu
+def test_host_zalesak_equals_oracle(host_bin, oracle_lib, tmp_path):
+    # the rotating disc through the library with its NEUMANN2 frame, against the oracle
+    # advanced from the same initial averages and frame
+    nx, ny, tend = 32, 32, 2e-3
+    ic, out = str(tmp_path / "ic.bin"), str(tmp_path / "u.bin")
+    kv = ("TESTCASE=8", f"ELEMNUMX={nx}", f"ELEMNUMY={ny}", "PRECISION=FP64_STRICT", "REFSLABS=4",
+          "RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=1", "PPlimiter=1")
+    assert run_host(host_bin, *kv, dump_ic=ic).returncode == 0
+    cp = run_host(host_bin, *kv, f"ENDTIME={tend}", f"OUTPUT={out}")
+    assert cp.returncode == 0, cp.stderr
+    U0, mine = to_soa(np.fromfile(ic), nx, ny), to_soa(np.fromfile(out), nx, ny)
+    F = np.fromfile(ic + ".frame").reshape(4, ny + 8, nx + 8)
+    p = Problem(nx=nx, ny=ny, bc=3, frame=F, rho10=1000.0, rho20=1.0, sound1=70.0, sound2=70.0, scheme=1, recon=1,
+                flux=1, limiter=1, ref_slabs=4, rk=2, cfl=0.5)
     V, n, t, _ = oracle_lib.advance(p, U0, t_end=tend)
     assert n > 0 and abs(t - tend) <= 1e-10
     assert np.array_equal(mine, V)

@@ -12,8 +12,10 @@
 // run, because it stops on their boundary kind (src/WENOFV.cpp:2286-2292): DAMBREAK,
 // DAMBREAK2, DAMBREAK3, RTI and STANDING_WAVE (include/Equations.hpp:747-973), with the
 // library's NEUMANN walls and the gravity of assembleSourceTerm (src/WENOFV.cpp:1831-1872).
-// ZALESAK needs NEUMANN2 (boundary from the initial data), which the library does not
-// provide; it throws std::invalid_argument, like an unknown case does in the reference (:975).
+// ZALESAK (:690-745), a disc of radius 0.15 in solid-body rotation about the centre, selects
+// NEUMANN2 (boundary from the initial data): CWENOFV builds the fixed ghost frame from the
+// initial averages of the 4 cell layers around the domain.  Other cases throw
+// std::invalid_argument, like an unknown case does in the reference (:975).
 #pragma once
 #include <cmath>
 #include <stdexcept>
@@ -109,9 +111,14 @@ public:
             set_phase(1000.0, 1.0, 100.0, 100.0, 0.0, 0.0, 1e-5, 1e4);
             walls(9.81);
             break;
+        case ZALESAK: // (:690-745)
+            set_box(0.0, 1.0, 0.0, 1.0);
+            outputTimes = {2};
+            set_phase(1000.0, 1.0, 70.0, 70.0, 1.0, 1.0, 1e-8);
+            boundaryCondition = NEUMANN2;
+            break;
         default:
-            throw std::invalid_argument(std::string("test case ") + TESTCASETYPE_STRINGS[type] +
-                                        " needs the NEUMANN2 boundary (from the initial data), which the CUDA backend does not provide");
+            throw std::invalid_argument(std::string("test case ") + std::to_string((int)type) + " is not supported");
         }
     }
 
@@ -149,6 +156,10 @@ public:
                 return (x >= xL && x <= xL + L0 && y >= yL && y <= yL + H0) ? 1.0 - g_epsa : g_epsa;
             return (x >= xR - L0 && x <= xR && y >= yL && y <= yL + H0) ? 1.0 - g_epsa : g_epsa;
         }
+        case ZALESAK: { // disc of radius 0.15 at (0.5, 0.5) (:717-723)
+            const double x0 = 0.5, y0 = 0.5, r = 0.15;
+            return (std::pow(x - x0, 2) + std::pow(y - y0, 2) < std::pow(r, 2)) ? 1 - g_epsa : g_epsa;
+        }
         default:
             return g_epsa;
         }
@@ -175,12 +186,14 @@ public:
     double u_0(double x, double y) const
     {
         // VORTEX adds r*0 + theta*0 + L*0 to g_u0 (:589-604), which is g_u0 for finite r
-        (void)x; (void)y;
+        if (testcase == ZALESAK) return M_PI * (0.5 - y); // rotation at omega = pi (:729-733)
+        (void)x;
         return g_u0;
     }
     double v_0(double x, double y) const
     {
-        (void)x; (void)y;
+        if (testcase == ZALESAK) return M_PI * (x - 0.5); // (:734-738)
+        (void)y;
         return g_v0;
     }
 

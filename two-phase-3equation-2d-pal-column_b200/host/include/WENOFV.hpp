@@ -72,6 +72,7 @@ public:
     RECONSTRUCTIONTYPE m_reconstructionType = CHARACTERISTIC;
 
     std::vector<double> m_Uh;  // interior cell averages, [i][j][r]
+    std::vector<double> m_frame; // NEUMANN2: ghost averages, SoA [r][ny+8][nx+8] (wenofv_set_frame)
     std::vector<double> m_rhs; // the last assembleRHS result, [i][j][r]
 
     int m_precision = WENOFV_FP64;

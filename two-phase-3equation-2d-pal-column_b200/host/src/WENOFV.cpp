@@ -117,6 +117,29 @@ void CWENOFV::initializeAve()
             for (int r = 0; r < m_varNum; r++) Uh(i, j, r) = acc[r] / area;
         }
     }
+    m_frame.clear();
+    if (equation->boundaryCondition != NEUMANN2) return;
+    // NEUMANN2 ("boundary from the initial data"): the same 4x4 average over the 4 cell layers
+    // around the domain, on the uniform grid extended past its edges; held fixed by the library
+    const int fw = m_worldElemNumX + 8, fh = m_worldElemNumY + 8;
+    m_frame.assign((size_t)m_varNum * fw * fh, 0.0);
+    for (int fj = 0; fj < fh; fj++)
+        for (int fi = 0; fi < fw; fi++) {
+            const int i = fi - 4, j = fj - 4;
+            if (i >= 0 && i < m_worldElemNumX && j >= 0 && j < m_worldElemNumY) continue;
+            const double xl = equation->xL + i * m_deltaX, xr = xl + m_deltaX;
+            const double yl = equation->yL + j * m_deltaY, yr = yl + m_deltaY;
+            const double xc = (xl + xr) / 2, xd = xr - xl, yc = (yl + yr) / 2, yd = yr - yl;
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int a = 0; a < 4; a++)
+                for (int b = 0; b < 4; b++) {
+                    const double gx = xc + 0.5 * xd * kGLegX[a], gy = yc + 0.5 * yd * kGLegX[b];
+                    const double wx = 0.5 * xd * kGLegW[a], wy = 0.5 * yd * kGLegW[b];
+                    equation->getU0(gx, gy, U0);
+                    for (int r = 0; r < m_varNum; r++) acc[r] += U0[r] * wx * wy;
+                }
+            for (int r = 0; r < m_varNum; r++) m_frame[((size_t)r * fh + fj) * fw + fi] = acc[r] / (xd * yd);
+        }
 }
 
 wenofv_config CWENOFV::config() const
@@ -153,6 +176,7 @@ void CWENOFV::initializeSolver()
         m_ctx = nullptr;
     }
     check(wenofv_create(&c, &p, &m_ctx), "wenofv_create");
+    if (!m_frame.empty()) check(wenofv_set_frame(m_ctx, m_frame.data()), "wenofv_set_frame");
     uploadUh();
     m_now = 0.0;
     m_stepCount = 0;

@@ -4,8 +4,8 @@
 //
 // reads the settings file (default ./config/settings.cfg), lets KEY=VALUE arguments
 // override its keys, builds TwoPhaseEquation and CWENOFV and runs the solver on one GPU.
-// --dump-ic FILE writes the initial cell averages ([i][j][r], FP64) and exits without
-// touching the GPU.  No MPI: the whole domain is one GPU's.
+// --dump-ic FILE writes the initial cell averages ([i][j][r], FP64), and for NEUMANN2 the
+// ghost frame to FILE.frame ([r][ny+8][nx+8]), and exits without touching the GPU.  No MPI: the whole domain is one GPU's.
 #include <cstring>
 #include <fstream>
 #include <iostream>
@@ -38,8 +38,14 @@ int main(int argc, char *argv[])
             solver.initializeAve();
             std::ofstream f(dump_ic, std::ios::binary);
             f.write(reinterpret_cast<const char *>(solver.m_Uh.data()), (std::streamsize)(solver.m_Uh.size() * sizeof(double)));
+            bool ok = (bool)f;
+            if (!solver.m_frame.empty()) { // NEUMANN2: the ghost frame beside it, FILE.frame
+                std::ofstream g(dump_ic + ".frame", std::ios::binary);
+                g.write(reinterpret_cast<const char *>(solver.m_frame.data()), (std::streamsize)(solver.m_frame.size() * sizeof(double)));
+                ok = ok && (bool)g;
+            }
             delete equation;
-            return f ? 0 : 1;
+            return ok ? 0 : 1;
         }
         solver.run();
     } catch (const std::exception &e) {
