@@ -246,10 +246,9 @@ __device__ __forceinline__ int map_index_po(int k, int n, int bc)
     return k < 0 ? k + n : k;
 }
 
-// the wall form of load_row: ghost cells are plain loads with the momentum signs (kept out
-// of line, so that the periodic and outflow loads keep their own register allocation)
+// the wall form of load_row: ghost cells are plain loads with the momentum signs
 template <int EQ, int H>
-__device__ __noinline__ void load_row_walls(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
+__device__ __forceinline__ void load_row_walls(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
                                             int i0, InstState *st)
 {
     constexpr int P = StageGeom<EQ, H>::P, NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
@@ -277,7 +276,7 @@ __device__ __noinline__ void load_row_walls(double (*dst)[StageSmem<EQ, H>::PS],
 // [-GH, ny+GH) with GH <= 4; columns past nx+4 only occur in a strip's unused tail and are
 // clamped into the frame.
 template <int EQ, int H>
-__device__ __noinline__ void load_row_frame(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
+__device__ __forceinline__ void load_row_frame(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
                                             int i0, InstState *st)
 {
     constexpr int P = StageGeom<EQ, H>::P, NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
@@ -306,6 +305,16 @@ __device__ __noinline__ void load_row_frame(double (*dst)[StageSmem<EQ, H>::PS],
     }
 }
 
+// the two ghost rules that are not an index map (walls, NEUMANN2 frame), behind one out-of-line
+// call so that the periodic and outflow loads keep the stage kernel's register allocation
+template <int EQ, int H>
+__device__ __noinline__ void load_row_other(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
+                                            int i0, InstState *st)
+{
+    if (D.bc == 3) load_row_frame<EQ, H>(dst, buf, D, row, i0, st);
+    else load_row_walls<EQ, H>(dst, buf, D, row, i0, st);
+}
+
 // one row of NV x P stage values into shared memory (ghost fill = index map), cp.async 8 B
 template <int EQ, int H>
 __device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
@@ -330,11 +339,7 @@ __device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ, H>::PS], co
         }
         return;
     }
-    if (D.bc == 3) {
-        load_row_frame<EQ, H>(dst, buf, D, row, i0, st);
-        return;
-    }
-    load_row_walls<EQ, H>(dst, buf, D, row, i0, st);
+    load_row_other<EQ, H>(dst, buf, D, row, i0, st);
 }
 
 // value of a reconstruction: in the deviation form the anchor plus the FP32 deviation, in
