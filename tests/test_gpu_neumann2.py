@@ -39,6 +39,7 @@ def _runs(nx, ny):
     return [(Problem(nx=nx, ny=ny, bc=BC_NEUMANN2, frame=fr(F0), scheme=1, flux=1, recon=1, limiter=1, gravity=9.81, **prm), U0),
             (Problem(nx=nx, ny=ny, bc=BC_NEUMANN2, frame=fr(F0), scheme=2, flux=0, recon=0, limiter=1, **prm), U0),
             (Problem(nx=nx, ny=ny, bc=BC_NEUMANN2, frame=fr(F0), scheme=1, flux=1, recon=3, limiter=1, **prm), U0),
+            (Problem(nx=nx, ny=ny, bc=BC_NEUMANN2, frame=fr(F0), scheme=2, flux=1, recon=2, limiter=1, **prm), U0),
             (Problem(nx=nx, ny=ny, bc=BC_NEUMANN2, frame=fr(EF), eq_kind=EQ_EULER, scheme=1, flux=1, recon=1, cfl=0.4), E0),
             (Problem(nx=nx, ny=ny, bc=BC_NEUMANN2, frame=fr(A0[:, ::-1].copy()), eq_kind=EQ_LINEAR_ADV, scheme=0, flux=0,
                      recon=0), A0)]

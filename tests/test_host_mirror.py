@@ -280,3 +280,28 @@ def test_host_zalesak_equals_oracle(host_bin, oracle_lib, tmp_path):
     V, n, t, _ = oracle_lib.advance(p, U0, t_end=tend)
     assert n > 0 and abs(t - tend) <= 1e-10
     assert np.array_equal(mine, V)
+
+
+@pytest.mark.gpu
+def test_host_sharp_oscillation_output(host_bin, tmp_path):
+    # SHARP writes outputUPoscillation's file at the initial and final moments: the velocity
+    # and pressure deviations from the uniform flow (1, 1), consistent with average_*.plt
+    out = tmp_path / "out"
+    cp = run_host(host_bin, "TESTCASE=2", "ELEMNUMX=32", "ELEMNUMY=32", "REFSLABS=4", "ENDTIME=0.002",
+                  "PRECISION=FP64_STRICT", "RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=1", "PPlimiter=1", f"OUTPUTDIR={out}")
+    assert cp.returncode == 0, cp.stderr
+    for moment in ("initial", "final"):
+        lines = (out / f"UPoscillation_{moment}.plt").read_text().splitlines()
+        assert lines[0] == "TITLE=FvSolution"
+        assert lines[1].split() == ["VARIABLES=X", "Y", "Speed_oscillation", "P_oscillation", "U_oscillation", "V_oscillation"]
+        assert lines[2].startswith("ZONE T=TA, I=32, J=32")
+        osc = np.array([list(map(float, ln.split())) for ln in lines[3:]])
+        ave = np.array([list(map(float, ln.split())) for ln in (out / f"average_{moment}.plt").read_text().splitlines()[3:]])
+        assert osc.shape == (32 * 32, 6)
+        assert np.array_equal(osc[:, :2], ave[:, :2])
+        u, v, p = ave[:, 8], ave[:, 9], ave[:, 10]
+        # the printed columns carry 6 significant digits
+        assert np.allclose(osc[:, 4], np.abs(u - 1) / 70.0, rtol=1e-4, atol=1e-9)
+        assert np.allclose(osc[:, 5], np.abs(v - 1) / 70.0, rtol=1e-4, atol=1e-9)
+        assert np.allclose(osc[:, 3], np.abs(p) / 1000.0 / 70.0 ** 2, rtol=1e-4, atol=1e-12)
+        assert np.allclose(osc[:, 2], np.hypot(osc[:, 4], osc[:, 5]), rtol=1e-4, atol=1e-9)

@@ -216,9 +216,11 @@ void CWENOFV::outputResults(int count, double now, const std::string &specialCas
     if (specialCase == "initial") {
         outputAve("initial");
         if (exact) outputAccuracy("initial", now);
+        if (m_testcase == SHARP) outputUPoscillation("initial");
     } else if (specialCase == "final") {
         outputAve("final");
         if (exact) outputAccuracy("final", now);
+        if (m_testcase == SHARP) outputUPoscillation("final"); // outputSpecialTestCasebyCell (:3381-3391)
     } else if (specialCase == "intermediate") {
         outputAve(num_str(now) + "_intermediate");
     }
@@ -245,6 +247,33 @@ void CWENOFV::outputAve(const std::string &prefix)
             f << (xl + xr) / 2 << " " << (yl + yr) / 2 << " " << U[0] << " " << U[1] << " " << z1 << " " << U[0] / z1
               << " " << U[1] / (1.0 - z1) << " " << rho << " " << U[2] / rho << " " << U[3] / rho << " "
               << pressure(*equation, U, z1) << " " << std::endl;
+        }
+    }
+}
+
+// outputUPoscillation (src/WENOFV.cpp:2739-2805): for the SHARP square advected at (1, 1), each
+// cell's deviation from that uniform flow: |(u-1, v-1)| / c1, |p| / (rho10 c1^2), |u-1| / c1
+// and |v-1| / c1, in the layout of outputAve
+void CWENOFV::outputUPoscillation(const std::string &prefix)
+{
+    const std::string filename = m_outputDir + "UPoscillation_" + prefix + ".plt";
+    std::ofstream f(filename);
+    if (!f) throw std::runtime_error("cannot write " + filename);
+    f << "TITLE=FvSolution" << std::endl;
+    f << "VARIABLES=X Y Speed_oscillation P_oscillation U_oscillation V_oscillation " << std::endl;
+    f << "ZONE T=TA, I=" << m_worldElemNumY << ", J=" << m_worldElemNumX << ", DATAPACKING = POINT" << std::endl;
+    const int G = m_ghostCellNum;
+    const double c1 = equation->g_sound1;
+    for (int i = 0; i < m_worldElemNumX; i++) {
+        const double xl = equation->xL - G * m_deltaX + (i + G) * m_deltaX, xr = equation->xL - G * m_deltaX + (i + G + 1) * m_deltaX;
+        for (int j = 0; j < m_worldElemNumY; j++) {
+            const double yl = equation->yL - G * m_deltaY + (j + G) * m_deltaY, yr = equation->yL - G * m_deltaY + (j + G + 1) * m_deltaY;
+            const double *U = &m_Uh[((size_t)i * m_worldElemNumY + j) * m_varNum];
+            const double rho = U[0] + U[1], u = U[2] / rho, v = U[3] / rho;
+            const double p = pressure(*equation, U, volume_frac(*equation, U));
+            f << (xl + xr) / 2 << " " << (yl + yr) / 2 << " " << std::fabs(std::sqrt(std::pow(u - 1, 2) + std::pow(v - 1, 2))) / c1
+              << " " << std::fabs(p) / equation->g_rho10 / std::pow(c1, 2) << " " << std::fabs(u - 1) / c1 << " "
+              << std::fabs(v - 1) / c1 << " " << std::endl;
         }
     }
 }
