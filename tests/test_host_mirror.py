@@ -9,6 +9,7 @@ state of SMOOTH and SHARP bit for bit.
 """
 from __future__ import annotations
 
+import json
 import os
 import subprocess
 
@@ -287,9 +288,24 @@ def test_host_sharp_oscillation_output(host_bin, tmp_path):
     # SHARP writes outputUPoscillation's file at the initial and final moments: the velocity
     # and pressure deviations from the uniform flow (1, 1), consistent with average_*.plt
     out = tmp_path / "out"
-    cp = run_host(host_bin, "TESTCASE=2", "ELEMNUMX=32", "ELEMNUMY=32", "REFSLABS=4", "ENDTIME=0.002",
-                  "PRECISION=FP64_STRICT", "RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=1", "PPlimiter=1", f"OUTPUTDIR={out}")
+    kv = ("TESTCASE=2", "ELEMNUMX=32", "ELEMNUMY=32", "REFSLABS=4", "ENDTIME=0.05", "PRECISION=FP64_STRICT",
+          "RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=1", "PPlimiter=1")
+    cp = run_host(host_bin, *kv, f"OUTPUTDIR={out}")
     assert cp.returncode == 0, cp.stderr
+    # the time series of outputUPoscillationByTime at step 1 and every 200th step, the same
+    # from the device loop (run in pieces) and from the host loop
+    steps = json.loads(cp.stdout.strip().splitlines()[-1])["steps"]
+    assert steps >= 200
+    out_h = tmp_path / "out_host"
+    cp = run_host(host_bin, *kv, "STEPMODE=1", f"OUTPUTDIR={out_h}")
+    assert cp.returncode == 0, cp.stderr
+    ts = (out / "oscillationByTime_32.plt").read_text()
+    assert ts == (out_h / "oscillationByTime_32.plt").read_text()
+    ts = ts.splitlines()
+    assert ts[0] == "TITLE=FvSolution" and ts[2] == "ZONE T=TA"
+    assert ts[1].split() == ["VARIABLES=Time", "Speed_oscillation", "P_oscillation", "U_oscillation", "V_oscillation"]
+    series = np.array([list(map(float, ln.split())) for ln in ts[3:]])
+    assert series.shape == (1 + steps // 200, 5) and np.all(np.diff(series[:, 0]) > 0) and np.all(series[:, 1:3] >= 0)
     for moment in ("initial", "final"):
         lines = (out / f"UPoscillation_{moment}.plt").read_text().splitlines()
         assert lines[0] == "TITLE=FvSolution"

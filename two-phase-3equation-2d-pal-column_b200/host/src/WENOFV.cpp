@@ -278,6 +278,36 @@ void CWENOFV::outputUPoscillation(const std::string &prefix)
     }
 }
 
+// outputSpecialTestCasebyTime (src/WENOFV.cpp:3363-3379) for SHARP: outputUPoscillationByTime
+// (:2865-2941) appends the maxima over the cells of the pressure, speed, u and v deviations
+// to oscillationByTime_<nx>.plt.  The reference's header names the columns Speed, P, U, V
+// but writes them in the order P, Speed, U, V, and takes the signed u and v deviations (maxima
+// from 0); both are kept, so that files from the two programs read alike.
+void CWENOFV::outputSpecialTestCasebyTime(double now)
+{
+    if (m_testcase != SHARP) return;
+    const std::string filename = m_outputDir + "oscillationByTime_" + std::to_string(m_worldElemNumX) + ".plt";
+    const bool exists = std::filesystem::exists(filename);
+    std::ofstream f(filename, std::ios::app);
+    if (!f) throw std::runtime_error("cannot write " + filename);
+    if (!exists)
+        f << "TITLE=FvSolution" << std::endl
+          << "VARIABLES=Time Speed_oscillation P_oscillation U_oscillation V_oscillation " << std::endl
+          << "ZONE T=TA" << std::endl;
+    const double c1 = equation->g_sound1;
+    double pmax = 0, smax = 0, umax = 0, vmax = 0;
+    for (int i = 0; i < m_worldElemNumX; i++)
+        for (int j = 0; j < m_worldElemNumY; j++) {
+            const double *U = &m_Uh[((size_t)i * m_worldElemNumY + j) * m_varNum];
+            const double rho = U[0] + U[1], u = U[2] / rho, v = U[3] / rho;
+            pmax = std::max(pmax, std::fabs(pressure(*equation, U, volume_frac(*equation, U))) / equation->g_rho10 / std::pow(c1, 2));
+            smax = std::max(smax, std::sqrt(std::pow(u - 1, 2) + std::pow(v - 1, 2)) / c1);
+            umax = std::max(umax, (u - 1) / c1);
+            vmax = std::max(vmax, (v - 1) / c1);
+        }
+    f << now << " " << pmax << " " << smax << " " << umax << " " << vmax << std::endl;
+}
+
 // outputAccuracy (src/WENOFV.cpp:3152-3251): z1 against the 4x4 Gauss-Legendre average of
 // the initial volume fraction translated by (u0, v0) t
 void CWENOFV::outputAccuracy(const std::string &prefix, double now)
@@ -356,6 +386,7 @@ void CWENOFV::run()
     outputResults(0, m_now, "initial");
     const auto t1 = std::chrono::steady_clock::now();
     const bool hostLoop = opt("STEPMODE", "0") == "1";
+    const bool byTime = !m_outputDir.empty() && m_testcase == SHARP; // the time series built here
     for (size_t k = 1; k < m_timeMoments.size(); k++) {
         const double targetTime = m_timeMoments[k];
         if (hostLoop) {
@@ -368,6 +399,29 @@ void CWENOFV::run()
                 performTimeIntegration(timestep);
                 m_now += timestep;
                 n++;
+                if (byTime && (m_stepCount == 1 || m_stepCount % 200 == 0)) {
+                    downloadUh();
+                    outputSpecialTestCasebyTime(m_now);
+                }
+            }
+        } else if (byTime) {
+            // the device loop in pieces that end at the steps where the reference writes its
+            // time series (step 1 and every 200th, src/WENOFV.cpp:2486-2497)
+            int64_t done = 0;
+            while (std::abs(m_now - targetTime) > 1e-10 && (m_maxSteps <= 0 || done < m_maxSteps)) {
+                int64_t piece = m_stepCount < 1 ? 1 : 200 - m_stepCount % 200;
+                if (m_maxSteps > 0) piece = std::min<int64_t>(piece, m_maxSteps - done);
+                double tout = m_now;
+                int64_t n = 0;
+                check(wenofv_advance(m_ctx, m_now, targetTime, piece, &tout, &n), "run");
+                m_now = tout;
+                m_stepCount += n;
+                done += n;
+                if (n == 0) break;
+                if (m_stepCount == 1 || m_stepCount % 200 == 0) {
+                    downloadUh();
+                    outputSpecialTestCasebyTime(m_now);
+                }
             }
         } else {
             double tout = m_now;
