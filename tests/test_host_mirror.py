@@ -321,3 +321,27 @@ def test_host_sharp_oscillation_output(host_bin, tmp_path):
         assert np.allclose(osc[:, 5], np.abs(v - 1) / 70.0, rtol=1e-4, atol=1e-9)
         assert np.allclose(osc[:, 3], np.abs(p) / 1000.0 / 70.0 ** 2, rtol=1e-4, atol=1e-12)
         assert np.allclose(osc[:, 2], np.hypot(osc[:, 4], osc[:, 5]), rtol=1e-4, atol=1e-9)
+
+
+@pytest.mark.gpu
+def test_host_dambreak_pressure_probes(host_bin, tmp_path):
+    # DAMBREAK's outputPressureByTime: wall pressures at 3, 15, 30 and 80 mm over rho10 g H0,
+    # at step 1 and every 200th step; the same from the device loop and the host loop
+    kv = ("TESTCASE=3", "ELEMNUMX=32", "ELEMNUMY=16", "REFSLABS=4", "ENDTIME=0.06", "PRECISION=FP64_STRICT",
+          "RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=1", "PPlimiter=1")
+    out, out_h = tmp_path / "out", tmp_path / "out_host"
+    cp = run_host(host_bin, *kv, f"OUTPUTDIR={out}")
+    assert cp.returncode == 0, cp.stderr
+    steps = json.loads(cp.stdout.strip().splitlines()[-1])["steps"]
+    assert steps >= 200
+    cp = run_host(host_bin, *kv, "STEPMODE=1", f"OUTPUTDIR={out_h}")
+    assert cp.returncode == 0, cp.stderr
+    text = (out / "pressureByTime.plt").read_text()
+    assert text == (out_h / "pressureByTime.plt").read_text()
+    lines = text.splitlines()
+    assert lines[:4] == ["TITLE=FvSolution", "VARIABLES=Time P_y3mm P_y15mm P_y30mm P_y80mm", "", "ZONE T=TA"]
+    series = np.array([list(map(float, ln.split())) for ln in lines[4:]])
+    assert series.shape == (1 + steps // 200, 5) and np.all(np.diff(series[:, 0]) > 0)
+    # getPressure of the linearised model is the deviation from g_preb, which starts at 0:
+    # after one step it is still far below the hydrostatic scale (1 on this axis)
+    assert np.all(np.abs(series[0, 1:]) < 1e-3)

@@ -101,7 +101,8 @@ public:
     void outputAve(const std::string &prefix);
     void outputAccuracy(const std::string &prefix, double now);
     void outputUPoscillation(const std::string &prefix); // SHARP's velocity/pressure deviation
-    void outputSpecialTestCasebyTime(double now);      // SHARP's oscillation time series
+    void outputSpecialTestCasebyTime(double now);      // SHARP's and DAMBREAK's time series
+    void outputPressureByTime(double now);             // DAMBREAK's wall pressure probes
     std::string m_outputDir;
     double &Uh(int i, int j, int r) { return m_Uh[((size_t)i * m_worldElemNumY + j) * m_varNum + r]; }
     wenofv_config config() const;

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <filesystem>
 #include <fstream>
+#include <limits>
 #include <iomanip>
 #include <iostream>
 #include <sstream>
@@ -285,6 +286,10 @@ void CWENOFV::outputUPoscillation(const std::string &prefix)
 // from 0); both are kept, so that files from the two programs read alike.
 void CWENOFV::outputSpecialTestCasebyTime(double now)
 {
+    if (m_testcase == DAMBREAK) {
+        outputPressureByTime(now);
+        return;
+    }
     if (m_testcase != SHARP) return;
     const std::string filename = m_outputDir + "oscillationByTime_" + std::to_string(m_worldElemNumX) + ".plt";
     const bool exists = std::filesystem::exists(filename);
@@ -306,6 +311,57 @@ void CWENOFV::outputSpecialTestCasebyTime(double now)
             vmax = std::max(vmax, (v - 1) / c1);
         }
     f << now << " " << pmax << " " << smax << " " << umax << " " << vmax << std::endl;
+}
+
+// outputPressureByTime (src/WENOFV.cpp:2942-3048) for DAMBREAK: the pressure on the left wall
+// at y = 3, 15, 30 and 80 mm over rho10 g H0 (g = 9.81, H0 = 0.3), against t sqrt(g / H0).  For
+// each height, the cell pressures of a 5x5 block around (first column, row floor(y / dy)) are
+// reconstructed by WENO-JS across x to the wall face (Gauss-Lobatto point 0), then across y
+// to the 4 points of the row's cell; the point nearest y is taken.  Cells beyond the domain
+// are the mirror images that the library's NEUMANN walls use (the pressure keeps its sign).
+// The reconstructions run through the library's WENO probe, so they are the solver's own.
+void CWENOFV::outputPressureByTime(double now)
+{
+    const std::string filename = m_outputDir + "pressureByTime.plt";
+    const bool exists = std::filesystem::exists(filename);
+    std::ofstream f(filename, std::ios::app);
+    if (!f) throw std::runtime_error("cannot write " + filename);
+    if (!exists) f << "TITLE=FvSolution" << std::endl << "VARIABLES=Time P_y3mm P_y15mm P_y30mm P_y80mm\n" << std::endl << "ZONE T=TA" << std::endl;
+    auto mirror = [](int k, int n) {
+        for (int it = 0; it < 64 && (k < 0 || k >= n); it++) k = k < 0 ? -1 - k : 2 * n - 1 - k;
+        return std::min(std::max(k, 0), n - 1);
+    };
+    const double heights_mm[4] = {3.0, 15.0, 30.0, 80.0};
+    const double gl[4] = {-1.0, -std::sqrt(0.2), std::sqrt(0.2), 1.0}; // Gauss-Lobatto points on [-1, 1]
+    std::vector<double> xst(4 * 25), xout(4 * 20), yst(4 * 5), yout(4 * 4);
+    int rows[4];
+    for (int h = 0; h < 4; h++) {
+        const double y_m = heights_mm[h] / 1000.0;
+        rows[h] = (int)std::floor(y_m / m_deltaY);
+        for (int b = 0; b < 5; b++)     // row offset b - 2: one x-stencil per row
+            for (int a = 0; a < 5; a++) { // column offset a - 2 from the first column
+                const int i = mirror(a - 2, m_worldElemNumX), j = mirror(rows[h] + b - 2, m_worldElemNumY);
+                const double *U = &m_Uh[((size_t)i * m_worldElemNumY + j) * m_varNum];
+                xst[(h * 5 + b) * 5 + a] = pressure(*equation, U, volume_frac(*equation, U)) / equation->g_rho10 / 9.81 / 0.3;
+            }
+    }
+    check(wenofv_probe_weno(0, WENOFV_FP64_STRICT, xst.data(), 20, xout.data(), m_device), "wenofv_probe_weno");
+    for (int h = 0; h < 4; h++)
+        for (int b = 0; b < 5; b++) yst[h * 5 + b] = xout[(h * 5 + b) * 4 + 0];
+    check(wenofv_probe_weno(0, WENOFV_FP64_STRICT, yst.data(), 4, yout.data(), m_device), "wenofv_probe_weno");
+    f << now * std::sqrt(9.81 / 0.3);
+    for (int h = 0; h < 4; h++) {
+        const double y_m = heights_mm[h] / 1000.0;
+        const double yc = equation->yL + (rows[h] + 0.5) * m_deltaY;
+        int best = 0;
+        double diff = std::numeric_limits<double>::max();
+        for (int k = 0; k < 4; k++) {
+            const double d = std::fabs(yc + 0.5 * m_deltaY * gl[k] - y_m);
+            if (d < diff) { diff = d; best = k; }
+        }
+        f << " " << yout[h * 4 + best];
+    }
+    f << std::endl;
 }
 
 // outputAccuracy (src/WENOFV.cpp:3152-3251): z1 against the 4x4 Gauss-Legendre average of
@@ -386,7 +442,7 @@ void CWENOFV::run()
     outputResults(0, m_now, "initial");
     const auto t1 = std::chrono::steady_clock::now();
     const bool hostLoop = opt("STEPMODE", "0") == "1";
-    const bool byTime = !m_outputDir.empty() && m_testcase == SHARP; // the time series built here
+    const bool byTime = !m_outputDir.empty() && (m_testcase == SHARP || m_testcase == DAMBREAK); // the series built here
     for (size_t k = 1; k < m_timeMoments.size(); k++) {
         const double targetTime = m_timeMoments[k];
         if (hostLoop) {
