@@ -306,6 +306,14 @@ def test_host_sharp_oscillation_output(host_bin, tmp_path):
     assert ts[1].split() == ["VARIABLES=Time", "Speed_oscillation", "P_oscillation", "U_oscillation", "V_oscillation"]
     series = np.array([list(map(float, ln.split())) for ln in ts[3:]])
     assert series.shape == (1 + steps // 200, 5) and np.all(np.diff(series[:, 0]) > 0) and np.all(series[:, 1:3] >= 0)
+    # outputThincknessByTime at the same steps: 1 / the largest z1 jump, about 1 cell for the
+    # sharp square after one step, growing as the scheme smears it
+    th = (out / "thincknessByTime.plt").read_text()
+    assert th == (out_h / "thincknessByTime.plt").read_text()
+    th = th.splitlines()
+    assert th[:4] == ["TITLE=FvSolution", "VARIABLES=time thinckness", "", "ZONE T=TA"]
+    thick = np.array([list(map(float, ln.split())) for ln in th[4:]])
+    assert np.array_equal(thick[:, 0], series[:, 0]) and 1.0 <= thick[0, 1] < 2.0 and thick[-1, 1] >= thick[0, 1]
     for moment in ("initial", "final"):
         lines = (out / f"UPoscillation_{moment}.plt").read_text().splitlines()
         assert lines[0] == "TITLE=FvSolution"
@@ -345,3 +353,21 @@ def test_host_dambreak_pressure_probes(host_bin, tmp_path):
     # getPressure of the linearised model is the deviation from g_preb, which starts at 0:
     # after one step it is still far below the hydrostatic scale (1 on this axis)
     assert np.all(np.abs(series[0, 1:]) < 1e-3)
+
+
+@pytest.mark.gpu
+def test_host_rti_symmetry_error(host_bin, tmp_path):
+    # RTI's outputSymmetryErr: z1 of the left half against its mirror image, at step 1 and
+    # every 200th step.  The initial interface is mirror-symmetric; the 4-slab grid metric is
+    # not to the last bit, and the Rayleigh-Taylor instability amplifies that rounding-level
+    # asymmetry (about 1e-12 after one step, 2e-8 after 200 on this grid)
+    kv = ("TESTCASE=6", "ELEMNUMX=16", "ELEMNUMY=32", "REFSLABS=4", "ENDTIME=0.07", "PRECISION=FP64_STRICT",
+          "RECONSTRUCTIONTYPE=1", "RIEMANNFLUX=1", "PPlimiter=1")
+    out = tmp_path / "out"
+    cp = run_host(host_bin, *kv, f"OUTPUTDIR={out}")
+    assert cp.returncode == 0, cp.stderr
+    steps = json.loads(cp.stdout.strip().splitlines()[-1])["steps"]
+    assert steps >= 200
+    err = np.array([list(map(float, ln.split())) for ln in (out / "symmetry_err.plt").read_text().splitlines()])
+    assert err.shape == (1 + steps // 200, 2) and np.all(np.diff(err[:, 0]) > 0)
+    assert np.all(err[:, 1] >= 0) and err[0, 1] < 1e-10 and np.all(err[:, 1] < 1e-6)

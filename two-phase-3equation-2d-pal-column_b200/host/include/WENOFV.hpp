@@ -103,6 +103,8 @@ public:
     void outputUPoscillation(const std::string &prefix); // SHARP's velocity/pressure deviation
     void outputSpecialTestCasebyTime(double now);      // SHARP's and DAMBREAK's time series
     void outputPressureByTime(double now);             // DAMBREAK's wall pressure probes
+    void outputThicknessByTime(double now);            // SHARP's interface thickness
+    void outputSymmetryErr(double now);                // RTI's left-right symmetry error
     std::string m_outputDir;
     double &Uh(int i, int j, int r) { return m_Uh[((size_t)i * m_worldElemNumY + j) * m_varNum + r]; }
     wenofv_config config() const;

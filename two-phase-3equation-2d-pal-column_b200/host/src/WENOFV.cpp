@@ -279,8 +279,9 @@ void CWENOFV::outputUPoscillation(const std::string &prefix)
     }
 }
 
-// outputSpecialTestCasebyTime (src/WENOFV.cpp:3363-3379) for SHARP: outputUPoscillationByTime
-// (:2865-2941) appends the maxima over the cells of the pressure, speed, u and v deviations
+// outputSpecialTestCasebyTime (src/WENOFV.cpp:3363-3379): DAMBREAK's pressure probes, RTI's
+// symmetry error, and for SHARP the interface thickness and outputUPoscillationByTime
+// (:2865-2941), which appends the maxima over the cells of the pressure, speed, u and v deviations
 // to oscillationByTime_<nx>.plt.  The reference's header names the columns Speed, P, U, V
 // but writes them in the order P, Speed, U, V, and takes the signed u and v deviations (maxima
 // from 0); both are kept, so that files from the two programs read alike.
@@ -290,7 +291,12 @@ void CWENOFV::outputSpecialTestCasebyTime(double now)
         outputPressureByTime(now);
         return;
     }
+    if (m_testcase == RTI) {
+        outputSymmetryErr(now);
+        return;
+    }
     if (m_testcase != SHARP) return;
+    outputThicknessByTime(now);
     const std::string filename = m_outputDir + "oscillationByTime_" + std::to_string(m_worldElemNumX) + ".plt";
     const bool exists = std::filesystem::exists(filename);
     std::ofstream f(filename, std::ios::app);
@@ -311,6 +317,47 @@ void CWENOFV::outputSpecialTestCasebyTime(double now)
             vmax = std::max(vmax, (v - 1) / c1);
         }
     f << now << " " << pmax << " " << smax << " " << umax << " " << vmax << std::endl;
+}
+
+// outputThincknessByTime (src/WENOFV.cpp:3049-3108) for SHARP: 1 / the largest jump of z1
+// between neighbouring cells in x or y (the right and upper neighbours, wrapped periodically
+// as the reference's ghost cells are), an interface thickness in cells, appended to
+// thincknessByTime.plt under the reference's file and column names
+void CWENOFV::outputThicknessByTime(double now)
+{
+    const std::string filename = m_outputDir + "thincknessByTime.plt";
+    const bool exists = std::filesystem::exists(filename);
+    std::ofstream f(filename, std::ios::app);
+    if (!f) throw std::runtime_error("cannot write " + filename);
+    if (!exists) f << "TITLE=FvSolution" << std::endl << "VARIABLES=time thinckness\n" << std::endl << "ZONE T=TA" << std::endl;
+    const int nx = m_worldElemNumX, ny = m_worldElemNumY;
+    auto z1 = [&](int i, int j) { return volume_frac(*equation, &m_Uh[((size_t)(i % nx) * ny + (j % ny)) * m_varNum]); };
+    double maxDiff = 0;
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++) {
+            const double z = z1(i, j);
+            maxDiff = std::max(maxDiff, std::max(std::fabs(z - z1(i + 1, j)), std::fabs(z - z1(i, j + 1))));
+        }
+    f << now << " " << 1.0 / maxDiff << std::endl;
+}
+
+// outputSymmetryErr (src/WENOFV.cpp:3109-3151) for RTI: the largest difference of z1 between
+// each cell of the left half and its mirror image across x = (xL + xR) / 2, appended to
+// symmetry_err.plt (no header, as the reference writes it; its running maximum starts
+// uninitialised there and at 0 here)
+void CWENOFV::outputSymmetryErr(double now)
+{
+    std::ofstream f(m_outputDir + "symmetry_err.plt", std::ios::app);
+    if (!f) throw std::runtime_error("cannot write " + m_outputDir + "symmetry_err.plt");
+    const int nx = m_worldElemNumX, ny = m_worldElemNumY;
+    double maxErr = 0;
+    for (int i = 0; i < nx / 2; i++)
+        for (int j = 0; j < ny; j++) {
+            const double a = volume_frac(*equation, &m_Uh[((size_t)i * ny + j) * m_varNum]);
+            const double b = volume_frac(*equation, &m_Uh[((size_t)(nx - 1 - i) * ny + j) * m_varNum]);
+            maxErr = std::max(maxErr, std::fabs(a - b));
+        }
+    f << now << " " << maxErr << std::endl;
 }
 
 // outputPressureByTime (src/WENOFV.cpp:2942-3048) for DAMBREAK: the pressure on the left wall
@@ -442,7 +489,7 @@ void CWENOFV::run()
     outputResults(0, m_now, "initial");
     const auto t1 = std::chrono::steady_clock::now();
     const bool hostLoop = opt("STEPMODE", "0") == "1";
-    const bool byTime = !m_outputDir.empty() && (m_testcase == SHARP || m_testcase == DAMBREAK); // the series built here
+    const bool byTime = !m_outputDir.empty() && (m_testcase == SHARP || m_testcase == DAMBREAK || m_testcase == RTI);
     for (size_t k = 1; k < m_timeMoments.size(); k++) {
         const double targetTime = m_timeMoments[k];
         if (hostLoop) {
