@@ -64,15 +64,12 @@ def flops_per_cell_stage(name: str) -> float:
     raise KeyError(name)
 
 
-def workload(name: str, wb, form: int):
-    """(U0, config, eq, description dict) of a named workload"""
+def workload_desc(name: str) -> dict:
+    """the description of a named workload (its `config` in the JSON line, both arms)"""
     if name in ("column1024", "column1024_exp", "column1024_prim3"):
         sch = 2 if name == "column1024_exp" else 1
         rec = 4 if name == "column1024_prim3" else 1
-        U0, prm = cases.liquid_column(1024, 1024, seed=3)
-        cfg = wb.make_config(1024, 1024, rk=2, cfl=0.5, scheme=sch, limiter=1, flux=1, recon=rec, precision=form)
-        eq = wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"])
-        desc = dict(workload="liquid_column_1024_ref_eos" + {"column1024": "", "column1024_exp": "_wenoexp",
+        return dict(workload="liquid_column_1024_ref_eos" + {"column1024": "", "column1024_exp": "_wenoexp",
                                                              "column1024_prim3": "_primitive3"}[name], grid="1024x1024",
                     equation="two-phase 3-equation, linear EOS "
                     "linearised from stiffened gas (g1=4.4, pinf1=6e3, g2=1.4, pinf2=0) at p=1, density ratio 1000",
@@ -80,39 +77,62 @@ def workload(name: str, wb, form: int):
                     flux="HLLC", reconstruction="primitive3 (z1, p, u, v)" if rec == 4 else "characteristic", limiter=True,
                     rk="SSP-RK3", cfl=0.5, ic="disk r=0.2 tanh-smoothed over 2 cells, eps=1e-6, seeded periodic "
                     "Gaussian velocity field amplitude 1e-2 (seed 3)")
-    elif name == "column1024_sg":
-        U0, prm = cases.sg_column(1024, 1024, seed=3)
-        cfg = wb.make_config(1024, 1024, rk=2, cfl=0.5, scheme=1, limiter=1, flux=1, recon=1, precision=form)
-        eq = wb.make_eq(kind=wb.EQ_TWO_PHASE_SG, rho10=prm["rho10"], rho20=prm["rho20"], preb=prm["preb"],
-                        gamma1=prm["gamma1"], pinf1=prm["pinf1"], gamma2=prm["gamma2"], pinf2=prm["pinf2"])
-        desc = dict(workload="liquid_column_1024_stiffened_gas", grid="1024x1024",
+    if name == "column1024_sg":
+        return dict(workload="liquid_column_1024_stiffened_gas", grid="1024x1024",
                     equation="two-phase 3-equation, stiffened-gas phases on their isentropes (g1=4.4, pinf1=6e3; "
                     "g2=1.4, pinf2=0) through p=1, density ratio 1000, Newton pressure equilibrium",
                     bc="periodic", scheme="WENO-Z", flux="HLLC", reconstruction="characteristic", limiter=True,
                     rk="SSP-RK3", cfl=0.5, ic="disk r=0.2 tanh-smoothed over 2 cells, eps=1e-6, p=1, seeded periodic "
                     "Gaussian velocity field amplitude 1e-2 (seed 3)")
+    if name == "euler512":
+        return dict(workload="euler_quadrants_512", grid="512x512", equation="Euler gamma=1.4", bc="outflow",
+                    scheme="WENO-Z", flux="HLLC", reconstruction="conservative", limiter=False, rk="SSP-RK3", cfl=0.4,
+                    ic="four quadrants, (rho,u,v,p) from seed 2")
+    if name == "advection128":
+        return dict(workload="linear_advection_128", grid="128x128", equation="u_t+u_x+u_y=0", bc="periodic",
+                    scheme="WENO-JS", flux="LLF", reconstruction="conservative", limiter=False, rk="SSP-RK3", cfl=0.5,
+                    ic="sin(2 pi (x+y))")
+    raise SystemExit(f"unknown workload {name}")
+
+
+def workload_config(name: str, form: str, world: int) -> dict:
+    """the `config` object of the JSON line: identical in the GPU arm and the reference arm"""
+    return dict(workload_desc(name), form=form, l2="flushed between steps by a 256 MiB write outside the timed events",
+                parallelism=f"replicas x{world}")
+
+
+def workload(name: str, wb, form: int):
+    """(U0, config, eq, description dict) of a named workload"""
+    desc = workload_desc(name)
+    if name in ("column1024", "column1024_exp", "column1024_prim3"):
+        sch = 2 if name == "column1024_exp" else 1
+        rec = 4 if name == "column1024_prim3" else 1
+        U0, prm = cases.liquid_column(1024, 1024, seed=3)
+        cfg = wb.make_config(1024, 1024, rk=2, cfl=0.5, scheme=sch, limiter=1, flux=1, recon=rec, precision=form)
+        eq = wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"])
+    elif name == "column1024_sg":
+        U0, prm = cases.sg_column(1024, 1024, seed=3)
+        cfg = wb.make_config(1024, 1024, rk=2, cfl=0.5, scheme=1, limiter=1, flux=1, recon=1, precision=form)
+        eq = wb.make_eq(kind=wb.EQ_TWO_PHASE_SG, rho10=prm["rho10"], rho20=prm["rho20"], preb=prm["preb"],
+                        gamma1=prm["gamma1"], pinf1=prm["pinf1"], gamma2=prm["gamma2"], pinf2=prm["pinf2"])
     elif name == "euler512":
         U0, _ = cases.euler_quadrants(512, 512, seed=2)
         cfg = wb.make_config(512, 512, bc=wb.BC_OUTFLOW, rk=2, cfl=0.4, scheme=1, flux=1, recon=0, precision=form)
         eq = wb.make_eq(kind=wb.EQ_EULER, gamma=1.4)
-        desc = dict(workload="euler_quadrants_512", grid="512x512", equation="Euler gamma=1.4", bc="outflow",
-                    scheme="WENO-Z", flux="HLLC", reconstruction="conservative", limiter=False, rk="SSP-RK3", cfl=0.4,
-                    ic="four quadrants, (rho,u,v,p) from seed 2")
-    elif name == "advection128":
+    else:  # advection128
         U0 = cases.advection_sine(128, 128)
         cfg = wb.make_config(128, 128, rk=2, cfl=0.5, scheme=0, flux=0, recon=0, precision=form)
         eq = wb.make_eq(kind=wb.EQ_LINEAR_ADV)
-        desc = dict(workload="linear_advection_128", grid="128x128", equation="u_t+u_x+u_y=0", bc="periodic",
-                    scheme="WENO-JS", flux="LLF", reconstruction="conservative", limiter=False, rk="SSP-RK3", cfl=0.5,
-                    ic="sin(2 pi (x+y))")
-    else:
-        raise SystemExit(f"unknown workload {name}")
     return U0, cfg, eq, desc
 
 
 # ---- host CPU baseline ------------------------------------------------------------------------
-def cpu_baseline(name: str, steps: int, warmup: int, sample_n: int = 256):
-    """The reference (or, where it cannot run the workload, the oracle port) on the host cores."""
+def cpu_baseline(name: str, steps: int, warmup: int, sample_n: int = 1024, single_core: bool = False):
+    """The reference (or, where it cannot run the workload, the oracle port) on the host cores.
+
+    The reference runs the workload at its full size (sample_n = 1024 for the columns): as
+    many concurrent processes as the host has groups of 4 cores, each the unmodified solver
+    with its 4 slab ranks on 4 threads, each timing `steps` SSP-RK3 steps after `warmup`."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
@@ -120,19 +140,23 @@ def cpu_baseline(name: str, steps: int, warmup: int, sample_n: int = 256):
     sch = "2" if name == "column1024_exp" else "1"
     rec = "4" if name == "column1024_prim3" else "1"
     if name in ("column1024", "column1024_exp", "column1024_prim3") and O.reference_available():
-        U0, prm = cases.liquid_column(sample_n, sample_n, seed=3)
-        nproc = max(1, ncores // 4)
-        with tempfile.TemporaryDirectory() as d:
-            U0.tofile(os.path.join(d, "u0.bin"))
-            args = [O.REF_BIN, "--testcase", "2", "--nx", str(sample_n), "--ny", str(sample_n), "--rk", "2",
+        def ref_args(n, d, U, nsteps, nwarm):
+            U.tofile(os.path.join(d, "u0.bin"))
+            prm = cases.column_params()
+            return [O.REF_BIN, "--testcase", "2", "--nx", str(n), "--ny", str(n), "--rk", "2",
                     "--cfl", "0.5", "--scheme", sch, "--limiter", "1", "--flux", "1", "--recon", rec,
                     "--rho10", O._f(prm["rho10"]), "--rho20", O._f(prm["rho20"]), "--sound1", O._f(prm["sound1"]),
-                    "--sound2", O._f(prm["sound2"]), "--u0", os.path.join(d, "u0.bin"), "--steps", str(steps),
-                    "--warmup", str(warmup), "--time"]
+                    "--sound2", O._f(prm["sound2"]), "--u0", os.path.join(d, "u0.bin"), "--steps", str(nsteps),
+                    "--warmup", str(nwarm), "--time"]
+
+        U0, _ = cases.liquid_column(sample_n, sample_n, seed=3)
+        nproc = max(1, ncores // 4)
+        with tempfile.TemporaryDirectory() as d:
+            args = ref_args(sample_n, d, U0, steps, warmup)
             t0 = time.perf_counter()
             procs = [subprocess.Popen(args, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
                      for _ in range(nproc)]
-            outs = [pr.communicate(timeout=1800) for pr in procs]
+            outs = [pr.communicate(timeout=3600) for pr in procs]
             wall = time.perf_counter() - t0
             secs = []
             for (o, e), pr in zip(outs, procs):
@@ -141,25 +165,25 @@ def cpu_baseline(name: str, steps: int, warmup: int, sample_n: int = 256):
                 secs.append(json.loads(o.strip().splitlines()[-1])["seconds"])
         units = nproc * sample_n * sample_n * 3 * steps
         single = None
-        if shutil.which("taskset"):
-            # the same reference process pinned to one core (its 4 slab ranks share it)
+        if single_core and shutil.which("taskset"):
+            # one reference process pinned to one core (its 4 slab ranks share it), 256^2
             with tempfile.TemporaryDirectory() as d1:
-                U0.tofile(os.path.join(d1, "u0.bin"))
-                a1 = list(args)
-                a1[a1.index("--u0") + 1] = os.path.join(d1, "u0.bin")
-                a1[a1.index("--steps") + 1] = "2"
-                cp = subprocess.run(["taskset", "-c", "0"] + a1, capture_output=True, text=True, timeout=1800)
+                U1, _ = cases.liquid_column(256, 256, seed=3)
+                cp = subprocess.run(["taskset", "-c", "0"] + ref_args(256, d1, U1, 1, 0), capture_output=True,
+                                    text=True, timeout=1800)
                 if cp.returncode == 0:
                     s1 = json.loads(cp.stdout.strip().splitlines()[-1])["seconds"]
-                    single = dict(value=sample_n * sample_n * 3 * 2 / s1, cores=1, steps=2)
+                    single = dict(value=256 * 256 * 3 / s1, cores=1, steps=1, grid="256x256")
         return dict(value=units / max(secs), unit="cell-stage updates/s", cores=4 * nproc, kind="reference",
-                    single_core=single,
+                    single_core=single, steps=steps, warmup=warmup,
                     sample=f"{nproc} concurrent processes of the unmodified reference (4 slab ranks each, "
-                           f"threads over an in-process MPI shim), {steps} timed SSP-RK3 steps after {warmup} "
-                           f"warm-up steps each, on the same workload at {sample_n}x{sample_n} "
-                           f"(same equation, options and initial data); {ncores} host cores; wall {wall:.1f} s",
+                           f"threads over an in-process MPI shim) on the same workload at its full size "
+                           f"{sample_n}x{sample_n} (same equation, options and initial data), {steps} timed "
+                           f"SSP-RK3 step(s) after {warmup} warm-up step(s) each; {ncores} host cores; "
+                           f"wall {wall:.1f} s",
                     seconds=max(secs))
     # the oracle port on all host threads (the reference has no Euler or scalar advection)
+    sample_n = min(sample_n, 256)
     if name == "euler512":
         U0, _ = cases.euler_quadrants(sample_n, sample_n, seed=2)
         p = O.Problem(nx=sample_n, ny=sample_n, bc=O.BC_OUTFLOW, eq_kind=O.EQ_EULER, rk=2, cfl=0.4, scheme=1,
@@ -368,6 +392,8 @@ def run_ours(args, rank, world, dist):
     hbm_peak = measured.get("hbm_gbs", 6650.0)
     roofline = dict(bound="fp32" if form == wb.FP32_BULK else "fp64", achieved=achieved_tf, peak=peak,
                     unit="TFLOP/s", frac=achieved_tf / peak, traffic=read_traffic(args.workload),
+                    traffic_source=f"not measured live: DRAM bytes read + written per stage launch from one ncu "
+                                   f"capture of this command, committed in profiles/stage_kernel_{args.workload}.md",
                     kernel="wenofv::stage_kernel", launch_ms=launch_ms, flops_per_launch=fpcs * ncells,
                     flops_per_cell_stage=fpcs,
                     peak_source=f"FMA throughput of the {'FP32' if form == wb.FP32_BULK else 'FP64'} CUDA-core pipe "
@@ -379,22 +405,61 @@ def run_ours(args, rank, world, dist):
                steps=args.steps, warmup=args.warmup, ms_per_step=total_ms / args.steps, higher_is_better=True,
                scaling="weak", vs_baseline=None,
                dtype={"fp64": "f64", "fp64_strict": "f64", "fp32_bulk": "f32+f64"}[args.form], data="synthetic",
-               config=dict(desc, form=args.form, l2="flushed between steps by a 256 MiB write outside the timed "
-                           "events", parallelism=f"replicas x{world}"),
+               config=workload_config(args.workload, args.form, world),
                roofline=roofline, e2e=e2e, gpu_launches=args.steps * nstages, status_flags=flags)
     if fp32:
         fp32["roofline"] = dict(bound="fp64+fp32", achieved=fpcs * ncells / (fp32["launch_ms"] * 1e-3) / 1e12,
                                 unit="TFLOP/s", note="counted flops of the FP64 algorithm per launch / launch time; "
                                 "the FP32-bulk form mixes both pipes, so no single peak bounds it")
+        fp32["speedup_vs_fp64_per_launch"] = launch_ms / fp32["launch_ms"]
         out["fp32_bulk"] = fp32
     out["clocks"] = clk.summary()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(args.workload, steps=args.cpu_steps, warmup=1)
+        out["cpu_baseline"] = cpu_baseline(args.workload, steps=args.cpu_steps, warmup=0)
     s.close()
     return out
 
 
+def run_steps(wb, cfg, eq, U0, dt, nsteps, precision):
+    """the state after nsteps manual RK steps of fixed dt in the given form"""
+    c = wb.Config.from_buffer_copy(cfg)
+    c.precision = precision
+    with wb.Solver(c, eq) as s:
+        s.upload(U0)
+        for _ in range(nsteps):
+            s.step(dt)
+        return s.download()
+
+
+def rel_l1(a, b):
+    return float(np.abs(a - b).sum() / np.abs(b).sum())
+
+
+def oracle_check(wb, cfg, eq, U0, dt, nsteps, threads):
+    """FP64_STRICT against the CPU oracle over the first nsteps steps of the same run: the
+    strict form is the oracle's arithmetic bit for bit, so it stands in for the oracle over
+    the whole run (the oracle at full size takes seconds per step)"""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    strict = run_steps(wb, cfg, eq, U0, dt, nsteps, wb.FP64_STRICT)
+    p = O.Problem(nx=cfg.nx, ny=cfg.ny, xl=cfg.xl, xr=cfg.xr, yl=cfg.yl, yr=cfg.yr, bc=cfg.bc, rk=cfg.rk_method,
+                  cfl=cfg.cfl, scheme=cfg.scheme, limiter=cfg.pp_limiter, flux=cfg.riemann_flux,
+                  recon=cfg.reconstruction, ref_slabs=cfg.ref_slabs, threads=threads, eq_kind=eq.eq_kind,
+                  rho10=eq.rho10, rho20=eq.rho20, sound1=eq.sound1, sound2=eq.sound2, gamma=eq.gamma)
+    orc = O.Oracle()
+    V = U0
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        V = orc.step(p, V, dt)
+    return dict(steps=nsteps, bit_identical=bool(np.array_equal(strict, V)), oracle_threads=threads,
+                oracle_seconds=time.perf_counter() - t0)
+
+
 def compare_fp32(args, wb, cfg, eq, U0, dt, U64, ncells, nstages, flush, barrier, dist, world, local):
+    """FP32-bulk beside FP64: the same steps from the same state and dt, device-timed the same
+    way; its error, and the FP64 form's, against the FP64 oracle's arithmetic (FP64_STRICT on the
+    device, checked bit for bit against the CPU oracle over a prefix of the same run)"""
     import torch
 
     cfg32 = wb.Config.from_buffer_copy(cfg)
@@ -422,14 +487,23 @@ def compare_fp32(args, wb, cfg, eq, U0, dt, U64, ncells, nstages, flush, barrier
     U32 = s.download()
     flags, _ = s.status()
     s.close()
-    per = [float(np.abs(U32[v] - U64[v]).sum() / max(np.abs(U64[v]).sum(), 1e-300)) for v in range(U64.shape[0])]
-    return dict(value=world * ncells * nstages * args.steps / (total_ms * 1e-3), unit="cell-stage updates/s",
-                ms_per_step=total_ms / args.steps, launch_ms=total_ms / (args.steps * nstages),
-                gpu_launches=args.steps * nstages,
-                rel_l1_vs_fp64=float(np.abs(U32 - U64).sum() / np.abs(U64).sum()), rel_l1_vs_fp64_per_var=per,
-                error_note=f"relative L1 of the FP32-bulk state against the FP64 state after the same "
-                           f"{args.warmup + args.steps} steps from the same initial data and dt",
-                status_flags=flags)
+    nsteps = args.warmup + args.steps
+    Ustrict = run_steps(wb, cfg, eq, U0, dt, nsteps, wb.FP64_STRICT)
+    per = [float(np.abs(U32[v] - Ustrict[v]).sum() / max(np.abs(Ustrict[v]).sum(), 1e-300)) for v in range(U64.shape[0])]
+    out = dict(value=world * ncells * nstages * args.steps / (total_ms * 1e-3), unit="cell-stage updates/s",
+               ms_per_step=total_ms / args.steps, launch_ms=total_ms / (args.steps * nstages),
+               gpu_launches=args.steps * nstages,
+               speedup_vs_fp64_per_launch=None,
+               rel_l1_vs_oracle=rel_l1(U32, Ustrict), rel_l1_vs_oracle_per_var=per,
+               fp64_rel_l1_vs_oracle=rel_l1(U64, Ustrict), rel_l1_vs_fp64=rel_l1(U32, U64),
+               min_partial_density=[float(U32[0].min()), float(U32[1].min())] if U32.shape[0] == 4 else None,
+               error_note=f"pooled relative L1 of the final state after the same {nsteps} steps from the same "
+                          f"initial data and dt, against the FP64 oracle's arithmetic (FP64_STRICT on the device; "
+                          f"see oracle_check) and, for the spread of the scheme's own roundoff, the FP64 form's",
+               status_flags=flags)
+    if not args.no_oracle_check:
+        out["oracle_check"] = oracle_check(wb, cfg, eq, U0, dt, 2, os.cpu_count() or 1)
+    return out
 
 
 def _load_package():
@@ -601,13 +675,22 @@ def run_serve(args, rank, world, dist):
 
 
 def run_reference_arm(args):
-    cb = cpu_baseline(args.workload, steps=max(1, args.steps), warmup=args.warmup)
+    """the reference's CPU implementation on the same workload and config as the GPU arm.  At
+    1024^2 one reference step takes tens of seconds, so the arm times a bounded prefix: at most
+    REF_MAX_STEPS steps after at most one warm-up step (the line's steps and warmup say what ran)."""
+    REF_MAX_STEPS = 2
+    steps = max(1, min(args.steps, REF_MAX_STEPS))
+    warmup = min(args.warmup, 1)
+    cb = cpu_baseline(args.workload, steps=steps, warmup=warmup, single_core=True)
     return dict(metric="cell-stage updates/s", value=cb["value"], unit="cell-stage updates/s", n_gpus=args.gpus,
-                steps=args.steps, warmup=args.warmup, ms_per_step=1e3 * cb["seconds"] / max(1, args.steps),
+                steps=steps, warmup=warmup, ms_per_step=1e3 * cb["seconds"] / steps,
                 higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
-                impl="reference", config=dict(workload=args.workload, sample=cb["sample"]),
+                impl="reference", config=workload_config(args.workload, args.form, args.gpus),
+                requested=dict(steps=args.steps, warmup=args.warmup,
+                               note=f"bounded prefix: {steps} timed step(s) after {warmup} warm-up step(s) of the "
+                                    f"full-size workload on every reference process"),
                 cpu_baseline=dict(value=cb["value"], unit=cb["unit"], cores=cb["cores"], kind=cb["kind"],
-                                  sample=cb["sample"]),
+                                  sample=cb["sample"], single_core=cb.get("single_core")),
                 e2e=dict(value=cb["value"], unit=cb["unit"], h2d_bytes_per_step=0, d2h_bytes_per_step=0))
 
 
@@ -625,9 +708,10 @@ def main():
     ap.add_argument("--max-steps", type=int, default=2000, help="serve: most steps of a request")
     ap.add_argument("--hbm-budget-gb", type=int, default=150, help="serve: HBM budget of the server")
     ap.add_argument("--form", default="fp64", choices=["fp64", "fp64_strict", "fp32_bulk"])
-    ap.add_argument("--cpu-steps", type=int, default=12)
+    ap.add_argument("--cpu-steps", type=int, default=1, help="timed reference steps of the cpu_baseline leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-bulk comparison of the FP64 form")
+    ap.add_argument("--no-oracle-check", action="store_true", help="skip the CPU oracle check of the strict form")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 

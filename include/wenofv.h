@@ -171,6 +171,20 @@ void *wenofv_stream(wenofv_ctx *ctx);
 /* device pointer of the current interior state, SoA with row pitch *pitch doubles and
  * plane stride pitch*ny (valid until the next step) */
 int wenofv_device_state(wenofv_ctx *ctx, double **U, int *pitch);
+/* the per-cell record of useBoundPreservingLimiter (src/WENOFV.cpp:1906-1909), m_totalTheta
+ * as getWorldTheta gathers it for the theta column of outputAve / outputSliceAve
+ * (src/WENOFV.cpp:2587, :2725): out[cell] = 1 where the final RK stage of the latest step
+ * limited the cell (theta < 1 - 1e-8), else 0; nx*ny bytes, [j][i] (SOA) or [i][j]
+ * (REF_AOS).  All 0 without PPlimiter (the reference never writes it then). */
+int wenofv_theta_flags(wenofv_ctx *ctx, uint8_t *out, int layout);
+/* Asynchronous snapshot of the current state for output (the gathers of outputResults,
+ * src/WENOFV.cpp:2447-2523): the state is copied on the device at this point of the
+ * context's stream, then read back into host on a separate copy stream, so the read-back
+ * overlaps later steps.  host must stay valid until wenofv_snapshot_wait returns (pinned
+ * memory makes the copy a DMA; pageable memory is also accepted).  One snapshot in flight
+ * per context (WENOFV_EBUSY otherwise). */
+int wenofv_snapshot_begin(wenofv_ctx *ctx, double *host, int layout);
+int wenofv_snapshot_wait(wenofv_ctx *ctx);
 
 /* The reference's periodic test cases (TESTCASE 0 SMOOTH, 1 VORTEX, 2 SHARP) with the
  * velocity and volume-fraction floor of TwoPhaseEquation::setEquationParameters
@@ -200,7 +214,9 @@ int wenofv_accuracy(wenofv_ctx *ctx, const wenofv_testcase *tc, double t, double
  * the array: calls whose work overlaps on the GPU race.  The call synchronises `stream`
  * (a cudaStream_t, NULL = default stream) once after its host-to-device set-up copies, and
  * again at the end when flags is non-NULL (then *flags receives the WENOFV_FLAG_* word).
- * No counterpart in the reference. */
+ * The caller's current device is the same on return as on entry.  The step takes dt from the
+ * caller (finite, >= 0) and does not return the CFL step of the new state: a caller that
+ * needs it calls wenofv_compute_dt on a context.  No counterpart in the reference. */
 int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_params *eq, const double *d_U, double *d_U_next,
                         int pitch, double dt, void *stream, uint32_t *flags);
 

@@ -15,6 +15,9 @@
 //                   [--rhs FILE]       one assembleRHS of the initial state, SoA FP64
 //                   [--faces FILE]     face states after that assembleRHS [cell][B,T,L,R][v][gp]
 //                   [--out FILE] [--dts FILE] [--time]
+//                   [--output-ave DIR] after the steps, the reference's own outputAve("final") and
+//                                      outputSliceAve("final") into DIR (average_final.plt,
+//                                      slice_final.plt), to compare the host mirror's files with
 //                   [--source-case N]  after initialisation, the test case that assembleSourceTerm
 //                                      sees (DAMBREAK/RTI: g = 9.81, STANDING_WAVE: 2 pi), so that
 //                                      its gravity runs on a periodic case's grid and boundaries
@@ -42,7 +45,7 @@ namespace {
 struct Args {
     std::map<std::string, std::string> opt;
     double rho10 = -1, rho20 = -1, sound1 = -1, sound2 = -1;
-    std::string u0, dump_u0, rhs, faces, out, dts;
+    std::string u0, dump_u0, rhs, faces, out, dts, output_ave;
     long steps = -1, warmup = 0;
     double tend = -1;
     bool time = false;
@@ -147,6 +150,11 @@ void rank_main(int rank, const Args &a, Shared &sh, const std::vector<double> &u
         for (int ej = solver.m_startElemY; ej != solver.m_endElemY; ++ej)
             for (int v = 0; v < nv; ++v)
                 sh.U[idx(v, ej - solver.m_startElemY, x0 + ei - solver.m_startElemX)] = solver.m_Uh[ei][ej].vector[v];
+    if (!a.output_ave.empty()) { // every rank takes part in the gathers; rank 0 writes
+        solver.m_outputDir = a.output_ave + "/";
+        solver.outputAve("final");
+        solver.outputSliceAve("final");
+    }
 }
 
 } // namespace
@@ -180,13 +188,14 @@ int main(int argc, char **argv)
         else if (s == "--tend") { a.tend = std::atof(val); k++; }
         else if (s == "--time") { a.time = true; }
         else if (s == "--source-case") { a.source_case = std::atoi(val); k++; }
+        else if (s == "--output-ave") { a.output_ave = val; k++; }
         else { std::fprintf(stderr, "unknown argument %s\n", s.c_str()); return 2; }
     }
     if (a.steps < 0 && a.tend <= 0) a.steps = 0;
 
     // absolute paths before leaving the caller's directory
     auto absp = [](std::string &p) { if (!p.empty()) p = std::filesystem::absolute(p).string(); };
-    absp(a.u0); absp(a.dump_u0); absp(a.rhs); absp(a.faces); absp(a.out); absp(a.dts);
+    absp(a.u0); absp(a.dump_u0); absp(a.rhs); absp(a.faces); absp(a.out); absp(a.dts); absp(a.output_ave);
 
     Shared sh;
     sh.nx = std::atoi(a.opt["ELEMNUMX"].c_str());

@@ -169,11 +169,39 @@ def test_host_writes_the_reference_output_files(host_bin, tmp_path):
     assert lines[0] == "TITLE=FvSolution" and lines[1].split()[:4] == ["VARIABLES=X", "Y", "RHO1Z1", "RHO2Z2"]
     assert lines[2].startswith("ZONE T=TA, I=100, J=100")
     rows = [list(map(float, ln.split())) for ln in lines[3:]]
-    assert len(rows) == 100 * 100 and all(len(r) == 11 for r in rows)
+    assert len(rows) == 100 * 100 and all(len(r) == 13 for r in rows)  # ... PRE theta Pr
     acc = (out / "accuracy_final.csv").read_text().splitlines()
     assert acc[0] == "Cell Number, Linf-norm, L1-norm, L2-norm"
     vals = [float(x) for x in acc[1].split(",")]
     assert vals[0] == 100 and np.allclose(vals[1:], SMOOTH_KNOWN[0][1], rtol=1e-6, atol=0)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not reference_available(), reason="the compiled reference binary is not present")
+@pytest.mark.parametrize("recon", [1, 0])
+def test_host_output_files_equal_reference(host_bin, tmp_path, recon):
+    """average_final.plt and slice_final.plt of the mirror against the files the compiled
+    reference's own outputAve / outputSliceAve write on the same run (SHARP 32^2 to t = 0.01 with
+    the limiter, which limits some cells there, so the theta column is exercised)"""
+    nx, tend = 32, 0.01
+    out = tmp_path / "mine"
+    cp = run_host(host_bin, "TESTCASE=2", f"ELEMNUMX={nx}", f"ELEMNUMY={nx}", "PRECISION=FP64_STRICT", "REFSLABS=4",
+                  f"ENDTIME={tend}", f"RECONSTRUCTIONTYPE={recon}", "RIEMANNFLUX=1", "PPlimiter=1", "SCHEME=1",
+                  f"OUTPUTDIR={out}", "SLICEOUTPUT=1")
+    assert cp.returncode == 0, cp.stderr
+    ref = tmp_path / "ref"
+    ref.mkdir()
+    from oracle import REF_BIN
+    rp = subprocess.run([REF_BIN, "--testcase", "2", "--nx", str(nx), "--ny", str(nx), "--rk", "2", "--cfl", "0.5",
+                         "--scheme", "1", "--limiter", "1", "--flux", "1", "--recon", str(recon), "--tend", repr(tend),
+                         "--output-ave", str(ref)], capture_output=True, text=True, timeout=600)
+    assert rp.returncode == 0, rp.stderr[-2000:]
+    for name in ("average_final.plt", "slice_final.plt"):
+        a = (out / name).read_text().splitlines()
+        b = (ref / name).read_text().splitlines()
+        assert [x.rstrip() for x in a] == [x.rstrip() for x in b], name
+    theta = [int(float(ln.split()[11])) for ln in (ref / "average_final.plt").read_text().splitlines()[3:]]
+    assert 0 < sum(theta) < nx * nx  # some cells limited, not all
 
 
 # the periodic cases' (u0, v0, epsa): include/Equations.hpp:490-689

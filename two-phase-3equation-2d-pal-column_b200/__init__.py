@@ -30,7 +30,8 @@ EXPORTS = (
     "wenofv_abi_version", "wenofv_strerror", "wenofv_last_error", "wenofv_default_config",
     "wenofv_create", "wenofv_destroy", "wenofv_upload", "wenofv_set_frame", "wenofv_download", "wenofv_compute_dt",
     "wenofv_step", "wenofv_rhs", "wenofv_advance", "wenofv_status", "wenofv_synchronize",
-    "wenofv_stream", "wenofv_device_state", "wenofv_step_noalloc", "wenofv_init_testcase", "wenofv_accuracy",
+    "wenofv_stream", "wenofv_device_state", "wenofv_theta_flags", "wenofv_snapshot_begin", "wenofv_snapshot_wait",
+    "wenofv_step_noalloc", "wenofv_init_testcase", "wenofv_accuracy",
     "wenofv_batch_create", "wenofv_batch_destroy", "wenofv_batch_upload", "wenofv_batch_set_frame", "wenofv_batch_download",
     "wenofv_batch_advance", "wenofv_batch_set_tiling", "wenofv_batch_stream", "wenofv_batch_autotune",
     "wenofv_server_create", "wenofv_server_destroy", "wenofv_server_submit", "wenofv_server_poll",
@@ -110,6 +111,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.wenofv_stream.restype = P
     L.wenofv_stream.argtypes = [P]
     L.wenofv_device_state.argtypes = [P, C.POINTER(P), C.POINTER(I)]
+    L.wenofv_theta_flags.argtypes = [P, C.POINTER(C.c_uint8), I]
+    L.wenofv_snapshot_begin.argtypes = [P, DP, I]
+    L.wenofv_snapshot_wait.argtypes = [P]
     L.wenofv_batch_create.argtypes = [I, C.POINTER(Config), C.POINTER(EqParams), C.POINTER(P)]
     L.wenofv_batch_destroy.argtypes = [P]
     L.wenofv_batch_upload.argtypes = [P, I, DP, I]
@@ -257,6 +261,24 @@ class Solver:
 
     def stream(self) -> int:
         return self.L.wenofv_stream(self.h) or 0
+
+    def theta_flags(self, layout=LAYOUT_SOA) -> np.ndarray:
+        """the final stage's per-cell limiter record (1 where theta < 1 - 1e-8)"""
+        out = np.zeros((self.cfg.ny, self.cfg.nx) if layout == LAYOUT_SOA else (self.cfg.nx, self.cfg.ny), np.uint8)
+        _check(self.L.wenofv_theta_flags(self.h, out.ctypes.data_as(C.POINTER(C.c_uint8)), layout), "wenofv_theta_flags")
+        return out
+
+    def snapshot_begin(self, out: np.ndarray, layout=LAYOUT_SOA):
+        """asynchronous copy of the current state into out (kept alive until snapshot_wait)"""
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != int(np.prod(self.shape)):
+            raise ValueError("need a C-contiguous float64 array of the state's size")
+        self._snap = out
+        _check(self.L.wenofv_snapshot_begin(self.h, _dp(out), layout), "wenofv_snapshot_begin")
+
+    def snapshot_wait(self) -> np.ndarray:
+        _check(self.L.wenofv_snapshot_wait(self.h), "wenofv_snapshot_wait")
+        out, self._snap = getattr(self, "_snap", None), None
+        return out
 
     def device_state(self):
         p = C.c_void_p()

@@ -102,6 +102,24 @@ int wenofv_download(wenofv_ctx *ctx, double *U, int layout)
     if (!ctx) { set_error("null context"); return WENOFV_EINVAL; }
     return ctx->eng.download(0, U, layout);
 }
+int wenofv_theta_flags(wenofv_ctx *ctx, uint8_t *out, int layout)
+{
+    if (!ctx) { set_error("null context"); return WENOFV_EINVAL; }
+    return ctx->eng.theta_flags(0, out, layout);
+}
+
+int wenofv_snapshot_begin(wenofv_ctx *ctx, double *host, int layout)
+{
+    if (!ctx) { set_error("null context"); return WENOFV_EINVAL; }
+    return ctx->eng.snapshot_begin(0, host, layout);
+}
+
+int wenofv_snapshot_wait(wenofv_ctx *ctx)
+{
+    if (!ctx) { set_error("null context"); return WENOFV_EINVAL; }
+    return ctx->eng.snapshot_wait();
+}
+
 int wenofv_compute_dt(wenofv_ctx *ctx, double *dt)
 {
     if (!ctx || !dt) { set_error("null argument"); return WENOFV_EINVAL; }

@@ -168,6 +168,7 @@ Engine::~Engine()
 {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
+    if (copy_stream_) cudaStreamSynchronize(copy_stream_);
     drop_graphs();
     free_work();
     for (int i = 0; i < cap_; i++) free_instance(i);
@@ -176,6 +177,11 @@ Engine::~Engine()
     cudaFree(d_rhs_);
     if (h_state_) cudaFreeHost(h_state_);
     if (h_stage_) cudaFreeHost(h_stage_);
+    cudaFree(d_snap_);
+    if (h_snap_) cudaFreeHost(h_snap_);
+    if (snap_ready_) cudaEventDestroy(snap_ready_);
+    if (snap_done_) cudaEventDestroy(snap_done_);
+    if (copy_stream_) cudaStreamDestroy(copy_stream_);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -203,6 +209,7 @@ int Engine::init_slots(int capacity, int dev, int rk_method)
     dmem_.assign(cap_, nullptr);
     dmetric_.assign(cap_, nullptr);
     dframe_.assign(cap_, nullptr);
+    dtheta_.assign(cap_, nullptr);
     frame_set_.assign(cap_, 0);
     live_.assign(cap_, 0);
     WENOFV_CUDA(cudaMalloc(&d_desc_, cap_ * sizeof(InstDesc)));
@@ -277,6 +284,11 @@ int Engine::alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params
         WENOFV_CUDA(cudaMalloc(&dframe_[i], frame_bytes(c, e)));
         d.frame = dframe_[i];
     }
+    if (!slot_mode && c.pp_limiter && e.eq_kind != WENOFV_EQ_LINEAR_ADV) { // the limiter's per-cell record
+        WENOFV_CUDA(cudaMalloc(&dtheta_[i], (size_t)c.nx * c.ny));
+        WENOFV_CUDA(cudaMemsetAsync(dtheta_[i], 0, (size_t)c.nx * c.ny, stream));
+        d.theta_flag = dtheta_[i];
+    }
     WENOFV_CUDA(cudaMemcpyAsync(d_desc_ + i, &d, sizeof(InstDesc), cudaMemcpyHostToDevice, stream));
     WENOFV_CUDA(cudaStreamSynchronize(stream)); // the metric staging above is a host local
     cfg_[i] = c;
@@ -293,9 +305,11 @@ void Engine::free_instance(int i)
     if (dmem_[i]) cudaFree(dmem_[i]);
     if (dmetric_[i]) cudaFree(dmetric_[i]);
     if (dframe_[i]) cudaFree(dframe_[i]);
+    if (dtheta_[i]) cudaFree(dtheta_[i]);
     dmem_[i] = nullptr;
     dmetric_[i] = nullptr;
     dframe_[i] = nullptr;
+    dtheta_[i] = nullptr;
     frame_set_[i] = 0;
     if (live_[i]) work_dirty_ = true;
     live_[i] = 0;
@@ -602,6 +616,86 @@ int Engine::download(int i, double *U, int layout)
     return WENOFV_OK;
 }
 
+int Engine::theta_flags(int i, unsigned char *out, int layout)
+{
+    if (!live(i) || !out) { set_error("bad instance index or null array"); return WENOFV_EINVAL; }
+    if (layout != WENOFV_LAYOUT_SOA && layout != WENOFV_LAYOUT_REF_AOS) { set_error("unknown layout"); return WENOFV_EINVAL; }
+    const int nx = cfg_[i].nx, ny = cfg_[i].ny;
+    if (!dtheta_[i]) { // no limiter: the record stays 0, as the reference's is never set
+        std::memset(out, 0, (size_t)nx * ny);
+        return WENOFV_OK;
+    }
+    WENOFV_CUDA(cudaSetDevice(device));
+    std::vector<unsigned char> tmp;
+    unsigned char *dst = out;
+    if (layout == WENOFV_LAYOUT_REF_AOS) {
+        tmp.resize((size_t)nx * ny);
+        dst = tmp.data();
+    }
+    WENOFV_CUDA(cudaMemcpyAsync(dst, dtheta_[i], (size_t)nx * ny, cudaMemcpyDeviceToHost, stream));
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    if (layout == WENOFV_LAYOUT_REF_AOS)
+        for (int x = 0; x < nx; x++)
+            for (int y = 0; y < ny; y++) out[(size_t)x * ny + y] = tmp[(size_t)y * nx + x];
+    return WENOFV_OK;
+}
+
+// The current state is copied on the compute stream into a snapshot buffer (device to
+// device, ~10 us for a 1024^2 two-phase state), then read back into pinned staging on a copy
+// stream, so the host-bound copy overlaps whatever the compute stream does next.
+// snapshot_wait touches only the snapshot's own members (events, staging, caller's array),
+// so a worker thread may wait for it while the owning thread keeps stepping the context.
+int Engine::snapshot_begin(int i, double *host, int layout)
+{
+    if (!live(i) || !host) { set_error("bad instance index or null array"); return WENOFV_EINVAL; }
+    if (layout != WENOFV_LAYOUT_SOA && layout != WENOFV_LAYOUT_REF_AOS) { set_error("unknown layout"); return WENOFV_EINVAL; }
+    if (snap_pending_) { set_error("a snapshot is in flight: call wenofv_snapshot_wait first"); return WENOFV_EBUSY; }
+    WENOFV_CUDA(cudaSetDevice(device));
+    const InstDesc &d = desc_[i];
+    const size_t bytes = (size_t)nvar_of(d.eq_kind) * d.ny * d.pitch * sizeof(double);
+    if (!copy_stream_) {
+        WENOFV_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+        WENOFV_CUDA(cudaEventCreateWithFlags(&snap_ready_, cudaEventDisableTiming));
+        WENOFV_CUDA(cudaEventCreateWithFlags(&snap_done_, cudaEventDisableTiming));
+    }
+    if (bytes > snap_bytes_) {
+        WENOFV_CUDA(cudaStreamSynchronize(stream));
+        WENOFV_CUDA(cudaStreamSynchronize(copy_stream_));
+        cudaFree(d_snap_);
+        if (h_snap_) cudaFreeHost(h_snap_);
+        d_snap_ = nullptr;
+        h_snap_ = nullptr;
+        snap_bytes_ = 0;
+        WENOFV_CUDA(cudaMalloc(&d_snap_, bytes));
+        WENOFV_CUDA(cudaMallocHost(&h_snap_, bytes));
+        snap_bytes_ = bytes;
+    }
+    const int b = slot_mode ? h_state_[i].cur_buf : cur_;
+    WENOFV_CUDA(cudaMemcpyAsync(d_snap_, d.buf[b], bytes, cudaMemcpyDeviceToDevice, stream));
+    WENOFV_CUDA(cudaEventRecord(snap_ready_, stream));
+    WENOFV_CUDA(cudaStreamWaitEvent(copy_stream_, snap_ready_, 0));
+    WENOFV_CUDA(cudaMemcpyAsync(h_snap_, d_snap_, bytes, cudaMemcpyDeviceToHost, copy_stream_));
+    WENOFV_CUDA(cudaEventRecord(snap_done_, copy_stream_));
+    snap_host_ = host;
+    snap_layout_ = layout;
+    snap_nv_ = nvar_of(d.eq_kind);
+    snap_nx_ = d.nx;
+    snap_ny_ = d.ny;
+    snap_pitch_ = d.pitch;
+    snap_pending_ = true;
+    return WENOFV_OK;
+}
+
+int Engine::snapshot_wait()
+{
+    if (!snap_pending_) return WENOFV_OK;
+    WENOFV_CUDA(cudaSetDevice(device));
+    snap_pending_ = false;
+    WENOFV_CUDA(cudaEventSynchronize(snap_done_));
+    from_pitch(h_snap_, snap_layout_, snap_nv_, snap_nx_, snap_ny_, snap_pitch_, snap_host_);
+    return WENOFV_OK;
+}
+
 namespace {
 struct Range { // one NVTX range for the lifetime of the object
     explicit Range(const char *name) { nvtxRangePushA(name); }
@@ -807,26 +901,75 @@ int Engine::device_state(int i, double **U, int *pitch)
     return WENOFV_OK;
 }
 
-// Times candidate tilings with a few manual steps on a copy of the current state and keeps
-// the fastest; the state is restored afterwards.
+namespace {
+// what autotune borrows, given back on every return path: the saved copies of the states,
+// the two timing events, and (when the search stops early) the tiling and the loop state
+struct TuneScope {
+    Engine &e;
+    std::vector<double *> saved;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rows0, ctas0, cur0;
+    std::vector<InstState> state0;
+    bool done = false;
+    TuneScope(Engine &eng, int rows, int ctas, int cur, const InstState *st, int cap)
+        : e(eng), saved(eng.n, nullptr), rows0(rows), ctas0(ctas), cur0(cur), state0(st, st + cap) {}
+    ~TuneScope()
+    {
+        if (!done) { // an error path: the caller's tiling, buffer and loop state as they were
+            cudaStreamSynchronize(e.stream);
+            e.restore_after_tune(rows0, ctas0, cur0, state0.data(), saved);
+        }
+        for (double *p : saved) cudaFree(p);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        (void)cudaGetLastError();
+    }
+};
+} // namespace
+
+// puts the saved states back into the current buffer and restores tiling and loop state
+void Engine::restore_after_tune(int rows, int ctas, int cur, const InstState *st, const std::vector<double *> &saved)
+{
+    cur_ = cur;
+    for (int i = 0; i < n && i < (int)saved.size(); i++) {
+        if (!saved[i]) continue;
+        const InstDesc &d = desc_[i];
+        const size_t bytes = (size_t)nvar_of(d.eq_kind) * d.ny * d.pitch * sizeof(double);
+        cudaMemcpyAsync(d.buf[cur_], saved[i], bytes, cudaMemcpyDeviceToDevice, stream);
+    }
+    std::memcpy(h_state_, st, cap_ * sizeof(InstState));
+    push_state();
+    cudaStreamSynchronize(stream);
+    rows_per_item_ = rows;
+    ctas_per_sm_ = ctas;
+    work_dirty_ = true;
+    ensure_work();
+}
+
+// Times candidate tilings (rows per work item x resident CTAs per SM) with manual steps on
+// the current state and keeps the fastest: one warm-up step, then TUNE_SAMPLES timed steps
+// per candidate, ranked by the median.  The states, the buffer rotation and the loop state
+// (status flags included) are put back afterwards, and on any error.
 int Engine::autotune(int *rows_out, int *ctas_out, double *best_ms)
 {
+    constexpr int TUNE_SAMPLES = 3;
     WENOFV_CUDA(cudaSetDevice(device));
-    std::vector<double *> saved(n, nullptr);
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    int rc = pull_state();
+    if (rc) return rc;
+    TuneScope T(*this, rows_per_item_, ctas_per_sm_, cur_, h_state_, cap_);
     for (int i = 0; i < n; i++) {
         const InstDesc &d = desc_[i];
         const size_t bytes = (size_t)nvar_of(d.eq_kind) * d.ny * d.pitch * sizeof(double);
-        WENOFV_CUDA(cudaMalloc(&saved[i], bytes));
-        WENOFV_CUDA(cudaMemcpyAsync(saved[i], d.buf[cur_], bytes, cudaMemcpyDeviceToDevice, stream));
+        WENOFV_CUDA(cudaMalloc(&T.saved[i], bytes));
+        WENOFV_CUDA(cudaMemcpyAsync(T.saved[i], d.buf[cur_], bytes, cudaMemcpyDeviceToDevice, stream));
     }
-    const int cur0 = cur_;
-    cudaEvent_t e0, e1;
-    WENOFV_CUDA(cudaEventCreate(&e0));
-    WENOFV_CUDA(cudaEventCreate(&e1));
+    WENOFV_CUDA(cudaEventCreate(&T.e0));
+    WENOFV_CUDA(cudaEventCreate(&T.e1));
     double dt = 0.0;
     {
         std::vector<double> dts(n);
-        const int rc = compute_dt(dts.data());
+        rc = compute_dt(dts.data());
         if (rc) return rc;
         dt = *std::min_element(dts.begin(), dts.end()) * 0.5;
     }
@@ -836,33 +979,29 @@ int Engine::autotune(int *rows_out, int *ctas_out, double *best_ms)
     int br = 32, bc = 0;
     for (int r : rows_c)
         for (int c : ctas_c) {
-            int rc = set_tiling(r, c);
+            rc = set_tiling(r, c);
             if (!rc) rc = step(dt); // warm-up
             if (rc) return rc;
-            WENOFV_CUDA(cudaEventRecord(e0, stream));
-            for (int k = 0; k < 2 && !rc; k++) rc = step(dt);
-            if (rc) return rc;
-            WENOFV_CUDA(cudaEventRecord(e1, stream));
-            WENOFV_CUDA(cudaEventSynchronize(e1));
-            float ms = 0;
-            WENOFV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best) { best = ms; br = r; bc = c; }
+            float ms[TUNE_SAMPLES];
+            for (int k = 0; k < TUNE_SAMPLES; k++) {
+                WENOFV_CUDA(cudaEventRecord(T.e0, stream));
+                rc = step(dt);
+                if (rc) return rc;
+                WENOFV_CUDA(cudaEventRecord(T.e1, stream));
+                WENOFV_CUDA(cudaEventSynchronize(T.e1));
+                WENOFV_CUDA(cudaEventElapsedTime(&ms[k], T.e0, T.e1));
+            }
+            std::sort(ms, ms + TUNE_SAMPLES);
+            const double med = ms[TUNE_SAMPLES / 2];
+            if (med < best) { best = med; br = r; bc = c; }
         }
-    cur_ = cur0;
-    for (int i = 0; i < n; i++) {
-        const InstDesc &d = desc_[i];
-        const size_t bytes = (size_t)nvar_of(d.eq_kind) * d.ny * d.pitch * sizeof(double);
-        WENOFV_CUDA(cudaMemcpyAsync(d.buf[cur_], saved[i], bytes, cudaMemcpyDeviceToDevice, stream));
-    }
     WENOFV_CUDA(cudaStreamSynchronize(stream));
-    for (double *p : saved) cudaFree(p);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    const int rc = set_tiling(br, bc);
-    if (rc) return rc;
+    T.done = true;
+    restore_after_tune(br, bc, T.cur0, T.state0.data(), T.saved);
+    if (const cudaError_t e = cudaGetLastError()) return cuda_fail(e, "autotune restore");
     if (rows_out) *rows_out = br;
     if (ctas_out) *ctas_out = bc;
-    if (best_ms) *best_ms = best / 2.0;
+    if (best_ms) *best_ms = best / stage_count(rk); // per stage launch
     return WENOFV_OK;
 }
 

@@ -52,8 +52,13 @@ public:
     int status(int i, uint32_t *flags, int64_t *cell);
     int set_tiling(int rows, int ctas_per_sm);
     int autotune(int *rows, int *ctas_per_sm, double *best_ms);
+    // puts states, buffer rotation, loop state and tiling back after a tuning search
+    void restore_after_tune(int rows, int ctas, int cur, const InstState *st, const std::vector<double *> &saved);
     int device_state(int i, double **U, int *pitch);
     int set_frame(int i, const double *frame); // NEUMANN2 ghost averages, SoA [v][ny+8][nx+8]
+    int theta_flags(int i, unsigned char *out, int layout); // the final stage's limiter record per cell
+    int snapshot_begin(int i, double *host, int layout);     // async copy of the current state
+    int snapshot_wait();                                     // blocks until that copy has landed
     int init_testcase(int i, const wenofv_testcase *tc);                      // wenofv_init.cu
     int accuracy(int i, const wenofv_testcase *tc, double t, double *norms); // wenofv_init.cu
 
@@ -105,6 +110,16 @@ private:
     std::vector<double *> dmem_;    // per instance: 3 state buffers
     std::vector<double *> dmetric_; // per instance: dxc, dxl, dy
     std::vector<double *> dframe_;  // per NEUMANN2 instance: its ghost frame
+    std::vector<unsigned char *> dtheta_; // per instance: the limiter's per-cell theta record [ny][nx]
+    // snapshot: a device copy of one state, read back on a copy stream while the next steps run
+    double *d_snap_ = nullptr;
+    double *h_snap_ = nullptr; // pinned read-back of the snapshot (pitched), repacked by snapshot_wait
+    size_t snap_bytes_ = 0;
+    cudaStream_t copy_stream_ = nullptr;
+    cudaEvent_t snap_ready_ = nullptr, snap_done_ = nullptr;
+    double *snap_host_ = nullptr;
+    int snap_layout_ = 0, snap_nv_ = 0, snap_nx_ = 0, snap_ny_ = 0, snap_pitch_ = 0;
+    bool snap_pending_ = false;
     std::vector<char> frame_set_;
     std::vector<char> live_;
     std::vector<Group> groups_;

@@ -55,6 +55,14 @@ constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
 unsigned char *g_addr[MAX_DEVICES] = {};
 
+// puts the caller's current device back on every return path: the step makes cfg->device
+// current for its copies and launches, and a framework caller's own device must not change
+struct DeviceGuard {
+    int saved = -1;
+    DeviceGuard() { if (cudaGetDevice(&saved) != cudaSuccess) { saved = -1; (void)cudaGetLastError(); } }
+    ~DeviceGuard() { if (saved >= 0) cudaSetDevice(saved); }
+};
+
 int scratch_address(int device, unsigned char **out)
 {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -80,7 +88,7 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
     if (rc) return rc;
     if (cfg->bc == WENOFV_BC_NEUMANN2) { set_error("NEUMANN2 needs a ghost frame: use a context (wenofv_set_frame)"); return WENOFV_ENOTSUP; }
     if (!d_U || !d_U_next || d_U == d_U_next) { set_error("need distinct device input and output states"); return WENOFV_EINVAL; }
-    if (!(dt >= 0.0)) { set_error("dt must be a non-negative number"); return WENOFV_EINVAL; }
+    if (!std::isfinite(dt) || dt < 0.0) { set_error("dt must be a finite non-negative number"); return WENOFV_EINVAL; }
     if (pitch < cfg->nx) { set_error("pitch (%d) must be at least nx (%d)", pitch, cfg->nx); return WENOFV_EINVAL; }
     const int nv = nvar_of(eq->eq_kind);
     const int recon = eq->eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : cfg->reconstruction;
@@ -100,6 +108,7 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
     if (nwork > NOALLOC_MAX_WORK) { set_error("the no-allocation step takes at most %d work items", NOALLOC_MAX_WORK); return WENOFV_EINVAL; }
 
     if (cfg->device < 0 || cfg->device >= MAX_DEVICES) { set_error("device ordinal out of range"); return WENOFV_EINVAL; }
+    const DeviceGuard device_guard;
     WENOFV_CUDA(cudaSetDevice(cfg->device));
     unsigned char *base = nullptr;
     rc = scratch_address(cfg->device, &base);

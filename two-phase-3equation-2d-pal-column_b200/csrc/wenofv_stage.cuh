@@ -490,7 +490,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
 //      limiter :1895-2000) -> face states (FP64 in every form) ------------------------------
 template <int EQ, int RECON, class R, int SCH>
 __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>::H> &S, const InstDesc &D, InstState *st, int r,
-                                             int i0, int TXe, const double *ring_raw)
+                                             int i0, int TXe, const double *ring_raw, bool flag_row)
 {
     using SR = typename ReconSel<R, SCH, RECON>::type;
     constexpr int H = SR::H, NS = SR::NS;
@@ -651,6 +651,15 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
         const double t0 = __shfl_sync(0xffffffffu, th, gbase + 0);
         const double t1 = __shfl_sync(0xffffffffu, th, gbase + (NLIM > 1 ? 1 : 0));
         const double theta = NLIM == 2 ? sc_min(t0, t1) : t0;
+        // the per-cell record of useBoundPreservingLimiter (src/WENOFV.cpp:1906-1909), kept
+        // from the final stage of a step for the average_*.plt theta column
+        if (flag_row && active && v == 0 && c >= 0 && c < TXe) {
+#if WENOFV_CHECK_BOUNDS
+            if (r < 0 || r >= D.ny || i0 + c >= D.nx) flag_error(st, 16u /* WENOFV_FLAG_BOUNDS */, (long long)r * D.nx + i0 + c);
+            else
+#endif
+                D.theta_flag[(size_t)r * D.nx + i0 + c] = theta < 1.0 - 1e-8 ? 1 : 0;
+        }
         if (theta >= 0.0 && theta <= 1.0) {
             const double u0 = ub[v];
 #pragma unroll
@@ -838,6 +847,7 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
         }
         const double *bin = D.buf[L.bin];
         const double *bun = D.buf[L.bun];
+        const bool flag_rows = D.theta_flag != nullptr && L.final_stage && !L.rhs_out;
         // rows j0-1-H .. j0-1+H, the stencils of the first iteration's row
 #pragma unroll 1
         for (int m = 0; m <= 2 * H; m++) load_row<EQ, H>(S.su[(it.j0 - 1 - H + m) & 7], bin, D, it.j0 - 1 - H + m, it.i0, st);
@@ -857,7 +867,7 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
             }
             phase_ysweep<EQ, RECON, R, SCH>(S, D, r, stage_dyn_smem, r == it.j0 - 1);
             __syncthreads();
-            phase_xsweep<EQ, RECON, R, SCH>(S, D, st, r, it.i0, TXe, stage_dyn_smem);
+            phase_xsweep<EQ, RECON, R, SCH>(S, D, st, r, it.i0, TXe, stage_dyn_smem, flag_rows && r >= it.j0 && r < it.j1);
             __syncthreads();
             phase_riemann<EQ, R, FLX, H>(S, D, st, r, it.i0, it.j0, it.j1, TXe);
             // the last warp, idle in the second round of Riemann units, prepares the next

@@ -25,6 +25,7 @@ struct InstDesc {
     double dx4; // pow(dX, 4) as the host C library rounds it: WENOEXP's smoothness threshold
     EqParams eq;
     const double *frame; // NEUMANN2: fixed ghost averages [v][ny+8][nx+8], interior at (4, 4)
+    unsigned char *theta_flag; // optional [ny][nx]: 1 where the final stage's limiter theta < 1 - 1e-8
 };
 
 // mutable per-instance state of the device-side time loop

@@ -26,8 +26,10 @@
 // as the reference loops; 0, the default: the loop on the device).
 #pragma once
 #include <cstdint>
+#include <exception>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "Equations.hpp"
@@ -98,19 +100,29 @@ public:
     // cell averages and the derived variables) and, for SMOOTH and VORTEX,
     // accuracy_<prefix>.csv (L_inf, L1, L2 of z1 against the translated initial data)
     void outputResults(int count, double now, const std::string &specialCase);
-    void outputAve(const std::string &prefix);
+    void outputAve(const std::string &prefix);      // with the limiter's theta record and Pr (= 0)
+    void outputSliceAve(const std::string &prefix); // the row j = 1 (key SLICEOUTPUT = 1)
     void outputAccuracy(const std::string &prefix, double now);
     void outputUPoscillation(const std::string &prefix); // SHARP's velocity/pressure deviation
-    void outputSpecialTestCasebyTime(double now);      // SHARP's and DAMBREAK's time series
-    void outputPressureByTime(double now);             // DAMBREAK's wall pressure probes
-    void outputThicknessByTime(double now);            // SHARP's interface thickness
-    void outputSymmetryErr(double now);                // RTI's left-right symmetry error
+    // the time series of SHARP, DAMBREAK and RTI from a state Us ([i][j][r], m_Uh or a snapshot)
+    void outputSpecialTestCasebyTime(double now, const double *Us);
+    void outputPressureByTime(double now, const double *Us);  // DAMBREAK's wall pressure probes
+    void outputThicknessByTime(double now, const double *Us); // SHARP's interface thickness
+    void outputSymmetryErr(double now, const double *Us);     // RTI's left-right symmetry error
+    std::vector<uint8_t> thetaFlags() const;                  // the limiter's per-cell record, [i][j]
     std::string m_outputDir;
     double &Uh(int i, int j, int r) { return m_Uh[((size_t)i * m_worldElemNumY + j) * m_varNum + r]; }
     wenofv_config config() const;
 
 private:
     wenofv_ctx *m_ctx = nullptr;
+    // asynchronous time-series output of the device loop: a snapshot of the state is read back
+    // on the library's copy stream and written by a worker thread while the next steps run
+    std::thread m_writer;
+    std::exception_ptr m_writerError;
+    std::vector<double> m_snapshot;
+    void startSeriesOutput(double now);
+    void finishSeriesOutput();
     std::string opt(const std::string &key, const std::string &dflt) const;
     void check(int rc, const char *what) const;
 };

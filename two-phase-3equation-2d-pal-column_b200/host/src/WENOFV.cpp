@@ -27,7 +27,37 @@ CWENOFV::CWENOFV(TwoPhaseEquation *eq, std::map<std::string, std::string> opts) 
 
 CWENOFV::~CWENOFV()
 {
+    if (m_writer.joinable()) m_writer.join();
     if (m_ctx) wenofv_destroy(m_ctx);
+}
+
+// joins the previous series writer and rethrows its error, if any
+void CWENOFV::finishSeriesOutput()
+{
+    if (m_writer.joinable()) m_writer.join();
+    if (m_writerError) {
+        std::exception_ptr e = m_writerError;
+        m_writerError = nullptr;
+        std::rethrow_exception(e);
+    }
+}
+
+// snapshot of the device state now (a device-side copy, then a read-back on the library's
+// copy stream) and a worker thread that waits for it and appends the time series, so that
+// the read-back and the file writing overlap the next piece of the device loop
+void CWENOFV::startSeriesOutput(double now)
+{
+    finishSeriesOutput();
+    m_snapshot.resize(m_Uh.size());
+    check(wenofv_snapshot_begin(m_ctx, m_snapshot.data(), WENOFV_LAYOUT_REF_AOS), "wenofv_snapshot_begin");
+    m_writer = std::thread([this, now] {
+        try {
+            check(wenofv_snapshot_wait(m_ctx), "wenofv_snapshot_wait");
+            outputSpecialTestCasebyTime(now, m_snapshot.data());
+        } catch (...) {
+            m_writerError = std::current_exception();
+        }
+    });
 }
 
 std::string CWENOFV::opt(const std::string &key, const std::string &dflt) const
@@ -214,29 +244,45 @@ void CWENOFV::outputResults(int count, double now, const std::string &specialCas
     (void)count;
     if (m_outputDir.empty()) return;
     const bool exact = m_testcase == SMOOTH || m_testcase == VORTEX;
+    const bool slice = opt("SLICEOUTPUT", "0") == "1";
     if (specialCase == "initial") {
         outputAve("initial");
+        if (slice) outputSliceAve("initial");
         if (exact) outputAccuracy("initial", now);
         if (m_testcase == SHARP) outputUPoscillation("initial");
     } else if (specialCase == "final") {
         outputAve("final");
+        if (slice) outputSliceAve("final");
         if (exact) outputAccuracy("final", now);
         if (m_testcase == SHARP) outputUPoscillation("final"); // outputSpecialTestCasebyCell (:3381-3391)
     } else if (specialCase == "intermediate") {
         outputAve(num_str(now) + "_intermediate");
+        if (slice) outputSliceAve(num_str(now) + "_intermediate");
     }
 }
 
-// outputAve (src/WENOFV.cpp:2525-2601): cell centres and the variables of getVitalVarVal
-// (include/Equations.hpp:1005-1043). The reference also writes the limiter's theta and a
-// pressure diagnostic of its primitive reconstructions per cell; those stay on the GPU here.
+// the per-cell theta record of the limiter's last call (getWorldTheta, m_worldTotalTheta),
+// in the [i][j] order of m_Uh
+std::vector<uint8_t> CWENOFV::thetaFlags() const
+{
+    std::vector<uint8_t> th((size_t)m_worldElemNumX * m_worldElemNumY, 0);
+    check(wenofv_theta_flags(m_ctx, th.data(), WENOFV_LAYOUT_REF_AOS), "wenofv_theta_flags");
+    return th;
+}
+
+// outputAve (src/WENOFV.cpp:2525-2601): cell centres, the variables of getVitalVarVal
+// (include/Equations.hpp:1005-1043), the limiter's per-cell theta record (1 where the last
+// limiter call scaled the cell: theta < 1 - 1e-8) and the Pr column.  The reference's Pr is
+// m_totalPr, which every getFlux_* sets to zero (src/WENOFV.cpp:637, :746, :904, :1063,
+// :1219) and nothing writes, so it is 0 here too.
 void CWENOFV::outputAve(const std::string &prefix)
 {
     const std::string filename = m_outputDir + "average_" + prefix + ".plt";
     std::ofstream f(filename);
     if (!f) throw std::runtime_error("cannot write " + filename);
+    const std::vector<uint8_t> th = thetaFlags();
     f << "TITLE=FvSolution" << std::endl;
-    f << "VARIABLES=X Y RHO1Z1 RHO2Z2 Z1 RHO1 RHO2 RHO U V PRE " << std::endl;
+    f << "VARIABLES=X Y RHO1Z1 RHO2Z2 Z1 RHO1 RHO2 RHO U V PRE theta Pr " << std::endl;
     f << "ZONE T=TA, I=" << m_worldElemNumY << ", J=" << m_worldElemNumX << ", DATAPACKING = POINT" << std::endl;
     const int G = m_ghostCellNum;
     for (int i = 0; i < m_worldElemNumX; i++) {
@@ -247,8 +293,32 @@ void CWENOFV::outputAve(const std::string &prefix)
             const double z1 = volume_frac(*equation, U), rho = U[0] + U[1];
             f << (xl + xr) / 2 << " " << (yl + yr) / 2 << " " << U[0] << " " << U[1] << " " << z1 << " " << U[0] / z1
               << " " << U[1] / (1.0 - z1) << " " << rho << " " << U[2] / rho << " " << U[3] / rho << " "
-              << pressure(*equation, U, z1) << " " << std::endl;
+              << pressure(*equation, U, z1) << " " << (int)th[(size_t)i * m_worldElemNumY + j] << " " << 0 << " "
+              << std::endl;
         }
+    }
+}
+
+// outputSliceAve (src/WENOFV.cpp:2668-2737): the row j = 1 (the reference's ej = ghost + 1)
+// in the columns of outputAve without Y.  The reference's outputResults never calls it; here
+// the key SLICEOUTPUT = 1 writes slice_<prefix>.plt beside every average_<prefix>.plt.
+void CWENOFV::outputSliceAve(const std::string &prefix)
+{
+    const std::string filename = m_outputDir + "slice_" + prefix + ".plt";
+    std::ofstream f(filename);
+    if (!f) throw std::runtime_error("cannot write " + filename);
+    const std::vector<uint8_t> th = thetaFlags();
+    f << "TITLE=FvSolution_Slice" << std::endl;
+    f << "VARIABLES=X RHO1Z1 RHO2Z2 Z1 RHO1 RHO2 RHO U V PRE theta Pr " << std::endl;
+    f << "ZONE T=TA, I=" << m_worldElemNumX << ", DATAPACKING = POINT" << std::endl;
+    const int G = m_ghostCellNum, j = std::min(1, m_worldElemNumY - 1);
+    for (int i = 0; i < m_worldElemNumX; i++) {
+        const double xl = equation->xL - G * m_deltaX + (i + G) * m_deltaX, xr = equation->xL - G * m_deltaX + (i + G + 1) * m_deltaX;
+        const double *U = &m_Uh[((size_t)i * m_worldElemNumY + j) * m_varNum];
+        const double z1 = volume_frac(*equation, U), rho = U[0] + U[1];
+        f << (xl + xr) / 2 << " " << U[0] << " " << U[1] << " " << z1 << " " << U[0] / z1 << " " << U[1] / (1.0 - z1)
+          << " " << rho << " " << U[2] / rho << " " << U[3] / rho << " " << pressure(*equation, U, z1) << " "
+          << (int)th[(size_t)i * m_worldElemNumY + j] << " " << 0 << " " << std::endl;
     }
 }
 
@@ -285,18 +355,18 @@ void CWENOFV::outputUPoscillation(const std::string &prefix)
 // to oscillationByTime_<nx>.plt.  The reference's header names the columns Speed, P, U, V
 // but writes them in the order P, Speed, U, V, and takes the signed u and v deviations (maxima
 // from 0); both are kept, so that files from the two programs read alike.
-void CWENOFV::outputSpecialTestCasebyTime(double now)
+void CWENOFV::outputSpecialTestCasebyTime(double now, const double *Us)
 {
     if (m_testcase == DAMBREAK) {
-        outputPressureByTime(now);
+        outputPressureByTime(now, Us);
         return;
     }
     if (m_testcase == RTI) {
-        outputSymmetryErr(now);
+        outputSymmetryErr(now, Us);
         return;
     }
     if (m_testcase != SHARP) return;
-    outputThicknessByTime(now);
+    outputThicknessByTime(now, Us);
     const std::string filename = m_outputDir + "oscillationByTime_" + std::to_string(m_worldElemNumX) + ".plt";
     const bool exists = std::filesystem::exists(filename);
     std::ofstream f(filename, std::ios::app);
@@ -309,7 +379,7 @@ void CWENOFV::outputSpecialTestCasebyTime(double now)
     double pmax = 0, smax = 0, umax = 0, vmax = 0;
     for (int i = 0; i < m_worldElemNumX; i++)
         for (int j = 0; j < m_worldElemNumY; j++) {
-            const double *U = &m_Uh[((size_t)i * m_worldElemNumY + j) * m_varNum];
+            const double *U = &Us[((size_t)i * m_worldElemNumY + j) * m_varNum];
             const double rho = U[0] + U[1], u = U[2] / rho, v = U[3] / rho;
             pmax = std::max(pmax, std::fabs(pressure(*equation, U, volume_frac(*equation, U))) / equation->g_rho10 / std::pow(c1, 2));
             smax = std::max(smax, std::sqrt(std::pow(u - 1, 2) + std::pow(v - 1, 2)) / c1);
@@ -320,10 +390,14 @@ void CWENOFV::outputSpecialTestCasebyTime(double now)
 }
 
 // outputThincknessByTime (src/WENOFV.cpp:3049-3108) for SHARP: 1 / the largest jump of z1
-// between neighbouring cells in x or y (the right and upper neighbours, wrapped periodically
-// as the reference's ghost cells are), an interface thickness in cells, appended to
-// thincknessByTime.plt under the reference's file and column names
-void CWENOFV::outputThicknessByTime(double now)
+// between neighbouring cells in x or y (the right and upper neighbours), an interface
+// thickness in cells, appended to thincknessByTime.plt under the reference's file and column
+// names.  The last column and row compare with the periodic wrap, a choice of this mirror:
+// the reference gathers the state without filling the gathered array's ghost cells
+// (getWorldUh, src/WENOFV.cpp:2059-2093), so its last column and row compare with unfilled
+// entries.  On SHARP the two agree in practice, because z1 there is the background's ~1e-8
+// on both sides of the periodic seam.
+void CWENOFV::outputThicknessByTime(double now, const double *Us)
 {
     const std::string filename = m_outputDir + "thincknessByTime.plt";
     const bool exists = std::filesystem::exists(filename);
@@ -331,7 +405,7 @@ void CWENOFV::outputThicknessByTime(double now)
     if (!f) throw std::runtime_error("cannot write " + filename);
     if (!exists) f << "TITLE=FvSolution" << std::endl << "VARIABLES=time thinckness\n" << std::endl << "ZONE T=TA" << std::endl;
     const int nx = m_worldElemNumX, ny = m_worldElemNumY;
-    auto z1 = [&](int i, int j) { return volume_frac(*equation, &m_Uh[((size_t)(i % nx) * ny + (j % ny)) * m_varNum]); };
+    auto z1 = [&](int i, int j) { return volume_frac(*equation, &Us[((size_t)(i % nx) * ny + (j % ny)) * m_varNum]); };
     double maxDiff = 0;
     for (int i = 0; i < nx; i++)
         for (int j = 0; j < ny; j++) {
@@ -345,7 +419,7 @@ void CWENOFV::outputThicknessByTime(double now)
 // each cell of the left half and its mirror image across x = (xL + xR) / 2, appended to
 // symmetry_err.plt (no header, as the reference writes it; its running maximum starts
 // uninitialised there and at 0 here)
-void CWENOFV::outputSymmetryErr(double now)
+void CWENOFV::outputSymmetryErr(double now, const double *Us)
 {
     std::ofstream f(m_outputDir + "symmetry_err.plt", std::ios::app);
     if (!f) throw std::runtime_error("cannot write " + m_outputDir + "symmetry_err.plt");
@@ -353,8 +427,8 @@ void CWENOFV::outputSymmetryErr(double now)
     double maxErr = 0;
     for (int i = 0; i < nx / 2; i++)
         for (int j = 0; j < ny; j++) {
-            const double a = volume_frac(*equation, &m_Uh[((size_t)i * ny + j) * m_varNum]);
-            const double b = volume_frac(*equation, &m_Uh[((size_t)(nx - 1 - i) * ny + j) * m_varNum]);
+            const double a = volume_frac(*equation, &Us[((size_t)i * ny + j) * m_varNum]);
+            const double b = volume_frac(*equation, &Us[((size_t)(nx - 1 - i) * ny + j) * m_varNum]);
             maxErr = std::max(maxErr, std::fabs(a - b));
         }
     f << now << " " << maxErr << std::endl;
@@ -367,7 +441,7 @@ void CWENOFV::outputSymmetryErr(double now)
 // to the 4 points of the row's cell; the point nearest y is taken.  Cells beyond the domain
 // are the mirror images that the library's NEUMANN walls use (the pressure keeps its sign).
 // The reconstructions run through the library's WENO probe, so they are the solver's own.
-void CWENOFV::outputPressureByTime(double now)
+void CWENOFV::outputPressureByTime(double now, const double *Us)
 {
     const std::string filename = m_outputDir + "pressureByTime.plt";
     const bool exists = std::filesystem::exists(filename);
@@ -388,7 +462,7 @@ void CWENOFV::outputPressureByTime(double now)
         for (int b = 0; b < 5; b++)     // row offset b - 2: one x-stencil per row
             for (int a = 0; a < 5; a++) { // column offset a - 2 from the first column
                 const int i = mirror(a - 2, m_worldElemNumX), j = mirror(rows[h] + b - 2, m_worldElemNumY);
-                const double *U = &m_Uh[((size_t)i * m_worldElemNumY + j) * m_varNum];
+                const double *U = &Us[((size_t)i * m_worldElemNumY + j) * m_varNum];
                 xst[(h * 5 + b) * 5 + a] = pressure(*equation, U, volume_frac(*equation, U)) / equation->g_rho10 / 9.81 / 0.3;
             }
     }
@@ -504,7 +578,7 @@ void CWENOFV::run()
                 n++;
                 if (byTime && (m_stepCount == 1 || m_stepCount % 200 == 0)) {
                     downloadUh();
-                    outputSpecialTestCasebyTime(m_now);
+                    outputSpecialTestCasebyTime(m_now, m_Uh.data());
                 }
             }
         } else if (byTime) {
@@ -521,10 +595,7 @@ void CWENOFV::run()
                 m_stepCount += n;
                 done += n;
                 if (n == 0) break;
-                if (m_stepCount == 1 || m_stepCount % 200 == 0) {
-                    downloadUh();
-                    outputSpecialTestCasebyTime(m_now);
-                }
+                if (m_stepCount == 1 || m_stepCount % 200 == 0) startSeriesOutput(m_now);
             }
         } else {
             double tout = m_now;
@@ -533,6 +604,7 @@ void CWENOFV::run()
             m_now = tout;
             m_stepCount += n;
         }
+        finishSeriesOutput();
         downloadUh();
         outputResults((int)m_stepCount, m_now, "intermediate");
     }
