@@ -414,6 +414,8 @@ def run_ours(args, rank, world, dist):
         fp32["speedup_vs_fp64_per_launch"] = launch_ms / fp32["launch_ms"]
         out["fp32_bulk"] = fp32
     out["clocks"] = clk.summary()
+    if not args.no_mix and args.workload == "column1024":
+        out.update(mixed_workloads(wb, local, dist, world))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args.workload, steps=args.cpu_steps, warmup=0)
     s.close()
@@ -506,6 +508,28 @@ def compare_fp32(args, wb, cfg, eq, U0, dt, U64, ncells, nstages, flush, barrier
     return out
 
 
+def mixed_workloads(wb, local, dist, world):
+    """bounded versions of the batched ensemble and the serving stream for the default line:
+    solves/s, latency percentiles, FP32-bulk against FP64, and both forms' errors against the
+    oracle's arithmetic"""
+    ens = cases.ensemble(64, seed=4)
+    res, _, cells = batch_measure(wb, ens, 50, 3, local, dist, world)
+    batch = dict(workload="batched_ensemble_64", instances=64, cells=cells, steps_per_solve=50,
+                 grids="U{64,96,128,192,256}^2 and {256x64, 512x128} (seed 4)",
+                 solves_per_s=res["fp64"]["solves_per_s"], fp64=res["fp64"], fp32_bulk=res["fp32_bulk"],
+                 fp64_strict=res["fp64_strict"], errors=res["errors"],
+                 oracle_check=batch_oracle_check(wb, ens, 10, os.cpu_count() or 1))
+    reqs = serve_requests(wb, 16, 7, 50, 400, nx_max=1024, ny_max=256)
+    sres = serve_measure(wb, reqs, 4.0, 8 << 30, 7, local, dist, world)
+    serve = dict(workload="serving_stream_16", requests=16, arrival="Poisson, mean 4 req/s (seed 7)",
+                 grids="nx log-uniform 64..1024, ny log-uniform 64..256", steps="uniform 50..400 per request",
+                 mix="Euler quadrants / two-phase columns 50/50", hbm_budget_gb=8,
+                 solves_per_s=sres["fp64"]["solves_per_s"], p50_latency_s=sres["fp64"]["p50_latency_s"],
+                 p99_latency_s=sres["fp64"]["p99_latency_s"], fp64=sres["fp64"], fp32_bulk=sres["fp32_bulk"],
+                 errors=sres["errors"])
+    return dict(batch=batch, serve=serve)
+
+
 def _load_package():
     import importlib.util
 
@@ -521,19 +545,39 @@ def _pctl(x, q):
 
 
 # ---- config 4: batched ensemble ------------------------------------------------------------------
-def run_batch(args, rank, world, dist):
-    """256 uneven two-phase instances, one persistent launch per RK stage for all of them,
-    captured step pairs, autotuned tiling; FP64 and FP32-bulk on the same inputs."""
+def per_instance_errors(finals, names=("fp64", "fp32_bulk"), ref="fp64_strict"):
+    """pooled relative L1 of each instance's final state against the FP64 oracle's arithmetic
+    (the strict form), per form: the FP64 form's spread is the scheme's own sensitivity to
+    rounding, against which FP32-bulk's error is read"""
+    out = {}
+    for name in names:
+        e = [rel_l1(a, b) for a, b in zip(finals[name], finals[ref]) if a is not None and b is not None]
+        out[name] = e
+    return out
+
+
+def summarize_errors(err, bar=1e-5):
+    e32, e64 = np.asarray(err["fp32_bulk"]), np.asarray(err["fp64"])
+    # an instance "within the scheme's spread": FP32's error at most 10x the FP64 form's
+    excused = [(a > bar and a <= 10 * b) for a, b in zip(e32, e64)]
+    return dict(fp32_vs_oracle=dict(median=_pctl(e32, 50), p90=_pctl(e32, 90), max=float(e32.max()) if len(e32) else None,
+                                    within_bar=int(np.sum(e32 <= bar)), n=int(len(e32))),
+                fp64_vs_oracle=dict(median=_pctl(e64, 50), p90=_pctl(e64, 90), max=float(e64.max()) if len(e64) else None),
+                over_bar_explained_by_fp64_spread=int(np.sum(excused)),
+                over_bar_unexplained=int(np.sum([(a > bar and not x) for a, x in zip(e32, excused)])),
+                bar=bar, note="pooled relative L1 per instance against FP64_STRICT (the oracle's arithmetic, "
+                              "bit for bit); an instance over the bar whose FP64-form spread is within 10x of its "
+                              "FP32-bulk error is the scheme's own roundoff sensitivity, not FP32's")
+
+
+def batch_measure(wb, ens, steps, warmup, local, dist, world, autotune=True):
+    """one persistent launch per RK stage for all instances, captured step pairs; FP64, FP32-bulk
+    and FP64_STRICT on the same inputs (the strict run is the oracle's arithmetic)"""
     import torch
 
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    wb = _load_package()
-    ens = cases.ensemble(args.instances, seed=4)
     cells = sum(prm["nx"] * prm["ny"] for _, prm in ens)
-    steps = args.steps
     res, finals = {}, {}
-    for name, form in (("fp64", wb.FP64), ("fp32_bulk", wb.FP32_BULK)):
+    for name, form in (("fp64", wb.FP64), ("fp32_bulk", wb.FP32_BULK), ("fp64_strict", wb.FP64_STRICT)):
         cfgs, eqs = [], []
         for U0, prm in ens:
             c = wb.make_config(prm["nx"], prm["ny"], rk=2, cfl=0.5, scheme=prm["scheme"], flux=1, recon=1, limiter=1,
@@ -544,61 +588,100 @@ def run_batch(args, rank, world, dist):
         b = wb.Batch(cfgs, eqs)
         for k, (U0, _) in enumerate(ens):
             b.upload(k, U0)
-        rows, ctas, tune_ms = b.autotune()
-        b.advance(1e9, max_steps=args.warmup)
-        for k, (U0, _) in enumerate(ens):
-            b.upload(k, U0)
+        tiling = None
+        if autotune and name != "fp64_strict":
+            rows, ctas, tune_ms = b.autotune()
+            tiling = dict(rows_per_item=rows, ctas_per_sm=ctas, autotune_best_stage_ms=tune_ms)
+        if name != "fp64_strict":
+            b.advance(1e9, max_steps=warmup)
+            for k, (U0, _) in enumerate(ens):
+                b.upload(k, U0)
         stream = torch.cuda.ExternalStream(b.stream())
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
         e0.record(stream)
-        ns = b.advance(1e9, max_steps=steps)
+        try:
+            ns = b.advance(1e9, max_steps=steps)
+            failed = []
+        except wb.WenofvError:
+            ns, failed = None, ["status flags raised"]
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        ms = max_over_ranks(ms, dist, local)
-        assert int(ns.min()) == int(ns.max()) == steps
+        ms = max_over_ranks(e0.elapsed_time(e1), dist, local)
         finals[name] = [b.download(k) for k in range(len(ens))]
         res[name] = dict(value=world * cells * 3 * steps / (ms * 1e-3), unit="cell-stage updates/s",
-                         solves_per_s=world * len(ens) / (ms * 1e-3), seconds=ms * 1e-3,
-                         tiling=dict(rows_per_item=rows, ctas_per_sm=ctas, autotune_best_stage_ms=tune_ms))
+                         solves_per_s=world * len(ens) / (ms * 1e-3), seconds=ms * 1e-3, tiling=tiling,
+                         all_steps_done=bool(ns is not None and int(ns.min()) == int(ns.max()) == steps),
+                         failures=failed)
         b.close()
-    errs = [float(np.abs(a - b_).sum() / np.abs(b_).sum()) for a, b_ in zip(finals["fp32_bulk"], finals["fp64"])]
-    res["fp32_bulk"]["rel_l1_vs_fp64"] = dict(median=_pctl(errs, 50), p90=_pctl(errs, 90), max=max(errs),
-                                             note="pooled relative L1 of each instance's final state")
-    out = dict(metric="cell-stage updates/s", value=res["fp64"]["value"], unit="cell-stage updates/s", n_gpus=world,
-               steps=steps, warmup=args.warmup, ms_per_step=res["fp64"]["seconds"] * 1e3 / steps,
-               higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
-               config=dict(workload=f"batched_ensemble_{len(ens)}", instances=len(ens), cells=cells,
-                           grids="U{64,96,128,192,256}^2 and {256x64, 512x128} (seed 4)",
-                           ic="liquid columns, radius U[0.1,0.3], density ratio U[10,1000], eps in {1e-8,1e-6}",
-                           scheme="WENO-JS/WENO-Z mixed", flux="HLLC", reconstruction="characteristic",
-                           limiter=True, rk="SSP-RK3", steps_per_solve=steps,
-                           l2=f"working set {cells * 32 * 3 / 1e6:.0f} MB > L2", parallelism=f"replicas x{world}"),
-               solves_per_s=res["fp64"]["solves_per_s"], fp64=res["fp64"], fp32_bulk=res["fp32_bulk"],
-               gpu_launches=2 * 3 * steps)
-    return out
+    res["fp64_strict"].pop("tiling")
+    err = per_instance_errors(finals)
+    res["fp32_bulk"]["speedup_vs_fp64"] = res["fp32_bulk"]["value"] / res["fp64"]["value"]
+    res["errors"] = summarize_errors(err)
+    return res, err, cells
 
 
-# ---- config 5: serving stream --------------------------------------------------------------------
-def run_serve(args, rank, world, dist):
-    """Poisson arrivals of mixed Euler / two-phase solves into the continuous-batching
-    server; latency from submission to completion on the server clock."""
+def batch_oracle_check(wb, ens, steps, threads):
+    """FP64_STRICT against the CPU oracle for the first two instances of the batch, solved alone"""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    ok = True
+    for U0, prm in ens[:2]:
+        p = O.Problem(nx=prm["nx"], ny=prm["ny"], rk=2, cfl=0.5, scheme=prm["scheme"], flux=1, recon=1, limiter=1,
+                      threads=threads, rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"],
+                      sound2=prm["sound2"])
+        V, *_ = O.Oracle().advance(p, U0, t_end=1e9, max_steps=steps)
+        cfg = wb.make_config(prm["nx"], prm["ny"], rk=2, cfl=0.5, scheme=prm["scheme"], flux=1, recon=1, limiter=1,
+                             precision=wb.FP64_STRICT)
+        eq = wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"])
+        with wb.Solver(cfg, eq) as s:
+            s.upload(U0)
+            s.advance(1e9, max_steps=steps)
+            ok = ok and bool(np.array_equal(s.download(), V))
+    return dict(instances=2, steps=steps, bit_identical=ok)
+
+
+def run_batch(args, rank, world, dist):
+    """config 4: 256 uneven two-phase instances"""
     import torch
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     wb = _load_package()
-    rng = np.random.default_rng(5 + rank)
-    n = args.requests
-    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
+    ens = cases.ensemble(args.instances, seed=4)
+    res, err, cells = batch_measure(wb, ens, args.steps, args.warmup, local, dist, world)
+    res["oracle_check"] = batch_oracle_check(wb, ens, min(args.steps, 20), os.cpu_count() or 1)
+    rows = [dict(k=k, nx=prm["nx"], ny=prm["ny"], ratio=round(prm["ratio"], 1), eps=prm["eps"], scheme=prm["scheme"],
+                 fp32=err["fp32_bulk"][k], fp64=err["fp64"][k]) for k, (_, prm) in enumerate(ens)]
+    rows.sort(key=lambda r: -r["fp32"])
+    out = dict(metric="cell-stage updates/s", value=res["fp64"]["value"], unit="cell-stage updates/s", n_gpus=world,
+               steps=args.steps, warmup=args.warmup, ms_per_step=res["fp64"]["seconds"] * 1e3 / args.steps,
+               higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+               config=dict(workload=f"batched_ensemble_{len(ens)}", instances=len(ens), cells=cells,
+                           grids="U{64,96,128,192,256}^2 and {256x64, 512x128} (seed 4)",
+                           ic="liquid columns, radius U[0.1,0.3], density ratio U[10,1000], eps in {1e-8,1e-6}",
+                           scheme="WENO-JS/WENO-Z mixed", flux="HLLC", reconstruction="characteristic",
+                           limiter=True, rk="SSP-RK3", steps_per_solve=args.steps,
+                           l2=f"working set {cells * 32 * 3 / 1e6:.0f} MB", parallelism=f"replicas x{world}"),
+               solves_per_s=res["fp64"]["solves_per_s"], fp64=res["fp64"], fp32_bulk=res["fp32_bulk"],
+               fp64_strict=res["fp64_strict"], errors=res["errors"], oracle_check=res["oracle_check"],
+               worst_fp32_instances=rows[:10], gpu_launches=2 * 3 * args.steps)
+    return out
+
+
+# ---- config 5: serving stream --------------------------------------------------------------------
+def serve_requests(wb, n, seed, min_steps, max_steps, nx_max=2048, ny_max=512):
+    """n requests: Euler quadrants (outflow, conservative) or two-phase columns (periodic,
+    characteristic, limiter) 50/50, nx log-uniform 64..nx_max, ny 64..ny_max, steps uniform"""
+    rng = np.random.default_rng(seed)
     reqs = []
     for k in range(n):
-        nx = int(round(2 ** rng.uniform(6, 11) / 8)) * 8
-        ny = int(round(2 ** rng.uniform(6, 9) / 8)) * 8
-        steps = int(rng.integers(args.min_steps, args.max_steps + 1))
+        nx = int(round(2 ** rng.uniform(6, np.log2(nx_max)) / 8)) * 8
+        ny = int(round(2 ** rng.uniform(6, np.log2(ny_max)) / 8)) * 8
+        steps = int(rng.integers(min_steps, max_steps + 1))
         if rng.uniform() < 0.5:
             U0, _ = cases.euler_quadrants(nx, ny, seed=100 + k)
             mk = lambda f, nx=nx, ny=ny: wb.make_config(nx, ny, bc=wb.BC_OUTFLOW, rk=2, cfl=0.4, scheme=1, flux=1,
@@ -612,65 +695,119 @@ def run_serve(args, rank, world, dist):
             eq = wb.make_eq(rho10=prm["rho10"], rho20=prm["rho20"], sound1=prm["sound1"], sound2=prm["sound2"])
             kind = "two_phase"
         reqs.append((mk, eq, U0, steps, nx * ny, kind))
+    return reqs
+
+
+def serve_stream(wb, reqs, arrivals, form, budget_bytes, local, dist, world):
+    """submits the requests at their arrival times (server clock) and polls until all are done"""
+    srv = wb.Server(local, hbm_budget_bytes=budget_bytes, max_slots=256)
+    if dist is not None:
+        dist.barrier()
+    n = len(reqs)
+    t0 = srv.clock()
+    ids, done, failed = [], {}, set()
+    k = 0
+    while len(done) < n:
+        now = srv.clock() - t0
+        while k < n and arrivals[k] <= now:
+            mk, eq, U0, steps, _, _ = reqs[k]
+            cfg = mk(form)
+            cfg.device = local
+            ids.append(srv.submit(cfg, eq, U0, 1e9, max_steps=steps))
+            k += 1
+        for j, rid in enumerate(ids):
+            if j in done:
+                continue
+            try:
+                got = srv.poll(rid)
+            except wb.WenofvError:  # a numerically failed solve is a result too
+                got = (None, None)
+                failed.add(j)
+            if got is not None:
+                done[j] = got
+        time.sleep(0.0005)
+    srv.close()
+    ok = [j for j in range(n) if j not in failed]
+    lat = [done[j][1].t_done - done[j][1].t_submit for j in ok]
+    qwait = [done[j][1].t_admit - done[j][1].t_submit for j in ok]
+    span = max(done[j][1].t_done for j in ok) - min(done[j][1].t_submit for j in ok)
+    span = max_over_ranks(span, dist, local)
+    assert all(done[j][1].steps == reqs[j][3] for j in ok)
+    work_ok = sum(reqs[j][3] * reqs[j][4] * 3 for j in ok)
+    stats = dict(value=world * work_ok / span, unit="cell-stage updates/s", solves_per_s=world * len(ok) / span,
+                 failed_requests=sorted(failed), p50_latency_s=_pctl(lat, 50), p99_latency_s=_pctl(lat, 99),
+                 p50_queue_s=_pctl(qwait, 50), makespan_s=span)
+    return stats, [done[j][0] for j in range(n)]
+
+
+def serve_alone_strict(wb, reqs, local):
+    """each request solved alone in FP64_STRICT (the oracle's arithmetic)"""
+    out = []
+    for mk, eq, U0, steps, _, _ in reqs:
+        cfg = mk(wb.FP64_STRICT)
+        cfg.device = local
+        with wb.Solver(cfg, eq) as s:
+            s.upload(U0)
+            try:
+                s.advance(1e9, max_steps=steps)
+                out.append(s.download())
+            except wb.WenofvError:
+                out.append(None)
+    return out
+
+
+def serve_measure(wb, reqs, rate, budget_bytes, seed, local, dist, world, forms=("fp64", "fp32_bulk")):
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
     res, finals = {}, {}
-    for name, form in (("fp64", wb.FP64), ("fp32_bulk", wb.FP32_BULK)):
-        srv = wb.Server(local, hbm_budget_bytes=args.hbm_budget_gb << 30, max_slots=256)
-        if dist is not None:
-            dist.barrier()
-        t0 = srv.clock()
-        ids, done, failed = [], {}, set()
-        k = 0
-        while len(done) < n:
-            now = srv.clock() - t0
-            while k < n and arrivals[k] <= now:
-                mk, eq, U0, steps, _, _ = reqs[k]
-                cfg = mk(form)
-                cfg.device = local
-                ids.append(srv.submit(cfg, eq, U0, 1e9, max_steps=steps))
-                k += 1
-            for j, rid in enumerate(ids):
-                if j in done:
-                    continue
-                try:
-                    got = srv.poll(rid)
-                except wb.WenofvError:  # a numerically failed solve is a result too
-                    got = (None, None)
-                    failed.add(j)
-                if got is not None:
-                    done[j] = got
-            time.sleep(0.0005)
-        ok = [j for j in range(n) if j not in failed]
-        lat = [done[j][1].t_done - done[j][1].t_submit for j in ok]
-        qwait = [done[j][1].t_admit - done[j][1].t_submit for j in ok]
-        span = max(done[j][1].t_done for j in ok) - min(done[j][1].t_submit for j in ok)
-        span = max_over_ranks(span, dist, local)
-        assert all(done[j][1].steps == reqs[j][3] for j in ok)
-        finals[name] = [done[j][0] for j in range(n)]
-        work_ok = sum(reqs[j][3] * reqs[j][4] * 3 for j in ok)
-        res[name] = dict(value=world * work_ok / span, unit="cell-stage updates/s", solves_per_s=world * len(ok) / span,
-                         failed_requests=sorted(failed),
-                         p50_latency_s=_pctl(lat, 50), p99_latency_s=_pctl(lat, 99), p50_queue_s=_pctl(qwait, 50),
-                         makespan_s=span)
-        srv.close()
-    errs = {"euler": [], "two_phase": []}
-    for j in range(n):
-        a, b_ = finals["fp32_bulk"][j], finals["fp64"][j]
-        if a is not None and b_ is not None:
-            errs[reqs[j][5]].append(float(np.abs(a - b_).sum() / np.abs(b_).sum()))
-    res["fp32_bulk"]["rel_l1_vs_fp64"] = {k: dict(median=_pctl(v, 50), max=max(v) if v else None, n=len(v))
-                                          for k, v in errs.items()}
+    for name in forms:
+        form = {"fp64": wb.FP64, "fp32_bulk": wb.FP32_BULK}[name]
+        res[name], finals[name] = serve_stream(wb, reqs, arrivals, form, budget_bytes, local, dist, world)
+    if "fp32_bulk" in res:
+        finals["fp64_strict"] = serve_alone_strict(wb, reqs, local)
+        # errors per request kind (results of failed requests are left out)
+        by = {"euler": {"fp64": [], "fp32_bulk": []}, "two_phase": {"fp64": [], "fp32_bulk": []}}
+        for j, r in enumerate(reqs):
+            a, b, c = finals["fp32_bulk"][j], finals["fp64"][j], finals["fp64_strict"][j]
+            if a is None or b is None or c is None:
+                continue
+            by[r[5]]["fp32_bulk"].append(rel_l1(a, c))
+            by[r[5]]["fp64"].append(rel_l1(b, c))
+        res["errors"] = {k: summarize_errors(v) for k, v in by.items() if v["fp64"]}
+        res["fp32_bulk"]["speedup_vs_fp64"] = res["fp32_bulk"]["value"] / res["fp64"]["value"]
+    return res
+
+
+def run_serve(args, rank, world, dist):
+    """config 5: Poisson arrivals of mixed Euler / two-phase solves into the continuous-batching
+    server at the configured rate, plus a load sweep at rates the GPU sustains"""
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    wb = _load_package()
+    reqs = serve_requests(wb, args.requests, 5 + rank, args.min_steps, args.max_steps)
+    budget = args.hbm_budget_gb << 30
+    res = serve_measure(wb, reqs, args.rate, budget, 5 + rank, local, dist, world)
+    sweep = []
+    for rate in [float(x) for x in args.rates.split(",") if x]:
+        r = serve_measure(wb, reqs, rate, budget, 6 + rank, local, dist, world, forms=("fp64",))
+        sweep.append(dict(rate=rate, **{k: r["fp64"][k] for k in ("solves_per_s", "p50_latency_s", "p99_latency_s",
+                                                                   "p50_queue_s", "value")}))
     out = dict(metric="cell-stage updates/s", value=res["fp64"]["value"], unit="cell-stage updates/s", n_gpus=world,
-               steps=n, warmup=0, ms_per_step=None, higher_is_better=True, scaling="weak", vs_baseline=None,
+               steps=args.requests, warmup=0, ms_per_step=None, higher_is_better=True, scaling="weak", vs_baseline=None,
                dtype="f64", data="synthetic",
-               config=dict(workload=f"serving_stream_{n}", requests=n, arrival=f"Poisson, mean {args.rate} req/s "
-                           f"(seed {5 + rank})", grids="nx log-uniform 64..2048, ny log-uniform 64..512 (multiples of 8)",
+               config=dict(workload=f"serving_stream_{args.requests}", requests=args.requests,
+                           arrival=f"Poisson, mean {args.rate} req/s (seed {5 + rank})",
+                           grids="nx log-uniform 64..2048, ny log-uniform 64..512 (multiples of 8)",
                            steps=f"uniform {args.min_steps}..{args.max_steps} per request",
                            mix="Euler quadrants (outflow, conservative WENO-Z/HLLC) and two-phase columns "
                                "(periodic, characteristic WENO-Z/HLLC/limiter), 50/50",
                            hbm_budget_gb=args.hbm_budget_gb, parallelism=f"replicas x{world}",
                            latency="server clock, submission to completion"),
                solves_per_s=res["fp64"]["solves_per_s"], p50_latency_s=res["fp64"]["p50_latency_s"],
-               p99_latency_s=res["fp64"]["p99_latency_s"], fp64=res["fp64"], fp32_bulk=res["fp32_bulk"])
+               p99_latency_s=res["fp64"]["p99_latency_s"], fp64=res["fp64"], fp32_bulk=res["fp32_bulk"],
+               errors=res["errors"], load_sweep=sweep)
     return out
 
 
@@ -707,6 +844,8 @@ def main():
     ap.add_argument("--min-steps", type=int, default=50, help="serve: fewest steps of a request")
     ap.add_argument("--max-steps", type=int, default=2000, help="serve: most steps of a request")
     ap.add_argument("--hbm-budget-gb", type=int, default=150, help="serve: HBM budget of the server")
+    ap.add_argument("--rates", default="1,2,4", help="serve: arrival rates (req/s) of the load sweep")
+    ap.add_argument("--no-mix", action="store_true", help="default line: skip the batch and serve objects")
     ap.add_argument("--form", default="fp64", choices=["fp64", "fp64_strict", "fp32_bulk"])
     ap.add_argument("--cpu-steps", type=int, default=1, help="timed reference steps of the cpu_baseline leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -248,6 +248,9 @@ typedef struct {
     uint32_t flags;
     int status;
 } wenofv_request_info;
+/* starts a server on `device` with up to max_slots requests on the GPU at once.  The slots'
+ * device memory is one arena allocated here: hbm_budget_bytes, or the device's free memory
+ * less 1 GiB when that is smaller; admitting a request then allocates nothing. */
 int wenofv_server_create(int device, size_t hbm_budget_bytes, int max_slots, wenofv_server **out);
 void wenofv_server_destroy(wenofv_server *s);
 /* queues a solve of U0 (SoA) from t=0 to t_end, or max_steps steps if that comes first

@@ -147,6 +147,60 @@ def test_server_alone_equals_mixed(wb):
     srv.close()
 
 
+# FP32-bulk requests served beside FP64 ones (four launch groups, each its own branch of the
+# captured graph): each served result equals the same solve alone through the single-grid API
+# to SERVE_FP32_RTOL of max |U| (the per-instance arithmetic does not depend on the mix, so in
+# practice the results are the same bits)
+SERVE_FP32_RTOL = 1e-12
+
+
+def test_server_alone_equals_mixed_fp32(wb):
+    rng = np.random.default_rng(12)
+    reqs = []
+    for k in range(12):
+        nx, ny = [(64, 64), (96, 48), (128, 64), (40, 40)][k % 4]
+        prec = wb.FP64 if k % 4 == 3 else wb.FP32_BULK
+        if k % 3 == 2:
+            U0, _ = cases.euler_quadrants(nx, ny, seed=k)
+            cfg = wb.make_config(nx, ny, bc=wb.BC_OUTFLOW, cfl=0.4, scheme=1, flux=1, recon=0, precision=prec)
+            eq = wb.make_eq(kind=wb.EQ_EULER)
+        else:
+            U0, prm = cases.liquid_column(nx, ny, seed=k)
+            cfg, eq = column_cfg(wb, nx, ny, prm, prec)
+        reqs.append((cfg, eq, U0, int(rng.integers(6, 40))))
+    srv = wb.Server(0, hbm_budget_bytes=4 << 20, max_slots=5)
+    ids = []
+    for cfg, eq, U0, ns in reqs:
+        ids.append(srv.submit(cfg, eq, U0, 1e9, max_steps=ns))
+        time.sleep(0.001 * rng.integers(0, 3))
+    res = _drain(srv, ids)
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["active"] == 0 and st["resident_bytes"] == 0
+    for rid, (cfg, eq, U0, ns) in zip(ids, reqs):
+        U, info = res[rid]
+        assert info.status == 0 and info.steps == ns
+        ref, n = alone(wb, cfg, eq, U0, max_steps=ns)
+        assert np.abs(U - ref).max() <= SERVE_FP32_RTOL * np.abs(ref).max()
+    srv.close()
+
+
+def test_server_admits_after_retirement_without_regrowth(wb):
+    # a stream of requests larger in total than the arena: slots and arena blocks are reused
+    U0, prm = cases.liquid_column(64, 64, seed=4)
+    cfg, eq = column_cfg(wb, 64, 64, prm, wb.FP64)
+    per = 3 * 4 * 64 * 64 * 8 + (2 * 64 + 64) * 8
+    srv = wb.Server(0, hbm_budget_bytes=3 * per + 4096, max_slots=8)
+    ids = [srv.submit(cfg, eq, U0, 1e9, max_steps=4 + (k % 3)) for k in range(9)]
+    res = _drain(srv, ids)
+    ref = {n: alone(wb, cfg, eq, U0, max_steps=n)[0] for n in (4, 5, 6)}
+    for k, rid in enumerate(ids):
+        U, info = res[rid]
+        assert info.status == 0 and info.steps == 4 + (k % 3)
+        assert np.array_equal(U, ref[4 + (k % 3)])
+    assert srv.stats()["resident_bytes"] == 0
+    srv.close()
+
+
 def test_server_rejects_and_isolates_failures(wb):
     srv = wb.Server(0, hbm_budget_bytes=1 << 20, max_slots=2)
     U0, prm = cases.liquid_column(256, 256, seed=1)

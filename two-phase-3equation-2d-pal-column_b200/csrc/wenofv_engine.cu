@@ -181,6 +181,8 @@ Engine::~Engine()
     if (h_snap_) cudaFreeHost(h_snap_);
     if (snap_ready_) cudaEventDestroy(snap_ready_);
     if (snap_done_) cudaEventDestroy(snap_done_);
+    if (fork_) cudaEventDestroy(fork_);
+    cudaFree(arena_);
     if (copy_stream_) cudaStreamDestroy(copy_stream_);
     if (stream) cudaStreamDestroy(stream);
 }
@@ -191,7 +193,7 @@ size_t Engine::bytes_needed(const wenofv_config &c, const wenofv_eq_params &e)
     return 3 * (size_t)nvar_of(e.eq_kind) * c.ny * pitch * sizeof(double) + (2 * (size_t)c.nx + c.ny) * sizeof(double);
 }
 
-int Engine::init_slots(int capacity, int dev, int rk_method)
+int Engine::init_slots(int capacity, int dev, int rk_method, size_t arena_bytes)
 {
     if (capacity < 1) { set_error("capacity must be positive"); return WENOFV_EINVAL; }
     device = dev;
@@ -220,7 +222,62 @@ int Engine::init_slots(int capacity, int dev, int rk_method)
         h_state_[i] = fresh_state(0);
         h_state_[i].done = 1; // an empty slot is never stepped
     }
+    slot_off_.assign(cap_, 0);
+    if (arena_bytes > 0) {
+        arena_bytes = arena_bytes / 256 * 256;
+        WENOFV_CUDA(cudaMalloc((void **)&arena_, arena_bytes));
+        arena_bytes_ = arena_bytes;
+        arena_freelist_.clear();
+        arena_freelist_[0] = arena_bytes;
+        arena_used_.clear();
+    }
     return push_state();
+}
+
+// first fit over the free blocks; neighbouring free blocks are merged on release
+int Engine::arena_alloc(size_t bytes, size_t *off)
+{
+    bytes = (bytes + 255) / 256 * 256;
+    for (auto it = arena_freelist_.begin(); it != arena_freelist_.end(); ++it) {
+        if (it->second < bytes) continue;
+        const size_t o = it->first, rest = it->second - bytes;
+        arena_freelist_.erase(it);
+        if (rest) arena_freelist_[o + bytes] = rest;
+        arena_used_[o] = bytes;
+        *off = o;
+        return WENOFV_OK;
+    }
+    set_error("the slot arena has no free block of %zu bytes", bytes);
+    return WENOFV_ENOMEM;
+}
+
+void Engine::arena_free(size_t off)
+{
+    auto u = arena_used_.find(off);
+    if (u == arena_used_.end()) return;
+    size_t o = off, sz = u->second;
+    arena_used_.erase(u);
+    auto nx = arena_freelist_.lower_bound(o);
+    if (nx != arena_freelist_.end() && nx->first == o + sz) { // merge with the block after
+        sz += nx->second;
+        nx = arena_freelist_.erase(nx);
+    }
+    if (nx != arena_freelist_.begin()) { // merge with the block before
+        auto pv = std::prev(nx);
+        if (pv->first + pv->second == o) {
+            o = pv->first;
+            sz += pv->second;
+            arena_freelist_.erase(pv);
+        }
+    }
+    arena_freelist_[o] = sz;
+}
+
+size_t Engine::arena_free_bytes() const
+{
+    size_t f = 0;
+    for (const auto &kv : arena_freelist_) f += kv.second;
+    return f;
 }
 
 // NEUMANN2's fixed ghost frame: every variable on the grid widened by 4 cells on each side
@@ -258,11 +315,20 @@ int Engine::alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params
     const int nv = nvar_of(e.eq_kind);
     const int pitch = (c.nx + 15) / 16 * 16;
     const size_t per = (size_t)nv * c.ny * pitch;
-    WENOFV_CUDA(cudaMalloc(&dmem_[i], 3 * per * sizeof(double)));
-    WENOFV_CUDA(cudaMemsetAsync(dmem_[i], 0, 3 * per * sizeof(double), stream));
     std::vector<double> met(2 * (size_t)c.nx + c.ny);
     grid_metric(c, met.data(), met.data() + c.nx, met.data() + 2 * c.nx);
-    WENOFV_CUDA(cudaMalloc(&dmetric_[i], met.size() * sizeof(double)));
+    if (arena_) { // one arena block: three state buffers, then the metric
+        size_t off = 0;
+        const int rc = arena_alloc(bytes_needed(c, e), &off);
+        if (rc) return rc;
+        slot_off_[i] = off;
+        dmem_[i] = (double *)(arena_ + off);
+        dmetric_[i] = dmem_[i] + 3 * per;
+    } else {
+        WENOFV_CUDA(cudaMalloc(&dmem_[i], 3 * per * sizeof(double)));
+        WENOFV_CUDA(cudaMalloc(&dmetric_[i], met.size() * sizeof(double)));
+    }
+    WENOFV_CUDA(cudaMemsetAsync(dmem_[i], 0, 3 * per * sizeof(double), stream));
     WENOFV_CUDA(cudaMemcpyAsync(dmetric_[i], met.data(), met.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
     InstDesc &d = desc_[i];
     std::memset(&d, 0, sizeof d);
@@ -289,8 +355,9 @@ int Engine::alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params
         WENOFV_CUDA(cudaMemsetAsync(dtheta_[i], 0, (size_t)c.nx * c.ny, stream));
         d.theta_flag = dtheta_[i];
     }
+    // from pageable host memory: both copies have read their sources when they return
     WENOFV_CUDA(cudaMemcpyAsync(d_desc_ + i, &d, sizeof(InstDesc), cudaMemcpyHostToDevice, stream));
-    WENOFV_CUDA(cudaStreamSynchronize(stream)); // the metric staging above is a host local
+    if (!arena_) WENOFV_CUDA(cudaStreamSynchronize(stream));
     cfg_[i] = c;
     eq_[i] = e;
     live_[i] = 1;
@@ -302,8 +369,12 @@ int Engine::alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params
 void Engine::free_instance(int i)
 {
     if (i < 0 || i >= cap_) return;
-    if (dmem_[i]) cudaFree(dmem_[i]);
-    if (dmetric_[i]) cudaFree(dmetric_[i]);
+    if (arena_) {
+        if (dmem_[i]) arena_free(slot_off_[i]);
+    } else {
+        if (dmem_[i]) cudaFree(dmem_[i]);
+        if (dmetric_[i]) cudaFree(dmetric_[i]);
+    }
     if (dframe_[i]) cudaFree(dframe_[i]);
     if (dtheta_[i]) cudaFree(dtheta_[i]);
     dmem_[i] = nullptr;
@@ -342,9 +413,8 @@ int Engine::init(int count, const wenofv_config *cfgs, const wenofv_eq_params *e
 int Engine::ensure_work()
 {
     if (!work_dirty_) return WENOFV_OK;
-    WENOFV_CUDA(cudaStreamSynchronize(stream));
-    drop_graphs();
-    const int rc = build_work();
+    WENOFV_CUDA(cudaStreamSynchronize(stream)); // the lists may be in use by queued launches
+    const int rc = build_work();                // drops the graphs when a buffer moved
     if (!rc) work_dirty_ = false;
     return rc;
 }
@@ -378,17 +448,7 @@ int Engine::remove(int slot)
 
 int Engine::start(int slot, double t_end, int64_t max_steps)
 {
-    if (!live(slot)) { set_error("slot %d is not live", slot); return WENOFV_EINVAL; }
-    WENOFV_CUDA(cudaSetDevice(device));
-    int rc = ensure_work();
-    if (rc) return rc;
-    h_state_[slot] = fresh_state(0);
-    h_state_[slot].mode = MODE_ADVANCE;
-    h_state_[slot].t_end = t_end;
-    h_state_[slot].max_steps = max_steps > 0 ? max_steps : 0;
-    WENOFV_CUDA(cudaMemcpyAsync(d_state_ + slot, &h_state_[slot], sizeof(InstState), cudaMemcpyHostToDevice, stream));
-    // the CFL pass also re-derives the (unchanged) step of the slots already running
-    return launch_cfl_all();
+    return start_many(std::vector<int>{slot}, std::vector<double>{t_end}, std::vector<int64_t>{max_steps});
 }
 
 int Engine::run_pairs(int K)
@@ -401,6 +461,14 @@ int Engine::run_pairs(int K)
     return rc;
 }
 
+int Engine::run_graph_pairs(int K)
+{
+    WENOFV_CUDA(cudaSetDevice(device));
+    const int rc = ensure_work();
+    if (rc) return rc;
+    return run_graph(K);
+}
+
 int Engine::refresh() { return pull_state(); }
 
 void Engine::free_work()
@@ -408,38 +476,82 @@ void Engine::free_work()
     for (Group &g : groups_) {
         cudaFree(g.d_work);
         cudaFree(g.d_fin);
+        cudaFree(g.d_counts);
+        cudaFree(g.d_init_work);
+        cudaFree(g.d_init_fin);
         cudaFree(g.d_counter);
+        if (g.gstream) cudaStreamDestroy(g.gstream);
+        if (g.joined) cudaEventDestroy(g.joined);
     }
     groups_.clear();
 }
 
-// one launch group per (form, equation, reconstruction); work items are strips of TX
-// columns by `seg` rows; the grid is a persistent one (at most the resident CTA count)
+// the template key of an instance's launch group: form, equation, reconstruction, scheme
+// (PRIMITIVE3 always on WENOEXP's 7-point geometry) and flux
+long Engine::group_key(int i) const
+{
+    const int strict = cfg_[i].precision == WENOFV_FP64_STRICT;
+    const int fp32 = cfg_[i].precision == WENOFV_FP32_BULK;
+    const int sch = desc_[i].recon == 4 ? 2 : desc_[i].scheme;
+    const int flx = desc_[i].eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : desc_[i].flux;
+    return ((long)strict << 32) | ((long)fp32 << 24) | (desc_[i].eq_kind << 16) | (desc_[i].recon << 8) | (sch << 4) | flx;
+}
+
+namespace {
+// grows a device array to at least n elements (capacity doubles); reports whether it moved
+template <class T> int grow(T **p, int *cap, int n, bool *moved)
+{
+    if (n <= *cap) return WENOFV_OK;
+    int c = std::max(64, *cap);
+    while (c < n) c *= 2;
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    WENOFV_CUDA(cudaMalloc(p, (size_t)c * sizeof(T)));
+    *cap = c;
+    *moved = true;
+    return WENOFV_OK;
+}
+} // namespace
+
+// One launch group per template key; work items are strips of TX columns by `seg` rows.  The
+// grid is persistent (at most the resident CTA count; in slot mode always that count, so that
+// a captured graph fits any later work list).  Work lists are rewritten in place; a new group
+// or a buffer that had to grow drops the captured graphs.
 int Engine::build_work()
 {
-    free_work();
-    std::map<long, int> key2g;
-    for (int i = 0; i < cap_; i++) {
-        if (!live_[i]) continue;
-        const int strict = cfg_[i].precision == WENOFV_FP64_STRICT;
-        const int fp32 = cfg_[i].precision == WENOFV_FP32_BULK;
-        // PRIMITIVE3 reconstructs on WENOEXP's 7-point geometry whatever SCHEME is
-        const int sch = desc_[i].recon == 4 ? 2 : desc_[i].scheme;
-        const int flx = desc_[i].eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : desc_[i].flux;
-        const long key = ((long)strict << 32) | ((long)fp32 << 24) | (desc_[i].eq_kind << 16) | (desc_[i].recon << 8) |
-                         (sch << 4) | flx;
-        auto it = key2g.find(key);
-        if (it == key2g.end()) {
-            Group g;
-            g.ns_strict = strict; g.fp32 = fp32; g.eq = desc_[i].eq_kind; g.recon = desc_[i].recon;
-            g.scheme = sch; g.flux = flx;
-            key2g[key] = (int)groups_.size();
-            groups_.push_back(g);
-            it = key2g.find(key);
-        }
-        groups_[it->second].inst.push_back(i);
+    std::map<long, std::vector<int>> members;
+    for (int i = 0; i < cap_; i++)
+        if (live_[i]) members[group_key(i)].push_back(i);
+    bool moved = false;
+    if (!slot_mode) { // contexts and batches: the groups of the current instances only
+        free_work();
+        moved = true;
+    }
+    for (auto &kv : members) {
+        bool found = false;
+        for (Group &g : groups_) found = found || g.key == kv.first;
+        if (found) continue;
+        Group g;
+        const int i = kv.second[0];
+        g.key = kv.first;
+        g.ns_strict = cfg_[i].precision == WENOFV_FP64_STRICT;
+        g.fp32 = cfg_[i].precision == WENOFV_FP32_BULK;
+        g.eq = desc_[i].eq_kind;
+        g.recon = desc_[i].recon;
+        g.scheme = desc_[i].recon == 4 ? 2 : desc_[i].scheme;
+        g.flux = desc_[i].eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : desc_[i].flux;
+        WENOFV_CUDA(cudaMalloc(&g.d_counts, 4 * sizeof(int)));
+        WENOFV_CUDA(cudaMalloc(&g.d_counter, sizeof(unsigned int)));
+        WENOFV_CUDA(cudaMemsetAsync(g.d_counter, 0, sizeof(unsigned int), stream));
+        WENOFV_CUDA(cudaStreamCreateWithFlags(&g.gstream, cudaStreamNonBlocking));
+        WENOFV_CUDA(cudaEventCreateWithFlags(&g.joined, cudaEventDisableTiming));
+        groups_.push_back(g);
+        moved = true;
     }
     for (Group &g : groups_) {
+        auto m = members.find(g.key);
+        g.inst = m == members.end() ? std::vector<int>() : m->second;
         const int tx = g.ns_strict ? strict::stage_tx(g.eq, g.scheme) : fast::stage_tx(g.eq, g.scheme);
         const int bps = std::max(1, g.ns_strict ? strict::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux)
                                                 : fast::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux));
@@ -458,14 +570,20 @@ int Engine::build_work()
                 for (int i0 = 0; i0 < cfg_[i].nx; i0 += tx)
                     work.push_back(WorkItem{i, i0, j0, std::min(cfg_[i].ny, j0 + seg)});
         g.nwork = (int)work.size();
-        g.grid = std::min(g.nwork, slots);
-        WENOFV_CUDA(cudaMalloc(&g.d_work, work.size() * sizeof(WorkItem)));
-        WENOFV_CUDA(cudaMemcpy(g.d_work, work.data(), work.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
-        WENOFV_CUDA(cudaMalloc(&g.d_fin, g.inst.size() * sizeof(int)));
-        WENOFV_CUDA(cudaMemcpy(g.d_fin, g.inst.data(), g.inst.size() * sizeof(int), cudaMemcpyHostToDevice));
-        WENOFV_CUDA(cudaMalloc(&g.d_counter, sizeof(unsigned int)));
-        WENOFV_CUDA(cudaMemset(g.d_counter, 0, sizeof(unsigned int)));
+        const int grid = slot_mode ? slots : std::max(1, std::min(g.nwork, slots));
+        if (grid != g.grid) moved = true;
+        g.grid = grid;
+        int rc = grow(&g.d_work, &g.cap_work, std::max(1, g.nwork), &moved);
+        if (!rc) rc = grow(&g.d_fin, &g.cap_fin, std::max(1, (int)g.inst.size()), &moved);
+        if (rc) return rc;
+        // pageable sources: each copy has read its source when it returns
+        if (g.nwork) WENOFV_CUDA(cudaMemcpyAsync(g.d_work, work.data(), work.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, stream));
+        if (!g.inst.empty())
+            WENOFV_CUDA(cudaMemcpyAsync(g.d_fin, g.inst.data(), g.inst.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+        const int counts[2] = {g.nwork, (int)g.inst.size()};
+        WENOFV_CUDA(cudaMemcpyAsync(g.d_counts, counts, sizeof counts, cudaMemcpyHostToDevice, stream));
     }
+    if (moved) drop_graphs();
     return WENOFV_OK;
 }
 
@@ -481,19 +599,28 @@ int Engine::pull_state()
     return WENOFV_OK;
 }
 
+// the launch arguments every stage and CFL launch of a group shares
+int Engine::group_launch(const Group &g, StageLaunch &L) const
+{
+    std::memset(&L, 0, sizeof L);
+    L.inst = d_desc_;
+    L.state = d_state_;
+    L.work = g.d_work;
+    L.nwork = g.nwork;
+    L.fin_ids = g.d_fin;
+    L.nfin = (int)g.inst.size();
+    L.counts = g.d_counts;
+    L.counter = g.d_counter;
+    return WENOFV_OK;
+}
+
+// one stage of every group; inside a graph capture each group launches on its own branch
 int Engine::launch_stage_all(int parity, int stage, double *rhs_out)
 {
     const Roles ro = stage_roles(rk, parity, stage);
     for (Group &g : groups_) {
         StageLaunch L;
-        std::memset(&L, 0, sizeof L);
-        L.inst = d_desc_;
-        L.state = d_state_;
-        L.work = g.d_work;
-        L.nwork = g.nwork;
-        L.fin_ids = g.d_fin;
-        L.nfin = (int)g.inst.size();
-        L.counter = g.d_counter;
+        group_launch(g, L);
         if (rhs_out) {
             L.bin = L.bun = L.bout = cur_;
             L.first_stage = 1;
@@ -506,8 +633,9 @@ int Engine::launch_stage_all(int parity, int stage, double *rhs_out)
             L.rk1 = rk == 0;
             stage_coeffs(rk, stage, L.A, L.B, L.C);
         }
-        const int rc = g.ns_strict ? strict::launch_stage(g.eq, g.recon, g.fp32, g.scheme, g.flux, L, g.grid, stream)
-                                   : fast::launch_stage(g.eq, g.recon, g.fp32, g.scheme, g.flux, L, g.grid, stream);
+        cudaStream_t s = capturing_ ? g.gstream : stream;
+        const int rc = g.ns_strict ? strict::launch_stage(g.eq, g.recon, g.fp32, g.scheme, g.flux, L, g.grid, s)
+                                   : fast::launch_stage(g.eq, g.recon, g.fp32, g.scheme, g.flux, L, g.grid, s);
         if (rc) return cuda_fail((cudaError_t)rc, "stage kernel launch");
     }
     return WENOFV_OK;
@@ -517,17 +645,58 @@ int Engine::launch_cfl_all()
 {
     for (Group &g : groups_) {
         StageLaunch L;
-        std::memset(&L, 0, sizeof L);
-        L.inst = d_desc_;
-        L.state = d_state_;
-        L.work = g.d_work;
-        L.nwork = g.nwork;
-        L.fin_ids = g.d_fin;
-        L.nfin = (int)g.inst.size();
-        L.counter = g.d_counter;
+        group_launch(g, L);
         const int rc = g.ns_strict ? strict::launch_cfl(g.eq, g.scheme, L, g.grid, stream)
                                    : fast::launch_cfl(g.eq, g.scheme, L, g.grid, stream);
         if (rc) return cuda_fail((cudaError_t)rc, "cfl kernel launch");
+    }
+    return WENOFV_OK;
+}
+
+// the CFL pass and loop set-up (FIN_INIT) of the given slots only: per group, a work list
+// of just their strips in the group's second pair of buffers
+int Engine::start_many(const std::vector<int> &slots, const std::vector<double> &t_end, const std::vector<int64_t> &max_steps)
+{
+    WENOFV_CUDA(cudaSetDevice(device));
+    int rc = ensure_work();
+    if (rc) return rc;
+    for (size_t k = 0; k < slots.size(); k++) {
+        const int sl = slots[k];
+        if (!live(sl)) { set_error("slot %d is not live", sl); return WENOFV_EINVAL; }
+        h_state_[sl] = fresh_state(0);
+        h_state_[sl].mode = MODE_ADVANCE;
+        h_state_[sl].t_end = t_end[k];
+        h_state_[sl].max_steps = max_steps[k] > 0 ? max_steps[k] : 0;
+        WENOFV_CUDA(cudaMemcpyAsync(d_state_ + sl, &h_state_[sl], sizeof(InstState), cudaMemcpyHostToDevice, stream));
+    }
+    for (Group &g : groups_) {
+        std::vector<int> fin;
+        std::vector<WorkItem> work;
+        const int tx = g.ns_strict ? strict::stage_tx(g.eq, g.scheme) : fast::stage_tx(g.eq, g.scheme);
+        for (int sl : slots) {
+            if (group_key(sl) != g.key) continue;
+            fin.push_back(sl);
+            for (int j0 = 0; j0 < cfg_[sl].ny; j0 += 32)
+                for (int i0 = 0; i0 < cfg_[sl].nx; i0 += tx) work.push_back(WorkItem{sl, i0, j0, std::min(cfg_[sl].ny, j0 + 32)});
+        }
+        if (fin.empty()) continue;
+        bool moved = false;
+        rc = grow(&g.d_init_work, &g.cap_init_work, (int)work.size(), &moved);
+        if (!rc) rc = grow(&g.d_init_fin, &g.cap_init_fin, (int)fin.size(), &moved);
+        if (rc) return rc;
+        WENOFV_CUDA(cudaMemcpyAsync(g.d_init_work, work.data(), work.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, stream));
+        WENOFV_CUDA(cudaMemcpyAsync(g.d_init_fin, fin.data(), fin.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+        StageLaunch L;
+        group_launch(g, L);
+        L.work = g.d_init_work;
+        L.nwork = (int)work.size();
+        L.fin_ids = g.d_init_fin;
+        L.nfin = (int)fin.size();
+        L.counts = nullptr;
+        const int grid = std::max(1, std::min(L.nwork, g.grid));
+        const int lrc = g.ns_strict ? strict::launch_cfl(g.eq, g.scheme, L, grid, stream)
+                                    : fast::launch_cfl(g.eq, g.scheme, L, grid, stream);
+        if (lrc) return cuda_fail((cudaError_t)lrc, "cfl kernel launch");
     }
     return WENOFV_OK;
 }
@@ -775,21 +944,35 @@ void Engine::drop_graphs()
     graph_defs_.clear();
 }
 
-// K captured pairs of RK steps (buffer roles return to buffer 0 after each pair)
+// K captured pairs of RK steps (buffer roles return to buffer 0 after each pair).  The
+// launch groups are independent of each other (their instances never share memory), so
+// each group's chain of stages is its own branch of the graph, forked from and joined back
+// into the context's stream: groups of different template keys run side by side.
 int Engine::run_graph(int K)
 {
     Range nvtx_range("wenofv::run_graph");
     auto it = graphs_.find(K);
     if (it == graphs_.end()) {
+        if (!fork_) WENOFV_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
         cudaGraph_t g;
         WENOFV_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         int rc = 0;
-        for (int k = 0; k < K && !rc; k++)
+        cudaError_t e = cudaEventRecord(fork_, stream);
+        for (Group &gr : groups_)
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(gr.gstream, fork_, 0);
+        capturing_ = true;
+        for (int k = 0; k < K && !rc && e == cudaSuccess; k++)
             for (int p = 0; p < 2 && !rc; p++)
                 for (int s = 0; s < stage_count(rk) && !rc; s++) rc = launch_stage_all(p, s, nullptr);
-        const cudaError_t e = cudaStreamEndCapture(stream, &g);
+        capturing_ = false;
+        for (Group &gr : groups_) {
+            if (e == cudaSuccess) e = cudaEventRecord(gr.joined, gr.gstream);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, gr.joined, 0);
+        }
+        const cudaError_t ee = cudaStreamEndCapture(stream, &g);
         if (rc) return rc;
-        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        if (e != cudaSuccess) return cuda_fail(e, "graph fork/join");
+        if (ee != cudaSuccess) return cuda_fail(ee, "cudaStreamEndCapture");
         cudaGraphExec_t ex;
         WENOFV_CUDA(cudaGraphInstantiate(&ex, g, 0));
         graph_defs_[K] = g;

@@ -63,12 +63,18 @@ public:
     int accuracy(int i, const wenofv_testcase *tc, double t, double *norms); // wenofv_init.cu
 
     // ---- slots (serving): capacity fixed at init_slots, instances added and removed ----
-    int init_slots(int capacity, int device, int rk_method);
+    // arena_bytes > 0: every slot's device memory comes from one arena allocated here, so that
+    // adding a slot calls no cudaMalloc
+    int init_slots(int capacity, int device, int rk_method, size_t arena_bytes = 0);
     int add(const wenofv_config &cfg, const wenofv_eq_params &eq, int *slot);
     int remove(int slot);
     int start(int slot, double t_end, int64_t max_steps); // device loop of one slot: t = 0 -> t_end
+    // start several slots at once: one CFL launch per launch group over the new slots only
+    int start_many(const std::vector<int> &slots, const std::vector<double> &t_end, const std::vector<int64_t> &max_steps);
     int run_pairs(int K);                                 // K pairs of steps of every live, unfinished slot
+    int run_graph_pairs(int K);                           // the same, as one captured graph
     int refresh();                                        // pull the device loop state
+    size_t arena_free_bytes() const;
     const InstState &slot_state(int slot) const { return h_state_[slot]; }
     bool live(int slot) const { return slot >= 0 && slot < cap_ && live_[slot]; }
     static size_t bytes_needed(const wenofv_config &cfg, const wenofv_eq_params &eq);
@@ -80,17 +86,33 @@ public:
     bool slot_mode = false; // serving: every slot keeps its own current buffer
 
 private:
+    // one persistent launch per RK stage for the instances of one template key; the work
+    // list, the finalize list and their counts live in device buffers that are rewritten in
+    // place while they fit, so a captured graph stays valid when instances come and go
     struct Group {
+        long key = 0;
         int ns_strict, fp32, eq, recon, scheme, flux;
         std::vector<int> inst;
         WorkItem *d_work = nullptr;
-        int nwork = 0;
+        int nwork = 0, cap_work = 0;
         int *d_fin = nullptr;
+        int cap_fin = 0;
+        int *d_counts = nullptr; // {nwork, nfin} (+ {init nwork, init nfin} for start_many)
+        WorkItem *d_init_work = nullptr;
+        int *d_init_fin = nullptr;
+        int cap_init_work = 0, cap_init_fin = 0;
         unsigned int *d_counter = nullptr;
         int grid = 0;
+        cudaStream_t gstream = nullptr; // the group's branch inside a captured graph
+        cudaEvent_t joined = nullptr;
     };
+    struct Block { size_t off, size; };
     int build_work();
     void free_work();
+    long group_key(int i) const;
+    int group_launch(const Group &g, StageLaunch &L) const;
+    int arena_alloc(size_t bytes, size_t *off);
+    void arena_free(size_t off);
     int ensure_work();
     int alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params &e);
     void free_instance(int i);
@@ -136,6 +158,14 @@ private:
     bool work_dirty_ = true;
     std::map<int, cudaGraphExec_t> graphs_;
     std::map<int, cudaGraph_t> graph_defs_;
+    cudaEvent_t fork_ = nullptr;
+    bool capturing_ = false; // launch_stage_all puts each group on its own branch
+    // slot arena: one allocation, first-fit blocks of 256-byte granularity
+    char *arena_ = nullptr;
+    size_t arena_bytes_ = 0;
+    std::map<size_t, size_t> arena_freelist_; // offset -> size of the free blocks
+    std::map<size_t, size_t> arena_used_;     // offset -> size of the allocated blocks
+    std::vector<size_t> slot_off_;            // per slot: offset of its block (arena mode)
 };
 
 } // namespace wenofv

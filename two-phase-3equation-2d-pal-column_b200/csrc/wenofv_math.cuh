@@ -1304,17 +1304,29 @@ __device__ __forceinline__ void riemann(const EqParams &P, int flux_arg, const d
             else tp_llf<R>(l, r, UL, UR, Fr, xdir);
         }
     } else if constexpr (EQ == EQ_EULER) {
-        EUState<R> l, r;
-        eu_state<R>(P.gamma, ULd, l);
-        eu_state<R>(P.gamma, URd, r);
-        if (flux == 1) eu_hllc<R>(P.gamma, l, r, UL, UR, Fr, xdir);
-        else eu_llf<R>(l, r, UL, UR, Fr, xdir);
+        if constexpr (F32) {
+            // FP32-bulk: the Euler flux stays FP64.  In FP32 the star flux F_K + S_K (U* - U_K)
+            // and the pressure terms round away the small flux differences between the two
+            // faces of a cell, which moved shock solutions by ~1e-4 (relative L1) within
+            // ~1000 steps; the reconstruction is the FP32 part of this equation's bulk form.
+            EUState<double> l, r;
+            eu_state<double>(P.gamma, ULd, l);
+            eu_state<double>(P.gamma, URd, r);
+            if (flux == 1) eu_hllc<double>(P.gamma, l, r, ULd, URd, F, xdir);
+            else eu_llf<double>(l, r, ULd, URd, F, xdir);
+        } else {
+            EUState<R> l, r;
+            eu_state<R>(P.gamma, ULd, l);
+            eu_state<R>(P.gamma, URd, r);
+            if (flux == 1) eu_hllc<R>(P.gamma, l, r, UL, UR, Fr, xdir);
+            else eu_llf<R>(l, r, UL, UR, Fr, xdir);
+        }
     } else {
         const R an = xdir ? (R(P.adv_u) * R(1.0) + R(P.adv_v) * R(0.0)) : (R(P.adv_u) * R(0.0) + R(P.adv_v) * R(1.0));
         const R ws = std_max(fabs(an), fabs(an));
         Fr[0] = R(0.5) * (an * UL[0] + an * UR[0] - ws * (UR[0] - UL[0]));
     }
-    if constexpr (!(F32 && IsTwoPhase<EQ>::value)) { // the FP32 two-phase fluxes write F themselves
+    if constexpr (!(F32 && (IsTwoPhase<EQ>::value || EQ == EQ_EULER))) { // those FP32 forms write F themselves
 #pragma unroll
         for (int v = 0; v < NV; v++) F[v] = (double)Fr[v];
     }

@@ -1,15 +1,25 @@
 // wenofv_server.cu -- continuous batching of solve requests on one GPU.
 //
-// A background engine thread owns one slot Engine.  Each round it
-//   1. admits queued requests in arrival order while a slot is free and the request's
-//      device state fits the HBM budget (three FP64 state buffers and the grid metric),
-//   2. runs a chunk of RK step pairs in which one batched launch per RK stage advances every
-//      running request (the stage kernel skips finished ones),
+// A background engine thread owns one slot Engine whose slot memory is a single arena
+// allocated when the server starts (the HBM budget, or what the device has free), so that
+// admitting a request calls no cudaMalloc.  Each round it
+//   1. admits queued requests in arrival order while a slot is free and the request's device
+//      state (three FP64 state buffers and the grid metric) fits in the arena: upload, then
+//      one CFL pass per launch group over the new slots only,
+//   2. runs a chunk of RK step pairs as one captured graph in which every launch group (one
+//      per template key: form, equation, reconstruction, scheme, flux) is its own branch, so
+//      groups of different keys run side by side; a persistent launch per RK stage advances
+//      every running request of its group, and a request that reaches its end time or step
+//      count stops inside the kernel (its work items are skipped) while the others go on.
+//      The chunk length follows the measured time per step pair (about CHUNK_TARGET_MS per
+//      round), not the shortest remaining request,
 //   3. reads the device loop state back, copies finished requests' results to host memory,
-//      frees their slots and budget.
-// Requests arriving while others run join at the next round boundary, so their work shares
-// launches with the requests already on the GPU.  submit/poll only touch the queue and the
-// result table under a mutex; they never call CUDA.
+//      frees their slots and arena blocks.
+// Work lists are rewritten in place in device buffers, so a captured graph stays valid while
+// requests come and go; it is re-captured only when a new template key appears or a list
+// outgrows its buffer.  Requests arriving while others run join at the next round boundary,
+// so their work shares launches with the requests already on the GPU.  submit/poll only touch
+// the queue and the result table under a mutex; they never call CUDA.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -60,6 +70,10 @@ struct wenofv_server {
     std::map<int64_t, Request *> all;
     std::vector<Request *> active; // by slot
     int64_t next_id = 1, admitted = 0, completed = 0;
+    static constexpr double CHUNK_TARGET_MS = 10.0;
+    static constexpr int CHUNK_MAX_PAIRS = 32;
+    double ms_per_pair = 1.0; // running estimate of one step pair of the current mix
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool stop = false;
     int fatal = 0;
     std::thread th;
@@ -76,23 +90,29 @@ int wenofv_server::round()
         std::lock_guard<std::mutex> lk(mu);
         int free_slots = 0;
         for (Request *r : active) free_slots += r == nullptr;
-        while (!queue.empty() && free_slots > 0 && resident + queue.front()->bytes <= budget) {
+        size_t arena_free = eng.arena_free_bytes();
+        while (!queue.empty() && free_slots > 0 && resident + queue.front()->bytes <= budget &&
+               (queue.front()->bytes + 255) / 256 * 256 <= arena_free) {
             Request *r = queue.front();
             queue.pop_front();
             resident += r->bytes;
+            arena_free -= (r->bytes + 255) / 256 * 256;
             admit.push_back(r);
             free_slots--;
         }
     }
+    std::vector<int> new_slots;
+    std::vector<double> new_tend;
+    std::vector<int64_t> new_max;
+    std::vector<Request *> started;
     for (Request *r : admit) {
         int slot = -1;
         int rc = eng.add(r->cfg, r->eq, &slot);
         if (!rc) rc = eng.upload(slot, r->U.data(), WENOFV_LAYOUT_SOA);
-        if (!rc) rc = eng.start(slot, r->t_end, r->max_steps);
         std::lock_guard<std::mutex> lk(mu);
         r->info.t_admit = now_s(t0);
         admitted++;
-        if (rc) {
+        if (rc) { // e.g. a fragmented arena: the request fails alone, the others go on
             if (slot >= 0) eng.remove(slot);
             resident -= r->bytes;
             r->info.status = rc;
@@ -104,29 +124,31 @@ int wenofv_server::round()
         }
         r->slot = slot;
         active[slot] = r;
+        new_slots.push_back(slot);
+        new_tend.push_back(r->t_end);
+        new_max.push_back(r->max_steps);
+    }
+    if (!new_slots.empty()) {
+        const int rc = eng.start_many(new_slots, new_tend, new_max);
+        if (rc) return rc;
     }
     int running = 0;
     for (Request *r : active) running += r != nullptr;
     if (running == 0) return 0;
 
-    // 2. a chunk of step pairs for every running request: the smallest remaining estimate
-    //    bounds the chunk so that finished requests leave (and queued ones enter) promptly
-    int rc = eng.refresh();
+    // 2. a chunk of step pairs for every running request, as one captured graph; its length
+    //    follows the measured time per pair so that a round takes about CHUNK_TARGET_MS
+    int K = 1;
+    while (K < CHUNK_MAX_PAIRS && K * ms_per_pair < CHUNK_TARGET_MS / 2) K *= 2;
+    cudaEventRecord(ev0, eng.stream);
+    int rc = eng.run_graph_pairs(K);
     if (rc) return rc;
-    double least = 1e30;
-    for (Request *r : active) {
-        if (!r) continue;
-        const InstState &s = eng.slot_state(r->slot);
-        if (s.done) { least = 0; continue; }
-        double left = s.dt > 0 ? (s.t_end - s.now) / s.dt : 1.0;
-        if (s.max_steps > 0) left = std::min(left, (double)(s.max_steps - s.nsteps));
-        least = std::min(least, left);
-    }
-    int K = (int)std::ceil(least / 2.0);
-    K = std::max(1, std::min(K, 16));
-    if (least > 0) rc = eng.run_pairs(K);
-    if (!rc) rc = eng.refresh();
+    cudaEventRecord(ev1, eng.stream);
+    rc = eng.refresh();
     if (rc) return rc;
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess && ms > 0) ms_per_pair = 0.5 * ms_per_pair + 0.5 * ms / K;
+    (void)cudaGetLastError();
 
     // 3. collect finished requests
     for (size_t k = 0; k < active.size(); k++) {
@@ -191,7 +213,21 @@ int wenofv_server_create(int device, size_t hbm_budget_bytes, int max_slots, wen
     s->max_slots = max_slots;
     s->t0 = std::chrono::steady_clock::now();
     s->eng.slot_mode = true;
-    const int rc = s->eng.init_slots(max_slots, device, 2);
+    // the slot arena: the budget, or what the device has free less a margin for the
+    // engine's own buffers
+    size_t free_b = 0, total_b = 0;
+    if (cudaSetDevice(device) != cudaSuccess || cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        (void)cudaGetLastError();
+        delete s;
+        set_error("no CUDA device %d", device);
+        return WENOFV_EINVAL;
+    }
+    const size_t margin = (size_t)1 << 30;
+    const size_t arena = std::min(hbm_budget_bytes, free_b > 2 * margin ? free_b - margin : free_b / 2);
+    s->budget = arena;
+    int rc = s->eng.init_slots(max_slots, device, 2, arena);
+    if (!rc && cudaEventCreate(&s->ev0) != cudaSuccess) rc = WENOFV_ECUDA;
+    if (!rc && cudaEventCreate(&s->ev1) != cudaSuccess) rc = WENOFV_ECUDA;
     if (rc) { delete s; return rc; }
     s->active.assign(max_slots, nullptr);
     s->th = std::thread([s] { s->loop(); });
@@ -209,6 +245,8 @@ void wenofv_server_destroy(wenofv_server *s)
     }
     if (s->th.joinable()) s->th.join();
     for (auto &kv : s->all) delete kv.second;
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
     delete s;
 }
 
@@ -222,7 +260,7 @@ int wenofv_server_submit(wenofv_server *s, const wenofv_config *cfg, const wenof
     if (cfg->bc == WENOFV_BC_NEUMANN2) { set_error("the server takes no NEUMANN2 requests (they need a ghost frame)"); return WENOFV_ENOTSUP; }
     if (!(t_end > 0)) { set_error("t_end must be positive"); return WENOFV_EINVAL; }
     const size_t bytes = Engine::bytes_needed(*cfg, *eq);
-    if (bytes > s->budget) { set_error("request needs %zu bytes, over the HBM budget", bytes); return WENOFV_ENOMEM; }
+    if ((bytes + 255) / 256 * 256 > s->budget) { set_error("request needs %zu bytes, over the HBM budget", bytes); return WENOFV_ENOMEM; }
     Request *r = new (std::nothrow) Request;
     if (!r) { set_error("host allocation failed"); return WENOFV_ENOMEM; }
     const size_t n = (size_t)nvar_of(eq->eq_kind) * cfg->nx * cfg->ny;

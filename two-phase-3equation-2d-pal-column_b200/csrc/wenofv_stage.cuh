@@ -174,7 +174,8 @@ __device__ __forceinline__ void launch_epilogue(const StageLaunch &L, int fin_ki
     __syncthreads();
     if (*s_last) {
         __threadfence();
-        for (int k = threadIdx.x; k < L.nfin; k += blockDim.x) finalize_instance(&L.state[L.fin_ids[k]], fin_kind, L.bout);
+        const int nfin = L.counts ? L.counts[1] : L.nfin;
+        for (int k = threadIdx.x; k < nfin; k += blockDim.x) finalize_instance(&L.state[L.fin_ids[k]], fin_kind, L.bout);
         __syncthreads();
         if (threadIdx.x == 0) *L.counter = 0u;
     }
@@ -823,7 +824,8 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
     constexpr int TX = StageGeom<EQ, H>::TX;
     __shared__ StageSmem<EQ, H> S;
     extern __shared__ __align__(16) double stage_dyn_smem[]; // StageDynSmem bytes: the primitive ring
-    for (int w = blockIdx.x; w < L.nwork; w += gridDim.x) {
+    const int nwork = L.counts ? L.counts[0] : L.nwork;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         const WorkItem it = L.work[w];
         const InstDesc &D = L.inst[it.inst];
         InstState *st = &L.state[it.inst];
@@ -894,7 +896,8 @@ __global__ void __launch_bounds__(NT) cfl_kernel(const StageLaunch L)
     constexpr int NV = EqTraits<EQ>::NV;
     __shared__ double sred[NT / 32];
     __shared__ int s_last;
-    for (int w = blockIdx.x; w < L.nwork; w += gridDim.x) {
+    const int nwork = L.counts ? L.counts[0] : L.nwork;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         const WorkItem it = L.work[w];
         const InstDesc &D = L.inst[it.inst];
         InstState *st = &L.state[it.inst];

@@ -51,6 +51,8 @@ struct StageLaunch {
     int nwork;
     const int *fin_ids; // instances this launch finalizes
     int nfin;
+    const int *counts; // optional device copy of {nwork, nfin}: the serving engine updates its
+                       // work lists in place, so captured graphs keep fixed launch arguments
     unsigned int *counter;
     int bin, bun, bout; // buffer roles: stage input, U^n, output
     int first_stage, final_stage, rk1;
