@@ -552,7 +552,7 @@ int Engine::build_work()
     for (Group &g : groups_) {
         auto m = members.find(g.key);
         g.inst = m == members.end() ? std::vector<int>() : m->second;
-        const int tx = g.ns_strict ? strict::stage_tx(g.eq, g.scheme) : fast::stage_tx(g.eq, g.scheme);
+        const int tx = g.ns_strict ? strict::stage_tx(g.eq, g.recon, g.fp32, g.scheme) : fast::stage_tx(g.eq, g.recon, g.fp32, g.scheme);
         const int bps = std::max(1, g.ns_strict ? strict::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux)
                                                 : fast::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux));
         const int slots = sms_ * (ctas_per_sm_ > 0 ? std::min(ctas_per_sm_, bps) : bps);
@@ -646,8 +646,8 @@ int Engine::launch_cfl_all()
     for (Group &g : groups_) {
         StageLaunch L;
         group_launch(g, L);
-        const int rc = g.ns_strict ? strict::launch_cfl(g.eq, g.scheme, L, g.grid, stream)
-                                   : fast::launch_cfl(g.eq, g.scheme, L, g.grid, stream);
+        const int rc = g.ns_strict ? strict::launch_cfl(g.eq, g.recon, g.fp32, g.scheme, L, g.grid, stream)
+                                   : fast::launch_cfl(g.eq, g.recon, g.fp32, g.scheme, L, g.grid, stream);
         if (rc) return cuda_fail((cudaError_t)rc, "cfl kernel launch");
     }
     return WENOFV_OK;
@@ -672,7 +672,7 @@ int Engine::start_many(const std::vector<int> &slots, const std::vector<double> 
     for (Group &g : groups_) {
         std::vector<int> fin;
         std::vector<WorkItem> work;
-        const int tx = g.ns_strict ? strict::stage_tx(g.eq, g.scheme) : fast::stage_tx(g.eq, g.scheme);
+        const int tx = g.ns_strict ? strict::stage_tx(g.eq, g.recon, g.fp32, g.scheme) : fast::stage_tx(g.eq, g.recon, g.fp32, g.scheme);
         for (int sl : slots) {
             if (group_key(sl) != g.key) continue;
             fin.push_back(sl);
@@ -694,8 +694,8 @@ int Engine::start_many(const std::vector<int> &slots, const std::vector<double> 
         L.nfin = (int)fin.size();
         L.counts = nullptr;
         const int grid = std::max(1, std::min(L.nwork, g.grid));
-        const int lrc = g.ns_strict ? strict::launch_cfl(g.eq, g.scheme, L, grid, stream)
-                                    : fast::launch_cfl(g.eq, g.scheme, L, grid, stream);
+        const int lrc = g.ns_strict ? strict::launch_cfl(g.eq, g.recon, g.fp32, g.scheme, L, grid, stream)
+                                    : fast::launch_cfl(g.eq, g.recon, g.fp32, g.scheme, L, grid, stream);
         if (lrc) return cuda_fail((cudaError_t)lrc, "cfl kernel launch");
     }
     return WENOFV_OK;

@@ -21,11 +21,25 @@ namespace fast {
 #define WENOFV_HAS_FP32 1
 #endif
 
-// strip width of the work items: 5-point stencils (H = 2) or WENOEXP's 7-point ones (H = 3)
-int stage_tx(int eq, int scheme)
+// threads per CTA and strip width of the stage kernel of (eq, recon, form): StageThreads
+static int stage_threads(int eq, int recon, int fp32)
 {
-    if (scheme == 2) return eq == EQ_LINEAR_ADV ? StageGeom<EQ_LINEAR_ADV, 3>::TX : StageGeom<EQ_TWO_PHASE, 3>::TX;
-    return eq == EQ_LINEAR_ADV ? StageGeom<EQ_LINEAR_ADV, 2>::TX : StageGeom<EQ_TWO_PHASE, 2>::TX;
+    return (!fp32 && eq != EQ_LINEAR_ADV && eq != EQ_TWO_PHASE_SG && recon != 4) ? 256 : 128;
+}
+static_assert(StageThreads<EQ_TWO_PHASE, 1, double>::value == 256 && StageThreads<EQ_TWO_PHASE, 4, double>::value == 128 &&
+                  StageThreads<EQ_TWO_PHASE, 1, float>::value == 128 && StageThreads<EQ_LINEAR_ADV, 0, double>::value == 128 &&
+                  StageThreads<EQ_TWO_PHASE_SG, 1, double>::value == 128 && StageThreads<EQ_EULER, 0, double>::value == 256,
+              "stage_threads mirrors StageThreads");
+
+// strip width of the work items: 5-point stencils (H = 2) or WENOEXP's 7-point ones (H = 3)
+template <int NT> static int tx_of(int eq, int scheme)
+{
+    if (scheme == 2) return eq == EQ_LINEAR_ADV ? StageGeom<EQ_LINEAR_ADV, 3, NT>::TX : StageGeom<EQ_TWO_PHASE, 3, NT>::TX;
+    return eq == EQ_LINEAR_ADV ? StageGeom<EQ_LINEAR_ADV, 2, NT>::TX : StageGeom<EQ_TWO_PHASE, 2, NT>::TX;
+}
+int stage_tx(int eq, int recon, int fp32, int scheme)
+{
+    return stage_threads(eq, recon, fp32) == 256 ? tx_of<256>(eq, scheme) : tx_of<128>(eq, scheme);
 }
 
 template <int EQ, int RECON, class R, int SCH, int FLX> static const void *stage_fn()
@@ -88,13 +102,27 @@ static const void *pick_stage(int eq, int recon, int fp32, int scheme, int flux)
     return pick_eq<double>(eq, recon, scheme, flux);
 }
 
-// dynamic shared memory of a stage kernel (the primitive ring; the same for both geometries)
-static int stage_dyn_bytes(int eq, int recon)
+// dynamic shared memory of a stage kernel: its StageSmem block, then the primitive ring of
+// the primitive reconstructions (the same size for both geometries)
+template <int H, int NT> static int smem_of(int eq)
 {
-    static_assert(StageDynSmem<EQ_TWO_PHASE, 2, 2>::value == StageDynSmem<EQ_TWO_PHASE, 2, 3>::value, "ring size");
-    return (eq == EQ_TWO_PHASE && recon >= 2) ? StageDynSmem<EQ_TWO_PHASE, 2, 2>::value : 0;
+    return eq == EQ_TWO_PHASE      ? StageSmemBytes<EQ_TWO_PHASE, H, NT>::value
+         : eq == EQ_EULER          ? StageSmemBytes<EQ_EULER, H, NT>::value
+         : eq == EQ_TWO_PHASE_SG   ? StageSmemBytes<EQ_TWO_PHASE_SG, H, NT>::value
+                                   : StageSmemBytes<EQ_LINEAR_ADV, H, NT>::value;
 }
-// static plus dynamic shared memory passes the default 48 KB: opt in (not during a stream
+static int stage_dyn_bytes(int eq, int recon, int fp32, int scheme)
+{
+    static_assert(StageDynSmem<EQ_TWO_PHASE, 2, 2, 256>::value == StageDynSmem<EQ_TWO_PHASE, 2, 3, 256>::value, "ring size");
+    const int nt = stage_threads(eq, recon, fp32);
+    const int ring = (eq == EQ_TWO_PHASE && recon >= 2)
+                         ? (nt == 256 ? StageDynSmem<EQ_TWO_PHASE, 2, 2, 256>::value : StageDynSmem<EQ_TWO_PHASE, 2, 2, 128>::value)
+                         : 0;
+    const int base = nt == 256 ? (scheme == 2 ? smem_of<3, 256>(eq) : smem_of<2, 256>(eq))
+                               : (scheme == 2 ? smem_of<3, 128>(eq) : smem_of<2, 128>(eq));
+    return base + ring;
+}
+// dynamic shared memory past the default 48 KB needs an opt-in (not during a stream
 // capture, where the engine has already done it through stage_blocks_per_sm)
 static cudaError_t allow_dyn(const void *fn, int dyn)
 {
@@ -106,40 +134,42 @@ int launch_stage(int eq, int recon, int fp32, int scheme, int flux, const StageL
 {
     const void *fn = pick_stage(eq, recon, fp32, scheme, flux);
     if (!fn) return (int)cudaErrorInvalidValue;
-    const int dyn = stage_dyn_bytes(eq, recon);
-    if (dyn > 0) {
+    const int dyn = stage_dyn_bytes(eq, recon, fp32, scheme);
+    if (dyn > 48 * 1024) {
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         cudaError_t e = cudaStreamIsCapturing((cudaStream_t)stream, &cs);
         if (e != cudaSuccess) return (int)e;
         if (cs == cudaStreamCaptureStatusNone && (e = allow_dyn(fn, dyn)) != cudaSuccess) return (int)e;
     }
     void *args[] = {(void *)&L};
-    return (int)cudaLaunchKernel(fn, dim3(grid), dim3(NT), args, (size_t)dyn, (cudaStream_t)stream);
+    return (int)cudaLaunchKernel(fn, dim3(grid), dim3(stage_threads(eq, recon, fp32)), args, (size_t)dyn, (cudaStream_t)stream);
 }
 
-template <int H> static const void *cfl_fn(int eq)
+static const void *cfl_fn(int eq)
 {
-    return eq == EQ_TWO_PHASE      ? (const void *)cfl_kernel<EQ_TWO_PHASE, StageGeom<EQ_TWO_PHASE, H>::TX>
-         : eq == EQ_EULER          ? (const void *)cfl_kernel<EQ_EULER, StageGeom<EQ_EULER, H>::TX>
-         : eq == EQ_TWO_PHASE_SG   ? (const void *)cfl_kernel<EQ_TWO_PHASE_SG, StageGeom<EQ_TWO_PHASE_SG, H>::TX>
-                                   : (const void *)cfl_kernel<EQ_LINEAR_ADV, StageGeom<EQ_LINEAR_ADV, H>::TX>;
+    return eq == EQ_TWO_PHASE      ? (const void *)cfl_kernel<EQ_TWO_PHASE>
+         : eq == EQ_EULER          ? (const void *)cfl_kernel<EQ_EULER>
+         : eq == EQ_TWO_PHASE_SG   ? (const void *)cfl_kernel<EQ_TWO_PHASE_SG>
+                                   : (const void *)cfl_kernel<EQ_LINEAR_ADV>;
 }
 
-int launch_cfl(int eq, int scheme, const StageLaunch &L, int grid, void *stream)
+// the CFL pass over the work items of a launch group, whose strips are those of its stage kernel
+int launch_cfl(int eq, int recon, int fp32, int scheme, const StageLaunch &L, int grid, void *stream)
 {
-    const void *fn = scheme == 2 ? cfl_fn<3>(eq) : cfl_fn<2>(eq);
-    void *args[] = {(void *)&L};
-    return (int)cudaLaunchKernel(fn, dim3(grid), dim3(NT), args, 0, (cudaStream_t)stream);
+    StageLaunch Lc = L;
+    Lc.tx = stage_tx(eq, recon, fp32, scheme);
+    void *args[] = {(void *)&Lc};
+    return (int)cudaLaunchKernel(cfl_fn(eq), dim3(grid), dim3(CFL_NT), args, 0, (cudaStream_t)stream);
 }
 
 int stage_blocks_per_sm(int eq, int recon, int fp32, int scheme, int flux)
 {
     const void *fn = pick_stage(eq, recon, fp32, scheme, flux);
     if (!fn) return 0;
-    const int dyn = stage_dyn_bytes(eq, recon);
-    if (allow_dyn(fn, dyn) != cudaSuccess) return 0;
+    const int dyn = stage_dyn_bytes(eq, recon, fp32, scheme);
+    if (dyn > 48 * 1024 && allow_dyn(fn, dyn) != cudaSuccess) return 0;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, NT, (size_t)dyn) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, stage_threads(eq, recon, fp32), (size_t)dyn) != cudaSuccess) return 0;
     return n;
 }
 

@@ -103,7 +103,7 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
         set_error("the no-allocation step needs 2*nx + ny <= %d", NOALLOC_METRIC_DOUBLES);
         return WENOFV_EINVAL;
     }
-    const int tx = strictf ? strict::stage_tx(eq->eq_kind, sch) : fast::stage_tx(eq->eq_kind, sch);
+    const int tx = strictf ? strict::stage_tx(eq->eq_kind, recon, 0, sch) : fast::stage_tx(eq->eq_kind, recon, fp32, sch);
     const long nwork = (long)((cfg->nx + tx - 1) / tx) * ((cfg->ny + NOALLOC_ROWS - 1) / NOALLOC_ROWS);
     if (nwork > NOALLOC_MAX_WORK) { set_error("the no-allocation step takes at most %d work items", NOALLOC_MAX_WORK); return WENOFV_EINVAL; }
 

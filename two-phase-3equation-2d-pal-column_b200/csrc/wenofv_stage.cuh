@@ -14,7 +14,7 @@
 // cells whose stencils contain it (the reference recomputes it per cell,
 // src/WENOFV.cpp:670-687 and :796-833, with identical operands).
 //
-// Thread mapping (NT = 128 threads): a unit of the y-sweep is (position, variable), of the
+// Thread mapping (NT threads, StageThreads): a unit of the y-sweep is (position, variable), of the
 // x-sweep (cell, variable), of the Riemann phase (face, Gauss point) and of the update
 // (cell, variable); groups of NV (or 4) consecutive lanes belong to the same position, cell
 // or face, so characteristic projections, the limiter's theta and the GL quadrature sums
@@ -37,7 +37,19 @@ namespace strict {
 namespace fast {
 #endif
 
-constexpr int NT = 128;
+// threads per CTA of a stage kernel.  256 (strips of 58 columns, 2 CTAs per SM at 128
+// registers) for the FP64 forms of the 4-variable systems: the halo positions and the idle
+// lanes of the x-sweep, Riemann and update phases drop from ~19 % to ~9 % of the thread
+// slots, measured 9 % faster per stage than 3 CTAs of 128 threads at 168 registers (and 10 %
+// faster than 4 CTAs of 128 at 128 registers).  128 for FP32-bulk (5 CTAs per SM at 96
+// registers measured best), for PRIMITIVE3 (its variable-major y-sweep maps 4 warps to 32
+// positions), for scalar advection (strips of 122 columns already) and for the stiffened gas
+// (whose Newton equilibrium spills at 128 registers).
+template <int EQ, int RECON, class R> struct StageThreads {
+    static constexpr int value =
+        (sizeof(R) == sizeof(double) && EqTraits<EQ>::NV == 4 && RECON != 4 && EQ != EQ_TWO_PHASE_SG) ? 256 : 128;
+};
+constexpr int CFL_NT = 128; // threads per CTA of cfl_kernel
 
 // the reconstruction of one stencil at the Gauss-Lobatto points, by scheme: the 5-point
 // WENO-JS/Z (half-width H = 2) or the 7-point WENOEXP (H = 3, FP64 only)
@@ -204,7 +216,7 @@ __device__ __forceinline__ double block_min(double v, double *s_red)
 // H positions on each side of it and its neighbours', so the strip carries GH = H + 1
 // halo positions on each side (GH = 3 is the reference's ghost layer count,
 // src/WENOFV.cpp:59)
-template <int EQ, int H> struct StageGeom {
+template <int EQ, int H, int NT> struct StageGeom {
     static constexpr int NV = EqTraits<EQ>::NV;
     static constexpr int GH = H + 1;
     static constexpr int TX = NT / NV - 2 * GH; // interior columns per strip
@@ -212,8 +224,8 @@ template <int EQ, int H> struct StageGeom {
 };
 
 // shared memory of one CTA (doubles)
-template <int EQ, int H> struct StageSmem {
-    static constexpr int NV = StageGeom<EQ, H>::NV, TX = StageGeom<EQ, H>::TX, P = StageGeom<EQ, H>::P;
+template <int EQ, int H, int NT> struct StageSmem {
+    static constexpr int NV = StageGeom<EQ, H, NT>::NV, TX = StageGeom<EQ, H, NT>::TX, P = StageGeom<EQ, H, NT>::P;
     // Strides are padded so that the lanes of a half-warp (8-byte accesses are served 16
     // lanes at a time) hit distinct bank pairs: rows of 4 variables at P+4 doubles
     // (variable v of 4 neighbouring positions: banks 8v + 2p), positions and cells at an odd
@@ -239,6 +251,11 @@ template <int EQ, int H> struct StageSmem {
     int s_last;
 };
 
+// bytes of a CTA's StageSmem, rounded to 16 (the primitive ring follows it)
+template <int EQ, int H, int NT> struct StageSmemBytes {
+    static constexpr int value = (int)((sizeof(StageSmem<EQ, H, NT>) + 15) / 16 * 16);
+};
+
 // periodic wrap or outflow clamp (the ghost fill of the non-wall kinds)
 __device__ __forceinline__ int map_index_po(int k, int n, int bc)
 {
@@ -248,11 +265,11 @@ __device__ __forceinline__ int map_index_po(int k, int n, int bc)
 }
 
 // the wall form of load_row: ghost cells are plain loads with the momentum signs
-template <int EQ, int H>
-__device__ __forceinline__ void load_row_walls(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
+template <int EQ, int H, int NT>
+__device__ __forceinline__ void load_row_walls(double (*dst)[StageSmem<EQ, H, NT>::PS], const double *buf, const InstDesc &D, int row,
                                             int i0, InstState *st)
 {
-    constexpr int P = StageGeom<EQ, H>::P, NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
+    constexpr int P = StageGeom<EQ, H, NT>::P, NV = StageGeom<EQ, H, NT>::NV, GH = StageGeom<EQ, H, NT>::GH;
     const size_t plane = (size_t)D.ny * D.pitch;
     (void)st;
     int fy;
@@ -276,11 +293,11 @@ __device__ __forceinline__ void load_row_walls(double (*dst)[StageSmem<EQ, H>::P
 // loads of the instance's fixed frame [v][ny+8][nx+8] (interior at (4, 4)).  Rows stay in
 // [-GH, ny+GH) with GH <= 4; columns past nx+4 only occur in a strip's unused tail and are
 // clamped into the frame.
-template <int EQ, int H>
-__device__ __forceinline__ void load_row_frame(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
+template <int EQ, int H, int NT>
+__device__ __forceinline__ void load_row_frame(double (*dst)[StageSmem<EQ, H, NT>::PS], const double *buf, const InstDesc &D, int row,
                                             int i0, InstState *st)
 {
-    constexpr int P = StageGeom<EQ, H>::P, NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
+    constexpr int P = StageGeom<EQ, H, NT>::P, NV = StageGeom<EQ, H, NT>::NV, GH = StageGeom<EQ, H, NT>::GH;
     static_assert(GH <= 4, "the frame holds 4 ghost layers");
     const size_t plane = (size_t)D.ny * D.pitch;
     const int fw = D.nx + 8;
@@ -308,20 +325,20 @@ __device__ __forceinline__ void load_row_frame(double (*dst)[StageSmem<EQ, H>::P
 
 // the two ghost rules that are not an index map (walls, NEUMANN2 frame), behind one out-of-line
 // call so that the periodic and outflow loads keep the stage kernel's register allocation
-template <int EQ, int H>
-__device__ __noinline__ void load_row_other(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
+template <int EQ, int H, int NT>
+__device__ __noinline__ void load_row_other(double (*dst)[StageSmem<EQ, H, NT>::PS], const double *buf, const InstDesc &D, int row,
                                             int i0, InstState *st)
 {
-    if (D.bc == 3) load_row_frame<EQ, H>(dst, buf, D, row, i0, st);
-    else load_row_walls<EQ, H>(dst, buf, D, row, i0, st);
+    if (D.bc == 3) load_row_frame<EQ, H, NT>(dst, buf, D, row, i0, st);
+    else load_row_walls<EQ, H, NT>(dst, buf, D, row, i0, st);
 }
 
 // one row of NV x P stage values into shared memory (ghost fill = index map), cp.async 8 B
-template <int EQ, int H>
-__device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ, H>::PS], const double *buf, const InstDesc &D, int row,
+template <int EQ, int H, int NT>
+__device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ, H, NT>::PS], const double *buf, const InstDesc &D, int row,
                                          int i0, InstState *st)
 {
-    constexpr int P = StageGeom<EQ, H>::P, NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
+    constexpr int P = StageGeom<EQ, H, NT>::P, NV = StageGeom<EQ, H, NT>::NV, GH = StageGeom<EQ, H, NT>::GH;
     const size_t plane = (size_t)D.ny * D.pitch;
     (void)st;
     if (D.bc == 0 || D.bc == 5) {
@@ -340,7 +357,7 @@ __device__ __forceinline__ void load_row(double (*dst)[StageSmem<EQ, H>::PS], co
         }
         return;
     }
-    load_row_other<EQ, H>(dst, buf, D, row, i0, st);
+    load_row_other<EQ, H, NT>(dst, buf, D, row, i0, st);
 }
 
 // value of a reconstruction: in the deviation form the anchor plus the FP32 deviation, in
@@ -354,10 +371,10 @@ template <bool DEV, class R> __device__ __forceinline__ double anchor(double c, 
 // ---- phase 0: the per-cell eigensystem data (L/R rows, wave speeds) of row r at the
 // strip's P positions, computed once per cell by one thread each (threads t0 .. t0+n-1)
 // instead of by every lane that needs it.  Identical arithmetic to the per-lane form.
-template <int EQ, int RECON, int H>
-__device__ __forceinline__ void phase_eigen(StageSmem<EQ, H> &S, const InstDesc &D, int r, int t0, int n)
+template <int EQ, int RECON, int H, int NT>
+__device__ __forceinline__ void phase_eigen(StageSmem<EQ, H, NT> &S, const InstDesc &D, int r, int t0, int n)
 {
-    constexpr int NV = StageGeom<EQ, H>::NV, P = StageGeom<EQ, H>::P;
+    constexpr int NV = StageGeom<EQ, H, NT>::NV, P = StageGeom<EQ, H, NT>::P;
     if constexpr (NV > 1) {
         if (!(RECON == 1 || D.limiter)) return;
         for (int p = (int)threadIdx.x - t0; p < P; p += n) {
@@ -382,17 +399,17 @@ __device__ __forceinline__ void phase_eigen(StageSmem<EQ, H> &S, const InstDesc 
 // FP64.
 // bytes of dynamic shared memory of a stage kernel: the primitive-variable ring of the
 // primitive reconstructions (8 rows of the 4 primitives at the strip's positions)
-template <int EQ, int RECON, int H> struct StageDynSmem {
-    static constexpr int value = (RECON >= 2 && EqTraits<EQ>::NV == 4) ? 8 * 4 * StageSmem<EQ, H>::PS * (int)sizeof(double) : 0;
+template <int EQ, int RECON, int H, int NT> struct StageDynSmem {
+    static constexpr int value = (RECON >= 2 && EqTraits<EQ>::NV == 4) ? 8 * 4 * StageSmem<EQ, H, NT>::PS * (int)sizeof(double) : 0;
 };
 
-template <int EQ, int RECON, class R, int SCH>
-__device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>::H> &S, const InstDesc &D, int r, double *ring_raw,
+template <int EQ, int RECON, class R, int SCH, int NT>
+__device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>::H, NT> &S, const InstDesc &D, int r, double *ring_raw,
                                              bool first)
 {
     using SR = typename ReconSel<R, SCH, RECON>::type;
     constexpr int H = SR::H, NS = SR::NS;
-    constexpr int NV = StageGeom<EQ, H>::NV;
+    constexpr int NV = StageGeom<EQ, H, NT>::NV;
     constexpr bool DEV = sizeof(R) < sizeof(double); // deviation form
     const int t = threadIdx.x;
     // PRIMITIVE3 reconstructs z1 with another kernel than p, u, v: one warp per variable (the
@@ -400,7 +417,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
     // variables of a position on 4 lanes, so that the two kernels do not diverge in a warp
     const int p = RECON == 4 ? (t & 31) : t / NV;
     const int v = RECON == 4 ? (((t >> 5) + r) & 3) : t - p * NV;
-    static_assert(RECON != 4 || (NV == 4 && StageGeom<EQ, H>::P == 32 && NT == 128), "variable-major y-sweep");
+    static_assert(RECON != 4 || (NV == 4 && StageGeom<EQ, H, NT>::P == 32 && NT == 128), "variable-major y-sweep");
     if (RECON != 1 || NV == 1) {
         // conservative: the averages; primitive (RECONSTRUCTIONTYPE 2-4): the primitive
         // variables of each of the NS cells (src/WENOFV.cpp:944-979).  Each (position,
@@ -411,7 +428,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
 #pragma unroll
         for (int m = 0; m < NS; m++) {
             if constexpr (RECON >= 2 && NV == 4) {
-                auto ring = reinterpret_cast<double (*)[4][StageSmem<EQ, H>::PS]>(ring_raw);
+                auto ring = reinterpret_cast<double (*)[4][StageSmem<EQ, H, NT>::PS]>(ring_raw);
                 const int row = r - H + m;
                 if (first || m == NS - 1) {
                     double U4[4], W4[4];
@@ -489,13 +506,13 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
 
 // ---- phase 2: x-direction sweep + limiter of row r (src/WENOFV.cpp:690-721, :836-880,
 //      limiter :1895-2000) -> face states (FP64 in every form) ------------------------------
-template <int EQ, int RECON, class R, int SCH>
-__device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>::H> &S, const InstDesc &D, InstState *st, int r,
+template <int EQ, int RECON, class R, int SCH, int NT>
+__device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>::H, NT> &S, const InstDesc &D, InstState *st, int r,
                                              int i0, int TXe, const double *ring_raw, bool flag_row)
 {
     using SR = typename ReconSel<R, SCH, RECON>::type;
     constexpr int H = SR::H, NS = SR::NS;
-    constexpr int NV = StageGeom<EQ, H>::NV, TX = StageGeom<EQ, H>::TX, GH = StageGeom<EQ, H>::GH;
+    constexpr int NV = StageGeom<EQ, H, NT>::NV, TX = StageGeom<EQ, H, NT>::TX, GH = StageGeom<EQ, H, NT>::GH;
     constexpr bool DEV = sizeof(R) < sizeof(double);
     const int t = threadIdx.x;
     const int cu = t / NV, v = t - cu * NV;
@@ -511,7 +528,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
         // its points back to conserved variables, and shuffles hand every lane its variable
         // at the 12 boundary points.  Lanes 1 and 2 also evaluate the inner points (unused)
         // to keep the lanes converged.
-        auto ring = reinterpret_cast<const double (*)[4][StageSmem<EQ, H>::PS]>(ring_raw);
+        auto ring = reinterpret_cast<const double (*)[4][StageSmem<EQ, H, NT>::PS]>(ring_raw);
         const int gj = v;
         double pv[4][4]; // [gpi][variable] at (gpi, gj)
 #pragma unroll
@@ -692,11 +709,11 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
 // x-faces of row r (when r is an interior row of the item) and y-faces between rows r-1
 // and r (when r-1 >= j0-1 and r <= j1).  Four consecutive lanes hold the four Gauss
 // points of one face; lane gp = 0 sums them in the reference's order.
-template <int EQ, class R, int FLX, int H>
-__device__ __forceinline__ void phase_riemann(StageSmem<EQ, H> &S, const InstDesc &D, InstState *st, int r, int i0, int j0, int j1,
+template <int EQ, class R, int FLX, int H, int NT>
+__device__ __forceinline__ void phase_riemann(StageSmem<EQ, H, NT> &S, const InstDesc &D, InstState *st, int r, int i0, int j0, int j1,
                                               int TXe)
 {
-    constexpr int NV = StageGeom<EQ, H>::NV, TX = StageGeom<EQ, H>::TX;
+    constexpr int NV = StageGeom<EQ, H, NT>::NV, TX = StageGeom<EQ, H, NT>::TX;
     const int nxf = (r >= j0 && r < j1) ? (TX + 1) * 4 : 0;
     const int nyf = (r >= j0 && r <= j1) ? TX * 4 : 0;
     const int total = nxf + nyf;
@@ -746,11 +763,11 @@ __device__ __forceinline__ void phase_riemann(StageSmem<EQ, H> &S, const InstDes
 
 // ---- phase 4: RHS scatter (src/WENOFV.cpp:1802-1827) + SSP-RK combination (:376-473)
 //      of row q = r-1, and on the final stage the per-cell CFL step (:486-514) ---------
-template <int EQ, int H>
-__device__ __forceinline__ double phase_update(StageSmem<EQ, H> &S, const InstDesc &D, InstState *st, const StageLaunch &L,
+template <int EQ, int H, int NT>
+__device__ __forceinline__ double phase_update(StageSmem<EQ, H, NT> &S, const InstDesc &D, InstState *st, const StageLaunch &L,
                                                int q, int i0, int TXe, double dt, double cmin)
 {
-    constexpr int NV = StageGeom<EQ, H>::NV, GH = StageGeom<EQ, H>::GH;
+    constexpr int NV = StageGeom<EQ, H, NT>::NV, GH = StageGeom<EQ, H, NT>::GH;
     const int t = threadIdx.x;
     const int cu = t / NV, v = t - cu * NV;
     const bool act = cu < TXe;
@@ -809,21 +826,28 @@ __device__ __forceinline__ double phase_update(StageSmem<EQ, H> &S, const InstDe
 }
 
 // resident CTAs per SM the register allocation is bounded for (measured best): the FP64
-// forms at 3 keep all values in registers (4 spills and runs slower); the FP32-bulk form
-// runs 4 (conservative) or 5 (characteristic, a few spilled values) CTAs
-template <int RECON, class R> struct StageMinBlocks {
-    static constexpr int value = sizeof(R) < sizeof(double) ? (RECON == 1 ? 5 : 4) : 3;
+// forms of 256 threads at 2 (128 registers, a few spilled values); PRIMITIVE3 (128 threads)
+// at 3, which keeps all values in registers (4 spills and runs slower); the FP32-bulk form
+// runs 4 (conservative) or 5 (characteristic, a few spilled values) CTAs of 128
+template <int EQ, int RECON, class R> struct StageMinBlocks {
+    static constexpr int value = sizeof(R) < sizeof(double) ? (RECON == 1 ? 5 : 4)
+                                                              : (StageThreads<EQ, RECON, R>::value == 256 ? 2 : 3);
 };
 
 // SCH, FLX: the scheme (0 WENO-JS, 1 WENO-Z, 2 WENOEXP) and flux (0 LLF, 1 HLLC) of every
 // instance of the launch, as compile-time constants (the engine groups instances by them)
 template <int EQ, int RECON, class R, int SCH, int FLX>
-__global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_kernel(const StageLaunch L)
+__global__ void __launch_bounds__(StageThreads<EQ, RECON, R>::value, StageMinBlocks<EQ, RECON, R>::value)
+    stage_kernel(const StageLaunch L)
 {
+    constexpr int NT = StageThreads<EQ, RECON, R>::value;
     constexpr int H = StencilRecon<R, SCH>::H;
-    constexpr int TX = StageGeom<EQ, H>::TX;
-    __shared__ StageSmem<EQ, H> S;
-    extern __shared__ __align__(16) double stage_dyn_smem[]; // StageDynSmem bytes: the primitive ring
+    constexpr int TX = StageGeom<EQ, H, NT>::TX;
+    // the CTA's shared block is dynamic shared memory (it outgrows the 48 KB static limit for
+    // wider strips): StageSmem, then StageDynSmem bytes of the primitive ring
+    extern __shared__ __align__(16) unsigned char stage_smem_raw[];
+    StageSmem<EQ, H, NT> &S = *reinterpret_cast<StageSmem<EQ, H, NT> *>(stage_smem_raw);
+    double *stage_dyn_smem = reinterpret_cast<double *>(stage_smem_raw + StageSmemBytes<EQ, H, NT>::value);
     const int nwork = L.counts ? L.counts[0] : L.nwork;
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         const WorkItem it = L.work[w];
@@ -852,7 +876,7 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
         const bool flag_rows = D.theta_flag != nullptr && L.final_stage && !L.rhs_out;
         // rows j0-1-H .. j0-1+H, the stencils of the first iteration's row
 #pragma unroll 1
-        for (int m = 0; m <= 2 * H; m++) load_row<EQ, H>(S.su[(it.j0 - 1 - H + m) & 7], bin, D, it.j0 - 1 - H + m, it.i0, st);
+        for (int m = 0; m <= 2 * H; m++) load_row<EQ, H, NT>(S.su[(it.j0 - 1 - H + m) & 7], bin, D, it.j0 - 1 - H + m, it.i0, st);
         cp_async_commit();
         double cmin = __longlong_as_double(0x7ff0000000000000LL);
 #pragma unroll 1
@@ -860,23 +884,23 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
             cp_async_wait_all();
             __syncthreads();
             // row r+H+1 into the slot of row r-H-1 (8 slots: rows r-H .. r+H in use, one in flight)
-            if (r + H + 1 <= it.j1 + H) load_row<EQ, H>(S.su[(r + H + 1) & 7], bin, D, r + H + 1, it.i0, st);
-            if (!L.first_stage && r >= it.j0 && r < it.j1) load_row<EQ, H>(S.sun[r & 1], bun, D, r, it.i0, st);
+            if (r + H + 1 <= it.j1 + H) load_row<EQ, H, NT>(S.su[(r + H + 1) & 7], bin, D, r + H + 1, it.i0, st);
+            if (!L.first_stage && r >= it.j0 && r < it.j1) load_row<EQ, H, NT>(S.sun[r & 1], bun, D, r, it.i0, st);
             cp_async_commit();
             if (r == it.j0 - 1) { // eigensystems of the first row; later rows come from phase 3
-                phase_eigen<EQ, RECON, H>(S, D, r, 0, NT);
+                phase_eigen<EQ, RECON, H, NT>(S, D, r, 0, NT);
                 __syncthreads();
             }
-            phase_ysweep<EQ, RECON, R, SCH>(S, D, r, stage_dyn_smem, r == it.j0 - 1);
+            phase_ysweep<EQ, RECON, R, SCH, NT>(S, D, r, stage_dyn_smem, r == it.j0 - 1);
             __syncthreads();
-            phase_xsweep<EQ, RECON, R, SCH>(S, D, st, r, it.i0, TXe, stage_dyn_smem, flag_rows && r >= it.j0 && r < it.j1);
+            phase_xsweep<EQ, RECON, R, SCH, NT>(S, D, st, r, it.i0, TXe, stage_dyn_smem, flag_rows && r >= it.j0 && r < it.j1);
             __syncthreads();
-            phase_riemann<EQ, R, FLX, H>(S, D, st, r, it.i0, it.j0, it.j1, TXe);
+            phase_riemann<EQ, R, FLX, H, NT>(S, D, st, r, it.i0, it.j0, it.j1, TXe);
             // the last warp, idle in the second round of Riemann units, prepares the next
             // row's eigensystems (row r+1 is resident; se is not read until the next row)
-            if (threadIdx.x >= NT - 32) phase_eigen<EQ, RECON, H>(S, D, r + 1, NT - 32, 32);
+            if (threadIdx.x >= NT - 32) phase_eigen<EQ, RECON, H, NT>(S, D, r + 1, NT - 32, 32);
             __syncthreads();
-            if (r - 1 >= it.j0) cmin = phase_update<EQ, H>(S, D, st, L, r - 1, it.i0, TXe, dt, cmin);
+            if (r - 1 >= it.j0) cmin = phase_update<EQ, H, NT>(S, D, st, L, r - 1, it.i0, TXe, dt, cmin);
         }
         if (L.final_stage && !L.rhs_out) {
             const double m = block_min(cmin, S.sred);
@@ -888,12 +912,12 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<RECON, R>::value) stage_ker
 }
 
 // calculateDeltaT of the current state (src/WENOFV.cpp:474-540) for every instance of the
-// launch, then the loop bookkeeping (FIN_INIT) by the last CTA.  TXW: the strip width of the
-// launch's work items.
-template <int EQ, int TXW>
-__global__ void __launch_bounds__(NT) cfl_kernel(const StageLaunch L)
+// launch, then the loop bookkeeping (FIN_INIT) by the last CTA.  L.tx: the strip width of the
+// launch's work items (that of the instances' stage kernel).
+template <int EQ>
+__global__ void __launch_bounds__(CFL_NT) cfl_kernel(const StageLaunch L)
 {
-    constexpr int NV = EqTraits<EQ>::NV;
+    constexpr int NV = EqTraits<EQ>::NV, NT = CFL_NT;
     __shared__ double sred[NT / 32];
     __shared__ int s_last;
     const int nwork = L.counts ? L.counts[0] : L.nwork;
@@ -904,7 +928,7 @@ __global__ void __launch_bounds__(NT) cfl_kernel(const StageLaunch L)
         if (st->done) continue;
         const double *U = D.buf[st->cur_buf];
         const size_t plane = (size_t)D.ny * D.pitch;
-        const int width = min(TXW, D.nx - it.i0);
+        const int width = min(L.tx, D.nx - it.i0);
         double cmin = __longlong_as_double(0x7ff0000000000000LL);
         for (int e = threadIdx.x; e < width * (it.j1 - it.j0); e += NT) {
             const int j = it.j0 + e / width, i = it.i0 + e % width;

@@ -58,15 +58,16 @@ struct StageLaunch {
     int first_stage, final_stage, rk1;
     double A, B, C;  // U_out = (A*U^n + B*U) + (C*dt)*rhs
     double *rhs_out; // non-null: write the RHS (layout of instance 0) instead of the update
+    int tx;          // strip width of the work items (the CFL pass reads it)
 };
 
 // host launchers exported by each build of wenofv_kernels.cu
 #define WENOFV_DECLARE_LAUNCHERS(NS)                                                                     \
     namespace NS {                                                                                       \
-    int stage_tx(int eq, int scheme);                                                                    \
+    int stage_tx(int eq, int recon, int fp32, int scheme);                                               \
     int launch_stage(int eq, int recon, int fp32, int scheme, int flux, const StageLaunch &L, int grid,  \
                      void *stream);                                                                     \
-    int launch_cfl(int eq, int scheme, const StageLaunch &L, int grid, void *stream);                   \
+    int launch_cfl(int eq, int recon, int fp32, int scheme, const StageLaunch &L, int grid, void *stream); \
     int stage_blocks_per_sm(int eq, int recon, int fp32, int scheme, int flux);                          \
     int probe_weno(int scheme, int fp32, const double *d_st, int n, double *d_out, void *stream);       \
     int probe_weno_exp(const double *d_st, int n, double dx4, double *d_out, void *stream);             \
