@@ -559,10 +559,26 @@ int Engine::build_work()
         long strips_rows = 0;
         for (int i : g.inst) strips_rows += (long)((cfg_[i].nx + tx - 1) / tx) * cfg_[i].ny;
         int seg = rows_per_item_;
-        if (seg <= 0) {
-            // rows per item: long enough to amortise the 2 halo rows, short enough to fill the GPU
+        if (seg <= 0 && slots > 2 * sms_) {
+            // many resident CTAs per SM (the 128-thread kernels): long enough to amortise the 2
+            // halo rows, short enough to fill the GPU (measured best on the 1024^2 column)
             seg = 32;
             while (seg > 8 && strips_rows / seg < 2L * slots) seg /= 2;
+        } else if (seg <= 0) {
+            // 1-2 resident CTAs per SM: the CTAs take items in waves, and an item of s rows
+            // costs about s + 2 halo rows + 3 rows' worth of start-up (its first 2H+1 rows load
+            // before the loop; measured: 8 % of a 32-row item); pick the s of the shortest
+            // waves x (s + 5).  On the 1024^2 column it picks 64 rows: 0.897 ms per stage
+            // against 0.972 for 16 and 0.924 for 32 (measured).
+            double best = 1e300;
+            seg = 32;
+            for (int s : {8, 16, 24, 32, 48, 64}) {
+                long items = 0;
+                for (int i : g.inst) items += (long)((cfg_[i].nx + tx - 1) / tx) * ((cfg_[i].ny + s - 1) / s);
+                const double waves = std::ceil((double)items / slots);
+                const double cost = waves * (s + 5);
+                if (cost < best - 1e-9) { best = cost; seg = s; }
+            }
         }
         std::vector<WorkItem> work;
         for (int i : g.inst)
