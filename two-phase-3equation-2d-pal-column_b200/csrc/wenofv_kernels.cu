@@ -24,10 +24,11 @@ namespace fast {
 // threads per CTA and strip width of the stage kernel of (eq, recon, form): StageThreads
 static int stage_threads(int eq, int recon, int fp32)
 {
-    return (eq != EQ_LINEAR_ADV && eq != EQ_TWO_PHASE_SG && recon != 4 && (!fp32 || eq == EQ_EULER)) ? 256 : 128;
+    (void)fp32;
+    return (eq != EQ_LINEAR_ADV && eq != EQ_TWO_PHASE_SG && recon != 4) ? 256 : 128;
 }
 static_assert(StageThreads<EQ_TWO_PHASE, 1, double>::value == 256 && StageThreads<EQ_TWO_PHASE, 4, double>::value == 128 &&
-                  StageThreads<EQ_TWO_PHASE, 1, float>::value == 128 && StageThreads<EQ_LINEAR_ADV, 0, double>::value == 128 &&
+                  StageThreads<EQ_TWO_PHASE, 1, float>::value == 256 && StageThreads<EQ_LINEAR_ADV, 0, double>::value == 128 &&
                   StageThreads<EQ_TWO_PHASE_SG, 1, double>::value == 128 && StageThreads<EQ_EULER, 0, double>::value == 256 &&
                   StageThreads<EQ_EULER, 0, float>::value == 256,
               "stage_threads mirrors StageThreads");

@@ -37,18 +37,18 @@ namespace strict {
 namespace fast {
 #endif
 
-// threads per CTA of a stage kernel.  256 (strips of 58 columns, 2 CTAs per SM at 128
-// registers) for the FP64 forms of the 4-variable systems: the halo positions and the idle
-// lanes of the x-sweep, Riemann and update phases drop from ~19 % to ~9 % of the thread
-// slots, measured 9 % faster per stage than 3 CTAs of 128 threads at 168 registers (and 10 %
-// faster than 4 CTAs of 128 at 128 registers).  128 for FP32-bulk (5 CTAs per SM at 96
-// registers measured best; the Euler FP32-bulk form, whose flux stays FP64, runs 3 CTAs of
-// 256 threads, 16 % faster than 5 of 128), for PRIMITIVE3 (its variable-major y-sweep maps 4 warps to 32
-// positions), for scalar advection (strips of 122 columns already) and for the stiffened gas
-// (whose Newton equilibrium spills at 128 registers).
+// threads per CTA of a stage kernel.  256 (strips of 58 columns) for the 4-variable systems:
+// the halo positions and the idle lanes of the x-sweep, Riemann and update phases drop from
+// ~19 % to ~9 % of the thread slots.  The FP64 forms run 2 CTAs per SM at 128 registers
+// (0.892 ms per stage of the 1024^2 column, against 1.053 for 3 CTAs of 128 threads at 168
+// registers), FP32-bulk 2 CTAs as well (0.776 against 0.838 for 5 CTAs of 128 at 96
+// registers) and the Euler FP32-bulk form, whose flux stays FP64, 3.  128 for PRIMITIVE3 (its
+// variable-major y-sweep maps 4 warps to 32 positions), for scalar advection (strips of 122
+// columns already) and for the stiffened gas (whose Newton equilibrium spills at 128
+// registers).
 template <int EQ, int RECON, class R> struct StageThreads {
     static constexpr int value =
-        (EqTraits<EQ>::NV == 4 && RECON != 4 && EQ != EQ_TWO_PHASE_SG && (sizeof(R) == sizeof(double) || EQ == EQ_EULER)) ? 256 : 128;
+        (EqTraits<EQ>::NV == 4 && RECON != 4 && EQ != EQ_TWO_PHASE_SG) ? 256 : 128;
 };
 constexpr int CFL_NT = 128; // threads per CTA of cfl_kernel
 
@@ -831,7 +831,7 @@ __device__ __forceinline__ double phase_update(StageSmem<EQ, H, NT> &S, const In
 // at 3, which keeps all values in registers (4 spills and runs slower); the FP32-bulk form
 // runs 4 (conservative) or 5 (characteristic, a few spilled values) CTAs of 128
 template <int EQ, int RECON, class R> struct StageMinBlocks {
-    static constexpr int value = sizeof(R) < sizeof(double) ? (StageThreads<EQ, RECON, R>::value == 256 ? 3 : (RECON == 1 ? 5 : 4))
+    static constexpr int value = sizeof(R) < sizeof(double) ? (StageThreads<EQ, RECON, R>::value == 256 ? (EQ == EQ_EULER ? 3 : 2) : (RECON == 1 ? 5 : 4))
                                                               : (StageThreads<EQ, RECON, R>::value == 256 ? 2 : 3);
 };
 
