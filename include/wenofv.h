@@ -236,7 +236,15 @@ int wenofv_batch_advance(wenofv_batch *b, const double *t_end, int64_t max_steps
 /* rows per work item and CTAs per SM of the persistent stage kernel (0 = automatic) */
 int wenofv_batch_set_tiling(wenofv_batch *b, int rows_per_item, int ctas_per_sm);
 int wenofv_batch_stream(wenofv_batch *b, void **stream);
-/* measures candidate tilings on the batch's current state (state unchanged) and keeps the best */
+/* threads per CTA of the stage kernels: 0 (the default) chooses per instance, 256 (strips of 58
+ * columns) where the grid's width fills them well, else 128 (26 columns); 128 or 256 forces that
+ * width for every instance that has it (PRIMITIVE3, the stiffened gas and scalar advection run
+ * 128 only) */
+int wenofv_batch_set_threads(wenofv_batch *b, int threads_per_cta);
+/* the current tiling settings (0 = automatic) */
+int wenofv_batch_tiling(wenofv_batch *b, int *rows_per_item, int *ctas_per_sm, int *threads_per_cta);
+/* measures candidate tilings (threads per CTA x rows per work item x CTAs per SM) on the
+ * batch's current state (state unchanged) and keeps the best; wenofv_batch_tiling reports it */
 int wenofv_batch_autotune(wenofv_batch *b, int *rows_per_item, int *ctas_per_sm, double *best_ms);
 
 /* ---- serving: continuous batching of solve requests under an HBM budget (no

@@ -101,6 +101,33 @@ def test_batch_autotune_keeps_state(wb):
     b.close()
 
 
+def test_batch_cta_width_keeps_results(wb):
+    # the same instances with the stage kernels of 128 and of 256 threads (strips of 26 and 58
+    # columns), and with the per-instance choice: FP64_STRICT results equal the instances
+    # solved alone bit for bit, whatever the width and the tiling
+    ens = cases.ensemble(4, seed=9, grids=[(64, 64), (256, 64), (96, 96), (200, 40)])
+    cfgs, eqs = [], []
+    for U0, prm in ens:
+        c, e = column_cfg(wb, prm["nx"], prm["ny"], prm, wb.FP64_STRICT, scheme=prm["scheme"])
+        cfgs.append(c)
+        eqs.append(e)
+    refs = [alone(wb, c, e, U0, max_steps=4)[0] for c, e, (U0, _) in zip(cfgs, eqs, ens)]
+    b = wb.Batch(cfgs, eqs)
+    for nt, rows in ((128, 16), (256, 64), (0, 0), (256, 8)):
+        b.set_threads(nt)
+        b.set_tiling(rows, 0)
+        assert b.tiling() == (rows, 0, nt)
+        for k, (U0, _) in enumerate(ens):
+            b.upload(k, U0)
+        b.advance(1e9, max_steps=4)
+        for k in range(len(ens)):
+            assert np.array_equal(b.download(k), refs[k]), (nt, rows, k)
+    with pytest.raises(wb.WenofvError) as e:
+        b.set_threads(192)
+    assert e.value.code == wb.EINVAL
+    b.close()
+
+
 def _drain(srv, ids, timeout=300.0):
     out = {}
     t0 = time.time()

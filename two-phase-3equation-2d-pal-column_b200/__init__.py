@@ -34,6 +34,7 @@ EXPORTS = (
     "wenofv_step_noalloc", "wenofv_init_testcase", "wenofv_accuracy",
     "wenofv_batch_create", "wenofv_batch_destroy", "wenofv_batch_upload", "wenofv_batch_set_frame", "wenofv_batch_download",
     "wenofv_batch_advance", "wenofv_batch_set_tiling", "wenofv_batch_stream", "wenofv_batch_autotune",
+    "wenofv_batch_set_threads", "wenofv_batch_tiling",
     "wenofv_server_create", "wenofv_server_destroy", "wenofv_server_submit", "wenofv_server_poll",
     "wenofv_server_clock", "wenofv_server_stats",
     "wenofv_probe_weno", "wenofv_probe_weno_exp", "wenofv_probe_riemann", "wenofv_probe_eigen", "wenofv_probe_fma_peak",
@@ -122,6 +123,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.wenofv_batch_set_tiling.argtypes = [P, I, I]
     L.wenofv_batch_stream.argtypes = [P, C.POINTER(P)]
     L.wenofv_batch_autotune.argtypes = [P, C.POINTER(I), C.POINTER(I), DP]
+    L.wenofv_batch_set_threads.argtypes = [P, I]
+    L.wenofv_batch_tiling.argtypes = [P, C.POINTER(I), C.POINTER(I), C.POINTER(I)]
     L.wenofv_server_create.argtypes = [I, C.c_size_t, I, C.POINTER(P)]
     L.wenofv_server_destroy.argtypes = [P]
     L.wenofv_server_submit.argtypes = [P, C.POINTER(Config), C.POINTER(EqParams), DP, D, I64, C.POINTER(I64)]
@@ -335,6 +338,16 @@ class Batch:
 
     def set_tiling(self, rows: int, ctas_per_sm: int = 0):
         _check(self.L.wenofv_batch_set_tiling(self.h, rows, ctas_per_sm), "wenofv_batch_set_tiling")
+
+    def set_threads(self, threads_per_cta: int):
+        """0: per instance (the default); 128 or 256: that CTA width wherever it exists"""
+        _check(self.L.wenofv_batch_set_threads(self.h, threads_per_cta), "wenofv_batch_set_threads")
+
+    def tiling(self):
+        """(rows per item, CTAs per SM, threads per CTA); 0 = automatic"""
+        r, c, t = C.c_int(), C.c_int(), C.c_int()
+        _check(self.L.wenofv_batch_tiling(self.h, C.byref(r), C.byref(c), C.byref(t)), "wenofv_batch_tiling")
+        return r.value, c.value, t.value
 
     def autotune(self):
         r, c, ms = C.c_int(), C.c_int(), C.c_double()

@@ -204,6 +204,19 @@ int wenofv_batch_stream(wenofv_batch *b, void **stream)
     *stream = (void *)b->eng.stream;
     return WENOFV_OK;
 }
+int wenofv_batch_set_threads(wenofv_batch *b, int threads_per_cta)
+{
+    if (!b) { set_error("null batch"); return WENOFV_EINVAL; }
+    return b->eng.set_threads(threads_per_cta);
+}
+
+int wenofv_batch_tiling(wenofv_batch *b, int *rows_per_item, int *ctas_per_sm, int *threads_per_cta)
+{
+    if (!b) { set_error("null batch"); return WENOFV_EINVAL; }
+    b->eng.tiling(rows_per_item, ctas_per_sm, threads_per_cta);
+    return WENOFV_OK;
+}
+
 int wenofv_batch_autotune(wenofv_batch *b, int *rows_per_item, int *ctas_per_sm, double *best_ms)
 {
     if (!b) { set_error("null batch"); return WENOFV_EINVAL; }

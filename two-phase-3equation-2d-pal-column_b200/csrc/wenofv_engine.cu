@@ -486,15 +486,38 @@ void Engine::free_work()
     groups_.clear();
 }
 
+// the CTA width of an instance's stage kernel: 256 (strips of 58 columns) or 128 (26 columns)
+// where both exist.  The wide kernel costs about 0.85 (FP64) or 0.93 (FP32-bulk) of the narrow
+// one per column-row it computes (measured on a 1024-wide grid), but rounds the grid's width up
+// to whole strips of 58; choose the width of the smaller cost x padded width.  The override
+// (wenofv_batch_set_threads, the autotuner) forces one width where it exists.
+int Engine::instance_nt(int i) const
+{
+    const int eqk = desc_[i].eq_kind, recon = desc_[i].recon;
+    const int strict = cfg_[i].precision == WENOFV_FP64_STRICT, fp32 = cfg_[i].precision == WENOFV_FP32_BULK;
+    const int wide = strict ? strict::stage_wide(eqk, recon) : fast::stage_wide(eqk, recon);
+    if (!wide) return 128;
+    if (nt_override_ == 128 || nt_override_ == 256) return nt_override_;
+    const int sch = recon == 4 ? 2 : desc_[i].scheme;
+    const int tn = strict ? strict::stage_tx(eqk, recon, fp32, sch, 128) : fast::stage_tx(eqk, recon, fp32, sch, 128);
+    const int tw = strict ? strict::stage_tx(eqk, recon, fp32, sch, 256) : fast::stage_tx(eqk, recon, fp32, sch, 256);
+    const int nx = cfg_[i].nx;
+    const double narrow = (double)((nx + tn - 1) / tn) * tn;
+    const double wide_cost = (fp32 ? 0.93 : 0.85) * (double)((nx + tw - 1) / tw) * tw;
+    return wide_cost < narrow ? 256 : 128;
+}
+
 // the template key of an instance's launch group: form, equation, reconstruction, scheme
-// (PRIMITIVE3 always on WENOEXP's 7-point geometry) and flux
+// (PRIMITIVE3 always on WENOEXP's 7-point geometry), flux and CTA width
 long Engine::group_key(int i) const
 {
     const int strict = cfg_[i].precision == WENOFV_FP64_STRICT;
     const int fp32 = cfg_[i].precision == WENOFV_FP32_BULK;
     const int sch = desc_[i].recon == 4 ? 2 : desc_[i].scheme;
     const int flx = desc_[i].eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : desc_[i].flux;
-    return ((long)strict << 32) | ((long)fp32 << 24) | (desc_[i].eq_kind << 16) | (desc_[i].recon << 8) | (sch << 4) | flx;
+    const int wide = instance_nt(i) == 256;
+    return ((long)wide << 40) | ((long)strict << 32) | ((long)fp32 << 24) | (desc_[i].eq_kind << 16) | (desc_[i].recon << 8) |
+           (sch << 4) | flx;
 }
 
 namespace {
@@ -541,6 +564,7 @@ int Engine::build_work()
         g.recon = desc_[i].recon;
         g.scheme = desc_[i].recon == 4 ? 2 : desc_[i].scheme;
         g.flux = desc_[i].eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : desc_[i].flux;
+        g.nt = instance_nt(i);
         WENOFV_CUDA(cudaMalloc(&g.d_counts, 4 * sizeof(int)));
         WENOFV_CUDA(cudaMalloc(&g.d_counter, sizeof(unsigned int)));
         WENOFV_CUDA(cudaMemsetAsync(g.d_counter, 0, sizeof(unsigned int), stream));
@@ -552,9 +576,9 @@ int Engine::build_work()
     for (Group &g : groups_) {
         auto m = members.find(g.key);
         g.inst = m == members.end() ? std::vector<int>() : m->second;
-        const int tx = g.ns_strict ? strict::stage_tx(g.eq, g.recon, g.fp32, g.scheme) : fast::stage_tx(g.eq, g.recon, g.fp32, g.scheme);
-        const int bps = std::max(1, g.ns_strict ? strict::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux)
-                                                : fast::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux));
+        const int tx = g.ns_strict ? strict::stage_tx(g.eq, g.recon, g.fp32, g.scheme, g.nt) : fast::stage_tx(g.eq, g.recon, g.fp32, g.scheme, g.nt);
+        const int bps = std::max(1, g.ns_strict ? strict::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux, g.nt)
+                                                : fast::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux, g.nt));
         const int slots = sms_ * (ctas_per_sm_ > 0 ? std::min(ctas_per_sm_, bps) : bps);
         long strips_rows = 0;
         for (int i : g.inst) strips_rows += (long)((cfg_[i].nx + tx - 1) / tx) * cfg_[i].ny;
@@ -650,8 +674,8 @@ int Engine::launch_stage_all(int parity, int stage, double *rhs_out)
             stage_coeffs(rk, stage, L.A, L.B, L.C);
         }
         cudaStream_t s = capturing_ ? g.gstream : stream;
-        const int rc = g.ns_strict ? strict::launch_stage(g.eq, g.recon, g.fp32, g.scheme, g.flux, L, g.grid, s)
-                                   : fast::launch_stage(g.eq, g.recon, g.fp32, g.scheme, g.flux, L, g.grid, s);
+        const int rc = g.ns_strict ? strict::launch_stage(g.eq, g.recon, g.fp32, g.scheme, g.flux, g.nt, L, g.grid, s)
+                                   : fast::launch_stage(g.eq, g.recon, g.fp32, g.scheme, g.flux, g.nt, L, g.grid, s);
         if (rc) return cuda_fail((cudaError_t)rc, "stage kernel launch");
     }
     return WENOFV_OK;
@@ -662,8 +686,8 @@ int Engine::launch_cfl_all()
     for (Group &g : groups_) {
         StageLaunch L;
         group_launch(g, L);
-        const int rc = g.ns_strict ? strict::launch_cfl(g.eq, g.recon, g.fp32, g.scheme, L, g.grid, stream)
-                                   : fast::launch_cfl(g.eq, g.recon, g.fp32, g.scheme, L, g.grid, stream);
+        const int rc = g.ns_strict ? strict::launch_cfl(g.eq, g.recon, g.fp32, g.scheme, g.nt, L, g.grid, stream)
+                                   : fast::launch_cfl(g.eq, g.recon, g.fp32, g.scheme, g.nt, L, g.grid, stream);
         if (rc) return cuda_fail((cudaError_t)rc, "cfl kernel launch");
     }
     return WENOFV_OK;
@@ -688,7 +712,7 @@ int Engine::start_many(const std::vector<int> &slots, const std::vector<double> 
     for (Group &g : groups_) {
         std::vector<int> fin;
         std::vector<WorkItem> work;
-        const int tx = g.ns_strict ? strict::stage_tx(g.eq, g.recon, g.fp32, g.scheme) : fast::stage_tx(g.eq, g.recon, g.fp32, g.scheme);
+        const int tx = g.ns_strict ? strict::stage_tx(g.eq, g.recon, g.fp32, g.scheme, g.nt) : fast::stage_tx(g.eq, g.recon, g.fp32, g.scheme, g.nt);
         for (int sl : slots) {
             if (group_key(sl) != g.key) continue;
             fin.push_back(sl);
@@ -710,8 +734,8 @@ int Engine::start_many(const std::vector<int> &slots, const std::vector<double> 
         L.nfin = (int)fin.size();
         L.counts = nullptr;
         const int grid = std::max(1, std::min(L.nwork, g.grid));
-        const int lrc = g.ns_strict ? strict::launch_cfl(g.eq, g.recon, g.fp32, g.scheme, L, grid, stream)
-                                    : fast::launch_cfl(g.eq, g.recon, g.fp32, g.scheme, L, grid, stream);
+        const int lrc = g.ns_strict ? strict::launch_cfl(g.eq, g.recon, g.fp32, g.scheme, g.nt, L, grid, stream)
+                                    : fast::launch_cfl(g.eq, g.recon, g.fp32, g.scheme, g.nt, L, grid, stream);
         if (lrc) return cuda_fail((cudaError_t)lrc, "cfl kernel launch");
     }
     return WENOFV_OK;
@@ -1092,6 +1116,23 @@ int Engine::set_tiling(int rows, int ctas)
     return ensure_work();
 }
 
+int Engine::set_threads(int nt)
+{
+    if (nt != 0 && nt != 128 && nt != 256) { set_error("threads per CTA must be 0 (automatic), 128 or 256"); return WENOFV_EINVAL; }
+    WENOFV_CUDA(cudaSetDevice(device));
+    WENOFV_CUDA(cudaStreamSynchronize(stream));
+    nt_override_ = nt;
+    work_dirty_ = true;
+    return ensure_work();
+}
+
+void Engine::tiling(int *rows, int *ctas, int *nt) const
+{
+    if (rows) *rows = rows_per_item_;
+    if (ctas) *ctas = ctas_per_sm_;
+    if (nt) *nt = nt_override_;
+}
+
 int Engine::device_state(int i, double **U, int *pitch)
 {
     if (!live(i)) { set_error("bad instance index"); return WENOFV_EINVAL; }
@@ -1107,16 +1148,16 @@ struct TuneScope {
     Engine &e;
     std::vector<double *> saved;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    int rows0, ctas0, cur0;
+    int rows0, ctas0, nt0, cur0;
     std::vector<InstState> state0;
     bool done = false;
-    TuneScope(Engine &eng, int rows, int ctas, int cur, const InstState *st, int cap)
-        : e(eng), saved(eng.n, nullptr), rows0(rows), ctas0(ctas), cur0(cur), state0(st, st + cap) {}
+    TuneScope(Engine &eng, int rows, int ctas, int nt, int cur, const InstState *st, int cap)
+        : e(eng), saved(eng.n, nullptr), rows0(rows), ctas0(ctas), nt0(nt), cur0(cur), state0(st, st + cap) {}
     ~TuneScope()
     {
         if (!done) { // an error path: the caller's tiling, buffer and loop state as they were
             cudaStreamSynchronize(e.stream);
-            e.restore_after_tune(rows0, ctas0, cur0, state0.data(), saved);
+            e.restore_after_tune(rows0, ctas0, nt0, cur0, state0.data(), saved);
         }
         for (double *p : saved) cudaFree(p);
         if (e0) cudaEventDestroy(e0);
@@ -1127,7 +1168,7 @@ struct TuneScope {
 } // namespace
 
 // puts the saved states back into the current buffer and restores tiling and loop state
-void Engine::restore_after_tune(int rows, int ctas, int cur, const InstState *st, const std::vector<double *> &saved)
+void Engine::restore_after_tune(int rows, int ctas, int nt, int cur, const InstState *st, const std::vector<double *> &saved)
 {
     cur_ = cur;
     for (int i = 0; i < n && i < (int)saved.size(); i++) {
@@ -1141,14 +1182,17 @@ void Engine::restore_after_tune(int rows, int ctas, int cur, const InstState *st
     cudaStreamSynchronize(stream);
     rows_per_item_ = rows;
     ctas_per_sm_ = ctas;
+    nt_override_ = nt;
     work_dirty_ = true;
     ensure_work();
 }
 
-// Times candidate tilings (rows per work item x resident CTAs per SM) with manual steps on
-// the current state and keeps the fastest: one warm-up step, then TUNE_SAMPLES timed steps
-// per candidate, ranked by the median.  The states, the buffer rotation and the loop state
-// (status flags included) are put back afterwards, and on any error.
+// Times candidate tilings (CTA width x rows per work item x resident CTAs per SM) with manual
+// steps on the current state and keeps the fastest: one warm-up step, then TUNE_SAMPLES timed
+// steps per candidate, ranked by the median.  The CTA width candidates are the per-instance
+// width model (0) and, where any instance has the 256-thread kernel, 128 and 256 for all.  The
+// states, the buffer rotation and the loop state (status flags included) are put back
+// afterwards, and on any error.
 int Engine::autotune(int *rows_out, int *ctas_out, double *best_ms)
 {
     constexpr int TUNE_SAMPLES = 3;
@@ -1156,7 +1200,7 @@ int Engine::autotune(int *rows_out, int *ctas_out, double *best_ms)
     WENOFV_CUDA(cudaStreamSynchronize(stream));
     int rc = pull_state();
     if (rc) return rc;
-    TuneScope T(*this, rows_per_item_, ctas_per_sm_, cur_, h_state_, cap_);
+    TuneScope T(*this, rows_per_item_, ctas_per_sm_, nt_override_, cur_, h_state_, cap_);
     for (int i = 0; i < n; i++) {
         const InstDesc &d = desc_[i];
         const size_t bytes = (size_t)nvar_of(d.eq_kind) * d.ny * d.pitch * sizeof(double);
@@ -1172,12 +1216,21 @@ int Engine::autotune(int *rows_out, int *ctas_out, double *best_ms)
         if (rc) return rc;
         dt = *std::min_element(dts.begin(), dts.end()) * 0.5;
     }
-    const int rows_c[] = {8, 16, 32, 64};
-    const int ctas_c[] = {0, 2, 1};
+    bool any_wide = false;
+    for (int i = 0; i < n; i++) {
+        const int st = cfg_[i].precision == WENOFV_FP64_STRICT;
+        any_wide = any_wide || (st ? strict::stage_wide(desc_[i].eq_kind, desc_[i].recon) : fast::stage_wide(desc_[i].eq_kind, desc_[i].recon));
+    }
+    std::vector<int> nt_c = {0};
+    if (any_wide) { nt_c.push_back(128); nt_c.push_back(256); }
+    const int rows_c[] = {16, 32, 64};
+    const int ctas_c[] = {0, 2};
     double best = 1e30;
-    int br = 32, bc = 0;
-    for (int r : rows_c)
+    int br = 32, bc = 0, bn = 0;
+    for (int w : nt_c)
+        for (int r : rows_c)
         for (int c : ctas_c) {
+            nt_override_ = w;
             rc = set_tiling(r, c);
             if (!rc) rc = step(dt); // warm-up
             if (rc) return rc;
@@ -1192,11 +1245,11 @@ int Engine::autotune(int *rows_out, int *ctas_out, double *best_ms)
             }
             std::sort(ms, ms + TUNE_SAMPLES);
             const double med = ms[TUNE_SAMPLES / 2];
-            if (med < best) { best = med; br = r; bc = c; }
+            if (med < best) { best = med; br = r; bc = c; bn = w; }
         }
     WENOFV_CUDA(cudaStreamSynchronize(stream));
     T.done = true;
-    restore_after_tune(br, bc, T.cur0, T.state0.data(), T.saved);
+    restore_after_tune(br, bc, bn, T.cur0, T.state0.data(), T.saved);
     if (const cudaError_t e = cudaGetLastError()) return cuda_fail(e, "autotune restore");
     if (rows_out) *rows_out = br;
     if (ctas_out) *ctas_out = bc;

@@ -53,7 +53,9 @@ public:
     int set_tiling(int rows, int ctas_per_sm);
     int autotune(int *rows, int *ctas_per_sm, double *best_ms);
     // puts states, buffer rotation, loop state and tiling back after a tuning search
-    void restore_after_tune(int rows, int ctas, int cur, const InstState *st, const std::vector<double *> &saved);
+    void restore_after_tune(int rows, int ctas, int nt, int cur, const InstState *st, const std::vector<double *> &saved);
+    int set_threads(int nt);                           // 0: per instance by the width model; 128 or 256
+    void tiling(int *rows, int *ctas, int *nt) const;  // the current settings (0 = automatic)
     int device_state(int i, double **U, int *pitch);
     int set_frame(int i, const double *frame); // NEUMANN2 ghost averages, SoA [v][ny+8][nx+8]
     int theta_flags(int i, unsigned char *out, int layout); // the final stage's limiter record per cell
@@ -91,7 +93,7 @@ private:
     // place while they fit, so a captured graph stays valid when instances come and go
     struct Group {
         long key = 0;
-        int ns_strict, fp32, eq, recon, scheme, flux;
+        int ns_strict, fp32, eq, recon, scheme, flux, nt = 128;
         std::vector<int> inst;
         WorkItem *d_work = nullptr;
         int nwork = 0, cap_work = 0;
@@ -110,6 +112,7 @@ private:
     int build_work();
     void free_work();
     long group_key(int i) const;
+    int instance_nt(int i) const;
     int group_launch(const Group &g, StageLaunch &L) const;
     int arena_alloc(size_t bytes, size_t *off);
     void arena_free(size_t off);
@@ -152,6 +155,7 @@ private:
     size_t h_stage_bytes_ = 0;
     double *d_rhs_ = nullptr;
     int rows_per_item_ = 0, ctas_per_sm_ = 0;
+    int nt_override_ = 0; // 0: CTA width per instance by the width model; 128 or 256: forced
     int sms_ = 148;
     int cap_ = 0;
     int cur_ = 0; // buffer holding every instance's state between calls (context/batch)

@@ -21,17 +21,14 @@ namespace fast {
 #define WENOFV_HAS_FP32 1
 #endif
 
-// threads per CTA and strip width of the stage kernel of (eq, recon, form): StageThreads
-static int stage_threads(int eq, int recon, int fp32)
-{
-    (void)fp32;
-    return (eq != EQ_LINEAR_ADV && eq != EQ_TWO_PHASE_SG && recon != 4) ? 256 : 128;
-}
-static_assert(StageThreads<EQ_TWO_PHASE, 1, double>::value == 256 && StageThreads<EQ_TWO_PHASE, 4, double>::value == 128 &&
-                  StageThreads<EQ_TWO_PHASE, 1, float>::value == 256 && StageThreads<EQ_LINEAR_ADV, 0, double>::value == 128 &&
-                  StageThreads<EQ_TWO_PHASE_SG, 1, double>::value == 128 && StageThreads<EQ_EULER, 0, double>::value == 256 &&
-                  StageThreads<EQ_EULER, 0, float>::value == 256,
-              "stage_threads mirrors StageThreads");
+// whether (eq, recon) has the 256-thread stage kernel too (StageWide)
+int stage_wide(int eq, int recon) { return eq != EQ_LINEAR_ADV && eq != EQ_TWO_PHASE_SG && recon != 4; }
+static_assert(StageWide<EQ_TWO_PHASE, 1, double>::value && !StageWide<EQ_TWO_PHASE, 4, double>::value &&
+                  StageWide<EQ_TWO_PHASE, 1, float>::value && !StageWide<EQ_LINEAR_ADV, 0, double>::value &&
+                  !StageWide<EQ_TWO_PHASE_SG, 1, double>::value && StageWide<EQ_EULER, 0, float>::value,
+              "stage_wide mirrors StageWide");
+// the width a launch runs: 256 where asked for and available, else 128
+static int width_of(int eq, int recon, int nt) { return (nt == 256 && stage_wide(eq, recon)) ? 256 : 128; }
 
 // strip width of the work items: 5-point stencils (H = 2) or WENOEXP's 7-point ones (H = 3)
 template <int NT> static int tx_of(int eq, int scheme)
@@ -39,53 +36,56 @@ template <int NT> static int tx_of(int eq, int scheme)
     if (scheme == 2) return eq == EQ_LINEAR_ADV ? StageGeom<EQ_LINEAR_ADV, 3, NT>::TX : StageGeom<EQ_TWO_PHASE, 3, NT>::TX;
     return eq == EQ_LINEAR_ADV ? StageGeom<EQ_LINEAR_ADV, 2, NT>::TX : StageGeom<EQ_TWO_PHASE, 2, NT>::TX;
 }
-int stage_tx(int eq, int recon, int fp32, int scheme)
+int stage_tx(int eq, int recon, int fp32, int scheme, int nt)
 {
-    return stage_threads(eq, recon, fp32) == 256 ? tx_of<256>(eq, scheme) : tx_of<128>(eq, scheme);
+    (void)fp32;
+    return width_of(eq, recon, nt) == 256 ? tx_of<256>(eq, scheme) : tx_of<128>(eq, scheme);
 }
 
-template <int EQ, int RECON, class R, int SCH, int FLX> static const void *stage_fn()
+template <int EQ, int RECON, class R, int SCH, int FLX, int NT> static const void *stage_fn()
 {
-    return (const void *)stage_kernel<EQ, RECON, R, SCH, FLX>;
+    return (const void *)stage_kernel<EQ, RECON, R, SCH, FLX, NT>;
 }
 // the scheme and flux of a launch group as template arguments (scalar advection has one flux)
 // (WENOEXP, scheme 2, only in FP64)
-template <int EQ, int RECON, class R> static const void *pick_sf(int scheme, int flux)
+template <int EQ, int RECON, class R, int NT> static const void *pick_sf(int scheme, int flux)
 {
-    if constexpr (RECON == 4) { // PRIMITIVE3: FP64, on the 7-point geometry (scheme 2) whatever SCHEME is
+    if constexpr (NT == 256 && !StageWide<EQ, RECON, R>::value) {
+        return nullptr;
+    } else if constexpr (RECON == 4) { // PRIMITIVE3: FP64, on the 7-point geometry (scheme 2) whatever SCHEME is
         if constexpr (EQ == EQ_TWO_PHASE && sizeof(R) == sizeof(double)) {
             if (scheme != 2) return nullptr;
-            return flux ? stage_fn<EQ, RECON, R, 2, 1>() : stage_fn<EQ, RECON, R, 2, 0>();
+            return flux ? stage_fn<EQ, RECON, R, 2, 1, NT>() : stage_fn<EQ, RECON, R, 2, 0, NT>();
         } else {
             return nullptr;
         }
     } else {
         if constexpr (sizeof(R) == sizeof(double)) {
             if (scheme == 2) {
-                if (EQ == EQ_LINEAR_ADV) return stage_fn<EQ, RECON, R, 2, 0>();
-                return flux ? stage_fn<EQ, RECON, R, 2, 1>() : stage_fn<EQ, RECON, R, 2, 0>();
+                if (EQ == EQ_LINEAR_ADV) return stage_fn<EQ, RECON, R, 2, 0, NT>();
+                return flux ? stage_fn<EQ, RECON, R, 2, 1, NT>() : stage_fn<EQ, RECON, R, 2, 0, NT>();
             }
         } else {
             if (scheme == 2) return nullptr;
         }
-        if (EQ == EQ_LINEAR_ADV) return scheme ? stage_fn<EQ, RECON, R, 1, 0>() : stage_fn<EQ, RECON, R, 0, 0>();
-        if (scheme) return flux ? stage_fn<EQ, RECON, R, 1, 1>() : stage_fn<EQ, RECON, R, 1, 0>();
-        return flux ? stage_fn<EQ, RECON, R, 0, 1>() : stage_fn<EQ, RECON, R, 0, 0>();
+        if (EQ == EQ_LINEAR_ADV) return scheme ? stage_fn<EQ, RECON, R, 1, 0, NT>() : stage_fn<EQ, RECON, R, 0, 0, NT>();
+        if (scheme) return flux ? stage_fn<EQ, RECON, R, 1, 1, NT>() : stage_fn<EQ, RECON, R, 1, 0, NT>();
+        return flux ? stage_fn<EQ, RECON, R, 0, 1, NT>() : stage_fn<EQ, RECON, R, 0, 0, NT>();
     }
 }
-template <class R> static const void *pick_eq(int eq, int recon, int scheme, int flux)
+template <class R, int NT> static const void *pick_eq(int eq, int recon, int scheme, int flux)
 {
     switch (eq) {
     case EQ_TWO_PHASE:
-        return recon == 1 ? pick_sf<EQ_TWO_PHASE, 1, R>(scheme, flux) : recon == 2 ? pick_sf<EQ_TWO_PHASE, 2, R>(scheme, flux)
-             : recon == 3 ? pick_sf<EQ_TWO_PHASE, 3, R>(scheme, flux) : recon == 4 ? pick_sf<EQ_TWO_PHASE, 4, R>(scheme, flux)
-                          : pick_sf<EQ_TWO_PHASE, 0, R>(scheme, flux);
-    case EQ_EULER: return recon ? pick_sf<EQ_EULER, 1, R>(scheme, flux) : pick_sf<EQ_EULER, 0, R>(scheme, flux);
-    case EQ_LINEAR_ADV: return pick_sf<EQ_LINEAR_ADV, 0, R>(scheme, flux);
+        return recon == 1 ? pick_sf<EQ_TWO_PHASE, 1, R, NT>(scheme, flux) : recon == 2 ? pick_sf<EQ_TWO_PHASE, 2, R, NT>(scheme, flux)
+             : recon == 3 ? pick_sf<EQ_TWO_PHASE, 3, R, NT>(scheme, flux) : recon == 4 ? pick_sf<EQ_TWO_PHASE, 4, R, NT>(scheme, flux)
+                          : pick_sf<EQ_TWO_PHASE, 0, R, NT>(scheme, flux);
+    case EQ_EULER: return recon ? pick_sf<EQ_EULER, 1, R, NT>(scheme, flux) : pick_sf<EQ_EULER, 0, R, NT>(scheme, flux);
+    case EQ_LINEAR_ADV: return pick_sf<EQ_LINEAR_ADV, 0, R, NT>(scheme, flux);
     case EQ_TWO_PHASE_SG: // FP64, conservative or characteristic reconstruction
         if constexpr (sizeof(R) == sizeof(double)) {
             if (recon > 1) return nullptr;
-            return recon ? pick_sf<EQ_TWO_PHASE_SG, 1, R>(scheme, flux) : pick_sf<EQ_TWO_PHASE_SG, 0, R>(scheme, flux);
+            return recon ? pick_sf<EQ_TWO_PHASE_SG, 1, R, NT>(scheme, flux) : pick_sf<EQ_TWO_PHASE_SG, 0, R, NT>(scheme, flux);
         } else {
             return nullptr;
         }
@@ -93,15 +93,16 @@ template <class R> static const void *pick_eq(int eq, int recon, int scheme, int
     }
 }
 
-static const void *pick_stage(int eq, int recon, int fp32, int scheme, int flux)
+static const void *pick_stage(int eq, int recon, int fp32, int scheme, int flux, int nt)
 {
     if (scheme < 0 || scheme > 2 || flux < 0 || flux > 1) return nullptr;
+    const bool wide = width_of(eq, recon, nt) == 256;
 #if WENOFV_HAS_FP32
-    if (fp32) return pick_eq<float>(eq, recon, scheme, flux);
+    if (fp32) return wide ? pick_eq<float, 256>(eq, recon, scheme, flux) : pick_eq<float, 128>(eq, recon, scheme, flux);
 #else
     if (fp32) return nullptr;
 #endif
-    return pick_eq<double>(eq, recon, scheme, flux);
+    return wide ? pick_eq<double, 256>(eq, recon, scheme, flux) : pick_eq<double, 128>(eq, recon, scheme, flux);
 }
 
 // dynamic shared memory of a stage kernel: its StageSmem block, then the primitive ring of
@@ -113,15 +114,15 @@ template <int H, int NT> static int smem_of(int eq)
          : eq == EQ_TWO_PHASE_SG   ? StageSmemBytes<EQ_TWO_PHASE_SG, H, NT>::value
                                    : StageSmemBytes<EQ_LINEAR_ADV, H, NT>::value;
 }
-static int stage_dyn_bytes(int eq, int recon, int fp32, int scheme)
+static int stage_dyn_bytes(int eq, int recon, int scheme, int nt)
 {
     static_assert(StageDynSmem<EQ_TWO_PHASE, 2, 2, 256>::value == StageDynSmem<EQ_TWO_PHASE, 2, 3, 256>::value, "ring size");
-    const int nt = stage_threads(eq, recon, fp32);
+    const bool wide = width_of(eq, recon, nt) == 256;
     const int ring = (eq == EQ_TWO_PHASE && recon >= 2)
-                         ? (nt == 256 ? StageDynSmem<EQ_TWO_PHASE, 2, 2, 256>::value : StageDynSmem<EQ_TWO_PHASE, 2, 2, 128>::value)
+                         ? (wide ? StageDynSmem<EQ_TWO_PHASE, 2, 2, 256>::value : StageDynSmem<EQ_TWO_PHASE, 2, 2, 128>::value)
                          : 0;
-    const int base = nt == 256 ? (scheme == 2 ? smem_of<3, 256>(eq) : smem_of<2, 256>(eq))
-                               : (scheme == 2 ? smem_of<3, 128>(eq) : smem_of<2, 128>(eq));
+    const int base = wide ? (scheme == 2 ? smem_of<3, 256>(eq) : smem_of<2, 256>(eq))
+                          : (scheme == 2 ? smem_of<3, 128>(eq) : smem_of<2, 128>(eq));
     return base + ring;
 }
 // dynamic shared memory past the default 48 KB needs an opt-in (not during a stream
@@ -132,11 +133,11 @@ static cudaError_t allow_dyn(const void *fn, int dyn)
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
 }
 
-int launch_stage(int eq, int recon, int fp32, int scheme, int flux, const StageLaunch &L, int grid, void *stream)
+int launch_stage(int eq, int recon, int fp32, int scheme, int flux, int nt, const StageLaunch &L, int grid, void *stream)
 {
-    const void *fn = pick_stage(eq, recon, fp32, scheme, flux);
+    const void *fn = pick_stage(eq, recon, fp32, scheme, flux, nt);
     if (!fn) return (int)cudaErrorInvalidValue;
-    const int dyn = stage_dyn_bytes(eq, recon, fp32, scheme);
+    const int dyn = stage_dyn_bytes(eq, recon, scheme, nt);
     if (dyn > 48 * 1024) {
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         cudaError_t e = cudaStreamIsCapturing((cudaStream_t)stream, &cs);
@@ -144,7 +145,7 @@ int launch_stage(int eq, int recon, int fp32, int scheme, int flux, const StageL
         if (cs == cudaStreamCaptureStatusNone && (e = allow_dyn(fn, dyn)) != cudaSuccess) return (int)e;
     }
     void *args[] = {(void *)&L};
-    return (int)cudaLaunchKernel(fn, dim3(grid), dim3(stage_threads(eq, recon, fp32)), args, (size_t)dyn, (cudaStream_t)stream);
+    return (int)cudaLaunchKernel(fn, dim3(grid), dim3(width_of(eq, recon, nt)), args, (size_t)dyn, (cudaStream_t)stream);
 }
 
 static const void *cfl_fn(int eq)
@@ -156,22 +157,22 @@ static const void *cfl_fn(int eq)
 }
 
 // the CFL pass over the work items of a launch group, whose strips are those of its stage kernel
-int launch_cfl(int eq, int recon, int fp32, int scheme, const StageLaunch &L, int grid, void *stream)
+int launch_cfl(int eq, int recon, int fp32, int scheme, int nt, const StageLaunch &L, int grid, void *stream)
 {
     StageLaunch Lc = L;
-    Lc.tx = stage_tx(eq, recon, fp32, scheme);
+    Lc.tx = stage_tx(eq, recon, fp32, scheme, nt);
     void *args[] = {(void *)&Lc};
     return (int)cudaLaunchKernel(cfl_fn(eq), dim3(grid), dim3(CFL_NT), args, 0, (cudaStream_t)stream);
 }
 
-int stage_blocks_per_sm(int eq, int recon, int fp32, int scheme, int flux)
+int stage_blocks_per_sm(int eq, int recon, int fp32, int scheme, int flux, int nt)
 {
-    const void *fn = pick_stage(eq, recon, fp32, scheme, flux);
+    const void *fn = pick_stage(eq, recon, fp32, scheme, flux, nt);
     if (!fn) return 0;
-    const int dyn = stage_dyn_bytes(eq, recon, fp32, scheme);
+    const int dyn = stage_dyn_bytes(eq, recon, scheme, nt);
     if (dyn > 48 * 1024 && allow_dyn(fn, dyn) != cudaSuccess) return 0;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, stage_threads(eq, recon, fp32), (size_t)dyn) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, width_of(eq, recon, nt), (size_t)dyn) != cudaSuccess) return 0;
     return n;
 }
 

@@ -34,6 +34,7 @@ constexpr size_t NOALLOC_STATE_DOUBLES = (size_t)4 << 17; // 4 MiB of FP64 state
 constexpr int NOALLOC_METRIC_DOUBLES = 8192;
 constexpr int NOALLOC_MAX_WORK = 8192;
 constexpr int NOALLOC_ROWS = 16; // rows per work item
+constexpr int NOALLOC_NT = 128;  // CTA width of its stage kernels (the grids it takes are narrow)
 
 // layout of the scratch array (each part 256-byte aligned)
 constexpr size_t OFF_DESC = 0;
@@ -103,7 +104,7 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
         set_error("the no-allocation step needs 2*nx + ny <= %d", NOALLOC_METRIC_DOUBLES);
         return WENOFV_EINVAL;
     }
-    const int tx = strictf ? strict::stage_tx(eq->eq_kind, recon, 0, sch) : fast::stage_tx(eq->eq_kind, recon, fp32, sch);
+    const int tx = strictf ? strict::stage_tx(eq->eq_kind, recon, 0, sch, NOALLOC_NT) : fast::stage_tx(eq->eq_kind, recon, fp32, sch, NOALLOC_NT);
     const long nwork = (long)((cfg->nx + tx - 1) / tx) * ((cfg->ny + NOALLOC_ROWS - 1) / NOALLOC_ROWS);
     if (nwork > NOALLOC_MAX_WORK) { set_error("the no-allocation step takes at most %d work items", NOALLOC_MAX_WORK); return WENOFV_EINVAL; }
 
@@ -176,8 +177,8 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
     int sms = 0;
     WENOFV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device));
     const int flx = eq->eq_kind == WENOFV_EQ_LINEAR_ADV ? 0 : cfg->riemann_flux;
-    const int bps = strictf ? strict::stage_blocks_per_sm(eq->eq_kind, recon, fp32, sch, flx)
-                            : fast::stage_blocks_per_sm(eq->eq_kind, recon, fp32, sch, flx);
+    const int bps = strictf ? strict::stage_blocks_per_sm(eq->eq_kind, recon, fp32, sch, flx, NOALLOC_NT)
+                            : fast::stage_blocks_per_sm(eq->eq_kind, recon, fp32, sch, flx, NOALLOC_NT);
     const int grid = (int)(k < (long)sms * (bps > 0 ? bps : 1) ? k : (long)sms * (bps > 0 ? bps : 1));
     for (int stage = 0; stage < stage_count(cfg->rk_method); stage++) {
         const Roles ro = stage_roles(cfg->rk_method, 0, stage);
@@ -195,8 +196,8 @@ extern "C" int wenofv_step_noalloc(const wenofv_config *cfg, const wenofv_eq_par
         L.final_stage = stage == stage_count(cfg->rk_method) - 1;
         L.rk1 = cfg->rk_method == 0;
         stage_coeffs(cfg->rk_method, stage, L.A, L.B, L.C);
-        const int lrc = strictf ? strict::launch_stage(eq->eq_kind, recon, 0, sch, flx, L, grid, stream)
-                                : fast::launch_stage(eq->eq_kind, recon, fp32, sch, flx, L, grid, stream);
+        const int lrc = strictf ? strict::launch_stage(eq->eq_kind, recon, 0, sch, flx, NOALLOC_NT, L, grid, stream)
+                                : fast::launch_stage(eq->eq_kind, recon, fp32, sch, flx, NOALLOC_NT, L, grid, stream);
         if (lrc) return cuda_fail((cudaError_t)lrc, "stage kernel launch");
     }
     if (flags) {

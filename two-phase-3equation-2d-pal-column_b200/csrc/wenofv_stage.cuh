@@ -14,7 +14,7 @@
 // cells whose stencils contain it (the reference recomputes it per cell,
 // src/WENOFV.cpp:670-687 and :796-833, with identical operands).
 //
-// Thread mapping (NT threads, StageThreads): a unit of the y-sweep is (position, variable), of the
+// Thread mapping (NT threads, 128 or 256): a unit of the y-sweep is (position, variable), of the
 // x-sweep (cell, variable), of the Riemann phase (face, Gauss point) and of the update
 // (cell, variable); groups of NV (or 4) consecutive lanes belong to the same position, cell
 // or face, so characteristic projections, the limiter's theta and the GL quadrature sums
@@ -37,18 +37,17 @@ namespace strict {
 namespace fast {
 #endif
 
-// threads per CTA of a stage kernel.  256 (strips of 58 columns) for the 4-variable systems:
-// the halo positions and the idle lanes of the x-sweep, Riemann and update phases drop from
-// ~19 % to ~9 % of the thread slots.  The FP64 forms run 2 CTAs per SM at 128 registers
-// (0.892 ms per stage of the 1024^2 column, against 1.053 for 3 CTAs of 128 threads at 168
-// registers), FP32-bulk 2 CTAs as well (0.776 against 0.838 for 5 CTAs of 128 at 96
-// registers) and the Euler FP32-bulk form, whose flux stays FP64, 3.  128 for PRIMITIVE3 (its
-// variable-major y-sweep maps 4 warps to 32 positions), for scalar advection (strips of 122
-// columns already) and for the stiffened gas (whose Newton equilibrium spills at 128
-// registers).
-template <int EQ, int RECON, class R> struct StageThreads {
-    static constexpr int value =
-        (EqTraits<EQ>::NV == 4 && RECON != 4 && EQ != EQ_TWO_PHASE_SG) ? 256 : 128;
+// Threads per CTA of a stage kernel: 128 (strips of 26 columns for the 4-variable systems)
+// or, for the 4-variable systems except PRIMITIVE3 and the stiffened gas, also 256 (strips of
+// 58 columns).  The wide form cuts the halo positions and idle lanes of the x-sweep, Riemann
+// and update phases from ~19 % to ~9 % of the thread slots, which makes it 15 % faster on a
+// 1024-wide grid (FP64: 0.892 ms per 1024^2 stage against 1.053; FP32-bulk 0.776 against
+// 0.838), but a narrow grid fills its last strip poorly (a 64-wide grid runs 58 + 6 columns),
+// so the engine chooses the width per instance.  PRIMITIVE3 stays at 128 (its variable-major
+// y-sweep maps 4 warps to 32 positions), as does the stiffened gas (whose Newton equilibrium
+// spills at 128 registers); scalar advection has strips of 122 columns at 128 already.
+template <int EQ, int RECON, class R> struct StageWide {
+    static constexpr bool value = EqTraits<EQ>::NV == 4 && RECON != 4 && EQ != EQ_TWO_PHASE_SG;
 };
 constexpr int CFL_NT = 128; // threads per CTA of cfl_kernel
 
@@ -826,22 +825,22 @@ __device__ __forceinline__ double phase_update(StageSmem<EQ, H, NT> &S, const In
     return cmin;
 }
 
-// resident CTAs per SM the register allocation is bounded for (measured best): the FP64
-// forms of 256 threads at 2 (128 registers, a few spilled values); PRIMITIVE3 (128 threads)
-// at 3, which keeps all values in registers (4 spills and runs slower); the FP32-bulk form
-// runs 4 (conservative) or 5 (characteristic, a few spilled values) CTAs of 128
-template <int EQ, int RECON, class R> struct StageMinBlocks {
-    static constexpr int value = sizeof(R) < sizeof(double) ? (StageThreads<EQ, RECON, R>::value == 256 ? (EQ == EQ_EULER ? 3 : 2) : (RECON == 1 ? 5 : 4))
-                                                              : (StageThreads<EQ, RECON, R>::value == 256 ? 2 : 3);
+// resident CTAs per SM the register allocation is bounded for (measured best).  128 threads:
+// the FP64 forms at 3, which keeps all values in registers (4 spills and runs slower), the
+// FP32-bulk form at 4 (conservative) or 5 (characteristic, a few spilled values).  256
+// threads: 2 (128 registers, a few spilled values), the Euler FP32-bulk form (its flux stays
+// FP64) 3
+template <int EQ, int RECON, class R, int NT> struct StageMinBlocks {
+    static constexpr int value = NT == 256 ? ((sizeof(R) < sizeof(double) && EQ == EQ_EULER) ? 3 : 2)
+                                           : (sizeof(R) < sizeof(double) ? (RECON == 1 ? 5 : 4) : 3);
 };
 
 // SCH, FLX: the scheme (0 WENO-JS, 1 WENO-Z, 2 WENOEXP) and flux (0 LLF, 1 HLLC) of every
 // instance of the launch, as compile-time constants (the engine groups instances by them)
-template <int EQ, int RECON, class R, int SCH, int FLX>
-__global__ void __launch_bounds__(StageThreads<EQ, RECON, R>::value, StageMinBlocks<EQ, RECON, R>::value)
-    stage_kernel(const StageLaunch L)
+template <int EQ, int RECON, class R, int SCH, int FLX, int NT>
+__global__ void __launch_bounds__(NT, StageMinBlocks<EQ, RECON, R, NT>::value) stage_kernel(const StageLaunch L)
 {
-    constexpr int NT = StageThreads<EQ, RECON, R>::value;
+    static_assert(NT == 128 || (NT == 256 && StageWide<EQ, RECON, R>::value), "stage kernel width");
     constexpr int H = StencilRecon<R, SCH>::H;
     constexpr int TX = StageGeom<EQ, H, NT>::TX;
     // the CTA's shared block is dynamic shared memory (it outgrows the 48 KB static limit for

@@ -64,11 +64,13 @@ struct StageLaunch {
 // host launchers exported by each build of wenofv_kernels.cu
 #define WENOFV_DECLARE_LAUNCHERS(NS)                                                                     \
     namespace NS {                                                                                       \
-    int stage_tx(int eq, int recon, int fp32, int scheme);                                               \
-    int launch_stage(int eq, int recon, int fp32, int scheme, int flux, const StageLaunch &L, int grid,  \
-                     void *stream);                                                                     \
-    int launch_cfl(int eq, int recon, int fp32, int scheme, const StageLaunch &L, int grid, void *stream); \
-    int stage_blocks_per_sm(int eq, int recon, int fp32, int scheme, int flux);                          \
+    int stage_wide(int eq, int recon);                                                                   \
+    int stage_tx(int eq, int recon, int fp32, int scheme, int nt);                                       \
+    int launch_stage(int eq, int recon, int fp32, int scheme, int flux, int nt, const StageLaunch &L,    \
+                     int grid, void *stream);                                                           \
+    int launch_cfl(int eq, int recon, int fp32, int scheme, int nt, const StageLaunch &L, int grid,      \
+                   void *stream);                                                                       \
+    int stage_blocks_per_sm(int eq, int recon, int fp32, int scheme, int flux, int nt);                  \
     int probe_weno(int scheme, int fp32, const double *d_st, int n, double *d_out, void *stream);       \
     int probe_weno_exp(const double *d_st, int n, double dx4, double *d_out, void *stream);             \
     int probe_riemann(const EqParams &P, int flux, int fp32, const double *d_UL, const double *d_UR,   \
