@@ -350,7 +350,7 @@ int Engine::alloc_instance(int i, const wenofv_config &c, const wenofv_eq_params
         WENOFV_CUDA(cudaMalloc(&dframe_[i], frame_bytes(c, e)));
         d.frame = dframe_[i];
     }
-    if (!slot_mode && c.pp_limiter && e.eq_kind != WENOFV_EQ_LINEAR_ADV) { // the limiter's per-cell record
+    if (theta_record && c.pp_limiter && e.eq_kind != WENOFV_EQ_LINEAR_ADV) { // the limiter's per-cell record
         WENOFV_CUDA(cudaMalloc(&dtheta_[i], (size_t)c.nx * c.ny));
         WENOFV_CUDA(cudaMemsetAsync(dtheta_[i], 0, (size_t)c.nx * c.ny, stream));
         d.theta_flag = dtheta_[i];

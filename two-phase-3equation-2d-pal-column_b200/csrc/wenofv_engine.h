@@ -85,7 +85,8 @@ public:
     int device = 0;
     int n = 0;
     int rk = 2;
-    bool slot_mode = false; // serving: every slot keeps its own current buffer
+    bool slot_mode = false;    // serving: every slot keeps its own current buffer
+    bool theta_record = false; // contexts: keep the limiter's per-cell record (wenofv_theta_flags)
 
 private:
     // one persistent launch per RK stage for the instances of one template key; the work
