@@ -560,6 +560,7 @@ struct ExpThinc {
 // run in FP64 (also in the FP32-bulk form): the cancellation in q - qs and the division by
 // z2 rho2 c2^2 near pure phases need it.
 struct TwoPhaseK {
+    static constexpr bool linear = true; // constant phase sound speeds
     double c1_2, c2_2, q, rho10, rho20;
     __device__ __forceinline__ explicit TwoPhaseK(const EqParams &p)
     {
@@ -669,6 +670,7 @@ struct TwoPhaseK {
 // CUDA's, so the results agree with the C library's to a few ulp, not bit for bit.
 constexpr int SG_NEWTON = 12;
 struct StiffK {
+    static constexpr bool linear = false;
     TwoPhaseK lin;
     double g1, g2, pi1, pi2, pref, rho10, rho20, a1, a2, ig1, ig2, lo, scale;
     __device__ __forceinline__ explicit StiffK(const EqParams &p) : lin(p)
@@ -980,8 +982,50 @@ template <class R> struct TPEigen {
     R z1rho1, z2rho2, rho, u, v, c, c2, sc1_2, sc2_2;
     R i2c2, i2c, irc2, idsc, irho, pad; // reciprocals of the contracted build; pad: odd size in smem
 };
+#if !WENOFV_STRICT
+// The linear model's eigensystem data in the contracted build, with two divisions and one
+// square root besides the state recovery (the strict build keeps the reference's expressions).
+// With A_k = z_k rho_k c_k^2 and S = z1^2 A2 + z2^2 A1 (the Wood sum of sound()):
+//   c^2 = A1 A2 / (rho S),  1/(2c^2) = rho S / (2 A1 A2),  1/(rho c^2) = S / (A1 A2),
+//   sc1^2 = c1^2 c2^2 z1 z2rho2 / S,  sc2^2 = c1^2 c2^2 z2 z1rho1 / S
+// (sc_k^2 = c_k^2/z_k - c_k^2/z_k zrho_k / (zrho1 + zrho2), zrho_k = z_krho_k c_k^2 / z_k^2,
+// multiplied through by z1^2 z2^2), and 1/(sc1^2 - sc2^2) = S / (c1^2 c2^2 (z1 z2rho2 - z2 z1rho1)).
+// W = 1/(A1 A2 S) yields both 1/(A1 A2) and 1/S.
+__device__ __forceinline__ void tp_eigen_prep_linear(const TwoPhaseK &K, const double *U, TPEigen<double> &e)
+{
+    const double m1 = U[0], m2 = U[1];
+    e.z1rho1 = m1; e.z2rho2 = m2;
+    e.rho = m1 + m2;
+    double z1, pd;
+    K.recover_rho(m1, m2, e.rho, e.irho, z1, pd);
+    e.u = U[2] * e.irho;
+    e.v = U[3] * e.irho;
+    const double z2 = 1.0 - z1;
+    const double A1 = m1 * K.c1_2, A2 = m2 * K.c2_2;
+    const double Sw = z1 * z1 * A2 + z2 * z2 * A1;
+    const double P = A1 * A2;
+    const double W = 1.0 / (P * Sw);
+    const double iS = P * W, iP = Sw * W;
+    e.c2 = P * iS * e.irho;
+    e.c = sqrt(e.c2);
+    e.i2c2 = 0.5 * e.rho * Sw * iP;
+    e.i2c = e.c * e.i2c2;
+    e.irc2 = Sw * iP;
+    const double B = K.c1_2 * K.c2_2;
+    const double d1 = z1 * m2, d2 = z2 * m1;
+    e.sc1_2 = B * d1 * iS;
+    e.sc2_2 = B * d2 * iS;
+    e.idsc = Sw / (B * (d1 - d2));
+}
+#endif
 template <class R, class KT> __device__ __forceinline__ void tp_eigen_prep(const KT &K, const double *U, TPEigen<R> &e)
 {
+#if !WENOFV_STRICT
+    if constexpr (sizeof(R) == sizeof(double) && KT::linear) {
+        tp_eigen_prep_linear(K, U, e);
+        return;
+    }
+#endif
     e.z1rho1 = (R)U[0]; e.z2rho2 = (R)U[1];
     e.rho = e.z1rho1 + e.z2rho2;
 #if WENOFV_STRICT

@@ -385,8 +385,15 @@ __device__ __forceinline__ void phase_eigen(StageSmem<EQ, H, NT> &S, const InstD
             if (D.limiter) { // src/WENOFV.cpp:1954-1957
                 double a1, a2;
                 max_eigs_of<EQ>(S.se[p], a1, a2);
+#if WENOFV_STRICT
                 S.smu[p][0] = (a1 / D.dX) / (a1 / D.dX + a2 / D.dY);
                 S.smu[p][1] = (a2 / D.dY) / (a1 / D.dX + a2 / D.dY);
+#else
+                // the same weights multiplied through by dX dY: one division
+                const double s1 = a1 * D.dY, s2 = a2 * D.dX, iv = 1.0 / (s1 + s2);
+                S.smu[p][0] = s1 * iv;
+                S.smu[p][1] = s2 * iv;
+#endif
             }
         }
     }
