@@ -594,10 +594,13 @@ struct TwoPhaseK {
         const double qs = z2rho2 * c2_2 - z1rho1 * c1_2;
         const double N = (q - qs) + sqrt((q - qs) * (q - qs) + 4.0 * z1rho1 * c1_2 * z2rho2 * c2_2);
         const double Dn = 2.0 * z2rho2 * c2_2;
-        z1 = N / (N + Dn);
+        const double ND = N + Dn;
+        const double Ng = N > 0.0 ? N : 1.0; // N = 0: z1 = 0, pre1 unused
+        const double inv = 1.0 / (ND * Ng);  // 1/(N + D) = Ng inv, 1/N = ND inv
+        z1 = N * (Ng * inv);
         const double z2 = 1.0 - z1;
         const double pre2 = c2_2 * (z2rho2 - rho20) + 0.5 * N; // c2^2 (z2rho2 / z2 - rho20)
-        const double pre1 = c1_2 * (z1rho1 + z1rho1 * Dn / N - rho10); // c1^2 (z1rho1 / z1 - rho10)
+        const double pre1 = c1_2 * (z1rho1 + z1rho1 * Dn * (ND * inv) - rho10); // c1^2 (z1rho1 / z1 - rho10)
         p = (z1 < z2) ? pre2 : pre1;
     }
     // recover plus 1/rho of the same state with one division for 1/rho and 1/(N+D)
@@ -608,12 +611,13 @@ struct TwoPhaseK {
         const double N = (q - qs) + sqrt((q - qs) * (q - qs) + 4.0 * z1rho1 * c1_2 * z2rho2 * c2_2);
         const double Dn = 2.0 * z2rho2 * c2_2;
         const double ND = N + Dn;
-        const double inv = 1.0 / (rho * ND);
-        irho = ND * inv;
-        z1 = N * (rho * inv);
+        const double Ng = N > 0.0 ? N : 1.0; // N = 0: z1 = 0, pre1 unused
+        const double inv = 1.0 / (rho * ND * Ng); // 1/rho = ND Ng inv, 1/ND = rho Ng inv, 1/N = rho ND inv
+        irho = ND * Ng * inv;
+        z1 = N * (rho * Ng * inv);
         const double z2 = 1.0 - z1;
         const double pre2 = c2_2 * (z2rho2 - rho20) + 0.5 * N;
-        const double pre1 = c1_2 * (z1rho1 + z1rho1 * Dn / N - rho10);
+        const double pre1 = c1_2 * (z1rho1 + z1rho1 * Dn * (rho * ND * inv) - rho10);
         p = (z1 < z2) ? pre2 : pre1;
     }
     // the strict order of tp_state: getVolumeFrac, then getPressure
