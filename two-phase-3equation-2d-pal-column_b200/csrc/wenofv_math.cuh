@@ -650,9 +650,13 @@ struct TwoPhaseK {
     {
 #if !WENOFV_STRICT
         if constexpr (sizeof(R) == sizeof(double)) {
-            // 1/c^2 = rho (z1^2/(z1rho1 c1^2) + z2^2/(z2rho2 c2^2)): one division, one sqrt
+            // 1/c^2 = rho (z1^2/(z1rho1 c1^2) + z2^2/(z2rho2 c2^2)) = T / P: c = sqrt(P/T) =
+            // |P| / sqrt(P T), one reciprocal square root, for either sign of P and T (a
+            // reconstructed partial density below 0 makes both negative); c = 0 where P = 0
             const double a1 = z1rho1 * c1_2, a2 = z2rho2 * c2_2;
-            return sqrt(a1 * a2 / ((z1rho1 + z2rho2) * (z1 * z1 * a2 + z2 * z2 * a1)));
+            const double P = a1 * a2;
+            const double T = (z1rho1 + z2rho2) * (z1 * z1 * a2 + z2 * z2 * a1);
+            return P == 0.0 ? 0.0 : fabs(P) * rsqrt(P * T);
         }
 #endif
         const R rho = z1rho1 + z2rho2;
@@ -762,7 +766,8 @@ template <> struct TPKOf<EQ_TWO_PHASE_SG> { using type = StiffK; };
 // reference recomputes getVolumeFrac per call; the values are identical).
 template <class R> struct TPState {
     R z1rho1, z2rho2, rhou, rhov, rho, u, v, pre, c;
-    double pd; // the FP64 pressure (pre is pd rounded to R)
+    double pd;   // the FP64 pressure (pre is pd rounded to R)
+    double irho; // 1/rho (contracted FP64 build)
 };
 
 // The state comes in FP64 in every form: the volume fraction and the pressure are
@@ -780,10 +785,9 @@ __device__ __forceinline__ void tp_state(const KT &K, const double *U, TPState<R
 #else
     double z1;
     if constexpr (sizeof(R) == sizeof(double)) {
-        double ir;
-        K.recover_rho(U[0], U[1], s.rho, ir, z1, s.pd);
-        s.u = s.rhou * ir;
-        s.v = s.rhov * ir;
+        K.recover_rho(U[0], U[1], s.rho, s.irho, z1, s.pd);
+        s.u = s.rhou * s.irho;
+        s.v = s.rhov * s.irho;
     } else {
         const R ir = R(1) / s.rho;
         s.u = s.rhou * ir;
@@ -852,10 +856,21 @@ __device__ __forceinline__ void tp_hllc(const TPState<R> &L, const TPState<R> &R
     R c2_roe = (L.c * L.c * sL + Rs.c * Rs.c * sR) / (sL + sR);
     c2_roe += R(0.5) * sL * sR / (sL + sR) / (sL + sR) * (vn_R - vn_L) * (vn_R - vn_L);
 #else
-    const R is = R(1) / (sL + sR);
-    const R vn_roe = (vn_L * sL + vn_R * sR) * is;
-    R c2_roe = (L.c * L.c * sL + Rs.c * Rs.c * sR) * is;
-    c2_roe += R(0.5) * sL * sR * is * is * (vn_R - vn_L) * (vn_R - vn_L);
+    R vn_roe, c2_roe;
+    if constexpr (sizeof(R) == sizeof(double)) {
+        // Roe weights w_L = sL/(sL+sR) = 1/(1+t), w_R = t w_L with t = sqrt(rho_R/rho_L):
+        // one square root and one division
+        const R t = sqrt(Rs.rho * L.irho);
+        const R wL = R(1) / (R(1) + t), wR = t * wL;
+        vn_roe = vn_L * wL + vn_R * wR;
+        c2_roe = L.c * L.c * wL + Rs.c * Rs.c * wR;
+        c2_roe += R(0.5) * wL * wR * (vn_R - vn_L) * (vn_R - vn_L);
+    } else {
+        const R is = R(1) / (sL + sR);
+        vn_roe = (vn_L * sL + vn_R * sR) * is;
+        c2_roe = (L.c * L.c * sL + Rs.c * Rs.c * sR) * is;
+        c2_roe += R(0.5) * sL * sR * is * is * (vn_R - vn_L) * (vn_R - vn_L);
+    }
 #endif
     const R c_roe = sqrt(c2_roe);
     const R S_L = std_min(vn_L - L.c, vn_roe - c_roe);

@@ -232,8 +232,12 @@ template <int EQ, int H, int NT> struct StageSmem {
     // number of doubles (neighbouring positions 2 banks apart).
     static constexpr int PS = NV > 1 ? P + 4 : P; // row stride of su / sun
     static constexpr int YS = 4 * NV + 1;         // position stride of sy
-    static constexpr int FS = 8 * NV + 1;         // face stride of sxf
-    static constexpr int BS = 4 * NV + 1;         // cell stride of syb / syt
+    // face states of 4 variables: strides of 4 (mod 16) doubles with the variable slot rotated
+    // by the face index (face_slot), so that both the writers (4 cells x 4 variables of a
+    // half-warp, one point) and the readers (4 faces x 4 points, one variable) hit 16
+    // distinct banks
+    static constexpr int FS = NV == 4 ? 36 : 8 * NV + 1; // face stride of sxf
+    static constexpr int BS = NV == 4 ? 20 : 4 * NV + 1; // cell stride of syb / syt
     double su[8][NV][PS];   // ring of stage-input rows
     double sun[2][NV][PS];  // U^n rows (stages after the first)
     double sy[P][YS];       // y-sweep of the current row: [position][y GL point * NV + var]
@@ -250,6 +254,14 @@ template <int EQ, int H, int NT> struct StageSmem {
     double sred[NT / 32];
     int s_last;
 };
+
+// slot of variable v in the face-state records of face (or cell) f: rotated by f for 4
+// variables (the bank layout of StageSmem::FS / BS), the variable itself otherwise
+template <int NV> __device__ __forceinline__ int face_slot(int v, int f)
+{
+    if constexpr (NV == 4) return (v + f) & 3;
+    else return v;
+}
 
 // bytes of a CTA's StageSmem, rounded to 16 (the primitive ring follows it)
 template <int EQ, int H, int NT> struct StageSmemBytes {
@@ -702,11 +714,11 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
     if (active) {
 #pragma unroll
         for (int gp = 0; gp < 4; gp++) {
-            if (c >= 0) S.sxf[c][(4 + gp) * NV + v] = fv[0][gp];     // left face: plus side of face c
-            if (c < TX) S.sxf[c + 1][gp * NV + v] = fv[3][gp]; // right face: minus side of face c+1
+            if (c >= 0) S.sxf[c][(4 + gp) * NV + face_slot<NV>(v, c)] = fv[0][gp];     // left face: plus side of face c
+            if (c < TX) S.sxf[c + 1][gp * NV + face_slot<NV>(v, c + 1)] = fv[3][gp]; // right face: minus side of face c+1
             if (c >= 0 && c < TX) {
-                S.syb[c][gp * NV + v] = fv[gp][0];
-                S.syt[r & 1][c][gp * NV + v] = fv[gp][3];
+                S.syb[c][gp * NV + face_slot<NV>(v, c)] = fv[gp][0];
+                S.syt[r & 1][c][gp * NV + face_slot<NV>(v, c)] = fv[gp][3];
             }
         }
     }
@@ -738,10 +750,18 @@ __device__ __forceinline__ void phase_riemann(StageSmem<EQ, H, NT> &S, const Ins
         double UL[NV], UR[NV], F[NV];
         if (xf) {
 #pragma unroll
-            for (int v = 0; v < NV; v++) { UL[v] = S.sxf[f][gp * NV + v]; UR[v] = S.sxf[f][(4 + gp) * NV + v]; }
+            for (int v = 0; v < NV; v++) {
+                const int k = face_slot<NV>(v, f);
+                UL[v] = S.sxf[f][gp * NV + k];
+                UR[v] = S.sxf[f][(4 + gp) * NV + k];
+            }
         } else {
 #pragma unroll
-            for (int v = 0; v < NV; v++) { UL[v] = S.syt[(r - 1) & 1][f][gp * NV + v]; UR[v] = S.syb[f][gp * NV + v]; }
+            for (int v = 0; v < NV; v++) {
+                const int k = face_slot<NV>(v, f);
+                UL[v] = S.syt[(r - 1) & 1][f][gp * NV + k];
+                UR[v] = S.syb[f][gp * NV + k];
+            }
         }
         riemann<EQ, R, FLX>(D.eq, D.flux, UL, UR, F, xf);
         // gWeight = m_gweights_ref[gp] * (cell size) / 2.0 (src/WENOFV.cpp:1774, :1793)
