@@ -231,7 +231,7 @@ template <int EQ, int H, int NT> struct StageSmem {
     // (variable v of 4 neighbouring positions: banks 8v + 2p), positions and cells at an odd
     // number of doubles (neighbouring positions 2 banks apart).
     static constexpr int PS = NV > 1 ? P + 4 : P; // row stride of su / sun
-    static constexpr int YS = 4 * NV + 1;         // position stride of sy
+    static constexpr int YS = NV == 4 ? 20 : 4 * NV + 1; // position stride of sy (see sy_index)
     // face states of 4 variables: strides of 4 (mod 16) doubles with the variable slot rotated
     // by the face index (face_slot), so that both the writers (4 cells x 4 variables of a
     // half-warp, one point) and the readers (4 faces x 4 points, one variable) hit 16
@@ -240,7 +240,7 @@ template <int EQ, int H, int NT> struct StageSmem {
     static constexpr int BS = NV == 4 ? 20 : 4 * NV + 1; // cell stride of syb / syt
     double su[8][NV][PS];   // ring of stage-input rows
     double sun[2][NV][PS];  // U^n rows (stages after the first)
-    double sy[P][YS];       // y-sweep of the current row: [position][y GL point * NV + var]
+    double sy[P * YS];      // y-sweep of the current row by (position, y GL point, variable): sy_index
     double sxf[TX + 1][FS]; // x-face states: [face][(minus/plus side * 4 + GL point) * NV + var]
     double syb[TX][BS];     // bottom face states of the current row: [cell][GL point * NV + var]
     double syt[2][TX][BS];  // top face states of the current and previous row
@@ -261,6 +261,17 @@ template <int NV> __device__ __forceinline__ int face_slot(int v, int f)
 {
     if constexpr (NV == 4) return (v + f) & 3;
     else return v;
+}
+
+// element (position p, y Gauss point g, variable v) of StageSmem::sy.  Conservative and
+// characteristic sweeps (4 variables): position stride 20 (4 mod 16 doubles), so that the
+// writers and the x-sweep's readers, 4 positions x 4 variables of a half-warp each, hit 16
+// distinct banks; primitive sweeps (whose x-sweep lanes read one point of 4 variables per
+// cell, 4 cells x 4 points) stride 4 NV + 1.
+template <int RECON, int NV> __device__ __forceinline__ int sy_index(int p, int g, int v)
+{
+    if constexpr (NV == 4 && RECON < 2) return p * 20 + g * 4 + v;
+    else return p * (4 * NV + 1) + g * NV + v;
 }
 
 // bytes of a CTA's StageSmem, rounded to 16 (the primitive ring follows it)
@@ -473,7 +484,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
         R o[4];
         W.eval4(o);
 #pragma unroll
-        for (int gp = 0; gp < 4; gp++) S.sy[p][gp * NV + v] = anchor<DEV>(c0, o[gp]);
+        for (int gp = 0; gp < 4; gp++) S.sy[sy_index<RECON, NV>(p, gp, v)] = anchor<DEV>(c0, o[gp]);
     } else {
         // characteristic: project with L(U_centre, y), reconstruct, project back with R(U_centre, y).
         // The eigenvectors and the forward projection are FP64 in every form: the two-phase
@@ -512,12 +523,12 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
                 R s = R(0);
 #pragma unroll
                 for (int k = 0; k < NV; k++) s += (R)Rrow[k] * __shfl_sync(0xffffffffu, cg[gp], gbase + k);
-                S.sy[p][gp * NV + v] = Uc[v] + (double)s;
+                S.sy[sy_index<RECON, NV>(p, gp, v)] = Uc[v] + (double)s;
             } else {
                 double s = 0.0;
 #pragma unroll
                 for (int k = 0; k < NV; k++) s += Rrow[k] * (double)__shfl_sync(0xffffffffu, cg[gp], gbase + k);
-                S.sy[p][gp * NV + v] = s;
+                S.sy[sy_index<RECON, NV>(p, gp, v)] = s;
             }
         }
     }
@@ -555,7 +566,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
             const double ck = DEV ? ring[r & 7][k][c + GH] : 0.0; // deviation anchor: the primitive average
             R sv[NS];
 #pragma unroll
-            for (int m = 0; m < NS; m++) sv[m] = (R)(S.sy[c + 1 + m][gj * NV + k] - ck);
+            for (int m = 0; m < NS; m++) sv[m] = (R)(S.sy[sy_index<RECON, NV>(c + 1 + m, gj, k)] - ck);
             SR W;
             W.init(sv, D.scheme, k, D.dx4);
             R o[4];
@@ -592,7 +603,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
             // the stencil of cell c: positions c+GH-H .. c+GH+H = c+1 .. c+1+2H
             R sv[NS];
 #pragma unroll
-            for (int m = 0; m < NS; m++) sv[m] = (R)(S.sy[c + 1 + m][gpj * NV + v] - cc);
+            for (int m = 0; m < NS; m++) sv[m] = (R)(S.sy[sy_index<RECON, NV>(c + 1 + m, gpj, v)] - cc);
             SR W;
             W.init(sv, D.scheme, v, D.dx4);
             if (gpj == 0 || gpj == 3) {
@@ -626,7 +637,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
             for (int m = 0; m < NS; m++) {
                 double s = 0.0;
 #pragma unroll
-                for (int j = 0; j < NV; j++) s += Lrow[j] * S.sy[c + 1 + m][gpj * NV + j];
+                for (int j = 0; j < NV; j++) s += Lrow[j] * S.sy[sy_index<RECON, NV>(c + 1 + m, gpj, j)];
                 pr[m] = DEV ? (R)(s - lc) : (R)s;
             }
             SR W;
