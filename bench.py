@@ -560,11 +560,14 @@ def summarize_errors(err, bar=1e-5):
     e32, e64 = np.asarray(err["fp32_bulk"]), np.asarray(err["fp64"])
     # an instance "within the scheme's spread": FP32's error at most 10x the FP64 form's
     excused = [(a > bar and a <= 10 * b) for a, b in zip(e32, e64)]
+    unexplained = [dict(k=k, fp32=float(a), fp64=float(b)) for k, (a, b, x) in enumerate(zip(e32, e64, excused))
+                   if a > bar and not x]
+    unexplained.sort(key=lambda r: -r["fp32"])
     return dict(fp32_vs_oracle=dict(median=_pctl(e32, 50), p90=_pctl(e32, 90), max=float(e32.max()) if len(e32) else None,
                                     within_bar=int(np.sum(e32 <= bar)), n=int(len(e32))),
                 fp64_vs_oracle=dict(median=_pctl(e64, 50), p90=_pctl(e64, 90), max=float(e64.max()) if len(e64) else None),
                 over_bar_explained_by_fp64_spread=int(np.sum(excused)),
-                over_bar_unexplained=int(np.sum([(a > bar and not x) for a, x in zip(e32, excused)])),
+                over_bar_unexplained=len(unexplained), unexplained_instances=unexplained[:16],
                 bar=bar, note="pooled relative L1 per instance against FP64_STRICT (the oracle's arithmetic, "
                               "bit for bit); an instance over the bar whose FP64-form spread is within 10x of its "
                               "FP32-bulk error is the scheme's own roundoff sensitivity, not FP32's")
