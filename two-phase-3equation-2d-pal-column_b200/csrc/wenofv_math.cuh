@@ -603,22 +603,36 @@ struct TwoPhaseK {
         const double pre1 = c1_2 * (z1rho1 + z1rho1 * Dn * (ND * inv) - rho10); // c1^2 (z1rho1 / z1 - rho10)
         p = (z1 < z2) ? pre2 : pre1;
     }
-    // recover plus 1/rho of the same state with one division for 1/rho and 1/(N+D)
+    // recover plus 1/rho of the same state with one division for 1/rho, 1/(N+D) and 1/N, in two
+    // halves so that two states can share the division (recover_pair)
+    struct Rec { double N, Dn, ND, Ng, X; };
+    __device__ __forceinline__ Rec recover_a(double z1rho1, double z2rho2, double rho) const
+    {
+        Rec a;
+        const double qs = z2rho2 * c2_2 - z1rho1 * c1_2;
+        a.N = (q - qs) + sqrt((q - qs) * (q - qs) + 4.0 * z1rho1 * c1_2 * z2rho2 * c2_2);
+        a.Dn = 2.0 * z2rho2 * c2_2;
+        a.ND = a.N + a.Dn;
+        a.Ng = a.N > 0.0 ? a.N : 1.0; // N = 0: z1 = 0, pre1 unused
+        a.X = rho * a.ND * a.Ng;
+        return a;
+    }
+    // inv = 1/X: 1/rho = ND Ng inv, 1/ND = rho Ng inv, 1/N = rho ND inv
+    __device__ __forceinline__ void recover_b(const Rec &a, double inv, double z1rho1, double z2rho2, double rho, double &irho,
+                                              double &z1, double &p) const
+    {
+        irho = a.ND * a.Ng * inv;
+        z1 = a.N * (rho * a.Ng * inv);
+        const double z2 = 1.0 - z1;
+        const double pre2 = c2_2 * (z2rho2 - rho20) + 0.5 * a.N;
+        const double pre1 = c1_2 * (z1rho1 + z1rho1 * a.Dn * (rho * a.ND * inv) - rho10);
+        p = (z1 < z2) ? pre2 : pre1;
+    }
     __device__ __forceinline__ void recover_rho(double z1rho1, double z2rho2, double rho, double &irho, double &z1,
                                                 double &p) const
     {
-        const double qs = z2rho2 * c2_2 - z1rho1 * c1_2;
-        const double N = (q - qs) + sqrt((q - qs) * (q - qs) + 4.0 * z1rho1 * c1_2 * z2rho2 * c2_2);
-        const double Dn = 2.0 * z2rho2 * c2_2;
-        const double ND = N + Dn;
-        const double Ng = N > 0.0 ? N : 1.0; // N = 0: z1 = 0, pre1 unused
-        const double inv = 1.0 / (rho * ND * Ng); // 1/rho = ND Ng inv, 1/ND = rho Ng inv, 1/N = rho ND inv
-        irho = ND * Ng * inv;
-        z1 = N * (rho * Ng * inv);
-        const double z2 = 1.0 - z1;
-        const double pre2 = c2_2 * (z2rho2 - rho20) + 0.5 * N;
-        const double pre1 = c1_2 * (z1rho1 + z1rho1 * Dn * (rho * ND * inv) - rho10);
-        p = (z1 < z2) ? pre2 : pre1;
+        const Rec a = recover_a(z1rho1, z2rho2, rho);
+        recover_b(a, 1.0 / a.X, z1rho1, z2rho2, rho, irho, z1, p);
     }
     // the strict order of tp_state: getVolumeFrac, then getPressure
     __device__ __forceinline__ void state(double z1rho1, double z2rho2, double &z1, double &p) const
@@ -797,6 +811,59 @@ __device__ __forceinline__ void tp_state(const KT &K, const double *U, TPState<R
 #endif
     s.pre = (R)s.pd;
     s.c = K.template sound_p<R>(s.z1rho1, s.z2rho2, (R)z1, (R)(1.0 - z1), s.pd);
+}
+
+// the two face states of a Riemann problem: in the contracted FP64 build of the linear model
+// their recoveries share one division (1/(X_L X_R) gives 1/X_L and 1/X_R), otherwise tp_state
+// twice
+template <class R, class KT>
+__device__ __forceinline__ void tp_state_pair(const KT &K, const double *UL, const double *UR, TPState<R> &l, TPState<R> &r)
+{
+#if !WENOFV_STRICT
+    if constexpr (sizeof(R) == sizeof(double) && KT::linear) {
+        l.z1rho1 = UL[0]; l.z2rho2 = UL[1]; l.rhou = UL[2]; l.rhov = UL[3];
+        r.z1rho1 = UR[0]; r.z2rho2 = UR[1]; r.rhou = UR[2]; r.rhov = UR[3];
+        l.rho = l.z1rho1 + l.z2rho2;
+        r.rho = r.z1rho1 + r.z2rho2;
+        const typename KT::Rec a = K.recover_a(UL[0], UL[1], l.rho), b = K.recover_a(UR[0], UR[1], r.rho);
+        const double inv = 1.0 / (a.X * b.X);
+        double z1l, z1r;
+        K.recover_b(a, b.X * inv, UL[0], UL[1], l.rho, l.irho, z1l, l.pd);
+        K.recover_b(b, a.X * inv, UR[0], UR[1], r.rho, r.irho, z1r, r.pd);
+        l.u = l.rhou * l.irho; l.v = l.rhov * l.irho;
+        r.u = r.rhou * r.irho; r.v = r.rhov * r.irho;
+        l.pre = l.pd; r.pre = r.pd;
+        l.c = K.template sound_p<R>(l.z1rho1, l.z2rho2, z1l, 1.0 - z1l, l.pd);
+        r.c = K.template sound_p<R>(r.z1rho1, r.z2rho2, z1r, 1.0 - z1r, r.pd);
+        return;
+    }
+    if constexpr (sizeof(R) < sizeof(double) && KT::linear) {
+        // FP32-bulk: the FP64 recoveries (z1, p) share one division (rho = 1 in the halves:
+        // 1/(N+D) and 1/N only), the rest as tp_state
+        TPState<R> *s2[2] = {&l, &r};
+        const double *U2[2] = {UL, UR};
+        const typename KT::Rec a = K.recover_a(UL[0], UL[1], 1.0), b = K.recover_a(UR[0], UR[1], 1.0);
+        const double inv = 1.0 / (a.X * b.X);
+        double z1[2], dummy;
+        K.recover_b(a, b.X * inv, UL[0], UL[1], 1.0, dummy, z1[0], l.pd);
+        K.recover_b(b, a.X * inv, UR[0], UR[1], 1.0, dummy, z1[1], r.pd);
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            TPState<R> &s = *s2[k];
+            const double *U = U2[k];
+            s.z1rho1 = (R)U[0]; s.z2rho2 = (R)U[1]; s.rhou = (R)U[2]; s.rhov = (R)U[3];
+            s.rho = s.z1rho1 + s.z2rho2;
+            const R ir = R(1) / s.rho;
+            s.u = s.rhou * ir;
+            s.v = s.rhov * ir;
+            s.pre = (R)s.pd;
+            s.c = K.template sound_p<R>(s.z1rho1, s.z2rho2, (R)z1[k], (R)(1.0 - z1[k]), s.pd);
+        }
+        return;
+    }
+#endif
+    tp_state<R>(K, UL, l);
+    tp_state<R>(K, UR, r);
 }
 
 // getMaxEigenValue, include/Equations.hpp:149-156 (u from U[2]/(U[0]+U[1]) as there)
@@ -1357,8 +1424,7 @@ __device__ __forceinline__ void riemann(const EqParams &P, int flux_arg, const d
     if constexpr (IsTwoPhase<EQ>::value) {
         const typename TPKOf<EQ>::type K(P);
         TPState<R> l, r;
-        tp_state<R>(K, ULd, l);
-        tp_state<R>(K, URd, r);
+        tp_state_pair<R>(K, ULd, URd, l, r);
         if constexpr (F32) {
             if (flux == 1) tp_hllc_f32(l, r, F, xdir);
             else tp_llf_f32(l, r, ULd, URd, F, xdir);

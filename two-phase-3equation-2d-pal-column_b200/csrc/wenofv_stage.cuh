@@ -685,7 +685,11 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
                 rem -= omega1 * w / 2 * mu1 * fv[0][gp];
                 rem -= omega1 * w / 2 * mu1 * fv[3][gp];
             }
+#if WENOFV_STRICT
             rem /= omegaR;
+#else
+            rem *= 1.0 / omegaR; // a constant
+#endif
             double mloc = rem;
 #pragma unroll
             for (int gp = 0; gp < 4; gp++) {
