@@ -782,6 +782,30 @@ __device__ __forceinline__ void phase_riemann(StageSmem<EQ, H, NT> &S, const Ins
         // gWeight = m_gweights_ref[gp] * (cell size) / 2.0 (src/WENOFV.cpp:1774, :1793)
         const double wq = xf ? gl_weight(gp) * dyr / 2.0 : gl_weight(gp) * S.sdxc[f] / 2.0;
         bool bad = false;
+#if !WENOFV_STRICT
+        if constexpr (NV == 4) {
+            // contracted build: a reduce-scatter over the face's 4 lanes, after which lane gp
+            // holds the quadrature sum of variable gp, (p0 + p2) + (p1 + p3): three shuffles
+            // for the four variables
+            double pv[4];
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                pv[v] = F[v] * wq;
+                bad |= isnan(pv[v]);
+            }
+            const bool hi = (gp & 2) != 0, odd = (gp & 1) != 0;
+            const double k0 = hi ? pv[2] : pv[0], k1 = hi ? pv[3] : pv[1];
+            const double s0 = hi ? pv[0] : pv[2], s1 = hi ? pv[1] : pv[3];
+            const double r0 = k0 + __shfl_xor_sync(0xffffffffu, s0, 2);
+            const double r1 = k1 + __shfl_xor_sync(0xffffffffu, s1, 2);
+            const double sum = (odd ? r1 : r0) + __shfl_xor_sync(0xffffffffu, odd ? r0 : r1, 1);
+            if (act) {
+                if (xf) S.sfx[r & 1][f][gp] = sum;
+                else S.sfy[r & 1][f][gp] = sum;
+            }
+        } else
+#endif
+        {
 #pragma unroll
         for (int v = 0; v < NV; v++) {
             const double pv = F[v] * wq;
@@ -798,6 +822,7 @@ __device__ __forceinline__ void phase_riemann(StageSmem<EQ, H, NT> &S, const Ins
                 if (xf) S.sfx[r & 1][f][v] = ave;
                 else S.sfy[r & 1][f][v] = ave;
             }
+        }
         }
         if (bad && act && f < TXe + (xf ? 1 : 0)) flag_error(st, 4u, (long long)map_index(r, D.ny, D.bc) * D.nx + i0 + (f < TXe ? f : TXe - 1));
     }
