@@ -274,6 +274,18 @@ template <int RECON, int NV> __device__ __forceinline__ int sy_index(int p, int 
     else return p * (4 * NV + 1) + g * NV + v;
 }
 
+// the 4 values at q (16-byte aligned) by 16-byte shared-memory loads
+template <class R> __device__ __forceinline__ void load4(const R *q, R *o)
+{
+    if constexpr (sizeof(R) == sizeof(double)) {
+        const double2 a = reinterpret_cast<const double2 *>(q)[0], b = reinterpret_cast<const double2 *>(q)[1];
+        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+    } else {
+        const float4 a = reinterpret_cast<const float4 *>(q)[0];
+        o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+    }
+}
+
 // bytes of a CTA's StageSmem, rounded to 16 (the primitive ring follows it)
 template <int EQ, int H, int NT> struct StageSmemBytes {
     static constexpr int value = (int)((sizeof(StageSmem<EQ, H, NT>) + 15) / 16 * 16);
@@ -515,6 +527,39 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
         R cg[4];
         W.eval4(cg);
         const int lane = t & 31, gbase = lane & ~(NV - 1);
+        (void)gbase;
+        if constexpr (NV == 4) {
+            // the 4 characteristic values of a point reach the position's 4 lanes through the
+            // warp's own rows of sy (positions 8w .. 8w+7, written by no other warp), as R at the
+            // element offsets of sy_index; the results overwrite them afterwards
+            R *xs = reinterpret_cast<R *>(&S.sy[sy_index<RECON, NV>(p, 0, 0)]);
+#pragma unroll
+            for (int gp = 0; gp < 4; gp++) xs[gp * 4 + v] = cg[gp];
+            __syncwarp();
+            double out[4];
+#pragma unroll
+            for (int gp = 0; gp < 4; gp++) {
+                R q[4];
+                load4<R>(xs + gp * 4, q);
+                // back-projection: FP32 in the bulk form (it adds an error of the same order as
+                // the FP32 WENO's own, eps * sum_k |R_vk w_k|), FP64 otherwise
+                if constexpr (DEV) {
+                    R s = R(0);
+#pragma unroll
+                    for (int k = 0; k < NV; k++) s += (R)Rrow[k] * q[k];
+                    out[gp] = Uc[v] + (double)s;
+                } else {
+                    double s = 0.0;
+#pragma unroll
+                    for (int k = 0; k < NV; k++) s += Rrow[k] * (double)q[k];
+                    out[gp] = s;
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int gp = 0; gp < 4; gp++) S.sy[sy_index<RECON, NV>(p, gp, v)] = out[gp];
+            return;
+        }
 #pragma unroll
         for (int gp = 0; gp < 4; gp++) {
             // back-projection: FP32 in the bulk form (it adds an error of the same order as the
@@ -628,6 +673,10 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
 #pragma unroll
             for (int j = 0; j < NV; j++) lc += Lrow[j] * Uc[j];
         }
+        // exchange area of this warp's cells (inactive lanes read cell slot 0): element stride
+        // 20 per cell (4 mod 16 doubles: the 16 writers of a half-warp hit distinct banks)
+        R *xs = reinterpret_cast<R *>(&S.sxf[8 * (t >> 5)][0]) + (active ? (lane >> 2) : 0) * 20;
+        (void)xs;
         // per y Gauss point: project, reconstruct, and project back at once, so that only
         // that point's characteristic values are live (not all twelve)
 #pragma unroll
@@ -646,6 +695,35 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
             const bool all4 = gpj == 0 || gpj == 3;
             if (all4) W.eval4(cg);
             else W.eval03(cg[0], cg[3]);
+            if constexpr (NV == 4) {
+                // the cell's 4 characteristic values of a point through this warp's faces
+                // 8w .. 8w+6 of sxf: only this warp writes them (at the end of this phase), and
+                // the previous row's face states there were read before the last barrier
+                __syncwarp(); // the previous point's reads are done
+                if (active) {
+#pragma unroll
+                    for (int gpi = 0; gpi < 4; gpi++)
+                        if (gpi == 0 || gpi == 3 || all4) xs[gpi * 4 + v] = cg[gpi];
+                }
+                __syncwarp();
+#pragma unroll
+                for (int gpi = 0; gpi < 4; gpi++) {
+                    if (!(gpi == 0 || gpi == 3 || all4)) continue;
+                    R q[4];
+                    load4<R>(xs + gpi * 4, q);
+                    if constexpr (DEV) { // as in the y-sweep
+                        R s = R(0);
+#pragma unroll
+                        for (int k = 0; k < NV; k++) s += (R)Rrow[k] * q[k];
+                        fv[gpi][gpj] = Uc[v] + (double)s;
+                    } else {
+                        double s = 0.0;
+#pragma unroll
+                        for (int k = 0; k < NV; k++) s += Rrow[k] * (double)q[k];
+                        fv[gpi][gpj] = s;
+                    }
+                }
+            } else {
 #pragma unroll
             for (int gpi = 0; gpi < 4; gpi++) {
                 if (!(gpi == 0 || gpi == 3 || all4)) continue;
@@ -661,7 +739,9 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
                     fv[gpi][gpj] = s;
                 }
             }
+            }
         }
+        if constexpr (NV == 4) __syncwarp(); // the exchange area is written below
     }
 
     // bound-preserving limiter: theta from the partial densities, in FP64 in every form
@@ -910,6 +990,11 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<EQ, RECON, R, NT>::value) s
     static_assert(NT == 128 || (NT == 256 && StageWide<EQ, RECON, R>::value), "stage kernel width");
     constexpr int H = StencilRecon<R, SCH>::H;
     constexpr int TX = StageGeom<EQ, H, NT>::TX;
+    using SmemT = StageSmem<EQ, H, NT>;
+    static_assert(offsetof(SmemT, sy) % 16 == 0 && offsetof(SmemT, sxf) % 16 == 0, "16-byte exchange loads");
+    // the last warp's exchange area (its active cells, from face 8 (NT/32 - 1) on) inside sxf
+    static_assert(EqTraits<EQ>::NV != 4 || 8 * (NT / 32 - 1) * SmemT::FS + (TX + 1 - 8 * (NT / 32 - 1)) * 20 + 16 <= (TX + 1) * SmemT::FS,
+                  "exchange area of the last warp");
     // the CTA's shared block is dynamic shared memory (it outgrows the 48 KB static limit for
     // wider strips): StageSmem, then StageDynSmem bytes of the primitive ring
     extern __shared__ __align__(16) unsigned char stage_smem_raw[];
