@@ -660,6 +660,8 @@ def run_batch(args, rank, world, dist):
     res["oracle_check"] = batch_oracle_check(wb, ens, min(args.steps, 20), os.cpu_count() or 1)
     rows = [dict(k=k, nx=prm["nx"], ny=prm["ny"], ratio=round(prm["ratio"], 1), eps=prm["eps"], scheme=prm["scheme"],
                  fp32=err["fp32_bulk"][k], fp64=err["fp64"][k]) for k, (_, prm) in enumerate(ens)]
+    for u in res["errors"].get("unexplained_instances", []):
+        u.update({key: rows[u["k"]][key] for key in ("nx", "ny", "ratio", "eps", "scheme")})
     rows.sort(key=lambda r: -r["fp32"])
     out = dict(metric="cell-stage updates/s", value=res["fp64"]["value"], unit="cell-stage updates/s", n_gpus=world,
                steps=args.steps, warmup=args.warmup, ms_per_step=res["fp64"]["seconds"] * 1e3 / args.steps,
