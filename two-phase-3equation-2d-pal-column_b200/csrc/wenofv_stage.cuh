@@ -17,9 +17,9 @@
 // Thread mapping (NT threads, 128 or 256): a unit of the y-sweep is (position, variable), of the
 // x-sweep (cell, variable), of the Riemann phase (face, Gauss point) and of the update
 // (cell, variable); groups of NV (or 4) consecutive lanes belong to the same position, cell
-// or face, so characteristic projections, the limiter's theta and the GL quadrature sums
-// exchange values by warp shuffles.  TX = NT/NV - 2(H+1) makes the y-sweep exactly one unit
-// per thread.
+// or face.  The limiter's theta and the GL quadrature sums are exchanged by warp shuffles;
+// the characteristic values of a point pass between a cell's lanes through the warp's own
+// shared-memory rows.  TX = NT/NV - 2(H+1) makes the y-sweep exactly one unit per thread.
 #pragma once
 #include "wenofv_math.cuh"
 
@@ -822,7 +822,8 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
 // ---- phase 3: Riemann fluxes + Gauss-Lobatto quadrature (src/WENOFV.cpp:1707-1799) -----
 // x-faces of row r (when r is an interior row of the item) and y-faces between rows r-1
 // and r (when r-1 >= j0-1 and r <= j1).  Four consecutive lanes hold the four Gauss
-// points of one face; lane gp = 0 sums them in the reference's order.
+// points of one face.  FP64_STRICT: lane gp = 0 sums them in the reference's order; the
+// contracted build: a reduce-scatter leaves the sum of variable gp on lane gp.
 template <int EQ, class R, int FLX, int H, int NT>
 __device__ __forceinline__ void phase_riemann(StageSmem<EQ, H, NT> &S, const InstDesc &D, InstState *st, int r, int i0, int j0, int j1,
                                               int TXe)
