@@ -917,8 +917,8 @@ __device__ __forceinline__ void tp_hllc(const TPState<R> &L, const TPState<R> &R
     FUR[1] = Rs.z2rho2 * vn_R;
     FUR[2] = Rs.rhou * vn_R + Rs.pre * nx;
     FUR[3] = Rs.rhov * vn_R + Rs.pre * ny;
-    const R sL = sqrt(L.rho), sR = sqrt(Rs.rho);
 #if WENOFV_STRICT
+    const R sL = sqrt(L.rho), sR = sqrt(Rs.rho);
     const R vn_roe = (vn_L * sL + vn_R * sR) / (sL + sR);
     R c2_roe = (L.c * L.c * sL + Rs.c * Rs.c * sR) / (sL + sR);
     c2_roe += R(0.5) * sL * sR / (sL + sR) / (sL + sR) * (vn_R - vn_L) * (vn_R - vn_L);
@@ -933,6 +933,7 @@ __device__ __forceinline__ void tp_hllc(const TPState<R> &L, const TPState<R> &R
         c2_roe = L.c * L.c * wL + Rs.c * Rs.c * wR;
         c2_roe += R(0.5) * wL * wR * (vn_R - vn_L) * (vn_R - vn_L);
     } else {
+        const R sL = sqrt(L.rho), sR = sqrt(Rs.rho);
         const R is = R(1) / (sL + sR);
         vn_roe = (vn_L * sL + vn_R * sR) * is;
         c2_roe = (L.c * L.c * sL + Rs.c * Rs.c * sR) * is;
