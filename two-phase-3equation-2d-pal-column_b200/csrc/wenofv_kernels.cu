@@ -22,8 +22,8 @@ namespace fast {
 #endif
 
 // whether (eq, recon) has the 256-thread stage kernel too (StageWide)
-int stage_wide(int eq, int recon) { return eq != EQ_LINEAR_ADV && eq != EQ_TWO_PHASE_SG && recon != 4; }
-static_assert(StageWide<EQ_TWO_PHASE, 1, double>::value && !StageWide<EQ_TWO_PHASE, 4, double>::value &&
+int stage_wide(int eq, int recon) { (void)recon; return eq != EQ_LINEAR_ADV && eq != EQ_TWO_PHASE_SG; }
+static_assert(StageWide<EQ_TWO_PHASE, 1, double>::value && StageWide<EQ_TWO_PHASE, 4, double>::value &&
                   StageWide<EQ_TWO_PHASE, 1, float>::value && !StageWide<EQ_LINEAR_ADV, 0, double>::value &&
                   !StageWide<EQ_TWO_PHASE_SG, 1, double>::value && StageWide<EQ_EULER, 0, float>::value,
               "stage_wide mirrors StageWide");

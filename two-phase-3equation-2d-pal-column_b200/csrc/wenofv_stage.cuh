@@ -47,7 +47,7 @@ namespace fast {
 // y-sweep maps 4 warps to 32 positions), as does the stiffened gas (whose Newton equilibrium
 // spills at 128 registers); scalar advection has strips of 122 columns at 128 already.
 template <int EQ, int RECON, class R> struct StageWide {
-    static constexpr bool value = EqTraits<EQ>::NV == 4 && RECON != 4 && EQ != EQ_TWO_PHASE_SG;
+    static constexpr bool value = EqTraits<EQ>::NV == 4 && EQ != EQ_TWO_PHASE_SG;
 };
 constexpr int CFL_NT = 128; // threads per CTA of cfl_kernel
 
@@ -457,9 +457,9 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
     // PRIMITIVE3 reconstructs z1 with another kernel than p, u, v: one warp per variable (the
     // strip's 32 positions on its lanes, the z1 warp rotating with the row) instead of the 4
     // variables of a position on 4 lanes, so that the two kernels do not diverge in a warp
-    const int p = RECON == 4 ? (t & 31) : t / NV;
+    const int p = RECON == 4 ? (t & 31) + 32 * (t >> 7) : t / NV; // PRIMITIVE3: warps 4-7 take positions 32-63
     const int v = RECON == 4 ? (((t >> 5) + r) & 3) : t - p * NV;
-    static_assert(RECON != 4 || (NV == 4 && StageGeom<EQ, H, NT>::P == 32 && NT == 128), "variable-major y-sweep");
+    static_assert(RECON != 4 || (NV == 4 && StageGeom<EQ, H, NT>::P == NT / 4), "variable-major y-sweep");
     if (RECON != 1 || NV == 1) {
         // conservative: the averages; primitive (RECONSTRUCTIONTYPE 2-4): the primitive
         // variables of each of the NS cells (src/WENOFV.cpp:944-979).  Each (position,
