@@ -237,9 +237,9 @@ int wenofv_batch_advance(wenofv_batch *b, const double *t_end, int64_t max_steps
 int wenofv_batch_set_tiling(wenofv_batch *b, int rows_per_item, int ctas_per_sm);
 int wenofv_batch_stream(wenofv_batch *b, void **stream);
 /* threads per CTA of the stage kernels: 0 (the default) chooses per instance, 256 (strips of 58
- * columns) where the grid's width fills them well, else 128 (26 columns); 128 or 256 forces that
- * width for every instance that has it (PRIMITIVE3, the stiffened gas and scalar advection run
- * 128 only) */
+ * columns, 56 on the 7-point geometry) where the grid's width fills them well, else 128 (26 or
+ * 24 columns); 128 or 256 forces that width for every instance that has it (the stiffened gas
+ * and scalar advection run 128 only) */
 int wenofv_batch_set_threads(wenofv_batch *b, int threads_per_cta);
 /* the current tiling settings (0 = automatic) */
 int wenofv_batch_tiling(wenofv_batch *b, int *rows_per_item, int *ctas_per_sm, int *threads_per_cta);
