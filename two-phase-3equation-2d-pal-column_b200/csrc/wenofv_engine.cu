@@ -588,6 +588,9 @@ int Engine::build_work()
             // halo rows, short enough to fill the GPU (measured best on the 1024^2 column)
             seg = 32;
             while (seg > 8 && strips_rows / seg < 2L * slots) seg /= 2;
+            // a grid that leaves SMs idle even at 8 rows: shorter items, since each CTA's time
+            // is its rows in sequence (latency-bound), not the work
+            while (seg > 2 && strips_rows / seg < sms_) seg /= 2;
         } else if (seg <= 0) {
             // 1-2 resident CTAs per SM: the CTAs take items in waves, and an item of s rows
             // costs about s + 2 halo rows + 3 rows' worth of start-up (its first 2H+1 rows load
@@ -596,7 +599,7 @@ int Engine::build_work()
             // against 0.972 for 16 and 0.924 for 32 (measured).
             double best = 1e300;
             seg = 32;
-            for (int s : {8, 16, 24, 32, 48, 64}) {
+            for (int s : {2, 4, 8, 16, 24, 32, 48, 64}) {
                 long items = 0;
                 for (int i : g.inst) items += (long)((cfg_[i].nx + tx - 1) / tx) * ((cfg_[i].ny + s - 1) / s);
                 const double waves = std::ceil((double)items / slots);
