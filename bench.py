@@ -772,14 +772,24 @@ def serve_measure(wb, reqs, rate, budget_bytes, seed, local, dist, world, forms=
     if "fp32_bulk" in res:
         finals["fp64_strict"] = serve_alone_strict(wb, reqs, local)
         # errors per request kind (results of failed requests are left out)
-        by = {"euler": {"fp64": [], "fp32_bulk": []}, "two_phase": {"fp64": [], "fp32_bulk": []}}
+        by = {"euler": {"fp64": [], "fp32_bulk": [], "req": []}, "two_phase": {"fp64": [], "fp32_bulk": [], "req": []}}
         for j, r in enumerate(reqs):
             a, b, c = finals["fp32_bulk"][j], finals["fp64"][j], finals["fp64_strict"][j]
             if a is None or b is None or c is None:
                 continue
             by[r[5]]["fp32_bulk"].append(rel_l1(a, c))
             by[r[5]]["fp64"].append(rel_l1(b, c))
-        res["errors"] = {k: summarize_errors(v) for k, v in by.items() if v["fp64"]}
+            by[r[5]]["req"].append(j)
+        res["errors"] = {}
+        for kind, v in by.items():
+            if not v["fp64"]:
+                continue
+            summ = summarize_errors(v)
+            for u in summ["unexplained_instances"]:  # k: the request's index in the stream
+                j = v["req"][u["k"]]
+                nx, ny = reqs[j][2].shape[2], reqs[j][2].shape[1]
+                u.update(k=j, nx=int(nx), ny=int(ny), steps=int(reqs[j][3]))
+            res["errors"][kind] = summ
         res["fp32_bulk"]["speedup_vs_fp64"] = res["fp32_bulk"]["value"] / res["fp64"]["value"]
     return res
 
