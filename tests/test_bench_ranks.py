@@ -55,3 +55,17 @@ def test_single_process_has_no_reduction():
 
     assert bench.max_over_ranks(3.25, None) == 3.25
     assert bench.replica_value(1, 10.0, 2.0) == 5.0
+
+
+def test_error_summary_names_unexplained_instances():
+    """bench.summarize_errors: instances over the bar split into those the FP64 form's own
+    error explains (FP32-bulk within 10x of it) and those it does not, the latter listed"""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    err = {"fp32_bulk": [1e-7, 2e-5, 3e-4, 5e-5], "fp64": [1e-9, 1e-5, 1e-7, 6e-6]}
+    s = bench.summarize_errors(err, bar=1e-5)
+    assert s["fp32_vs_oracle"]["within_bar"] == 1 and s["fp32_vs_oracle"]["n"] == 4
+    assert s["over_bar_explained_by_fp64_spread"] == 2  # 2e-5 <= 10 * 1e-5, 5e-5 <= 10 * 6e-6
+    assert s["over_bar_unexplained"] == 1
+    assert s["unexplained_instances"] == [dict(k=2, fp32=3e-4, fp64=1e-7)]
