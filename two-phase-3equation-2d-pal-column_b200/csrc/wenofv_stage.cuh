@@ -626,19 +626,27 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
 #pragma unroll
             for (int k = 0; k < 4; k++) pv[gpi][k] = U4[k];
         }
+        // each lane's variable at the boundary points, through this warp's faces 8w .. 8w+6 of
+        // sxf (as in the characteristic sweep): per x point gpi, lane gj leaves its 4 variables
+        // at slot k*4 + ((gj + k) & 3) of its cell, so that the writers (4 cells x 4 points, one
+        // variable) and the readers (4 cells x 4 variables, one point) hit 16 distinct banks
+        double *xs = reinterpret_cast<double *>(&S.sxf[8 * (t >> 5)][0]) + (active ? (lane >> 2) : 0) * 20;
+        (void)gbase;
 #pragma unroll
-        for (int gpj = 0; gpj < 4; gpj++)
+        for (int gpi = 0; gpi < 4; gpi++) {
+            __syncwarp(); // the previous point's reads are done
+            if (active) {
 #pragma unroll
-            for (int gpi = 0; gpi < 4; gpi++) {
-                if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
-                double x = 0.0;
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const double y = __shfl_sync(0xffffffffu, pv[gpi][k], gbase + gpj);
-                    if (k == v) x = y;
-                }
-                fv[gpi][gpj] = x;
+                for (int k = 0; k < 4; k++) xs[k * 4 + ((gj + k) & 3)] = pv[gpi][k];
             }
+            __syncwarp();
+#pragma unroll
+            for (int gpj = 0; gpj < 4; gpj++) {
+                if (!(gpi == 0 || gpi == 3 || gpj == 0 || gpj == 3)) continue;
+                fv[gpi][gpj] = xs[v * 4 + ((gpj + v) & 3)];
+            }
+        }
+        __syncwarp(); // the exchange area is written below
     } else if (RECON != 1 || NV == 1) {
         (void)ring_raw;
         double cc = 0.0; // deviation anchor: the cell's own average
