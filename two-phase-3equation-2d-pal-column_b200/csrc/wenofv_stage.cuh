@@ -526,9 +526,7 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
         W.init(pr, D.scheme, v, D.dx4);
         R cg[4];
         W.eval4(cg);
-        const int lane = t & 31, gbase = lane & ~(NV - 1);
-        (void)gbase;
-        if constexpr (NV == 4) {
+        if constexpr (NV == 4) { // the characteristic sweeps have 4 variables
             // the 4 characteristic values of a point reach the position's 4 lanes through the
             // warp's own rows of sy (positions 8w .. 8w+7, written by no other warp), as R at the
             // element offsets of sy_index; the results overwrite them afterwards
@@ -558,23 +556,6 @@ __device__ __forceinline__ void phase_ysweep(StageSmem<EQ, StencilRecon<R, SCH>:
             __syncwarp();
 #pragma unroll
             for (int gp = 0; gp < 4; gp++) S.sy[sy_index<RECON, NV>(p, gp, v)] = out[gp];
-            return;
-        }
-#pragma unroll
-        for (int gp = 0; gp < 4; gp++) {
-            // back-projection: FP32 in the bulk form (it adds an error of the same order as the
-            // FP32 WENO's own, eps * sum_k |R_vk w_k|), FP64 otherwise
-            if constexpr (DEV) {
-                R s = R(0);
-#pragma unroll
-                for (int k = 0; k < NV; k++) s += (R)Rrow[k] * __shfl_sync(0xffffffffu, cg[gp], gbase + k);
-                S.sy[sy_index<RECON, NV>(p, gp, v)] = Uc[v] + (double)s;
-            } else {
-                double s = 0.0;
-#pragma unroll
-                for (int k = 0; k < NV; k++) s += Rrow[k] * (double)__shfl_sync(0xffffffffu, cg[gp], gbase + k);
-                S.sy[sy_index<RECON, NV>(p, gp, v)] = s;
-            }
         }
     }
 }
@@ -600,9 +581,9 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
         // primitive reconstructions (src/WENOFV.cpp:981-1025, :1137-1189, :1302-1354): lane v
         // of the cell reconstructs all 4 primitive variables at y Gauss point gj = v, so that
         // PRIMITIVE3's z1 kernel and WENO-Z do not diverge across the cell's lanes, converts
-        // its points back to conserved variables, and shuffles hand every lane its variable
-        // at the 12 boundary points.  Lanes 1 and 2 also evaluate the inner points (unused)
-        // to keep the lanes converged.
+        // its points back to conserved variables, and hands every lane its variable at the 12
+        // boundary points through shared memory (below).  Lanes 1 and 2 also evaluate the
+        // inner points (unused) to keep the lanes converged.
         auto ring = reinterpret_cast<const double (*)[4][StageSmem<EQ, H, NT>::PS]>(ring_raw);
         const int gj = v;
         double pv[4][4]; // [gpi][variable] at (gpi, gj)
@@ -631,7 +612,6 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
         // at slot k*4 + ((gj + k) & 3) of its cell, so that the writers (4 cells x 4 points, one
         // variable) and the readers (4 cells x 4 variables, one point) hit 16 distinct banks
         double *xs = reinterpret_cast<double *>(&S.sxf[8 * (t >> 5)][0]) + (active ? (lane >> 2) : 0) * 20;
-        (void)gbase;
 #pragma unroll
         for (int gpi = 0; gpi < 4; gpi++) {
             __syncwarp(); // the previous point's reads are done
@@ -684,7 +664,6 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
         // exchange area of this warp's cells (inactive lanes read cell slot 0): element stride
         // 20 per cell (4 mod 16 doubles: the 16 writers of a half-warp hit distinct banks)
         R *xs = reinterpret_cast<R *>(&S.sxf[8 * (t >> 5)][0]) + (active ? (lane >> 2) : 0) * 20;
-        (void)xs;
         // per y Gauss point: project, reconstruct, and project back at once, so that only
         // that point's characteristic values are live (not all twelve)
 #pragma unroll
@@ -703,7 +682,7 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
             const bool all4 = gpj == 0 || gpj == 3;
             if (all4) W.eval4(cg);
             else W.eval03(cg[0], cg[3]);
-            if constexpr (NV == 4) {
+            if constexpr (NV == 4) { // the characteristic sweeps have 4 variables
                 // the cell's 4 characteristic values of a point through this warp's faces
                 // 8w .. 8w+6 of sxf: only this warp writes them (at the end of this phase), and
                 // the previous row's face states there were read before the last barrier
@@ -731,25 +710,9 @@ __device__ __forceinline__ void phase_xsweep(StageSmem<EQ, StencilRecon<R, SCH>:
                         fv[gpi][gpj] = s;
                     }
                 }
-            } else {
-#pragma unroll
-            for (int gpi = 0; gpi < 4; gpi++) {
-                if (!(gpi == 0 || gpi == 3 || all4)) continue;
-                if constexpr (DEV) { // as in the y-sweep
-                    R s = R(0);
-#pragma unroll
-                    for (int k = 0; k < NV; k++) s += (R)Rrow[k] * __shfl_sync(0xffffffffu, cg[gpi], gbase + k);
-                    fv[gpi][gpj] = Uc[v] + (double)s;
-                } else {
-                    double s = 0.0;
-#pragma unroll
-                    for (int k = 0; k < NV; k++) s += Rrow[k] * (double)__shfl_sync(0xffffffffu, cg[gpi], gbase + k);
-                    fv[gpi][gpj] = s;
-                }
-            }
             }
         }
-        if constexpr (NV == 4) __syncwarp(); // the exchange area is written below
+        __syncwarp(); // the exchange area is written below
     }
 
     // bound-preserving limiter: theta from the partial densities, in FP64 in every form
