@@ -69,6 +69,7 @@ int wenofv_create(const wenofv_config *cfg, const wenofv_eq_params *eq, wenofv_c
     wenofv_ctx *c = new (std::nothrow) wenofv_ctx;
     if (!c) { set_error("host allocation failed"); return WENOFV_ENOMEM; }
     c->eng.theta_record = true;
+    c->eng.solo = true;
     const int rc = c->eng.init(1, cfg, eq);
     if (rc) { delete c; return rc; }
     *out = c;

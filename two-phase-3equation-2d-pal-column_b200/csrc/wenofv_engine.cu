@@ -486,11 +486,59 @@ void Engine::free_work()
     groups_.clear();
 }
 
+// rows per work item of a launch group whose instances `inst` have strips of tx columns and
+// `slots` resident CTAs (the tiling override when set)
+int Engine::item_rows(const std::vector<int> &inst, int tx, int slots) const
+{
+    if (rows_per_item_ > 0) return rows_per_item_;
+    long strips_rows = 0;
+    for (int i : inst) strips_rows += (long)((cfg_[i].nx + tx - 1) / tx) * cfg_[i].ny;
+    int seg = 32;
+    if (slots > 2 * sms_) {
+        // many resident CTAs per SM (the 128-thread kernels): long enough to amortise the 2
+        // halo rows, short enough to fill the GPU (measured best on the 1024^2 column)
+        while (seg > 8 && strips_rows / seg < 2L * slots) seg /= 2;
+        // a grid that leaves SMs idle even at 8 rows: shorter items, since each CTA's time
+        // is its rows in sequence (latency-bound), not the work
+        while (seg > 2 && strips_rows / seg < sms_) seg /= 2;
+        return seg;
+    }
+    // 1-2 resident CTAs per SM: the CTAs take items in waves, and an item of s rows costs
+    // about s + 2 halo rows + 3 rows' worth of start-up (its first 2H+1 rows load before the
+    // loop; measured: 8 % of a 32-row item); pick the s of the shortest waves x (s + 5).  On
+    // the 1024^2 column it picks 64 rows: 0.897 ms per stage against 0.972 for 16 and 0.924 for
+    // 32 (measured).
+    double best = 1e300;
+    for (int s : {2, 4, 8, 16, 24, 32, 48, 64}) {
+        const double cost = waves_of(inst, tx, slots, s) * (s + 5);
+        if (cost < best - 1e-9) { best = cost; seg = s; }
+    }
+    return seg;
+}
+
+// waves of work items of s rows over `slots` resident CTAs
+double Engine::waves_of(const std::vector<int> &inst, int tx, int slots, int s) const
+{
+    long items = 0;
+    for (int i : inst) items += (long)((cfg_[i].nx + tx - 1) / tx) * ((cfg_[i].ny + s - 1) / s);
+    return std::ceil((double)items / std::max(1, slots));
+}
+
 // the CTA width of an instance's stage kernel: 256 (strips of 58 columns) or 128 (26 columns)
-// where both exist.  The wide kernel costs about 0.85 (FP64) or 0.93 (FP32-bulk) of the narrow
-// one per column-row it computes (measured on a 1024-wide grid), but rounds the grid's width up
-// to whole strips of 58; choose the width of the smaller cost x padded width.  The override
-// (wenofv_batch_set_threads, the autotuner) forces one width where it exists.
+// where both exist.  The override (wenofv_batch_set_threads, the autotuner) forces one width
+// where it exists.
+//
+// Among many instances (batches, servers) the GPU is full, so the throughput decides: the
+// wide kernel costs about 0.85 (FP64) or 0.93 (FP32-bulk) of the narrow one per column-row it
+// computes (measured on a 1024-wide grid), but rounds the grid's width up to whole strips of
+// 58; the width of the smaller cost x padded width.
+//
+// A context's single instance is alone on the GPU, and a small grid does not fill it: its
+// stage takes the waves of work items of its own tiling (item_rows) x (rows + 5) row
+// iterations, and a row iteration of the wide kernel takes about 1.3 (FP64) or 1.1 (FP32-bulk)
+// of the narrow one's (measured on the 1024^2 and 256^2 columns: 0.725 against 0.896 ms per
+// FP64 stage at 1024^2, 0.119 against 0.098 ms at 256^2, where the narrow kernel's 10 strips
+// spread over more SMs than the wide kernel's 5).
 int Engine::instance_nt(int i) const
 {
     const int eqk = desc_[i].eq_kind, recon = desc_[i].recon;
@@ -501,6 +549,21 @@ int Engine::instance_nt(int i) const
     const int sch = recon == 4 ? 2 : desc_[i].scheme;
     const int tn = strict ? strict::stage_tx(eqk, recon, fp32, sch, 128) : fast::stage_tx(eqk, recon, fp32, sch, 128);
     const int tw = strict ? strict::stage_tx(eqk, recon, fp32, sch, 256) : fast::stage_tx(eqk, recon, fp32, sch, 256);
+    if (solo) {
+        const std::vector<int> one{i};
+        const int flx = eqk == WENOFV_EQ_LINEAR_ADV ? 0 : desc_[i].flux;
+        double rows_t[2];
+        const int nts[2] = {128, 256};
+        for (int k = 0; k < 2; k++) {
+            const int tx = k ? tw : tn;
+            const int bps = std::max(1, strict ? strict::stage_blocks_per_sm(eqk, recon, fp32, sch, flx, nts[k])
+                                               : fast::stage_blocks_per_sm(eqk, recon, fp32, sch, flx, nts[k]));
+            const int slots = sms_ * (ctas_per_sm_ > 0 ? std::min(ctas_per_sm_, bps) : bps);
+            const int seg = item_rows(one, tx, slots);
+            rows_t[k] = waves_of(one, tx, slots, seg) * (seg + 5);
+        }
+        return (fp32 ? 1.1 : 1.3) * rows_t[1] < rows_t[0] ? 256 : 128;
+    }
     const int nx = cfg_[i].nx;
     const double narrow = (double)((nx + tn - 1) / tn) * tn;
     const double wide_cost = (fp32 ? 0.93 : 0.85) * (double)((nx + tw - 1) / tw) * tw;
@@ -580,33 +643,7 @@ int Engine::build_work()
         const int bps = std::max(1, g.ns_strict ? strict::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux, g.nt)
                                                 : fast::stage_blocks_per_sm(g.eq, g.recon, g.fp32, g.scheme, g.flux, g.nt));
         const int slots = sms_ * (ctas_per_sm_ > 0 ? std::min(ctas_per_sm_, bps) : bps);
-        long strips_rows = 0;
-        for (int i : g.inst) strips_rows += (long)((cfg_[i].nx + tx - 1) / tx) * cfg_[i].ny;
-        int seg = rows_per_item_;
-        if (seg <= 0 && slots > 2 * sms_) {
-            // many resident CTAs per SM (the 128-thread kernels): long enough to amortise the 2
-            // halo rows, short enough to fill the GPU (measured best on the 1024^2 column)
-            seg = 32;
-            while (seg > 8 && strips_rows / seg < 2L * slots) seg /= 2;
-            // a grid that leaves SMs idle even at 8 rows: shorter items, since each CTA's time
-            // is its rows in sequence (latency-bound), not the work
-            while (seg > 2 && strips_rows / seg < sms_) seg /= 2;
-        } else if (seg <= 0) {
-            // 1-2 resident CTAs per SM: the CTAs take items in waves, and an item of s rows
-            // costs about s + 2 halo rows + 3 rows' worth of start-up (its first 2H+1 rows load
-            // before the loop; measured: 8 % of a 32-row item); pick the s of the shortest
-            // waves x (s + 5).  On the 1024^2 column it picks 64 rows: 0.897 ms per stage
-            // against 0.972 for 16 and 0.924 for 32 (measured).
-            double best = 1e300;
-            seg = 32;
-            for (int s : {2, 4, 8, 16, 24, 32, 48, 64}) {
-                long items = 0;
-                for (int i : g.inst) items += (long)((cfg_[i].nx + tx - 1) / tx) * ((cfg_[i].ny + s - 1) / s);
-                const double waves = std::ceil((double)items / slots);
-                const double cost = waves * (s + 5);
-                if (cost < best - 1e-9) { best = cost; seg = s; }
-            }
-        }
+        const int seg = item_rows(g.inst, tx, slots);
         std::vector<WorkItem> work;
         for (int i : g.inst)
             for (int j0 = 0; j0 < cfg_[i].ny; j0 += seg)

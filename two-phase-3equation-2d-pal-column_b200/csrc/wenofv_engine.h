@@ -87,6 +87,7 @@ public:
     int rk = 2;
     bool slot_mode = false;    // serving: every slot keeps its own current buffer
     bool theta_record = false; // contexts: keep the limiter's per-cell record (wenofv_theta_flags)
+    bool solo = false;         // contexts: one instance alone on the GPU (instance_nt)
 
 private:
     // one persistent launch per RK stage for the instances of one template key; the work
@@ -114,6 +115,8 @@ private:
     void free_work();
     long group_key(int i) const;
     int instance_nt(int i) const;
+    int item_rows(const std::vector<int> &inst, int tx, int slots) const;
+    double waves_of(const std::vector<int> &inst, int tx, int slots, int s) const;
     int group_launch(const Group &g, StageLaunch &L) const;
     int arena_alloc(size_t bytes, size_t *off);
     void arena_free(size_t off);
