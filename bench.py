@@ -594,7 +594,7 @@ def batch_measure(wb, ens, steps, warmup, local, dist, world, autotune=True):
         tiling = None
         if autotune and name != "fp64_strict":
             rows, ctas, tune_ms = b.autotune()
-            tiling = dict(rows_per_item=rows, ctas_per_sm=ctas, threads_per_cta=b.tiling()[2] or "per instance",
+            tiling = dict(rows_per_item=rows or "automatic", ctas_per_sm=ctas, threads_per_cta=b.tiling()[2] or "per instance",
                           autotune_best_stage_ms=tune_ms)
         if name != "fp64_strict":
             b.advance(1e9, max_steps=warmup)

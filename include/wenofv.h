@@ -243,8 +243,9 @@ int wenofv_batch_stream(wenofv_batch *b, void **stream);
 int wenofv_batch_set_threads(wenofv_batch *b, int threads_per_cta);
 /* the current tiling settings (0 = automatic) */
 int wenofv_batch_tiling(wenofv_batch *b, int *rows_per_item, int *ctas_per_sm, int *threads_per_cta);
-/* measures candidate tilings (threads per CTA x rows per work item x CTAs per SM) on the
- * batch's current state (state unchanged) and keeps the best; wenofv_batch_tiling reports it */
+/* measures candidate tilings (threads per CTA x rows per work item x CTAs per SM; rows 0 =
+ * the automatic choice among them) on the batch's current state (state unchanged) and keeps
+ * the best; wenofv_batch_tiling reports it */
 int wenofv_batch_autotune(wenofv_batch *b, int *rows_per_item, int *ctas_per_sm, double *best_ms);
 
 /* ---- serving: continuous batching of solve requests under an HBM budget (no

@@ -91,7 +91,7 @@ def test_batch_autotune_keeps_state(wb):
     for k, (U0, _) in enumerate(ens):
         b.upload(k, U0)
     rows, ctas, ms = b.autotune()
-    assert rows in (8, 16, 32, 64) and ms > 0
+    assert rows in (0, 16, 32, 64) and ms > 0  # 0: the automatic rows per item
     for k, (U0, _) in enumerate(ens):
         assert np.array_equal(b.download(k), U0)  # the autotuner restores the state
     b.advance([1e9] * len(ens), max_steps=3)

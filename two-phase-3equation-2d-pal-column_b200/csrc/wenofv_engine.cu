@@ -1263,7 +1263,7 @@ int Engine::autotune(int *rows_out, int *ctas_out, double *best_ms)
     }
     std::vector<int> nt_c = {0};
     if (any_wide) { nt_c.push_back(128); nt_c.push_back(256); }
-    const int rows_c[] = {16, 32, 64};
+    const int rows_c[] = {0, 16, 32, 64}; // 0: the automatic rows per item (item_rows)
     const int ctas_c[] = {0, 2};
     double best = 1e30;
     int br = 32, bc = 0, bn = 0;
